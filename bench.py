@@ -1,0 +1,310 @@
+#!/usr/bin/env python
+"""Benchmark: MD ion-steps/s of the N=24,000 polarisable silica Nose-Hoover-chain step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--precision fp64|mixed] [--solver cg|reference]
+
+A step is one MD step (src/md.c:229-241: prop_agate = NHC half-step, velocity-Verlet
+drift, force evaluation with the induced-dipole solve, kick, NHC half-step; then
+check_verletlist) of the seeded 24,000-ion system (8000 Si + 16000 O, beta-cristobalite
+10^3 supercell with 0.05 Å displacements, 2.20 g/cm^3, L = 71.3 Å, MB velocities at
+2500 K), Buckingham rc 7 Å, Ewald alpha 0.32, rc 10 Å, kmax 14, skin 1 Å, PIM with
+ASPC order 4 and residual 1e-6.
+
+ours      : state resident on the GPU; each timed step is bracketed by CUDA events on
+            the engine stream, with a 256 MB L2 flush between steps (not timed).
+            `e2e` repeats the measurement through the C ABI with host buffers:
+            positions and velocities uploaded, one step, positions, velocities and
+            forces downloaded, every step.
+reference : the reference's own CPU code (oracle/_ref, -O3 -Ofast -fopenmp) on all host
+            cores, on a bounded sample of steps of the same system.
+N > 1 GPUs: one process per GPU (torchrun), an independent replica per rank (the path
+has no collective; weak scaling); time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MD ion-steps/s & batched fit-gradients/s: mixed vs FP64 GPU at ≤1e-5 force err"
+WORKLOAD = ("pim_silica_nvt_24000: 8000 Si + 16000 O, 2.20 g/cm^3, L=71.3 A, Buckingham rc 7 A, "
+            "Ewald alpha 0.32 rc 10 A kmax 14, PIM alpha_O 1 A^3 TT-damped, SCF 1e-6 ASPC-4, NHC(3) 2500 K, "
+            "dt 1 fs, skin 1 A")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--solver", choices=["cg", "reference"], default="cg")
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--roof-kernel", default="k_rho")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms (read only)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self) -> dict:
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread is not None:
+            self.thread.join(timeout=2)
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ---------------------------------------------------------------------------- cpu baseline
+def cpu_baseline(system, nsteps: int = 2) -> dict:
+    """The reference's own code on the host cores, `nsteps` MD steps after its t=0 forces."""
+    from oracle import ref
+    threads = os.cpu_count() or 1
+    if ref.available("tim"):
+        r = ref.run(system, "md", nsteps, 0, 6, variant="tim", threads=threads, timeout=1800)
+        wall = float(r["wall"][0])
+        return {"value": system.nion * nsteps / wall, "unit": "ion-steps/s", "cores": threads,
+                "kind": "reference",
+                "sample": f"{nsteps} MD steps of the same 24000-ion system after its t=0 force evaluation, "
+                          f"mdff20 C code -O3 -Ofast -fopenmp, OMP_NUM_THREADS={threads}, {wall:.2f} s"}
+    from oracle.oracle import Oracle
+    o = Oracle(system)
+    o.gen_verletlist()
+    o.engforce()
+    t0 = time.perf_counter()
+    for s in range(1, nsteps + 1):
+        o.md_step(s)
+    wall = time.perf_counter() - t0
+    return {"value": system.nion * nsteps / wall, "unit": "ion-steps/s", "cores": 1, "kind": "port",
+            "sample": f"{nsteps} MD steps of the same system with the single-thread C restatement, {wall:.2f} s"}
+
+
+# ---------------------------------------------------------------------------- arms
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return world, rank, local, pg
+
+
+def run_reference(args):
+    world, rank, local, pg = dist_setup(args)
+    from mdff20_b200 import synth
+    if rank == 0:
+        s = synth.config5()
+        nsteps = max(1, min(args.steps, 2))
+        cb = cpu_baseline(s, nsteps)
+        line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "ion-steps/s",
+                "n_gpus": args.gpus, "steps": nsteps, "warmup": 0, "ms_per_step": 1000.0 * s.nion / cb["value"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic: seeded beta-cristobalite silica, MB velocities",
+                "config": {"workload": WORKLOAD, "nion": s.nion, "parallelism": "host OpenMP"},
+                "cpu_baseline": cb,
+                "e2e": {"value": cb["value"], "unit": "ion-steps/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    from mdff20_b200 import synth
+    from mdff20_b200.engine import FP64, MIXED, PIM_CG, PIM_REFERENCE, Engine, fma_peak_tflops
+    from mdff20_b200.cellmath import wrap_positions
+
+    world, rank, local, pg = dist_setup(args)
+    dev = local
+    torch.cuda.set_device(dev)
+    s = synth.config5()
+    pos = wrap_positions(s.cell, s.pos)
+    prec = MIXED if args.precision == "mixed" else FP64
+    solver = PIM_CG if args.solver == "cg" else PIM_REFERENCE
+    eng = Engine(s, positions=pos, device=dev, precision=prec, pim_solver=solver)
+    eng.gen_verletlist()
+    eng.engforce()                                    # forces at t=0 (src/md.c:209)
+    istep = 1
+    if args.warmup > 0:
+        eng.md_steps(istep, args.warmup)
+        istep += args.warmup
+    stream = torch.cuda.ExternalStream(eng.stream_handle(), device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{dev}")   # 256 MB > L2
+    peak = fma_peak_tflops(dev, prec)
+
+    # ------------------------------------------------ device-resident timed region
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    thermo = []
+    eng.profile(args.roof_kernel)
+    l0 = eng.launch_count()
+    if pg is not None:
+        pg.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(dev)
+    clocks.start()
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        evs[k][0].record(stream)
+        thermo.append(eng.md_steps(istep, 1)[0])
+        evs[k][1].record(stream)
+        istep += 1
+    torch.cuda.synchronize()
+    if pg is not None:
+        pg.barrier()
+    clk = clocks.stop()
+    launches = eng.launch_count() - l0
+    kms, kcount, kflops = eng.profile_result()
+    eng.profile(None)
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    total_ms = float(sum(step_ms))
+    if pg is not None:
+        t = torch.tensor([total_ms], device=f"cuda:{dev}", dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        total_ms = float(t.item())
+    th = np.array(thermo)
+    value = world * s.nion * args.steps / (total_ms / 1000.0)
+
+    # ------------------------------------------------ end to end through the C ABI
+    nE = max(1, args.e2e_steps)
+    r, v, f = eng.state()
+    r = np.ascontiguousarray(r)
+    v = np.ascontiguousarray(v)
+    e_evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(nE)]
+    if pg is not None:
+        pg.barrier()
+    torch.cuda.synchronize()
+    for k in range(nE):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        e_evs[k][0].record(stream)
+        eng.set_positions(r)
+        eng.set_velocities(v)
+        eng.md_steps(istep, 1)
+        r, v, f = eng.state()
+        e_evs[k][1].record(stream)
+        istep += 1
+    torch.cuda.synchronize()
+    e2e_ms = float(sum(a.elapsed_time(b) for a, b in e_evs))
+    if pg is not None:
+        t = torch.tensor([e2e_ms], device=f"cuda:{dev}", dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * s.nion * nE / (e2e_ms / 1000.0)
+    n = s.nion
+    h2d = 2 * n * 3 * 8
+    d2h = 3 * n * 3 * 8 + 12 * 8
+
+    if rank == 0:
+        achieved = (kflops / (kms / 1000.0) / 1e12) if kms > 0 else None
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tpath):
+            traffic = json.load(open(tpath)).get(f"{args.roof_kernel}:{args.precision}")
+        line = {
+            "metric": METRIC, "value": value, "unit": "ion-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if prec == FP64 else "f32+f64",
+            "data": "synthetic: seeded beta-cristobalite silica, MB velocities",
+            "config": {"workload": WORKLOAD, "nion": n, "kmax": 14, "nk": int(s.nk()),
+                       "precision": args.precision, "pim_solver": args.solver,
+                       "l2": "256 MB written between timed steps (untimed)",
+                       "parallelism": f"replicas x{world}"},
+            "e2e": {"value": e2e_value, "unit": "ion-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "steps": nE, "ms_per_step": e2e_ms / nE},
+            "roofline": {"kernel": args.roof_kernel, "bound": "fp64" if prec == FP64 else "fp32",
+                         "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                         "launches": kcount, "ms_per_launch": (kms / kcount) if kcount else None,
+                         "peak_source": "measured by mdffgpu_fma_peak (FMA chains) on this GPU",
+                         "share_of_step": (kms / total_ms) if world == 1 else None},
+            "clocks": clk,
+            "gpu_launches": launches,
+            "scf_iter_mean": float(th[:, 10].mean()),
+            "list_rebuilds": int(th[-1, 9] - th[0, 9]) + 1,
+            "finite": bool(np.isfinite(th).all()),
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            try:
+                line["cpu_baseline"] = cpu_baseline(s, 2)
+            except Exception as exc:  # reported, not fatal
+                line["cpu_baseline"] = {"value": None, "error": str(exc)[:200]}
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

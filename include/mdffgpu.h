@@ -1,0 +1,193 @@
+/* mdffgpu: B200 (sm_100a) engine for the mdff20 force field and MD step -- C ABI.
+ *
+ * The reference (mdff20, plain C) has no plugin interface: its "operator API" is a set
+ * of void functions that read and write process globals.  Each entry point below
+ * replaces one of them; the comment names the reference function (file:line inside
+ * the mdff20 repository) and what the call takes instead of the globals.  Shims with
+ * the reference's exact names, working on the reference's globals, are in
+ * mdff20_b200/host/mdff_shim.c.
+ *
+ * Conventions
+ *  - every call returns an int status (MDFFGPU_OK = 0); the reference prints and calls
+ *    exit(-1) instead (src/tools.c:63-67);
+ *  - a context holds one system resident on one GPU; calls on a context are
+ *    synchronous with respect to the host and must not be made from two threads at once;
+ *  - host arrays are plain C arrays: positions/velocities/forces as three SoA arrays of
+ *    length nion (the reference's rx,ry,rz / vx,vy,vz / fx,fy,fz, src/config.h:38-40);
+ *    per-ion vectors (dipoles, fields) as [nion][3], EFG as [nion][3][3], the stress
+ *    tensor as [3][3], all row-major doubles;
+ *  - units are the reference's: control-file values in the parameter block, internal
+ *    units (eV, Å, amu, Å*(amu/eV)^0.5) in the state arrays.
+ */
+#ifndef MDFFGPU_H
+#define MDFFGPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MDFFGPU_NTMAX 16
+
+/* status codes */
+#define MDFFGPU_OK 0
+#define MDFFGPU_ERR_ARG 1            /* bad argument or unsupported parameter */
+#define MDFFGPU_ERR_CUDA 2           /* a CUDA call failed */
+#define MDFFGPU_ERR_LIST_OVERFLOW 3  /* a neighbour list or cell exceeded its capacity */
+#define MDFFGPU_ERR_SCF 4            /* induced dipoles did not converge in max_scf_pim_iter */
+#define MDFFGPU_ERR_NONFINITE 5      /* a NaN/Inf appeared in positions, forces or dipoles */
+#define MDFFGPU_ERR_STATE 6          /* call out of order (e.g. forces before a list exists) */
+#define MDFFGPU_ERR_NOMEM 7          /* device allocation failed */
+#define MDFFGPU_ERR_CELL 8           /* cutoff + skin exceeds half the cell width */
+#define MDFFGPU_ERR_TIMEOUT 9        /* a device loop hit its iteration limit */
+
+/* precision of the pair, Ewald and k-space arithmetic */
+#define MDFFGPU_FP64 0
+#define MDFFGPU_MIXED 1   /* FP32 arithmetic, compensated FP32/FP64 sums */
+
+/* induced-dipole solver */
+#define MDFFGPU_PIM_REFERENCE 0 /* the reference's algo_pim (scf: Jacobi + ASPC, scfkO) */
+#define MDFFGPU_PIM_CG 1        /* preconditioned conjugate gradient on (alpha^-1 - T) mu = E_stat */
+
+/* Parameter block: the values the reference's parsers leave in its globals, in
+ * control-file units (read_global src/global.c:13-60, read_md src/md.c:29-98,
+ * read_field src/field.c:31-183, read_nmlj src/nmlj.c:39-107, read_bhmftd
+ * src/bhmftd.c:26-90, read_pim src/pim.c:28-69) plus the POSFF header (cell, ions
+ * per type, src/config.c:372-401).  Pair tables hold the upper triangle as read
+ * (entries [i][j] with j >= i); the engine symmetrises them as the reference does. */
+typedef struct mdffgpu_params {
+    int nion, ntype;
+    int nionit[MDFFGPU_NTMAX];
+    double massit[MDFFGPU_NTMAX];
+    double cell[3][3];                 /* simuCell.A: rows are the lattice vectors */
+    int lreduced, lverletL;
+    double skindiff, cutshortrange, cutlongrange;
+    int lnmlj, trunctype;              /* 0 no, 1 linear, 2 quadratic */
+    double sigmalj[MDFFGPU_NTMAX][MDFFGPU_NTMAX], epslj[MDFFGPU_NTMAX][MDFFGPU_NTMAX];
+    double plj[MDFFGPU_NTMAX][MDFFGPU_NTMAX], qlj[MDFFGPU_NTMAX][MDFFGPU_NTMAX];
+    int lbhmft, lbhmftd;
+    double Abhmftd[MDFFGPU_NTMAX][MDFFGPU_NTMAX], Bbhmftd[MDFFGPU_NTMAX][MDFFGPU_NTMAX];
+    double Cbhmftd[MDFFGPU_NTMAX][MDFFGPU_NTMAX], Dbhmftd[MDFFGPU_NTMAX][MDFFGPU_NTMAX];
+    double BDbhmftd[MDFFGPU_NTMAX][MDFFGPU_NTMAX];
+    int lcoulombic;
+    double qit[MDFFGPU_NTMAX], dipit[MDFFGPU_NTMAX][3], polit[MDFFGPU_NTMAX][3][3];
+    int lpoldamping[MDFFGPU_NTMAX][MDFFGPU_NTMAX][MDFFGPU_NTMAX];
+    double pol_damp_b[MDFFGPU_NTMAX][MDFFGPU_NTMAX][MDFFGPU_NTMAX];
+    double pol_damp_c[MDFFGPU_NTMAX][MDFFGPU_NTMAX][MDFFGPU_NTMAX];
+    int pol_damp_k[MDFFGPU_NTMAX][MDFFGPU_NTMAX][MDFFGPU_NTMAX];
+    double alphaES;
+    int kES[3];
+    int algo_pim, algo_extrapolate_dipole, extrapolate_order, min_scf_pim_iter, max_scf_pim_iter;
+    double conv_tol_ind, omegakO;
+    int egrator;                       /* 0 nve-lf, 1 nve-vv, 2 nvt-nhcn */
+    int nhc_n, nhc_mults, nhc_yosh_order, nequil, nequilT;
+    double dt, temp, timesca_thermo, tauTberendsen;
+} mdffgpu_params;
+
+/* The reference's thermodynamic globals (src/thermo.h:3-14) plus solver counters. */
+typedef struct mdffgpu_thermo {
+    double e_kin, e_nvt, u_lj, u_bhmftd, u_coul, u_pol;
+    double pvir_lj, pvir_bhmftd, pvir_coul;
+    double tau_lj[9], tau_bhmftd[9], tau_coul[9];
+    double utail, ptail, scf_rmsd;
+    int scf_iter, nlist_builds;
+} mdffgpu_thermo;
+
+typedef struct mdffgpu_ctx mdffgpu_ctx;
+
+/* Set-up: init_global/read_config/init_md/init_field/init_config
+ * (src/mdff20.c:74-82) for one system whose positions (Cartesian, as read_config
+ * leaves them after its wrap, src/config.c:442-444) and velocities are given as SoA
+ * host arrays (vx may be NULL: zero velocities).  device < 0 uses the current device. */
+int mdffgpu_create(const mdffgpu_params *p, const double *rx, const double *ry, const double *rz,
+                   const double *vx, const double *vy, const double *vz, int device, mdffgpu_ctx **out);
+int mdffgpu_destroy(mdffgpu_ctx *ctx);
+const char *mdffgpu_last_error(const mdffgpu_ctx *ctx);
+int mdffgpu_set_precision(mdffgpu_ctx *ctx, int precision);
+int mdffgpu_set_pim_solver(mdffgpu_ctx *ctx, int solver);
+
+/* State transfer (the reference's rx..fz globals, src/config.h:38-40). */
+int mdffgpu_set_positions(mdffgpu_ctx *ctx, const double *rx, const double *ry, const double *rz);
+int mdffgpu_set_velocities(mdffgpu_ctx *ctx, const double *vx, const double *vy, const double *vz);
+int mdffgpu_get_state(mdffgpu_ctx *ctx, double *rx, double *ry, double *rz, double *vx, double *vy,
+                      double *vz, double *fx, double *fy, double *fz);
+/* dipia_ind history used by the ASPC predictor, [nion][6][3] (src/config.h:48) */
+int mdffgpu_set_dipole_history(mdffgpu_ctx *ctx, const double *hist);
+int mdffgpu_get_dipole_history(mdffgpu_ctx *ctx, double *hist);
+/* Nose-Hoover chain state xi, vxi (nhc_n values each, src/md.h:26) */
+int mdffgpu_set_nhc(mdffgpu_ctx *ctx, const double *xi, const double *vxi);
+int mdffgpu_get_nhc(mdffgpu_ctx *ctx, double *xi, double *vxi);
+/* info_thermo's inputs (src/thermo.c:12-35) */
+int mdffgpu_get_thermo(mdffgpu_ctx *ctx, mdffgpu_thermo *t);
+
+/* gen_pbc_verletlist (src/verlet.c:54-122): builds the short-range and Coulomb
+ * neighbour lists from the current positions and stores them as list reference. */
+int mdffgpu_gen_verletlist(mdffgpu_ctx *ctx);
+/* check_verletlist (src/verlet.c:124-170): rebuilds when the largest plus second
+ * largest displacement since the last build exceeds skindiff; *rebuilt (may be NULL)
+ * tells whether it did. */
+int mdffgpu_check_verletlist(mdffgpu_ctx *ctx, int *rebuilt);
+/* The lists in the reference's CSR half-list format (verlet_nb / verlet_coul,
+ * src/verlet.h:8-16): which = 0 short range, 1 Coulomb; point[nion+1], list[cap];
+ * *count receives the number of pairs.  Pairs follow the reference's parity rule
+ * (src/verlet.c:82-83), ascending j within each row. */
+int mdffgpu_get_verletlist(mdffgpu_ctx *ctx, int which, int *point, int *list, int cap, int *count);
+
+/* engforce (src/field.c:352-407): zeroes forces, then n-m LJ, BHMFT(D), induced
+ * dipoles (get_dipoles, src/coulombic.c:67-130) and the multipole Ewald sum. */
+int mdffgpu_engforce(mdffgpu_ctx *ctx);
+/* engforce_nmlj_pbc (src/nmlj.c:254-385) and engforce_bhmftd_pbc
+ * (src/bhmftd.c:117-271): ADD this evaluator's forces to the context forces and
+ * return its energy, virial pressure and stress tensor [3][3]. */
+int mdffgpu_engforce_nmlj(mdffgpu_ctx *ctx, double *u, double *pvir, double *tau);
+int mdffgpu_engforce_bhmftd(mdffgpu_ctx *ctx, double *u, double *pvir, double *tau);
+/* multipole_ES (src/ewald.c:75-348) on host arrays q[nion], mu[nion][3]; flags use
+ * the bits below.  Outputs (any may be NULL): u, pvir, tau[3][3], ef[nion][3],
+ * efg[nion][3][3], and this call's forces f[nion][3] (x coul_unit) -- the reference
+ * adds them to its global forces.  alpha > 0 overrides alphaES (the kO inner loop
+ * uses 0.001, src/pim.c:694). */
+#define MDFFGPU_ES_LQ 1
+#define MDFFGPU_ES_LD 2
+#define MDFFGPU_ES_LDAMP 4
+#define MDFFGPU_ES_FORCES 8
+#define MDFFGPU_ES_STRESS 16
+#define MDFFGPU_ES_EF 32
+#define MDFFGPU_ES_EFG 64
+#define MDFFGPU_ES_DIR 128
+#define MDFFGPU_ES_REC 256
+int mdffgpu_multipole_es(mdffgpu_ctx *ctx, const double *q, const double *mu, int flags, double alpha,
+                         double *u, double *pvir, double *tau, double *ef, double *efg, double *f);
+/* get_dipoles (src/coulombic.c:67-130) with momentpolaSCF / momentpolaSCFkO
+ * (src/pim.c:177-306, 457-603) or CG: total dipoles mu[nion][3] (static + induced)
+ * and the polarisation energy u_pol. */
+int mdffgpu_get_dipoles(mdffgpu_ctx *ctx, double *mu, double *upol);
+
+/* prop_agate (src/integration.c:298-333) for step istep (1-based): one velocity
+ * Verlet, leap-frog or Nose-Hoover-chain step including the force evaluation. */
+int mdffgpu_prop_agate(mdffgpu_ctx *ctx, int istep);
+/* The MD loop body of run_md (src/md.c:229-241): for istep = first..first+nsteps-1,
+ * prop_agate then check_verletlist, all on the device.  thermo (may be NULL) receives
+ * nsteps records of 12 doubles: e_kin u_lj u_bhmftd u_coul u_pol e_nvt pvir_lj
+ * pvir_bhmftd pvir_coul nlist_builds scf_iter scf_rmsd. */
+int mdffgpu_md_steps(mdffgpu_ctx *ctx, int first, int nsteps, double *thermo);
+
+/* Number of kernel launches the engine made so far (for accounting).  No counterpart
+ * in the reference. */
+long long mdffgpu_launch_count(const mdffgpu_ctx *ctx);
+/* The cudaStream_t every call of this context runs on, so a caller can record CUDA
+ * events around a call.  No counterpart in the reference. */
+void *mdffgpu_stream(const mdffgpu_ctx *ctx);
+/* Diagnostic: time every launch of one kernel family ("k_rho", "k_rec_ion", "k_dir")
+ * with CUDA events on the context stream from now on (NULL stops and clears);
+ * profile_result returns the summed device time (ms), the number of launches and the
+ * algorithmic flops of those launches.  No counterpart in the reference. */
+int mdffgpu_profile(mdffgpu_ctx *ctx, const char *kernel);
+int mdffgpu_profile_result(mdffgpu_ctx *ctx, double *ms, long long *count, double *flops);
+/* Diagnostic: measured fused-multiply-add throughput (TFLOP/s, 2 flops per FMA) of the
+ * FP64 (precision 0) or FP32 (1) pipe of `device`; the roofline of the pair and
+ * k-space kernels.  No counterpart in the reference. */
+int mdffgpu_fma_peak(int device, int precision, double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

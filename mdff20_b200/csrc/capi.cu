@@ -1,0 +1,326 @@
+// extern "C" entry points of libmdffgpu (declared in include/mdffgpu.h): argument
+// checks, host<->device transfer and conversion of engine exceptions to status codes.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "engine.cuh"
+
+using mdffgpu::Engine;
+using mdffgpu::Error;
+
+struct mdffgpu_ctx {
+    Engine *e;
+    std::string err;
+};
+
+namespace {
+
+template <typename F>
+int guarded(mdffgpu_ctx *ctx, F &&f) {
+    if (!ctx || !ctx->e) return MDFFGPU_ERR_ARG;
+    try {
+        f(*ctx->e);
+        return MDFFGPU_OK;
+    } catch (const Error &x) {
+        ctx->err = x.what();
+        return x.code;
+    } catch (const std::exception &x) {
+        ctx->err = x.what();
+        return MDFFGPU_ERR_CUDA;
+    }
+}
+
+void upload(Engine &e, void *dst, const void *src, size_t bytes) {
+    MDFF_CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, e.stream));
+}
+void download(Engine &e, void *dst, const void *src, size_t bytes) {
+    MDFF_CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, e.stream));
+}
+
+}  // namespace
+
+extern "C" {
+
+int mdffgpu_create(const mdffgpu_params *p, const double *rx, const double *ry, const double *rz, const double *vx,
+                   const double *vy, const double *vz, int device, mdffgpu_ctx **out) {
+    if (!p || !rx || !ry || !rz || !out) return MDFFGPU_ERR_ARG;
+    *out = nullptr;
+    mdffgpu_ctx *c = new mdffgpu_ctx();
+    c->e = nullptr;
+    try {
+        c->e = new Engine(*p, device);
+        c->e->set_positions(rx, ry, rz);
+        c->e->set_velocities(vx, vy, vz);
+    } catch (const Error &x) {
+        int code = x.code;
+        delete c->e;
+        delete c;
+        return code;
+    } catch (const std::exception &x) {
+        delete c->e;
+        delete c;
+        return MDFFGPU_ERR_CUDA;
+    }
+    *out = c;
+    return MDFFGPU_OK;
+}
+
+int mdffgpu_destroy(mdffgpu_ctx *ctx) {
+    if (!ctx) return MDFFGPU_ERR_ARG;
+    delete ctx->e;
+    delete ctx;
+    return MDFFGPU_OK;
+}
+
+const char *mdffgpu_last_error(const mdffgpu_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int mdffgpu_set_precision(mdffgpu_ctx *ctx, int precision) {
+    return guarded(ctx, [&](Engine &e) {
+        if (precision != MDFFGPU_FP64 && precision != MDFFGPU_MIXED) throw Error(MDFFGPU_ERR_ARG, "bad precision");
+        if (precision == MDFFGPU_MIXED && !mdffgpu::mixed_available())
+            throw Error(MDFFGPU_ERR_ARG, "mixed precision kernels are not built in this library");
+        e.precision = precision;
+    });
+}
+
+int mdffgpu_set_pim_solver(mdffgpu_ctx *ctx, int solver) {
+    return guarded(ctx, [&](Engine &e) {
+        if (solver != MDFFGPU_PIM_REFERENCE && solver != MDFFGPU_PIM_CG) throw Error(MDFFGPU_ERR_ARG, "bad solver");
+        e.pim_solver = solver;
+    });
+}
+
+int mdffgpu_set_positions(mdffgpu_ctx *ctx, const double *rx, const double *ry, const double *rz) {
+    if (!rx || !ry || !rz) return MDFFGPU_ERR_ARG;
+    return guarded(ctx, [&](Engine &e) { e.set_positions(rx, ry, rz); });
+}
+
+int mdffgpu_set_velocities(mdffgpu_ctx *ctx, const double *vx, const double *vy, const double *vz) {
+    return guarded(ctx, [&](Engine &e) { e.set_velocities(vx, vy, vz); });
+}
+
+int mdffgpu_get_state(mdffgpu_ctx *ctx, double *rx, double *ry, double *rz, double *vx, double *vy, double *vz,
+                      double *fx, double *fy, double *fz) {
+    return guarded(ctx, [&](Engine &e) { e.get_state(rx, ry, rz, vx, vy, vz, fx, fy, fz); });
+}
+
+int mdffgpu_set_dipole_history(mdffgpu_ctx *ctx, const double *hist) {
+    if (!hist) return MDFFGPU_ERR_ARG;
+    return guarded(ctx, [&](Engine &e) {
+        upload(e, e.d_hist, hist, sizeof(double) * 18 * (size_t)e.n);
+        MDFF_CK(cudaStreamSynchronize(e.stream));
+    });
+}
+
+int mdffgpu_get_dipole_history(mdffgpu_ctx *ctx, double *hist) {
+    if (!hist) return MDFFGPU_ERR_ARG;
+    return guarded(ctx, [&](Engine &e) {
+        download(e, hist, e.d_hist, sizeof(double) * 18 * (size_t)e.n);
+        MDFF_CK(cudaStreamSynchronize(e.stream));
+    });
+}
+
+int mdffgpu_set_nhc(mdffgpu_ctx *ctx, const double *xi, const double *vxi) {
+    if (!xi || !vxi) return MDFFGPU_ERR_ARG;
+    return guarded(ctx, [&](Engine &e) {
+        int k = e.p.nhc_n < 16 ? e.p.nhc_n : 16;
+        upload(e, e.d_nhc, xi, sizeof(double) * k);
+        upload(e, e.d_nhc + 16, vxi, sizeof(double) * k);
+        MDFF_CK(cudaStreamSynchronize(e.stream));
+    });
+}
+
+int mdffgpu_get_nhc(mdffgpu_ctx *ctx, double *xi, double *vxi) {
+    if (!xi || !vxi) return MDFFGPU_ERR_ARG;
+    return guarded(ctx, [&](Engine &e) {
+        int k = e.p.nhc_n < 16 ? e.p.nhc_n : 16;
+        download(e, xi, e.d_nhc, sizeof(double) * k);
+        download(e, vxi, e.d_nhc + 16, sizeof(double) * k);
+        MDFF_CK(cudaStreamSynchronize(e.stream));
+    });
+}
+
+int mdffgpu_get_thermo(mdffgpu_ctx *ctx, mdffgpu_thermo *t) {
+    if (!t) return MDFFGPU_ERR_ARG;
+    return guarded(ctx, [&](Engine &e) {
+        e.sync_scalars();
+        const mdffgpu::DevScalars &o = *e.h_out;
+        t->e_kin = o.e_kin;
+        t->e_nvt = o.e_nvt;
+        t->u_lj = o.u_lj;
+        t->u_bhmftd = o.u_bh;
+        t->u_coul = o.u_coul;
+        t->u_pol = o.u_pol;
+        t->pvir_lj = o.pvir_lj;
+        t->pvir_bhmftd = o.pvir_bh;
+        t->pvir_coul = o.pvir_coul;
+        memcpy(t->tau_lj, o.tau_lj, sizeof(double) * 9);
+        memcpy(t->tau_bhmftd, o.tau_bh, sizeof(double) * 9);
+        memcpy(t->tau_coul, o.tau_coul, sizeof(double) * 9);
+        t->utail = e.utail;
+        t->ptail = e.ptail;
+        t->scf_rmsd = e.last_rmsd;
+        t->scf_iter = e.last_scf_iter;
+        t->nlist_builds = o.nbuilds;
+    });
+}
+
+int mdffgpu_gen_verletlist(mdffgpu_ctx *ctx) {
+    return guarded(ctx, [&](Engine &e) { e.gen_verletlist(); });
+}
+
+int mdffgpu_check_verletlist(mdffgpu_ctx *ctx, int *rebuilt) {
+    return guarded(ctx, [&](Engine &e) {
+        int r = e.check_verletlist();
+        if (rebuilt) *rebuilt = r;
+    });
+}
+
+// the reference's half list from the full lists: keep (i, j) when the parity rule
+// of src/verlet.c:82-83 holds, ascending j
+int mdffgpu_get_verletlist(mdffgpu_ctx *ctx, int which, int *point, int *list, int cap, int *count) {
+    if (!point || (which != 0 && which != 1)) return MDFFGPU_ERR_ARG;
+    return guarded(ctx, [&](Engine &e) {
+        if (!e.list_ready) throw Error(MDFFGPU_ERR_STATE, "no Verlet list built");
+        int c = which ? e.cap_co : e.cap_nb;
+        std::vector<int> L((size_t)e.n * c), m(e.n);
+        download(e, L.data(), which ? e.d_co : e.d_nb, sizeof(int) * L.size());
+        download(e, m.data(), which ? e.d_con : e.d_nbn, sizeof(int) * e.n);
+        MDFF_CK(cudaStreamSynchronize(e.stream));
+        int tot = 0;
+        std::vector<int> row;
+        for (int i = 0; i < e.n; i++) {
+            point[i] = tot;
+            row.clear();
+            int mi = m[i] < c ? m[i] : c;
+            for (int k = 0; k < mi; k++) {
+                int j = L[(size_t)i * c + k];
+                if (((i > j) && ((i + j) % 2 == 0)) || ((i < j) && ((i + j) % 2 != 0))) row.push_back(j);
+            }
+            std::sort(row.begin(), row.end());
+            for (int j : row) {
+                if (list && tot < cap) list[tot] = j;
+                tot++;
+            }
+        }
+        point[e.n] = tot;
+        if (count) *count = tot;
+        if (list && tot > cap) throw Error(MDFFGPU_ERR_ARG, "list buffer too small");
+    });
+}
+
+int mdffgpu_engforce(mdffgpu_ctx *ctx) {
+    return guarded(ctx, [&](Engine &e) {
+        MDFF_CK(cudaMemsetAsync(e.d_status, 0, sizeof(unsigned), e.stream));
+        e.engforce();
+        e.sync_scalars();
+        e.check_status();
+    });
+}
+
+static int sr_call(mdffgpu_ctx *ctx, bool lj, double *u, double *pvir, double *tau) {
+    return guarded(ctx, [&](Engine &e) {
+        if (lj && !e.p.lnmlj) throw Error(MDFFGPU_ERR_STATE, "lnmlj is not set");
+        if (!lj && !(e.p.lbhmft || e.p.lbhmftd)) throw Error(MDFFGPU_ERR_STATE, "lbhmft/lbhmftd is not set");
+        e.ensure_lists();
+        mdffgpu::launch_kardir(e, e.d_r, e.d_s);
+        e.sr_forces(lj, nullptr, nullptr, nullptr);
+        e.sync_scalars();
+        const mdffgpu::DevScalars &o = *e.h_out;
+        if (u) *u = lj ? o.u_lj : o.u_bh;
+        if (pvir) *pvir = lj ? o.pvir_lj : o.pvir_bh;
+        if (tau) memcpy(tau, lj ? o.tau_lj : o.tau_bh, sizeof(double) * 9);
+    });
+}
+
+int mdffgpu_engforce_nmlj(mdffgpu_ctx *ctx, double *u, double *pvir, double *tau) {
+    return sr_call(ctx, true, u, pvir, tau);
+}
+
+int mdffgpu_engforce_bhmftd(mdffgpu_ctx *ctx, double *u, double *pvir, double *tau) {
+    return sr_call(ctx, false, u, pvir, tau);
+}
+
+int mdffgpu_multipole_es(mdffgpu_ctx *ctx, const double *q, const double *mu, int flags, double alpha, double *u,
+                         double *pvir, double *tau, double *ef, double *efg, double *f) {
+    if (!q || !mu) return MDFFGPU_ERR_ARG;
+    return guarded(ctx, [&](Engine &e) {
+        if (!e.p.lcoulombic) throw Error(MDFFGPU_ERR_STATE, "lcoulombic is not set");
+        size_t n = e.n;
+        double *dq = nullptr, *defg = nullptr;
+        double3 *dmu = nullptr, *def = nullptr, *df = nullptr;
+        MDFF_CK(cudaMalloc(&dq, sizeof(double) * n));
+        MDFF_CK(cudaMalloc(&dmu, sizeof(double3) * n));
+        MDFF_CK(cudaMalloc(&def, sizeof(double3) * n));
+        MDFF_CK(cudaMalloc(&df, sizeof(double3) * n));
+        MDFF_CK(cudaMalloc(&defg, sizeof(double) * 9 * n));
+        try {
+            upload(e, dq, q, sizeof(double) * n);
+            upload(e, dmu, mu, sizeof(double3) * n);
+            MDFF_CK(cudaMemsetAsync(df, 0, sizeof(double3) * n, e.stream));
+            double a = alpha > 0.0 ? alpha : e.p.alphaES;
+            e.multipole_es_dev(dq, dmu, a, flags, def, efg ? defg : nullptr, df);
+            e.sync_scalars();
+            if (ef) download(e, ef, def, sizeof(double3) * n);
+            if (efg) download(e, efg, defg, sizeof(double) * 9 * n);
+            if (f) download(e, f, df, sizeof(double3) * n);
+            MDFF_CK(cudaStreamSynchronize(e.stream));
+            if (u) *u = e.h_out->u_coul;
+            if (pvir) *pvir = e.h_out->pvir_coul;
+            if (tau) memcpy(tau, e.h_out->tau_coul, sizeof(double) * 9);
+        } catch (...) {
+            cudaFree(dq); cudaFree(dmu); cudaFree(def); cudaFree(df); cudaFree(defg);
+            throw;
+        }
+        cudaFree(dq); cudaFree(dmu); cudaFree(def); cudaFree(df); cudaFree(defg);
+    });
+}
+
+int mdffgpu_get_dipoles(mdffgpu_ctx *ctx, double *mu, double *upol) {
+    return guarded(ctx, [&](Engine &e) {
+        if (!e.p.lcoulombic) throw Error(MDFFGPU_ERR_STATE, "lcoulombic is not set");
+        e.ensure_lists();
+        mdffgpu::launch_kardir(e, e.d_r, e.d_s);
+        e.get_dipoles();
+        e.sync_scalars();
+        if (mu) download(e, mu, e.d_mu_tot, sizeof(double3) * e.n);
+        MDFF_CK(cudaStreamSynchronize(e.stream));
+        if (upol) *upol = e.h_out->u_pol;
+    });
+}
+
+int mdffgpu_prop_agate(mdffgpu_ctx *ctx, int istep) {
+    return guarded(ctx, [&](Engine &e) {
+        MDFF_CK(cudaMemsetAsync(e.d_status, 0, sizeof(unsigned), e.stream));
+        e.prop_agate(istep);
+        e.sync_scalars();
+        e.check_status();
+    });
+}
+
+int mdffgpu_md_steps(mdffgpu_ctx *ctx, int first, int nsteps, double *thermo) {
+    if (nsteps < 0) return MDFFGPU_ERR_ARG;
+    return guarded(ctx, [&](Engine &e) { e.md_steps(first, nsteps, thermo); });
+}
+
+long long mdffgpu_launch_count(const mdffgpu_ctx *ctx) { return (ctx && ctx->e) ? ctx->e->launches : -1; }
+
+void *mdffgpu_stream(const mdffgpu_ctx *ctx) { return (ctx && ctx->e) ? (void *)ctx->e->stream : nullptr; }
+
+int mdffgpu_profile(mdffgpu_ctx *ctx, const char *kernel) {
+    return guarded(ctx, [&](Engine &e) {
+        MDFF_CK(cudaStreamSynchronize(e.stream));
+        e.prof_name = kernel ? kernel : "";
+        e.prof_pairs.clear();
+        e.prof_next = 0;
+        e.prof_flops = 0.0;
+    });
+}
+
+int mdffgpu_profile_result(mdffgpu_ctx *ctx, double *ms, long long *count, double *flops) {
+    if (!ms || !count || !flops) return MDFFGPU_ERR_ARG;
+    return guarded(ctx, [&](Engine &e) { e.prof_result(ms, count, flops); });
+}
+
+}  // extern "C"

@@ -1,0 +1,112 @@
+// Shared device helpers for the mdffgpu engine (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <stdexcept>
+#include <string>
+
+#include "mdffgpu.h"
+
+namespace mdffgpu {
+
+constexpr int NT = MDFFGPU_NTMAX;
+constexpr double PI_D = 3.1415926535897932385;   // src/constants.h:11
+constexpr double TPI_D = 6.2831853071795864770;  // src/constants.h:12
+constexpr int ASPC_DEPTH = 6;                    // MAX_EXTRAPOLATE_ORDER + 1, src/pim.h:4
+
+// ------------------------------------------------------------------ errors
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+#define MDFF_CK(call)                                                                          \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            throw ::mdffgpu::Error(MDFFGPU_ERR_CUDA, std::string(#call) + ": " +               \
+                                                         cudaGetErrorString(e_) + " at " +     \
+                                                         __FILE__ + ":" + std::to_string(__LINE__)); \
+    } while (0)
+
+// device status word bits (set by kernels, read by the host after a step)
+enum StatusBits : unsigned {
+    ST_LIST_OVERFLOW = 1u,
+    ST_CELL_OVERFLOW = 2u,
+    ST_NONFINITE = 4u,
+    ST_SCF = 8u,
+};
+
+// ------------------------------------------------------------------ cell geometry
+// Lattice as in lattice() (src/cell.c:13-91); passed by value to kernels.
+struct Cell {
+    double A[3][3];   // rows: lattice vectors
+    double B[3][3];   // reciprocal rows, B[i] . A[j] = delta_ij
+    double omega, inveOmega, inveOmegaPU;
+    double w[3];      // perpendicular widths
+    int ortho;        // A and B diagonal
+};
+
+// Exactly-rounded FP64 products/sums: the reference's geometry is compiled without
+// FMA contraction (src/Makefile:17, no -mfma), and the neighbour-list pair set must
+// match it bit for bit, so these expressions are kept uncontracted.
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+
+// kardir (src/cell.c:125-143): fractional coordinates, v1 = x*B00 + y*B01 + z*B02
+__device__ __forceinline__ double3 kardir(const Cell &c, double x, double y, double z) {
+    double3 s;
+    s.x = dadd(dadd(dmul(x, c.B[0][0]), dmul(y, c.B[0][1])), dmul(z, c.B[0][2]));
+    s.y = dadd(dadd(dmul(x, c.B[1][0]), dmul(y, c.B[1][1])), dmul(z, c.B[1][2]));
+    s.z = dadd(dadd(dmul(x, c.B[2][0]), dmul(y, c.B[2][1])), dmul(z, c.B[2][2]));
+    return s;
+}
+
+// pbc (src/pbc.c:7-14): nearbyint in fractional space (round half to even = rint),
+// then back to Cartesian with A; returns the Cartesian minimum-image vector.
+__device__ __forceinline__ double3 pbc_frac(const Cell &c, double dx, double dy, double dz) {
+    double sx = dsub(dx, rint(dx));
+    double sy = dsub(dy, rint(dy));
+    double sz = dsub(dz, rint(dz));
+    double3 r;
+    r.x = dadd(dadd(dmul(sx, c.A[0][0]), dmul(sy, c.A[1][0])), dmul(sz, c.A[2][0]));
+    r.y = dadd(dadd(dmul(sx, c.A[0][1]), dmul(sy, c.A[1][1])), dmul(sz, c.A[2][1]));
+    r.z = dadd(dadd(dmul(sx, c.A[0][2]), dmul(sy, c.A[1][2])), dmul(sz, c.A[2][2]));
+    return r;
+}
+
+__device__ __forceinline__ double norm2_exact(double3 r) {
+    return dadd(dadd(dmul(r.x, r.x), dmul(r.y, r.y)), dmul(r.z, r.z));
+}
+
+// ------------------------------------------------------------------ warp helpers
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ float warp_sumf(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Neumaier (compensated) summation for FP32 accumulations in the mixed path
+struct KahanF {
+    float s, c;
+    __device__ __forceinline__ KahanF() : s(0.f), c(0.f) {}
+    __device__ __forceinline__ void add(float x) {
+        float t = s + x;
+        if (fabsf(s) >= fabsf(x)) c += (s - t) + x;
+        else c += (x - t) + s;
+        s = t;
+    }
+    __device__ __forceinline__ double value() const { return (double)s + (double)c; }
+};
+
+inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+}  // namespace mdffgpu

@@ -1,0 +1,1034 @@
+// Engine set-up and orchestration: the reference's engforce / get_dipoles /
+// prop_agate / check_verletlist sequences (src/field.c:352-407, src/coulombic.c:67-130,
+// src/integration.c:22-333, src/verlet.c:124-170) as launches on one CUDA stream.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "engine.cuh"
+
+namespace mdffgpu {
+
+// kernels defined in integrate.cu / lists.cu
+__global__ void k_reduce_slots(const double *, int, int, int, double *);
+__global__ void k_fill3(int n, double3 *a, double3 v);
+__global__ void k_copy3(int n, const double3 *a, double3 *b);
+__global__ void k_self_sums(int n, const double *q, const double3 *mu, double *part, int stride);
+__global__ void k_self_plus_dir(int n, double self2, const double3 *mu, const double3 *efd, double3 *ef);
+__global__ void k_axpy3(int n, double a, const double3 *x, double3 *y);
+__global__ void k_efg_self_dir(int n, double self2, const double *q, const double *efgd, double *efg);
+__global__ void k_finalize_sr(const double *scal, int slot, double inveOmegaPU, double *u, double *pvir,
+                              double *tau);
+struct CoulFin {
+    double alpha, coul, inveOmegaPU, ttpiV;
+    int do_dir, do_rec, do_stress;
+};
+__global__ void k_finalize_coul(const double *scal, CoulFin c, double *u, double *pvir, double *tau);
+__global__ void k_induced(int n, const int *polar, const double *pol, const double3 *ef, double3 *mu);
+__global__ void k_aspc_predict(int n, int e, int es, double *hist, double3 *mu);
+__global__ void k_aspc_correct(int n, double W, const int *polar, const double *pol, const double3 *ef,
+                               double3 *mu);
+__global__ void k_add3(int n, const double3 *a, const double3 *b, double3 *c);
+__global__ void k_pim_sums(int n, const int *polar, const double *pol, const double *invpol, const double3 *mu,
+                           const double3 *ef, double *part, int stride);
+__global__ void k_hist_store(int n, const double3 *mu, double *hist);
+__global__ void k_ko_find(int n, const int *polar, const double *invpol, const double3 *ef, const double3 *mu,
+                          double3 *find);
+__global__ void k_scale_add3(int n, double a, const double3 *x, double b, double3 *y);
+__global__ void k_cg_residual(int n, const int *polar, const double *invpol, const double3 *efs,
+                              const double3 *tx, const double3 *x, double3 *r);
+__global__ void k_cg_ap(int n, const int *polar, const double *invpol, const double3 *p, const double3 *tp,
+                        double3 *ap, double *part, int stride);
+__global__ void k_cg_rz(int n, const int *polar, const double *pol, const double3 *r, double3 *z, double *part,
+                        int stride);
+__global__ void k_cg_update(int n, const double *scal, const double3 *p, const double3 *ap, double3 *x, double3 *r);
+__global__ void k_cg_dir(int n, const double *scal, const double3 *z, double3 *p);
+__global__ void k_copy_slot(double *scal, int from, int to);
+__global__ void k_vv1(int n, double dt, double dtsq2, const double *invm, double4 *r, const double3 *v,
+                      const double3 *f, double3 *fs);
+__global__ void k_vv2(int n, double dt2, const double *invm, const double *mass, double3 *v, const double3 *f,
+                      const double3 *fs, double *part, int stride);
+__global__ void k_pv1(int n, double dt, double dt2, const double *invm, double4 *r, double3 *v, const double3 *f);
+__global__ void k_pv2(int n, double dt2, const double *invm, const double *mass, double3 *v, const double3 *f,
+                      double *part, int stride);
+__global__ void k_scale_kin(int n, const DevScalars *out, int scale, const double *mass, double3 *v, double *part,
+                            int stride);
+__global__ void k_lf(int n, double dtsq, double idt, const double *invm, const double *mass, double4 *r,
+                     double3 *rs, double3 *v, const double3 *f, double *part, int stride);
+struct NhcArgs {
+    int nn, yo, mults;
+    double dt, temp, L, w[7];
+};
+__global__ void k_nhc_chain(NhcArgs a, double *nhc, const double *scal, DevScalars *out);
+__global__ void k_nhc_energy(int nn, double L, double temp, const double *nhc, const double *scal,
+                             DevScalars *out);
+__global__ void k_set_ekin(const double *scal, DevScalars *out);
+__global__ void k_check_finite(int n, const double4 *r, const double3 *f, unsigned *status);
+__global__ void k_sort_cells(int ncell, int cell_cap, const int *start, const int *cnt, int *ions,
+                             const int *rebuild);
+
+template <typename T>
+static T *dalloc(size_t count) {
+    T *p = nullptr;
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc((void **)&p, sizeof(T) * count);
+    if (e != cudaSuccess) throw Error(MDFFGPU_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    cudaMemset(p, 0, sizeof(T) * count);
+    return p;
+}
+template <typename T>
+static void dfree(T *&p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+// 3x3 inverse by Gauss-Jordan with partial pivoting (1/a_ii for a diagonal input),
+// standing in for invertmatrix3x3 (src/inverse_matrix.c:5-20, src/config.c:171)
+static void invert3(const double in[3][3], double out[3][3]) {
+    double m[3][6];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            m[i][j] = in[i][j];
+            m[i][j + 3] = (i == j);
+        }
+    for (int c = 0; c < 3; c++) {
+        int p = c;
+        for (int r = c + 1; r < 3; r++)
+            if (std::fabs(m[r][c]) > std::fabs(m[p][c])) p = r;
+        if (m[p][c] == 0.0) continue;
+        if (p != c)
+            for (int j = 0; j < 6; j++) std::swap(m[c][j], m[p][j]);
+        double inv = 1.0 / m[c][c];
+        for (int j = 0; j < 6; j++) m[c][j] = (j == c) ? 1.0 : m[c][j] * inv;
+        for (int r = 0; r < 3; r++) {
+            if (r == c || m[r][c] == 0.0) continue;
+            double f = m[r][c];
+            for (int j = 0; j < 6; j++) m[r][j] -= f * m[c][j];
+        }
+    }
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) out[i][j] = m[i][j + 3];
+}
+
+// ---------------------------------------------------------------- set-up
+Engine::Engine(const mdffgpu_params &prm, int dev) : p(prm) {
+    if (p.nion <= 0 || p.ntype <= 0 || p.ntype > NT) throw Error(MDFFGPU_ERR_ARG, "bad nion/ntype");
+    int sum = 0;
+    for (int t = 0; t < p.ntype; t++) sum += p.nionit[t];
+    if (sum != p.nion) throw Error(MDFFGPU_ERR_ARG, "nionit does not sum to nion");  // src/config.c:112-121
+    n = p.nion;
+    nt = p.ntype;
+    if (dev >= 0) MDFF_CK(cudaSetDevice(dev));
+    MDFF_CK(cudaGetDevice(&device));
+    MDFF_CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    setup_units_and_cell();
+    setup_types();
+    // device buffers
+    d_r = dalloc<double4>(n);
+    d_s = dalloc<double4>(n);
+    d_v = dalloc<double3>(n);
+    d_f = dalloc<double3>(n);
+    d_f2 = dalloc<double3>(n);
+    d_rs = dalloc<double3>(n);
+    d_mu_ind = dalloc<double3>(n);
+    d_mu_tot = dalloc<double3>(n);
+    d_ef_stat = dalloc<double3>(n);
+    d_ef_ind = dalloc<double3>(n);
+    d_ef = dalloc<double3>(n);
+    d_cg_r = dalloc<double3>(n);
+    d_cg_p = dalloc<double3>(n);
+    d_cg_ap = dalloc<double3>(n);
+    d_mu_save = dalloc<double3>(n);
+    d_tmp3 = dalloc<double3>(n);
+    d_hist = dalloc<double>((size_t)n * ASPC_DEPTH * 3);
+    d_efg = dalloc<double>((size_t)n * 9);
+    d_qzero = dalloc<double>(n);
+    d_muzero = dalloc<double3>(n);
+    d_svl = dalloc<double4>(n);
+    d_rebuild = dalloc<int>(1);
+    d_status = dalloc<unsigned>(1);
+    d_scal = dalloc<double>(NSLOT);
+    d_out = dalloc<DevScalars>(1);
+    d_nhc = dalloc<double>(48);
+    MDFF_CK(cudaMallocHost((void **)&h_out, sizeof(DevScalars)));
+    MDFF_CK(cudaMallocHost((void **)&h_stage, sizeof(double) * 10 * (size_t)n));
+    memset(h_out, 0, sizeof(DevScalars));
+    if (p.lcoulombic) setup_kspace();
+    int nkb = nk > 0 ? ceil_div(nk, 256) : 1;
+    part_stride = std::max(ceil_div(n, 8), nkb) + 8;
+    d_part = dalloc<double>((size_t)NSLOT * part_stride);
+    // neighbour lists: initial capacities from the number density
+    double rho = n * cell.inveOmega;
+    double cnb = p.cutshortrange + (p.lverletL ? p.skindiff : 0.0);
+    double cco = p.cutlongrange + (p.lverletL ? p.skindiff : 0.0);
+    auto cap_for = [&](double cut) {
+        double e = rho * 4.0 / 3.0 * PI_D * cut * cut * cut;
+        int c = (int)(1.4 * e) + 64;
+        c = (c + 31) / 32 * 32;
+        return std::max(32, std::min(c, ((n + 31) / 32) * 32));
+    };
+    setup_cells();
+    alloc_lists(cap_for(cnb), cap_for(cco));
+    // NHC masses Q (src/integration.c:146-150)
+    double L = 3.0 * (double)n;
+    std::vector<double> nhc(48, 0.0);
+    for (int i = 0; i < p.nhc_n && i < 16; i++) nhc[32 + i] = timesca * timesca * temp;
+    nhc[32] *= L;
+    MDFF_CK(cudaMemcpy(d_nhc, nhc.data(), sizeof(double) * 48, cudaMemcpyHostToDevice));
+    MDFF_CK(cudaDeviceSynchronize());
+}
+
+Engine::~Engine() {
+    if (stream) cudaStreamSynchronize(stream);
+    for (auto ev : prof_pool) cudaEventDestroy(ev);
+    double4 *d4[] = {d_r, d_s, d_svl};
+    for (auto &x : d4) cudaFree(x);
+    double3 *d3[] = {d_v, d_f, d_f2, d_rs, d_mu_static, d_mu_ind, d_mu_tot, d_ef_stat, d_ef_ind, d_ef, d_cg_r,
+                     d_cg_p, d_cg_ap, d_mu_save, d_tmp3, d_muzero, d_kvec};
+    for (auto &x : d3) cudaFree(x);
+    double *dd[] = {d_mass, d_invmass, d_q, d_pol, d_invpol, d_hist, d_efg, d_qzero, d_Ak, d_kcoe, d_part, d_scal,
+                    d_nhc};
+    for (auto &x : dd) cudaFree(x);
+    int *di[] = {d_typ, d_polar, d_nb, d_nbn, d_co, d_con, d_cell_of, d_cell_cnt, d_cell_start, d_cell_cur,
+                 d_cell_ions, d_rebuild, d_tile_row, d_tile_k};
+    for (auto &x : di) cudaFree(x);
+    cudaFree(d_pair);
+    cudaFree(d_damp);
+    cudaFree(d_seg);
+    cudaFree(d_row);
+    cudaFree(d_rho_part);
+    cudaFree(d_rho);
+    cudaFree(d_out);
+    cudaFree(d_status);
+    if (h_out) cudaFreeHost(h_out);
+    if (h_stage) cudaFreeHost(h_stage);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+void Engine::setup_units_and_cell() {
+    if (p.lreduced) {
+        boltz_unit = time_unit = press_unit = coul_unit = 1.0;
+    } else {
+        boltz_unit = 8.61734229648141E-05;
+        time_unit = 98.2269514139276;
+        press_unit = 0.00624150964712042;
+        coul_unit = 14.3996441494161;
+    }
+    // lattice(), src/cell.c:13-91
+    Cell &c = cell;
+    memcpy(c.A, p.cell, sizeof(c.A));
+    auto cross = [](const double *a, const double *b, double *h) {
+        h[0] = a[1] * b[2] - a[2] * b[1];
+        h[1] = a[2] * b[0] - a[0] * b[2];
+        h[2] = a[0] * b[1] - a[1] * b[0];
+    };
+    cross(c.A[1], c.A[2], c.B[0]);
+    cross(c.A[2], c.A[0], c.B[1]);
+    cross(c.A[0], c.A[1], c.B[2]);
+    double omega = c.B[0][0] * c.A[0][0] + c.B[1][0] * c.A[1][0] + c.B[2][0] * c.A[2][0];
+    if (!(omega > 0.0)) throw Error(MDFFGPU_ERR_ARG, "cell volume must be positive");
+    c.omega = omega;
+    c.inveOmega = 1.0 / omega;
+    c.inveOmegaPU = 1.0 / (omega * press_unit);
+    for (int i = 0; i < 3; i++)
+        c.w[i] = omega / std::sqrt(c.B[0][i] * c.B[0][i] + c.B[1][i] * c.B[1][i] + c.B[2][i] * c.B[2][i]);
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) c.B[i][j] = c.B[i][j] * c.inveOmega;
+    c.ortho = 1;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++)
+            if (i != j && (c.A[i][j] != 0.0)) c.ortho = 0;
+    // check_md, src/md.c:120-127
+    tauT = p.tauTberendsen;
+    if (p.nequil > 0 && tauT == 0.0) tauT = p.dt;
+    temp = p.temp * boltz_unit;
+    dt = p.dt * time_unit;
+    tauT *= time_unit;
+    timesca = p.timesca_thermo * time_unit;
+    srcutsq = p.cutshortrange * p.cutshortrange;
+    lrcutsq = p.cutlongrange * p.cutlongrange;
+}
+
+void Engine::setup_types() {
+    // flags of read_field / info_field (src/field.c:97-108, 195-221)
+    for (int t = 0; t < nt; t++) {
+        lpolar[t] = 0;
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++)
+                if (p.polit[t][i][j] != 0.0) lpolar[t] = 1, lpol = 1;
+        if (p.qit[t] != 0.0) lqch = 1;
+        for (int j = 0; j < 3; j++)
+            if (p.dipit[t][j] != 0.0) ldip = 1;
+    }
+    // the damping tables' in-place symmetrisation loop, src/field.c:209-219
+    for (int it = 0; it < nt; it++)
+        for (int jt = 0; jt < nt; jt++)
+            for (int kt = 0; kt < nt; kt++) {
+                if (p.lpoldamping[jt][it][kt]) ldmp = 1;
+                p.lpoldamping[jt][kt][it] = p.lpoldamping[jt][it][kt];
+                p.pol_damp_b[jt][kt][it] = p.pol_damp_b[jt][it][kt];
+                p.pol_damp_c[jt][kt][it] = p.pol_damp_c[jt][it][kt];
+                p.pol_damp_k[jt][kt][it] = p.pol_damp_k[jt][it][kt];
+            }
+    for (int t = 0; t < nt; t++)
+        if (lpolar[t]) lpim = 1;
+    if (!p.lcoulombic) lqch = ldip = lpol = ldmp = lpim = 0;
+    for (int t = 0; t < nt; t++)
+        for (int i = 0; i < nt; i++)
+            for (int j = 0; j < nt; j++)
+                if (p.pol_damp_k[t][i][j] < 0 || p.pol_damp_k[t][i][j] > 8)
+                    throw Error(MDFFGPU_ERR_ARG, "pol_damp_k must be in 0..8 (MAX_TT_EXPANSION, src/tt_damp.h:3)");
+
+    // per ion (init_config, src/config.c:124-198)
+    h_typ.resize(n);
+    std::vector<double> mass(n), invm(n), q(n, 0.0), pol((size_t)n * 9, 0.0), invpol((size_t)n * 9, 0.0);
+    std::vector<double3> mus(n, make_double3(0, 0, 0));
+    std::vector<int> polar(n, 0);
+    int ia = 0;
+    for (int t = 0; t < nt; t++) {
+        double ip[3][3];
+        if (lpolar[t]) invert3(p.polit[t], ip);
+        for (int k = 0; k < p.nionit[t]; k++, ia++) {
+            h_typ[ia] = t;
+            mass[ia] = p.massit[t];
+            invm[ia] = 1.0 / p.massit[t];
+            if (p.lcoulombic) {
+                q[ia] = p.qit[t];
+                mus[ia] = make_double3(p.dipit[t][0], p.dipit[t][1], p.dipit[t][2]);
+                if (lpolar[t]) {
+                    polar[ia] = 1;
+                    for (int i = 0; i < 3; i++)
+                        for (int j = 0; j < 3; j++) {
+                            pol[(size_t)ia * 9 + 3 * i + j] = p.polit[t][i][j];
+                            invpol[(size_t)ia * 9 + 3 * i + j] = ip[i][j];
+                        }
+                }
+            }
+        }
+    }
+    npol = 0;
+    for (int i = 0; i < n; i++) npol += polar[i];
+    h_q = q;
+    d_typ = dalloc<int>(n);
+    d_mass = dalloc<double>(n);
+    d_invmass = dalloc<double>(n);
+    d_q = dalloc<double>(n);
+    d_pol = dalloc<double>((size_t)n * 9);
+    d_invpol = dalloc<double>((size_t)n * 9);
+    d_polar = dalloc<int>(n);
+    d_mu_static = dalloc<double3>(n);
+    MDFF_CK(cudaMemcpy(d_typ, h_typ.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    MDFF_CK(cudaMemcpy(d_mass, mass.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+    MDFF_CK(cudaMemcpy(d_invmass, invm.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+    MDFF_CK(cudaMemcpy(d_q, q.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+    MDFF_CK(cudaMemcpy(d_pol, pol.data(), sizeof(double) * 9 * n, cudaMemcpyHostToDevice));
+    MDFF_CK(cudaMemcpy(d_invpol, invpol.data(), sizeof(double) * 9 * n, cudaMemcpyHostToDevice));
+    MDFF_CK(cudaMemcpy(d_polar, polar.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    MDFF_CK(cudaMemcpy(d_mu_static, mus.data(), sizeof(double3) * n, cudaMemcpyHostToDevice));
+
+    // pair tables: init_nmlj (src/nmlj.c:198-247) and init_bhmftd (src/bhmftd.c:99-110)
+    std::vector<PairSR> pr((size_t)nt * nt);
+    if (p.lnmlj) {
+        double two16 = std::pow(2.0, 1.0 / 6.0);
+        double srcut3 = srcutsq * p.cutshortrange;
+        for (int it = 0; it < nt; it++)
+            for (int jt = 0; jt < nt; jt++) {
+                if (jt >= it) {
+                    p.plj[jt][it] = p.plj[it][jt];
+                    p.qlj[jt][it] = p.qlj[it][jt];
+                    p.sigmalj[jt][it] = p.sigmalj[it][jt];
+                    p.epslj[jt][it] = p.epslj[it][jt];
+                }
+                double pp = p.plj[it][jt], qq = p.qlj[it][jt];
+                PairSR &P = pr[(size_t)it * nt + jt];
+                P.epsqp = p.epslj[it][jt] / (qq - pp);
+                P.sigsq = two16 * two16 * p.sigmalj[it][jt] * p.sigmalj[it][jt];
+                P.fc = (pp * qq * P.epsqp) / P.sigsq;
+                P.ptwo = pp * 0.5;
+                P.qtwo = qq * 0.5;
+                P.plj = pp;
+                P.qlj = qq;
+                double sr2 = P.sigsq / srcutsq, sr = std::sqrt(sr2);
+                double srp = std::pow(sr, pp), srq = std::pow(sr, qq);
+                P.uc = P.epsqp * (pp * srq - qq * srp);
+                auto as_int = [](double x) { return (x == std::floor(x) && x >= 0 && x <= 64) ? (int)x : -1; };
+                P.ip = as_int(P.ptwo);
+                P.iq = as_int(P.qtwo);
+                double ut = P.epsqp * (pp * srq / (qq - 3.0) - qq * srp / (pp - 3.0));
+                double pt = pp * qq * P.epsqp * (srq / (qq - 3.0) - srp / (pp - 3.0));
+                ut *= srcut3 * TPI_D;
+                pt *= srcut3 * TPI_D;
+                if (p.nionit[it] && p.nionit[jt]) {
+                    utail += ut * p.nionit[it] * p.nionit[jt] * cell.inveOmega;
+                    ptail += pt * p.nionit[it] * p.nionit[jt] * cell.inveOmega;
+                }
+            }
+        ptail = ptail / (press_unit * 3.0);
+    }
+    if (p.lbhmft || p.lbhmftd) {
+        for (int it = 0; it < nt; it++)
+            for (int jt = it; jt < nt; jt++) {
+                p.Abhmftd[jt][it] = p.Abhmftd[it][jt];
+                p.Bbhmftd[jt][it] = p.Bbhmftd[it][jt];
+                p.Cbhmftd[jt][it] = p.Cbhmftd[it][jt];
+                p.Dbhmftd[jt][it] = p.Dbhmftd[it][jt];
+                p.BDbhmftd[jt][it] = p.BDbhmftd[it][jt];
+            }
+        for (int it = 0; it < nt; it++)
+            for (int jt = 0; jt < nt; jt++) {
+                PairSR &P = pr[(size_t)it * nt + jt];
+                P.A = p.Abhmftd[it][jt];
+                P.B = p.Bbhmftd[it][jt];
+                P.C = p.Cbhmftd[it][jt];
+                P.D = p.Dbhmftd[it][jt];
+                P.BD = p.BDbhmftd[it][jt];
+            }
+    }
+    d_pair = dalloc<PairSR>((size_t)nt * nt);
+    MDFF_CK(cudaMemcpy(d_pair, pr.data(), sizeof(PairSR) * nt * nt, cudaMemcpyHostToDevice));
+    std::vector<PairDamp> dm((size_t)nt * nt);
+    for (int a = 0; a < nt; a++)
+        for (int b = 0; b < nt; b++) {
+            PairDamp &D = dm[(size_t)a * nt + b];
+            D.ldamp = (p.lpoldamping[a][a][b] || p.lpoldamping[b][a][b]) ? 1 : 0;
+            D.b1 = p.pol_damp_b[a][a][b];
+            D.c1 = p.pol_damp_c[a][a][b];
+            D.k1 = p.pol_damp_k[a][a][b];
+            D.b2 = p.pol_damp_b[b][a][b];
+            D.c2 = p.pol_damp_c[b][a][b];
+            D.k2 = p.pol_damp_k[b][a][b];
+            D.pad = 0;
+        }
+    d_damp = dalloc<PairDamp>((size_t)nt * nt);
+    MDFF_CK(cudaMemcpy(d_damp, dm.data(), sizeof(PairDamp) * nt * nt, cudaMemcpyHostToDevice));
+}
+
+// k-vectors in the reference's generation order (set_param_kmesh, src/kspace.c:64-102),
+// grouped in rows of fixed (nx, ny)
+void Engine::setup_kspace() {
+    for (int d = 0; d < 3; d++) {
+        kmax[d] = p.kES[d];
+        if (kmax[d] < 0) throw Error(MDFFGPU_ERR_ARG, "kES must be >= 0");
+    }
+    int K0 = kmax[0], K1 = kmax[1], K2 = kmax[2];
+    nk = K2 + K1 * (2 * K2 + 1) + K0 * (2 * K1 + 1) * (2 * K2 + 1);
+    if (nk <= 0) throw Error(MDFFGPU_ERR_ARG, "empty k mesh");
+    std::vector<double3> kv(nk);
+    std::vector<double> Ak(nk), kcoe(nk);
+    std::vector<KRow> rows;
+    std::vector<KSeg> segs;
+    double alpha2 = p.alphaES * p.alphaES;
+    const Cell &c = cell;
+    int ik = 0;
+    for (int nx = 0; nx < K0 + 1; nx++) {
+        int nymin = (nx == 0) ? 0 : -K1;
+        for (int ny = nymin; ny < K1 + 1; ny++) {
+            int nzmin = (nx == 0 && ny == 0) ? 1 : -K2;
+            KRow R;
+            R.nx = nx;
+            R.ny = ny;
+            R.z0 = nzmin;
+            R.cnt = K2 - nzmin + 1;
+            R.koff = ik;
+            R.pad0 = R.pad1 = R.pad2 = 0;
+            if (R.cnt <= 0) continue;
+            rows.push_back(R);
+            for (int z0 = nzmin; z0 <= K2; z0 += KSEG) {
+                KSeg S;
+                S.nx = nx;
+                S.ny = ny;
+                S.z0 = z0;
+                S.cnt = std::min(KSEG, K2 - z0 + 1);
+                S.koff = ik + (z0 - nzmin);
+                S.pad0 = S.pad1 = S.pad2 = 0;
+                segs.push_back(S);
+            }
+            for (int nz = nzmin; nz < K2 + 1; nz++) {
+                double kx = TPI_D * ((double)nx * c.B[0][0] + (double)ny * c.B[0][1] + (double)nz * c.B[0][2]);
+                double ky = TPI_D * ((double)nx * c.B[1][0] + (double)ny * c.B[1][1] + (double)nz * c.B[1][2]);
+                double kz = TPI_D * ((double)nx * c.B[2][0] + (double)ny * c.B[2][1] + (double)nz * c.B[2][2]);
+                double kk = kx * kx + ky * ky + kz * kz;
+                kv[ik] = make_double3(kx, ky, kz);
+                Ak[ik] = std::exp(-kk * 0.25 / alpha2) / kk;
+                kcoe[ik] = 2.0 * (1.0 / kk + 1.0 / alpha2 / 4.0);
+                ik++;
+            }
+        }
+    }
+    nrow = (int)rows.size();
+    nseg = (int)segs.size();
+    // ion-pass tiles: whole rows, at most 2048 k per tile (32 KB of shared memory)
+    const int TILEK = 2048;
+    h_tile_row.clear();
+    h_tile_k.clear();
+    int r = 0;
+    tile_kmax = 0;
+    while (r < nrow) {
+        int k0 = rows[r].koff, cnt = 0, r1 = r;
+        while (r1 < nrow && cnt + rows[r1].cnt <= TILEK) {
+            cnt += rows[r1].cnt;
+            r1++;
+        }
+        if (r1 == r) throw Error(MDFFGPU_ERR_ARG, "k row longer than a tile");
+        h_tile_row.push_back(r);
+        h_tile_k.push_back(k0);
+        tile_kmax = std::max(tile_kmax, cnt);
+        r = r1;
+    }
+    h_tile_row.push_back(nrow);
+    h_tile_k.push_back(nk);
+    ntile = (int)h_tile_row.size() - 1;
+    d_kvec = dalloc<double3>(nk);
+    d_Ak = dalloc<double>(nk);
+    d_kcoe = dalloc<double>(nk);
+    d_row = dalloc<KRow>(nrow);
+    d_seg = dalloc<KSeg>(nseg);
+    d_tile_row = dalloc<int>(ntile + 1);
+    d_tile_k = dalloc<int>(ntile + 1);
+    MDFF_CK(cudaMemcpy(d_kvec, kv.data(), sizeof(double3) * nk, cudaMemcpyHostToDevice));
+    MDFF_CK(cudaMemcpy(d_Ak, Ak.data(), sizeof(double) * nk, cudaMemcpyHostToDevice));
+    MDFF_CK(cudaMemcpy(d_kcoe, kcoe.data(), sizeof(double) * nk, cudaMemcpyHostToDevice));
+    MDFF_CK(cudaMemcpy(d_row, rows.data(), sizeof(KRow) * nrow, cudaMemcpyHostToDevice));
+    MDFF_CK(cudaMemcpy(d_seg, segs.data(), sizeof(KSeg) * nseg, cudaMemcpyHostToDevice));
+    MDFF_CK(cudaMemcpy(d_tile_row, h_tile_row.data(), sizeof(int) * (ntile + 1), cudaMemcpyHostToDevice));
+    MDFF_CK(cudaMemcpy(d_tile_k, h_tile_k.data(), sizeof(int) * (ntile + 1), cudaMemcpyHostToDevice));
+    // rho pass grid: segment blocks x ion chunks, about two waves of the SMs
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+    int segblocks = ceil_div(nseg, 128);
+    int chunks = std::max(1, ceil_div(2 * nsm, segblocks));
+    chunks = std::min(chunks, std::max(1, ceil_div(n, 32)));
+    rho_chunk = ceil_div(n, chunks);
+    rho_chunks = ceil_div(n, rho_chunk);
+    d_rho_part = dalloc<double2>((size_t)rho_chunks * nk);
+    d_rho = dalloc<double2>(nk);
+}
+
+void Engine::setup_cells() {
+    double cnb = p.cutshortrange + (p.lverletL ? p.skindiff : 0.0);
+    double cco = p.cutlongrange + (p.lverletL ? p.skindiff : 0.0);
+    double cut = std::max(cnb, cco);
+    for (int d = 0; d < 3; d++) {
+        int c = cut > 0 ? (int)std::floor(cell.w[d] / cut) : 1;
+        nc[d] = (c >= 3 && cell.ortho) ? std::min(c, 64) : 1;
+    }
+    ncell = nc[0] * nc[1] * nc[2];
+    int cap = 4096;
+    if (ncell == 1) {
+        cap = 1;
+        while (cap < n) cap <<= 1;
+        if (cap > 12288) throw Error(MDFFGPU_ERR_CELL, "cell too small for a cell list and too many ions to scan");
+    }
+    cell_cap = cap;
+    if (cell_cap * sizeof(int) > 48 * 1024) {
+        MDFF_CK(cudaFuncSetAttribute(k_sort_cells, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(cell_cap * sizeof(int))));
+    }
+    d_cell_of = dalloc<int>(n);
+    d_cell_cnt = dalloc<int>(ncell);
+    d_cell_start = dalloc<int>(ncell);
+    d_cell_cur = dalloc<int>(ncell);
+    d_cell_ions = dalloc<int>(n);
+}
+
+void Engine::alloc_lists(int cnb, int cco) {
+    dfree(d_nb);
+    dfree(d_nbn);
+    dfree(d_co);
+    dfree(d_con);
+    cap_nb = cnb;
+    cap_co = cco;
+    d_nb = dalloc<int>((size_t)n * cap_nb);
+    d_nbn = dalloc<int>(n);
+    d_co = dalloc<int>((size_t)n * cap_co);
+    d_con = dalloc<int>(n);
+    list_ready = false;
+}
+
+// ---------------------------------------------------------------- state
+// host<->device transfers go through one pinned staging block h_stage (10 doubles/ion)
+void Engine::set_positions(const double *rx, const double *ry, const double *rz) {
+    double4 *r4 = (double4 *)h_stage;
+    for (int i = 0; i < n; i++) r4[i] = make_double4(rx[i], ry[i], rz[i], h_q[i]);
+    MDFF_CK(cudaMemcpyAsync(d_r, r4, sizeof(double4) * n, cudaMemcpyHostToDevice, stream));
+    MDFF_CK(cudaStreamSynchronize(stream));
+    if (!p.lverletL) list_ready = false;
+}
+
+void Engine::set_velocities(const double *vx, const double *vy, const double *vz) {
+    double3 *v = (double3 *)(h_stage + 4 * (size_t)n);
+    for (int i = 0; i < n; i++) v[i] = make_double3(vx ? vx[i] : 0.0, vy ? vy[i] : 0.0, vz ? vz[i] : 0.0);
+    MDFF_CK(cudaMemcpyAsync(d_v, v, sizeof(double3) * n, cudaMemcpyHostToDevice, stream));
+    MDFF_CK(cudaStreamSynchronize(stream));
+}
+
+void Engine::get_state(double *rx, double *ry, double *rz, double *vx, double *vy, double *vz, double *fx,
+                       double *fy, double *fz) {
+    double4 *r = (double4 *)h_stage;
+    double3 *v = (double3 *)(h_stage + 4 * (size_t)n);
+    double3 *f = (double3 *)(h_stage + 7 * (size_t)n);
+    if (rx || ry || rz) MDFF_CK(cudaMemcpyAsync(r, d_r, sizeof(double4) * n, cudaMemcpyDeviceToHost, stream));
+    if (vx || vy || vz) MDFF_CK(cudaMemcpyAsync(v, d_v, sizeof(double3) * n, cudaMemcpyDeviceToHost, stream));
+    if (fx || fy || fz) MDFF_CK(cudaMemcpyAsync(f, d_f, sizeof(double3) * n, cudaMemcpyDeviceToHost, stream));
+    MDFF_CK(cudaStreamSynchronize(stream));
+    for (int i = 0; i < n; i++) {
+        if (rx) rx[i] = r[i].x;
+        if (ry) ry[i] = r[i].y;
+        if (rz) rz[i] = r[i].z;
+        if (vx) vx[i] = v[i].x;
+        if (vy) vy[i] = v[i].y;
+        if (vz) vz[i] = v[i].z;
+        if (fx) fx[i] = f[i].x;
+        if (fy) fy[i] = f[i].y;
+        if (fz) fz[i] = f[i].z;
+    }
+}
+
+void Engine::sync_scalars() {
+    MDFF_CK(cudaMemcpyAsync(h_out, d_out, sizeof(DevScalars), cudaMemcpyDeviceToHost, stream));
+    MDFF_CK(cudaMemcpyAsync(&h_out->status, d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+    MDFF_CK(cudaStreamSynchronize(stream));
+}
+
+void Engine::check_status() {
+    unsigned st = (unsigned)h_out->status;
+    if (st & ST_CELL_OVERFLOW) throw Error(MDFFGPU_ERR_LIST_OVERFLOW, "a cell holds more ions than its capacity");
+    if (st & ST_NONFINITE) throw Error(MDFFGPU_ERR_NONFINITE, "non-finite positions or forces");
+}
+
+// ---------------------------------------------------------------- lists
+// build (forced) and grow the capacities until nothing overflows
+void Engine::gen_verletlist() {
+    for (int attempt = 0; attempt < 8; attempt++) {
+        MDFF_CK(cudaMemsetAsync(d_status, 0, sizeof(unsigned), stream));
+        launch_kardir(*this, d_r, d_s);
+        launch_build_lists(*this, true);
+        unsigned st = 0;
+        MDFF_CK(cudaMemcpyAsync(&st, d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+        MDFF_CK(cudaStreamSynchronize(stream));
+        if (st & ST_CELL_OVERFLOW) throw Error(MDFFGPU_ERR_LIST_OVERFLOW, "cell capacity exceeded");
+        if (!(st & ST_LIST_OVERFLOW)) {
+            list_ready = true;
+            return;
+        }
+        // read the largest counts and grow
+        std::vector<int> a(n), b(n);
+        MDFF_CK(cudaMemcpy(a.data(), d_nbn, sizeof(int) * n, cudaMemcpyDeviceToHost));
+        MDFF_CK(cudaMemcpy(b.data(), d_con, sizeof(int) * n, cudaMemcpyDeviceToHost));
+        int ma = *std::max_element(a.begin(), a.end()), mb = *std::max_element(b.begin(), b.end());
+        int na = std::max(cap_nb, (ma * 5 / 4 + 63) / 32 * 32), nb = std::max(cap_co, (mb * 5 / 4 + 63) / 32 * 32);
+        alloc_lists(na, nb);
+    }
+    throw Error(MDFFGPU_ERR_LIST_OVERFLOW, "neighbour list capacity could not be grown");
+}
+
+int Engine::check_verletlist() {
+    if (!list_ready) {
+        gen_verletlist();
+        return 1;
+    }
+    MDFF_CK(cudaMemsetAsync(d_status, 0, sizeof(unsigned), stream));
+    launch_kardir(*this, d_r, d_s);
+    launch_check_list(*this);
+    launch_build_lists(*this, false);
+    int rb = 0;
+    unsigned st = 0;
+    MDFF_CK(cudaMemcpyAsync(&rb, d_rebuild, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    MDFF_CK(cudaMemcpyAsync(&st, d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+    MDFF_CK(cudaStreamSynchronize(stream));
+    if (st & ST_LIST_OVERFLOW) {
+        gen_verletlist();   // positions unchanged: rebuild with larger capacity
+        return 1;
+    }
+    if (st & ST_CELL_OVERFLOW) throw Error(MDFFGPU_ERR_LIST_OVERFLOW, "cell capacity exceeded");
+    return rb;
+}
+
+void Engine::ensure_lists() {
+    if (!p.lverletL) {
+        gen_verletlist();   // the reference scans all pairs each call: rebuild at the cutoff itself
+        return;
+    }
+    if (!list_ready) throw Error(MDFFGPU_ERR_STATE, "no Verlet list: call gen_verletlist first");
+}
+
+// ---------------------------------------------------------------- force evaluation
+void Engine::sr_forces(bool lj, double *u, double *pvir, double *tau) {
+    launch_sr(*this, lj);
+    int slot = lj ? S_LJ_U : S_BH_U;
+    reduce(slot, 7, ceil_div(n, 8));
+    DevScalars *o = d_out;
+    if (lj)
+        MDFF_LAUNCH(*this, k_finalize_sr, 1, 1, 0, d_scal, slot, cell.inveOmegaPU, &o->u_lj, &o->pvir_lj, o->tau_lj);
+    else
+        MDFF_LAUNCH(*this, k_finalize_sr, 1, 1, 0, d_scal, slot, cell.inveOmegaPU, &o->u_bh, &o->pvir_bh, o->tau_bh);
+    (void)u;
+    (void)pvir;
+    (void)tau;
+}
+
+static double self2_of(double alpha) {
+    const double rpi = 1.7724538509055160273;
+    double selfa = alpha / rpi, selfa2 = 2.0 * selfa * alpha * alpha / 3.0;
+    return 2.0 * selfa2;
+}
+
+// electric field of (q, mu): self + direct + reciprocal, as multipole_ES with
+// do_ef only (src/ewald.c:75-348); no energy, no forces
+void Engine::field_of(const double *d_qv, const double3 *d_muv, bool lq, bool ld, bool damp, double3 *d_ef_out) {
+    launch_dir(*this, d_qv, d_muv, p.alphaES, lq, ld, damp, false, true, false, false, d_tmp3, nullptr, nullptr);
+    RecOut o;
+    o.ef = d_ef_out;
+    o.ef_dir = d_tmp3;
+    o.self2 = self2_of(p.alphaES);
+    o.self_mu = d_muv;
+    launch_rec(*this, d_qv, d_muv, lq, ld, o);
+}
+
+// momentpolaSCF (src/pim.c:177-306) with extrapolate_dipole_aspc (src/pim.c:314-424)
+void Engine::pim_reference() {
+    int nb = ceil_div(n, 256);
+    field_of(d_q, d_mu_static, lqch != 0, ldip != 0, ldmp != 0, d_ef_stat);
+    MDFF_CK(cudaMemcpyAsync(d_ef, d_ef_stat, sizeof(double3) * n, cudaMemcpyDeviceToDevice, stream));
+    int ord = p.extrapolate_order;
+    int e = (istep >= ord + 1) ? ord : (!istep ? 0 : istep - 1);
+    int es = (e != ord) ? e + 1 : e;
+    static const double Wt[6] = {0.0, 2.0 / 3.0, 0.6, 4.0 / 7.0, 5.0 / 9.0, 6.0 / 11.0};
+    if (ord < 0 || ord > 5) throw Error(MDFFGPU_ERR_ARG, "extrapolate_order must be 0..5");
+    int iscf = 0;
+    double rmsd = 1.0e300;
+    double upol_pre = 0.0;
+    while (((iscf < p.max_scf_pim_iter) && (rmsd > p.conv_tol_ind)) || (iscf < p.min_scf_pim_iter)) {
+        MDFF_CK(cudaMemsetAsync(d_mu_ind, 0, sizeof(double3) * n, stream));
+        if (!iscf) MDFF_LAUNCH(*this, k_aspc_predict, nb, 256, 0, n, e, es, d_hist, d_mu_ind);
+        else MDFF_LAUNCH(*this, k_induced, nb, 256, 0, n, d_polar, d_pol, d_ef, d_mu_ind);
+        if (!iscf) {  // u_pol of the predicted dipoles (src/pim.c:253), kept if the loop ends here
+            MDFF_LAUNCH(*this, k_pim_sums, nb, 256, 0, n, d_polar, d_pol, d_invpol, d_mu_ind, d_ef, d_part,
+                        part_stride);
+            reduce(S_UPOL, 1, nb);
+            MDFF_CK(cudaMemcpyAsync(&h_out->u_pol, d_scal + S_UPOL, sizeof(double), cudaMemcpyDeviceToHost, stream));
+        }
+        field_of(d_qzero, d_mu_ind, false, true, false, d_ef_ind);
+        MDFF_LAUNCH(*this, k_add3, nb, 256, 0, n, d_ef_stat, d_ef_ind, d_ef);
+        if (!iscf) MDFF_LAUNCH(*this, k_aspc_correct, nb, 256, 0, n, Wt[e], d_polar, d_pol, d_ef, d_mu_ind);
+        MDFF_LAUNCH(*this, k_pim_sums, nb, 256, 0, n, d_polar, d_pol, d_invpol, d_mu_ind, d_ef, d_part, part_stride);
+        reduce(S_UPOL, 2, nb);
+        double sc[2];
+        MDFF_CK(cudaMemcpyAsync(sc, d_scal + S_UPOL, sizeof(double) * 2, cudaMemcpyDeviceToHost, stream));
+        MDFF_CK(cudaStreamSynchronize(stream));
+        if (!iscf) upol_pre = h_out->u_pol;
+        rmsd = std::sqrt(sc[1] / (double)std::max(npol, 1));
+        if (!std::isfinite(rmsd)) throw Error(MDFFGPU_ERR_NONFINITE, "induced dipoles diverged");
+        iscf++;
+        h_out->u_pol = (iscf == 1) ? upol_pre : sc[0];
+    }
+    double upol = h_out->u_pol;
+    MDFF_LAUNCH(*this, k_hist_store, nb, 256, 0, n, d_mu_ind, d_hist);
+    last_scf_iter = iscf;
+    last_rmsd = rmsd;
+    double v = 0.5 * upol * coul_unit;   // get_upol returns 0.5*sum (src/pim.c:160)
+    MDFF_CK(cudaMemcpyAsync(&d_out->u_pol, &v, sizeof(double), cudaMemcpyHostToDevice, stream));
+    MDFF_CK(cudaStreamSynchronize(stream));
+}
+
+// preconditioned conjugate gradient on (alpha^-1 - T) mu = E_stat, polarisable ions;
+// initial guess from the ASPC predictor; stops when the reference's residual measure
+// sqrt(sum (mu/alpha - E)^2 / npol) (src/pim.c:431-449) is below conv_tol_ind
+void Engine::pim_cg() {
+    int nb = ceil_div(n, 256);
+    field_of(d_q, d_mu_static, lqch != 0, ldip != 0, ldmp != 0, d_ef_stat);
+    int ord = p.extrapolate_order;
+    if (ord < 0 || ord > 5) throw Error(MDFFGPU_ERR_ARG, "extrapolate_order must be 0..5");
+    int e = (istep >= ord + 1) ? ord : (!istep ? 0 : istep - 1);
+    int es = (e != ord) ? e + 1 : e;
+    MDFF_LAUNCH(*this, k_aspc_predict, nb, 256, 0, n, e, es, d_hist, d_mu_ind);
+    field_of(d_qzero, d_mu_ind, false, true, false, d_ef_ind);
+    MDFF_LAUNCH(*this, k_cg_residual, nb, 256, 0, n, d_polar, d_invpol, d_ef_stat, d_ef_ind, d_mu_ind, d_cg_r);
+    MDFF_LAUNCH(*this, k_cg_rz, nb, 256, 0, n, d_polar, d_pol, d_cg_r, d_mu_save, d_part, part_stride);
+    reduce(S_RZ, 2, nb);
+    MDFF_CK(cudaMemcpyAsync(d_cg_p, d_mu_save, sizeof(double3) * n, cudaMemcpyDeviceToDevice, stream));
+    double rr = 0.0;
+    MDFF_CK(cudaMemcpyAsync(&rr, d_scal + S_RR, sizeof(double), cudaMemcpyDeviceToHost, stream));
+    MDFF_CK(cudaStreamSynchronize(stream));
+    double rmsd = std::sqrt(rr / (double)std::max(npol, 1));
+    int it = 0;
+    int maxit = std::max(p.max_scf_pim_iter, 1);
+    while (rmsd > p.conv_tol_ind && it < maxit) {
+        field_of(d_qzero, d_cg_p, false, true, false, d_ef_ind);     // T p
+        MDFF_LAUNCH(*this, k_cg_ap, nb, 256, 0, n, d_polar, d_invpol, d_cg_p, d_ef_ind, d_cg_ap, d_part, part_stride);
+        reduce(S_PAP, 1, nb);
+        MDFF_LAUNCH(*this, k_copy_slot, 1, 1, 0, d_scal, (int)S_RZ, (int)S_RZOLD);
+        MDFF_LAUNCH(*this, k_cg_update, nb, 256, 0, n, d_scal, d_cg_p, d_cg_ap, d_mu_ind, d_cg_r);
+        MDFF_LAUNCH(*this, k_cg_rz, nb, 256, 0, n, d_polar, d_pol, d_cg_r, d_mu_save, d_part, part_stride);
+        reduce(S_RZ, 2, nb);
+        MDFF_CK(cudaMemcpyAsync(&rr, d_scal + S_RR, sizeof(double), cudaMemcpyDeviceToHost, stream));
+        MDFF_CK(cudaStreamSynchronize(stream));
+        rmsd = std::sqrt(rr / (double)std::max(npol, 1));
+        if (!std::isfinite(rmsd)) throw Error(MDFFGPU_ERR_NONFINITE, "CG diverged");
+        it++;
+        if (rmsd <= p.conv_tol_ind) break;
+        MDFF_LAUNCH(*this, k_cg_dir, nb, 256, 0, n, d_scal, d_mu_save, d_cg_p);
+    }
+    if (rmsd > p.conv_tol_ind) throw Error(MDFFGPU_ERR_SCF, "CG did not converge in max_scf_pim_iter");
+    MDFF_LAUNCH(*this, k_pim_sums, nb, 256, 0, n, d_polar, d_pol, d_invpol, d_mu_ind, d_ef_stat, d_part, part_stride);
+    reduce(S_UPOL, 1, nb);
+    double up = 0.0;
+    MDFF_CK(cudaMemcpyAsync(&up, d_scal + S_UPOL, sizeof(double), cudaMemcpyDeviceToHost, stream));
+    MDFF_CK(cudaStreamSynchronize(stream));
+    MDFF_LAUNCH(*this, k_hist_store, nb, 256, 0, n, d_mu_ind, d_hist);
+    last_scf_iter = it;
+    last_rmsd = rmsd;
+    double v = 0.5 * up * coul_unit;
+    MDFF_CK(cudaMemcpyAsync(&d_out->u_pol, &v, sizeof(double), cudaMemcpyHostToDevice, stream));
+    MDFF_CK(cudaStreamSynchronize(stream));
+}
+
+// get_dipoles (src/coulombic.c:67-130): mu = static + induced
+void Engine::get_dipoles() {
+    if (lpol) {
+        if (pim_solver == MDFFGPU_PIM_CG) pim_cg();
+        else if (p.algo_pim == 1) throw Error(MDFFGPU_ERR_ARG, "algo_pim scfkO runs through the reference solver");
+        else pim_reference();
+        int nb = ceil_div(n, 256);
+        MDFF_LAUNCH(*this, k_add3, nb, 256, 0, n, d_mu_static, d_mu_ind, d_mu_tot);
+    } else {
+        MDFF_CK(cudaMemcpyAsync(d_mu_tot, d_mu_static, sizeof(double3) * n, cudaMemcpyDeviceToDevice, stream));
+    }
+}
+
+void Engine::finalize_coul(bool stress) {
+    CoulFin cf;
+    cf.alpha = p.alphaES;
+    cf.coul = coul_unit;
+    cf.inveOmegaPU = cell.inveOmegaPU;
+    cf.ttpiV = 2.0 * TPI_D * cell.inveOmega;
+    cf.do_dir = 1;
+    cf.do_rec = 1;
+    cf.do_stress = stress;
+    MDFF_LAUNCH(*this, k_finalize_coul, 1, 1, 0, d_scal, cf, &d_out->u_coul, &d_out->pvir_coul, d_out->tau_coul);
+}
+
+// engforce, src/field.c:352-407
+void Engine::engforce() {
+    ensure_lists();
+    MDFF_CK(cudaMemsetAsync(d_f, 0, sizeof(double3) * n, stream));
+    launch_kardir(*this, d_r, d_s);
+    if (p.lnmlj) sr_forces(true, nullptr, nullptr, nullptr);
+    if (p.lbhmft || p.lbhmftd) sr_forces(false, nullptr, nullptr, nullptr);
+    if (p.lcoulombic) {
+        get_dipoles();
+        bool ld = (ldip || lpol);
+        // direct space: forces, energy, virial (do_forces, do_stress; src/field.c:381-383)
+        launch_dir(*this, d_q, d_mu_tot, p.alphaES, lqch != 0, ld, ldmp != 0, true, false, false, false, nullptr,
+                   nullptr, d_tmp3);
+        reduce(S_DIR_U, 7, ceil_div(n, 8));
+        RecOut o;
+        o.f = d_f;
+        o.f_dir = d_tmp3;
+        o.coul = coul_unit;
+        launch_rec(*this, d_q, d_mu_tot, lqch != 0, ld, o);
+        int nb = ceil_div(n, 256);
+        MDFF_LAUNCH(*this, k_self_sums, nb, 256, 0, n, d_q, d_mu_tot, d_part, part_stride);
+        reduce(S_Q2, 2, nb);
+        finalize_coul(true);
+    }
+    MDFF_LAUNCH(*this, k_check_finite, ceil_div(n, 256), 256, 0, n, d_r, d_f, d_status);
+}
+
+// multipole_ES on caller data (src/ewald.c:75-348)
+void Engine::multipole_es_dev(const double *d_qv, const double3 *d_muv, double alpha, int flags, double3 *d_ef_out,
+                              double *d_efg_out, double3 *d_f_out) {
+    bool lq = flags & MDFFGPU_ES_LQ, ld = flags & MDFFGPU_ES_LD, damp = flags & MDFFGPU_ES_LDAMP;
+    bool fo = flags & MDFFGPU_ES_FORCES, st = flags & MDFFGPU_ES_STRESS, ef = flags & MDFFGPU_ES_EF;
+    bool efg = flags & MDFFGPU_ES_EFG, dir = flags & MDFFGPU_ES_DIR, rec = flags & MDFFGPU_ES_REC;
+    ensure_lists();
+    launch_kardir(*this, d_r, d_s);
+    int nb = ceil_div(n, 256);
+    double self2 = self2_of(alpha);
+    // efg_dir accumulates the charge part when do_efg and the dipole part when do_efg
+    // or do_forces (src/ewald.c:724-757)
+    bool want_efg_dir = efg || (fo && ld);
+    double3 *efd = d_ef_ind, *fd = d_tmp3;
+    double *egd = d_efg;
+    MDFF_CK(cudaMemsetAsync(d_part + (size_t)S_DIR_U * part_stride, 0, sizeof(double) * 7 * part_stride, stream));
+    MDFF_CK(cudaMemsetAsync(d_scal, 0, sizeof(double) * NSLOT, stream));
+    MDFF_CK(cudaMemsetAsync(efd, 0, sizeof(double3) * n, stream));
+    MDFF_CK(cudaMemsetAsync(fd, 0, sizeof(double3) * n, stream));
+    MDFF_CK(cudaMemsetAsync(egd, 0, sizeof(double) * 9 * n, stream));
+    if (dir) {
+        launch_dir(*this, d_qv, d_muv, alpha, lq, ld, damp, fo || st, ef, want_efg_dir, efg, efd, egd, fd);
+        reduce(S_DIR_U, 7, ceil_div(n, 8));
+    }
+    if (rec) {
+        RecOut o;
+        o.ef = d_ef_out;
+        o.ef_dir = efd;
+        o.self2 = self2;
+        o.f = fo ? d_f_out : nullptr;
+        o.f_dir = fd;
+        o.coul = coul_unit;
+        o.efg = (d_efg_out && ef) ? d_efg_out : nullptr;   // do_ef passed as do_efg, src/ewald.c:169
+        o.efg_dir = egd;
+        o.self_q = d_qv;
+        o.self_mu = d_muv;
+        launch_rec(*this, d_qv, d_muv, lq, ld, o);
+        if (d_efg_out && !ef) MDFF_LAUNCH(*this, k_efg_self_dir, nb, 256, 0, n, self2, d_qv, egd, d_efg_out);
+    } else {
+        MDFF_LAUNCH(*this, k_self_plus_dir, nb, 256, 0, n, self2, d_muv, efd, d_ef_out);
+        if (fo) MDFF_LAUNCH(*this, k_axpy3, nb, 256, 0, n, coul_unit, fd, d_f_out);
+        if (d_efg_out) MDFF_LAUNCH(*this, k_efg_self_dir, nb, 256, 0, n, self2, d_qv, egd, d_efg_out);
+    }
+    MDFF_LAUNCH(*this, k_self_sums, nb, 256, 0, n, d_qv, d_muv, d_part, part_stride);
+    reduce(S_Q2, 2, nb);
+    CoulFin cf;
+    cf.alpha = alpha;
+    cf.coul = coul_unit;
+    cf.inveOmegaPU = cell.inveOmegaPU;
+    cf.ttpiV = 2.0 * TPI_D * cell.inveOmega;
+    cf.do_dir = dir;
+    cf.do_rec = rec;
+    cf.do_stress = st;
+    MDFF_CK(cudaMemsetAsync(d_out->tau_coul, 0, sizeof(double) * 9, stream));
+    MDFF_LAUNCH(*this, k_finalize_coul, 1, 1, 0, d_scal, cf, &d_out->u_coul, &d_out->pvir_coul, d_out->tau_coul);
+}
+
+// ---------------------------------------------------------------- kernel timing
+void Engine::prof_begin(const char *name, int *slot) {
+    *slot = -1;
+    if (prof_name.empty() || prof_name != name) return;
+    if (prof_next >= (int)prof_pool.size()) {
+        cudaEvent_t ev;
+        MDFF_CK(cudaEventCreate(&ev));
+        prof_pool.push_back(ev);
+    }
+    *slot = prof_next++;
+    MDFF_CK(cudaEventRecord(prof_pool[*slot], stream));
+}
+
+void Engine::prof_end(const char *name, int slot, double flops) {
+    if (slot < 0) return;
+    if (prof_next >= (int)prof_pool.size()) {
+        cudaEvent_t ev;
+        MDFF_CK(cudaEventCreate(&ev));
+        prof_pool.push_back(ev);
+    }
+    int s2 = prof_next++;
+    MDFF_CK(cudaEventRecord(prof_pool[s2], stream));
+    prof_pairs.push_back({slot, s2});
+    prof_flops += flops;
+    (void)name;
+}
+
+void Engine::prof_result(double *ms, long long *count, double *flops) {
+    MDFF_CK(cudaStreamSynchronize(stream));
+    double t = 0.0;
+    for (auto &pr : prof_pairs) {
+        float m = 0.f;
+        MDFF_CK(cudaEventElapsedTime(&m, prof_pool[pr.first], prof_pool[pr.second]));
+        t += m;
+    }
+    *ms = t;
+    *count = (long long)prof_pairs.size();
+    *flops = prof_flops;
+}
+
+// ---------------------------------------------------------------- integration
+void Engine::prop_agate(int step) {
+    istep = step;
+    int nb = ceil_div(n, 256);
+    switch (p.egrator) {
+    case 0: {  // prop_leap_frog, src/integration.c:93-137
+        engforce();
+        MDFF_LAUNCH(*this, k_lf, nb, 256, 0, n, dt * dt, 0.5 / dt, d_invmass, d_mass, d_r, d_rs, d_v, d_f, d_part,
+                    part_stride);
+        reduce(S_KIN, 1, nb);
+        MDFF_LAUNCH(*this, k_set_ekin, 1, 1, 0, d_scal, d_out);
+        break;
+    }
+    case 2: {  // nhcn, src/integration.c:140-182
+        NhcArgs a;
+        a.nn = p.nhc_n;
+        a.yo = p.nhc_yosh_order;
+        a.mults = p.nhc_mults;
+        a.dt = dt;
+        a.temp = temp;
+        a.L = 3.0 * (double)n;
+        for (int k = 0; k < 7; k++) a.w[k] = 0.0;
+        switch (a.yo) {  // Yoshida weights, src/integration.c:205-236
+        case 1: a.w[0] = 1.0; break;
+        case 3:
+            a.w[0] = 1.0 / (2.0 - std::pow(2.0, 1.0 / 3.0));
+            a.w[1] = 1.0 - 2.0 * a.w[0];
+            a.w[2] = a.w[0];
+            break;
+        case 5:
+            a.w[0] = 1.0 / (4.0 - std::pow(4.0, 1.0 / 3.0));
+            a.w[1] = a.w[2] = a.w[3] = a.w[0];
+            a.w[4] = 1.0 - 4.0 * a.w[0];
+            break;
+        case 7:
+            a.w[0] = .78451361047756;
+            a.w[1] = .235573213359357;
+            a.w[2] = -1.17767998417887;
+            a.w[3] = 1.0 - 2.0 * (a.w[0] + a.w[1] + a.w[2]);
+            a.w[4] = a.w[2];
+            a.w[5] = a.w[1];
+            a.w[6] = a.w[0];
+            break;
+        default: throw Error(MDFFGPU_ERR_ARG, "nhc_yosh_order must be 1, 3, 5 or 7");
+        }
+        if (a.nn < 2 || a.nn > 16) throw Error(MDFFGPU_ERR_ARG, "nhc_n must be in 2..16");
+        MDFF_LAUNCH(*this, k_scale_kin, nb, 256, 0, n, d_out, 0, d_mass, d_v, d_part, part_stride);
+        reduce(S_KIN, 1, nb);
+        MDFF_LAUNCH(*this, k_nhc_chain, 1, 1, 0, a, d_nhc, d_scal, d_out);
+        MDFF_LAUNCH(*this, k_scale_kin, nb, 256, 0, n, d_out, 1, d_mass, d_v, d_part, part_stride);
+        MDFF_LAUNCH(*this, k_pv1, nb, 256, 0, n, dt, dt * 0.5, d_invmass, d_r, d_v, d_f);
+        engforce();
+        MDFF_LAUNCH(*this, k_pv2, nb, 256, 0, n, dt * 0.5, d_invmass, d_mass, d_v, d_f, d_part, part_stride);
+        reduce(S_KIN, 1, nb);
+        MDFF_LAUNCH(*this, k_nhc_chain, 1, 1, 0, a, d_nhc, d_scal, d_out);
+        MDFF_LAUNCH(*this, k_scale_kin, nb, 256, 0, n, d_out, 1, d_mass, d_v, d_part, part_stride);
+        reduce(S_KIN, 1, nb);
+        MDFF_LAUNCH(*this, k_nhc_energy, 1, 1, 0, a.nn, a.L, temp, d_nhc, d_scal, d_out);
+        break;
+    }
+    default: {  // prop_velocity_verlet, src/integration.c:22-63
+        double dtsq2 = dt * dt * 0.5, dt2 = dt * 0.5;
+        MDFF_LAUNCH(*this, k_vv1, nb, 256, 0, n, dt, dtsq2, d_invmass, d_r, d_v, d_f, d_f2);
+        engforce();
+        MDFF_LAUNCH(*this, k_vv2, nb, 256, 0, n, dt2, d_invmass, d_mass, d_v, d_f, d_f2, d_part, part_stride);
+        reduce(S_KIN, 1, nb);
+        MDFF_LAUNCH(*this, k_set_ekin, 1, 1, 0, d_scal, d_out);
+        break;
+    }
+    }
+}
+
+// run_md's loop body (src/md.c:229-241)
+void Engine::md_steps(int first, int nsteps, double *thermo) {
+    if (p.lverletL && !list_ready) gen_verletlist();
+    for (int s = 0; s < nsteps; s++) {
+        MDFF_CK(cudaMemsetAsync(d_status, 0, sizeof(unsigned), stream));
+        prop_agate(first + s);
+        if (p.lverletL) check_verletlist();
+        sync_scalars();
+        check_status();
+        if (thermo) {
+            double *t = thermo + 12 * (size_t)s;
+            t[0] = h_out->e_kin;
+            t[1] = h_out->u_lj;
+            t[2] = h_out->u_bh;
+            t[3] = h_out->u_coul;
+            t[4] = h_out->u_pol;
+            t[5] = h_out->e_nvt;
+            t[6] = h_out->pvir_lj;
+            t[7] = h_out->pvir_bh;
+            t[8] = h_out->pvir_coul;
+            t[9] = (double)h_out->nbuilds;
+            t[10] = (double)last_scf_iter;
+            t[11] = last_rmsd;
+        }
+    }
+}
+
+}  // namespace mdffgpu

@@ -1,0 +1,233 @@
+// mdffgpu engine: device state of one system and the launchers of its kernels.
+#pragma once
+
+#include <vector>
+
+#include "common.cuh"
+
+namespace mdffgpu {
+
+// ---------------------------------------------------------------- per type-pair data
+// n-m LJ constants of init_nmlj (src/nmlj.c:198-236) and the BHMFT(D) table
+// (src/bhmftd.c:99-110), for the ordered pair (ti, tj).
+struct PairSR {
+    double sigsq, epsqp, fc, ptwo, qtwo, uc, plj, qlj;
+    double A, B, C, D, BD;
+    int ip, iq;   // ptwo/qtwo as integers when integral (fast power path), else -1
+};
+// Tang-Toennies damping of the charge->dipole field for the ordered pair (ita, jta)
+// (src/ewald.c:505-516): D1 from pol_damp_*[ita][ita][jta], D2 from [jta][ita][jta].
+struct PairDamp {
+    int ldamp, k1, k2, pad;
+    double b1, c1, b2, c2;
+};
+
+// one k-space row segment: up to KSEG consecutive nz values at fixed (nx, ny)
+constexpr int KSEG = 16;
+struct KSeg {
+    int nx, ny, z0, cnt;
+    int koff, pad0, pad1, pad2;
+};
+// one k-space row: all nz of a fixed (nx, ny)
+struct KRow {
+    int nx, ny, z0, cnt;
+    int koff, pad0, pad1, pad2;
+};
+
+// scalar slots (device array `scal`) written by the reduction kernels
+enum Slot : int {
+    S_LJ_U = 0, S_LJ_TAU = 1,      // 6 entries xx xy xz yy yz zz
+    S_BH_U = 7, S_BH_TAU = 8,
+    S_DIR_U = 14, S_DIR_TAU = 15,
+    S_REC_U = 21, S_REC_TAU = 22,
+    S_Q2 = 28, S_MU2 = 29,         // adjacent: written together
+    S_KIN = 30,
+    S_UPOL = 31, S_RMSD2 = 32,     // adjacent
+    S_RZ = 33, S_RR = 34,          // adjacent
+    S_PAP = 35, S_RZOLD = 36,
+    S_DISP1 = 37, S_DISP2 = 38,
+    NSLOT = 40
+};
+
+// values the host reads back in one copy after a step
+struct DevScalars {
+    double u_lj, pvir_lj, tau_lj[9];
+    double u_bh, pvir_bh, tau_bh[9];
+    double u_coul, pvir_coul, tau_coul[9];
+    double u_pol, e_kin, e_nvt, scf_rmsd;
+    double xi[16], vxi[16];
+    double nhc_s;
+    int scf_iter, nbuilds, rebuild, status;
+};
+
+struct Engine;
+
+// ---------------------------------------------------------------- launchers
+// lists.cu
+void launch_kardir(Engine &e, const double4 *r, double4 *s);
+void launch_check_list(Engine &e);             // sets e.d_rebuild on the device
+void launch_build_lists(Engine &e, bool force); // gated by d_rebuild unless force
+// pair.cu
+void launch_sr(Engine &e, bool lj);            // adds forces into e.d_f, partials into slots
+// real-space multipole sum on e.d_s (fractional positions); q, mu per ion.  forces:
+// per-ion force into out_f plus energy/virial partials (slots S_DIR_*); ef: field into
+// out_ef; efg: EFG into out_efg (efg_q adds the charge part, src/ewald.c:724-729).
+void launch_dir(Engine &e, const double *q, const double3 *mu, double alpha, bool lq, bool ld, bool damp,
+                bool forces, bool ef, bool efg, bool efg_q, double3 *out_ef, double *out_efg, double3 *out_f);
+// kspace.cu
+struct RecOut {
+    double3 *ef = nullptr;            // self2*mu + ef_dir + E_rec
+    const double3 *ef_dir = nullptr;
+    double self2 = 0.0;
+    const double *self_q = nullptr;   // charges and dipoles of the self terms
+    const double3 *self_mu = nullptr;
+    double3 *f = nullptr;             // f + f_dir*coul + F_rec*coul
+    const double3 *f_dir = nullptr;
+    double coul = 1.0;
+    double *efg = nullptr;            // self + efg_dir + EFG_rec (upper triangle)
+    const double *efg_dir = nullptr;
+};
+void launch_rec(Engine &e, const double *q, const double3 *mu, bool lq, bool ld, const RecOut &o);
+// integrate.cu
+void launch_reduce_slots(Engine &e, int first_slot, int nslots, int nparts);
+// true once the FP32 pair/k-space kernels exist in this build
+inline bool mixed_available() { return false; }
+
+// ---------------------------------------------------------------- engine state
+struct Engine {
+    mdffgpu_params p;
+    int n = 0, nt = 0, device = 0;
+    int precision = MDFFGPU_FP64;
+    int pim_solver = MDFFGPU_PIM_REFERENCE;
+    cudaStream_t stream = nullptr;
+    long long launches = 0;
+    std::string last_error;
+
+    // units (src/constants.c:8-18, reduced units :38-45)
+    double boltz_unit, time_unit, press_unit, coul_unit;
+    Cell cell;
+    // derived md parameters (check_md, src/md.c:120-141)
+    double dt, temp, tauT, timesca;
+    int lqch = 0, ldip = 0, lpol = 0, ldmp = 0, lpim = 0, npol = 0;
+    int lpolar[NT] = {0};
+    double srcutsq = 0, lrcutsq = 0;
+    double utail = 0, ptail = 0;
+
+    // ---- host copies of per-ion constants
+    std::vector<int> h_typ;
+    std::vector<double> h_q;
+    double *h_stage = nullptr;   // pinned staging for state transfers, 10 doubles per ion
+    // ---- device per-ion arrays
+    double4 *d_r = nullptr;      // Cartesian x y z, w = charge
+    double4 *d_s = nullptr;      // fractional (kardir) x y z, w = charge
+    double3 *d_v = nullptr, *d_f = nullptr, *d_f2 = nullptr;
+    double *d_mass = nullptr, *d_invmass = nullptr, *d_q = nullptr;
+    int *d_typ = nullptr;
+    double3 *d_mu_static = nullptr, *d_mu_ind = nullptr, *d_mu_tot = nullptr;
+    double *d_pol = nullptr, *d_invpol = nullptr;  // [n][9], zero for non-polarisable
+    int *d_polar = nullptr;
+    double3 *d_ef_stat = nullptr, *d_ef_ind = nullptr, *d_ef = nullptr;
+    double3 *d_cg_r = nullptr, *d_cg_p = nullptr, *d_cg_ap = nullptr, *d_mu_save = nullptr;
+    double3 *d_rs = nullptr;     // leap-frog r(t-dt)
+    double *d_hist = nullptr;    // ASPC history [n][6][3]
+    double *d_efg = nullptr;     // [n][9]
+    double3 *d_tmp3 = nullptr;   // scratch field / force
+    double *d_qzero = nullptr;
+    double3 *d_muzero = nullptr;
+    // pair tables
+    PairSR *d_pair = nullptr;
+    PairDamp *d_damp = nullptr;
+
+    // ---- neighbour lists (full lists, row-major [n][cap])
+    int cap_nb = 0, cap_co = 0;
+    int *d_nb = nullptr, *d_nbn = nullptr, *d_co = nullptr, *d_con = nullptr;
+    double4 *d_svl = nullptr;    // fractional positions at the last build
+    int nc[3] = {1, 1, 1}, ncell = 1, cell_cap = 4096;
+    int *d_cell_of = nullptr, *d_cell_cnt = nullptr, *d_cell_start = nullptr, *d_cell_cur = nullptr,
+        *d_cell_ions = nullptr;
+    int *d_rebuild = nullptr;    // 1 when the lists must be rebuilt this step
+    bool list_ready = false;
+
+    // ---- k space
+    int nk = 0, nseg = 0, nrow = 0, kmax[3] = {0, 0, 0};
+    double *d_Ak = nullptr, *d_kcoe = nullptr;
+    double3 *d_kvec = nullptr;
+    KSeg *d_seg = nullptr;
+    KRow *d_row = nullptr;
+    std::vector<int> h_tile_row;   // first row of each ion-pass tile (+ end)
+    std::vector<int> h_tile_k;     // first k of each tile (+ end)
+    int *d_tile_row = nullptr, *d_tile_k = nullptr;
+    int ntile = 0, tile_kmax = 0;
+    double2 *d_rho_part = nullptr, *d_rho = nullptr;   // partial per ion chunk, total (Ak-scaled)
+    int rho_chunks = 0, rho_chunk = 0;
+
+    // ---- reductions
+    double *d_part = nullptr;    // [NSLOT][part_stride]
+    int part_stride = 0;
+    double *d_scal = nullptr;    // [NSLOT]
+    DevScalars *d_out = nullptr; // composed results
+    DevScalars *h_out = nullptr; // pinned mirror
+    unsigned *d_status = nullptr;
+    double *d_nhc = nullptr;     // xi[16], vxi[16], Q[16]
+
+    // per-kernel timing of one chosen kernel family (CUDA events on `stream`)
+    std::string prof_name;
+    std::vector<cudaEvent_t> prof_pool;
+    std::vector<std::pair<int, int>> prof_pairs;   // indices into prof_pool
+    double prof_flops = 0.0;
+    int prof_next = 0;
+    void prof_begin(const char *name, int *slot);
+    void prof_end(const char *name, int slot, double flops);
+    void prof_result(double *ms, long long *count, double *flops);
+
+    // pim bookkeeping
+    int istep = 0;
+    int last_scf_iter = 0;
+    double last_rmsd = 0.0;
+    int nbuilds = 0;
+
+    explicit Engine(const mdffgpu_params &prm, int dev);
+    ~Engine();
+    Engine(const Engine &) = delete;
+    Engine &operator=(const Engine &) = delete;
+
+    // set-up pieces
+    void setup_units_and_cell();
+    void setup_types();
+    void setup_kspace();
+    void alloc_lists(int cap_nb_, int cap_co_);
+    void setup_cells();
+
+    // operations (engine.cu)
+    void set_positions(const double *rx, const double *ry, const double *rz);
+    void set_velocities(const double *vx, const double *vy, const double *vz);
+    void get_state(double *rx, double *ry, double *rz, double *vx, double *vy, double *vz, double *fx,
+                   double *fy, double *fz);
+    void gen_verletlist();
+    int check_verletlist();
+    void ensure_lists();
+    void engforce();
+    void sr_forces(bool lj, double *u, double *pvir, double *tau);
+    void multipole_es_dev(const double *d_qv, const double3 *d_muv, double alpha, int flags, double3 *d_ef_out,
+                          double *d_efg_out, double3 *d_f_out);
+    void field_of(const double *d_qv, const double3 *d_muv, bool lq, bool ld, bool damp, double3 *d_ef_out);
+    void get_dipoles();
+    void pim_reference();
+    void pim_cg();
+    void prop_agate(int step);
+    void md_steps(int first, int nsteps, double *thermo);
+    void sync_scalars();
+    void check_status();
+    void finalize_coul(bool stress);
+    void reduce(int first_slot, int nslots, int nparts) { launch_reduce_slots(*this, first_slot, nslots, nparts); }
+};
+
+// launch bookkeeping: every kernel launch goes through this
+#define MDFF_LAUNCH(eng, kernel, grid, block, smem, ...)                               \
+    do {                                                                               \
+        kernel<<<(grid), (block), (smem), (eng).stream>>>(__VA_ARGS__);                \
+        MDFF_CK(cudaGetLastError());                                                   \
+        (eng).launches++;                                                              \
+    } while (0)
+
+}  // namespace mdffgpu

@@ -1,0 +1,528 @@
+// Per-ion vector kernels: reductions, integrators (velocity Verlet, leap-frog,
+// Nose-Hoover chain), induced-dipole updates (Jacobi/ASPC, CG) and the composition of
+// the reference's energy/virial/stress globals.
+#include "engine.cuh"
+
+namespace mdffgpu {
+
+// ---------------------------------------------------------------- reductions
+// one block per slot; fixed-order tree over the block partials
+__global__ void k_reduce_slots(const double *__restrict__ part, int stride, int first, int nparts,
+                               double *__restrict__ scal) {
+    int slot = first + blockIdx.x;
+    const double *p = part + (size_t)slot * stride;
+    double a = 0.0;
+    for (int k = threadIdx.x; k < nparts; k += blockDim.x) a += p[k];
+    __shared__ double sh[32];
+    a = warp_sum(a);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = a;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double b = (threadIdx.x < (blockDim.x >> 5)) ? sh[threadIdx.x] : 0.0;
+        b = warp_sum(b);
+        if (threadIdx.x == 0) scal[slot] = b;
+    }
+}
+
+void launch_reduce_slots(Engine &e, int first_slot, int nslots, int nparts) {
+    MDFF_LAUNCH(e, k_reduce_slots, nslots, 256, 0, e.d_part, e.part_stride, first_slot, nparts, e.d_scal);
+}
+
+// block sums of NV per-thread values
+template <int NV>
+__device__ __forceinline__ void block_sum_to_part(double (&v)[NV], double *part, int slot, int stride) {
+    __shared__ double sh[32][NV];
+#pragma unroll
+    for (int k = 0; k < NV; k++) v[k] = warp_sum(v[k]);
+    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0)
+        for (int k = 0; k < NV; k++) sh[w][k] = v[k];
+    __syncthreads();
+    if (threadIdx.x < NV) {
+        double a = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); q++) a += sh[q][threadIdx.x];
+        part[(size_t)(slot + threadIdx.x) * stride + blockIdx.x] = a;
+    }
+}
+
+// ---------------------------------------------------------------- small helpers
+__global__ void k_fill3(int n, double3 *a, double3 v) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) a[i] = v;
+}
+
+__global__ void k_copy3(int n, const double3 *__restrict__ a, double3 *__restrict__ b) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = a[i];
+}
+
+// sum q^2 and |mu|^2 for the self terms (src/ewald.c:198-214)
+__global__ void k_self_sums(int n, const double *__restrict__ q, const double3 *__restrict__ mu, double *part,
+                            int stride) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double v[2] = {0.0, 0.0};
+    if (i < n) {
+        if (q) v[0] = q[i] * q[i];
+        if (mu) {
+            double3 m = mu[i];
+            v[1] = m.x * m.x + m.y * m.y + m.z * m.z;
+        }
+    }
+    block_sum_to_part<2>(v, part, S_Q2, stride);
+}
+
+// ef = self2*mu + ef_dir (used when the reciprocal part is skipped)
+__global__ void k_self_plus_dir(int n, double self2, const double3 *__restrict__ mu, const double3 *__restrict__ efd,
+                                double3 *__restrict__ ef) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double3 m = mu ? mu[i] : make_double3(0, 0, 0);
+    double3 d = efd ? efd[i] : make_double3(0, 0, 0);
+    ef[i] = make_double3(self2 * m.x + d.x, self2 * m.y + d.y, self2 * m.z + d.z);
+}
+
+// f += f_dir * coul (when the reciprocal part is skipped)
+__global__ void k_axpy3(int n, double a, const double3 *__restrict__ x, double3 *__restrict__ y) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double3 u = x[i], v = y[i];
+    y[i] = make_double3(v.x + u.x * a, v.y + u.y * a, v.z + u.z * a);
+}
+
+__global__ void k_efg_self_dir(int n, double self2, const double *__restrict__ q, const double *__restrict__ efgd,
+                               double *__restrict__ efg) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int p = 0; p < 3; p++)
+        for (int r = 0; r < 3; r++) {
+            double b = (p == r && q) ? -self2 * q[i] : 0.0;
+            if (efgd) b += efgd[(size_t)i * 9 + 3 * p + r];
+            efg[(size_t)i * 9 + 3 * p + r] = b;
+        }
+}
+
+// ---------------------------------------------------------------- composition
+// u, pvir, tau of a short-range evaluator from its slots (src/nmlj.c:351-363):
+// slot 0 holds the full-list energy sum (each pair twice), slots 1..6 the full-list
+// sum of r_a f_b + r_b f_a.
+__global__ void k_finalize_sr(const double *__restrict__ scal, int slot, double inveOmegaPU, double *u, double *pvir,
+                              double *tau) {
+    if (threadIdx.x || blockIdx.x) return;
+    *u = 0.5 * scal[slot];
+    double t[6];
+    for (int k = 0; k < 6; k++) t[k] = 0.25 * scal[slot + 1 + k] * inveOmegaPU;
+    double full[9] = {t[0], t[1], t[2], t[1], t[3], t[4], t[2], t[4], t[5]};
+    double pv = 0.0;
+    for (int k = 0; k < 9; k++) tau[k] = full[k];
+    for (int k = 0; k < 3; k++) pv += full[4 * k] * (1.0 / 3.0);
+    *pvir = pv;
+}
+
+// u_coul, tau_coul (src/ewald.c:209-307): dir (full-list sums), rec, self
+struct CoulFin {
+    double alpha, coul, inveOmegaPU, ttpiV;
+    int do_dir, do_rec, do_stress;
+};
+__global__ void k_finalize_coul(const double *__restrict__ scal, CoulFin c, double *u, double *pvir, double *tau) {
+    if (threadIdx.x || blockIdx.x) return;
+    const double rpi = 1.7724538509055160273;
+    double alpha2 = c.alpha * c.alpha, selfa = c.alpha / rpi, selfa2 = 2.0 * selfa * alpha2 / 3.0;
+    double u_self = -selfa * scal[S_Q2] + -selfa2 * scal[S_MU2];
+    double u_dir = c.do_dir ? 0.5 * scal[S_DIR_U] : 0.0;
+    double u_rec = c.do_rec ? scal[S_REC_U] * c.ttpiV : 0.0;
+    *u = (u_dir + u_rec + u_self) * c.coul;
+    if (c.do_stress) {
+        double td[6], tr[6];
+        for (int k = 0; k < 6; k++) {
+            td[k] = 0.25 * scal[S_DIR_TAU + k] * c.inveOmegaPU;
+            tr[k] = scal[S_REC_TAU + k] * c.ttpiV * c.inveOmegaPU;
+        }
+        int map[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+        for (int k = 0; k < 9; k++) {
+            double t = 0.0;
+            if (c.do_dir) t += td[map[k]] * c.coul;
+            if (c.do_rec) t += tr[map[k]] * c.coul;
+            tau[k] = t;
+        }
+    }
+    double pv = 0.0;
+    for (int k = 0; k < 3; k++) pv += tau[4 * k] * (1.0 / 3.0);
+    *pvir = pv;
+}
+
+// ---------------------------------------------------------------- PIM
+// induced_moment (src/pim.c:617-641): mu_i = sum_j pol[j][i] E_j, polarisable ions only
+__device__ __forceinline__ double3 pol_times(const double *P, double3 e) {
+    return make_double3(P[0] * e.x + P[3] * e.y + P[6] * e.z, P[1] * e.x + P[4] * e.y + P[7] * e.z,
+                        P[2] * e.x + P[5] * e.y + P[8] * e.z);
+}
+
+__global__ void k_induced(int n, const int *__restrict__ polar, const double *__restrict__ pol,
+                          const double3 *__restrict__ ef, double3 *__restrict__ mu) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !polar[i]) return;
+    mu[i] = pol_times(pol + (size_t)i * 9, ef[i]);
+}
+
+// extrapolate_dipole_aspc predictor (src/pim.c:381-400) for order `e`, then the
+// history shift by `es` places
+__global__ void k_aspc_predict(int n, int e, int es, double *__restrict__ hist, double3 *__restrict__ mu) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double Bt[6][6] = {{1.0, 0, 0, 0, 0, 0},
+                             {2.0, -1.0, 0, 0, 0, 0},
+                             {2.5, -2.0, 0.5, 0, 0, 0},
+                             {2.8, -2.8, 1.2, -0.2, 0, 0},
+                             {3.0, -24.0 / 7.0, 27.0 / 14.0, -4.0 / 7.0, 1.0 / 14.0, 0},
+                             {22.0 / 7.0, -55.0 / 14.0, 55.0 / 21.0, -22.0 / 21.0, 5.0 / 21.0, -1.0 / 42.0}};
+    double *h = hist + (size_t)i * ASPC_DEPTH * 3;
+    double m[3] = {0.0, 0.0, 0.0};
+    for (int k = 0; k < e + 1; k++)
+        for (int c = 0; c < 3; c++) m[c] += Bt[e][k] * h[3 * k + c];
+    for (int k = es; k > 0; k--)
+        for (int c = 0; c < 3; c++) h[3 * k + c] = h[3 * (k - 1) + c];
+    mu[i] = make_double3(m[0], m[1], m[2]);
+}
+
+// corrector (src/pim.c:403-420): mu = W * alpha E + (1 - W) * mu_pred
+__global__ void k_aspc_correct(int n, double W, const int *__restrict__ polar, const double *__restrict__ pol,
+                               const double3 *__restrict__ ef, double3 *__restrict__ mu) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double3 s = mu[i];
+    double3 m = polar[i] ? pol_times(pol + (size_t)i * 9, ef[i]) : s;
+    mu[i] = make_double3(m.x * W + (1.0 - W) * s.x, m.y * W + (1.0 - W) * s.y, m.z * W + (1.0 - W) * s.z);
+}
+
+// ef = a + b
+__global__ void k_add3(int n, const double3 *__restrict__ a, const double3 *__restrict__ b, double3 *__restrict__ c) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double3 x = a[i], y = b[i];
+    c[i] = make_double3(x.x + y.x, x.y + y.y, x.z + y.z);
+}
+
+// get_upol (src/pim.c:145-161) and get_rmsd_mu (src/pim.c:431-449) partial sums
+__global__ void k_pim_sums(int n, const int *__restrict__ polar, const double *__restrict__ pol,
+                           const double *__restrict__ invpol, const double3 *__restrict__ mu,
+                           const double3 *__restrict__ ef, double *part, int stride) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double v[2] = {0.0, 0.0};
+    if (i < n) {
+        double3 m3 = mu[i];
+        double m[3] = {m3.x, m3.y, m3.z};
+        const double *I = invpol + (size_t)i * 9;
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) v[0] += m[a] * I[3 * a + b] * m[b];
+        if (polar[i]) {
+            double3 e3 = ef[i];
+            double e[3] = {e3.x, e3.y, e3.z};
+            const double *P = pol + (size_t)i * 9;
+            for (int a = 0; a < 3; a++)
+                if (P[4 * a] != 0.0) {
+                    double d = m[a] / P[4 * a] - e[a];
+                    v[1] += d * d;
+                }
+        }
+    }
+    block_sum_to_part<2>(v, part, S_UPOL, stride);
+}
+
+__global__ void k_hist_store(int n, const double3 *__restrict__ mu, double *__restrict__ hist) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double3 m = mu[i];
+    double *h = hist + (size_t)i * ASPC_DEPTH * 3;
+    h[0] = m.x;
+    h[1] = m.y;
+    h[2] = m.z;
+}
+
+// kO: f_ind = ef - mu * invpol_ii on polarisable ions (src/pim.c:561-567)
+__global__ void k_ko_find(int n, const int *__restrict__ polar, const double *__restrict__ invpol,
+                          const double3 *__restrict__ ef, const double3 *__restrict__ mu, double3 *__restrict__ find) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || !polar[i]) return;
+    const double *I = invpol + (size_t)i * 9;
+    double3 e = ef[i], m = mu[i];
+    find[i] = make_double3(e.x - m.x * I[0], e.y - m.y * I[4], e.z - m.z * I[8]);
+}
+
+// kO inner loop updates (src/pim.c:684-729)
+__global__ void k_scale_add3(int n, double a, const double3 *__restrict__ x, double b, double3 *__restrict__ y) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double3 u = x[i], v = y[i];
+    y[i] = make_double3(a * u.x + b * v.x, a * u.y + b * v.y, a * u.z + b * v.z);
+}
+
+// ---- CG on (alpha^-1 - T) mu = E_stat over the polarisable ions (diagonal-alpha preconditioner)
+// r = ef_stat + T x - alpha^-1 x   with  T x  = field of x (incl. self term)
+__global__ void k_cg_residual(int n, const int *__restrict__ polar, const double *__restrict__ invpol,
+                              const double3 *__restrict__ efs, const double3 *__restrict__ tx,
+                              const double3 *__restrict__ x, double3 *__restrict__ r) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (!polar[i]) {
+        r[i] = make_double3(0, 0, 0);
+        return;
+    }
+    double3 e = efs[i], t = tx[i], m = x[i];
+    const double *I = invpol + (size_t)i * 9;
+    double3 ax = make_double3(I[0] * m.x + I[1] * m.y + I[2] * m.z, I[3] * m.x + I[4] * m.y + I[5] * m.z,
+                              I[6] * m.x + I[7] * m.y + I[8] * m.z);
+    r[i] = make_double3(e.x + t.x - ax.x, e.y + t.y - ax.y, e.z + t.z - ax.z);
+}
+
+// Ap = alpha^-1 p - T p ; partial sums of p.Ap
+__global__ void k_cg_ap(int n, const int *__restrict__ polar, const double *__restrict__ invpol,
+                        const double3 *__restrict__ p, const double3 *__restrict__ tp, double3 *__restrict__ ap,
+                        double *part, int stride) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double v[1] = {0.0};
+    if (i < n) {
+        if (polar[i]) {
+            double3 m = p[i], t = tp[i];
+            const double *I = invpol + (size_t)i * 9;
+            double3 a = make_double3(I[0] * m.x + I[1] * m.y + I[2] * m.z - t.x,
+                                     I[3] * m.x + I[4] * m.y + I[5] * m.z - t.y,
+                                     I[6] * m.x + I[7] * m.y + I[8] * m.z - t.z);
+            ap[i] = a;
+            v[0] = m.x * a.x + m.y * a.y + m.z * a.z;
+        } else {
+            ap[i] = make_double3(0, 0, 0);
+        }
+    }
+    block_sum_to_part<1>(v, part, S_PAP, stride);
+}
+
+// z = alpha r ; partial sums of r.z and r.r
+__global__ void k_cg_rz(int n, const int *__restrict__ polar, const double *__restrict__ pol,
+                        const double3 *__restrict__ r, double3 *__restrict__ z, double *part, int stride) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double v[2] = {0.0, 0.0};
+    if (i < n) {
+        if (polar[i]) {
+            double3 rr = r[i];
+            double3 zz = pol_times(pol + (size_t)i * 9, rr);  // pol symmetric in practice
+            z[i] = zz;
+            v[0] = rr.x * zz.x + rr.y * zz.y + rr.z * zz.z;
+            v[1] = rr.x * rr.x + rr.y * rr.y + rr.z * rr.z;
+        } else {
+            z[i] = make_double3(0, 0, 0);
+        }
+    }
+    block_sum_to_part<2>(v, part, S_RZ, stride);  // r.z, r.r
+}
+
+// x += a p ; r -= a Ap, with a = rz / pAp read on the device
+__global__ void k_cg_update(int n, const double *__restrict__ scal, const double3 *__restrict__ p,
+                            const double3 *__restrict__ ap, double3 *__restrict__ x, double3 *__restrict__ r) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double a = scal[S_RZOLD] / scal[S_PAP];
+    double3 pp = p[i], q = ap[i], xx = x[i], rr = r[i];
+    x[i] = make_double3(xx.x + a * pp.x, xx.y + a * pp.y, xx.z + a * pp.z);
+    r[i] = make_double3(rr.x - a * q.x, rr.y - a * q.y, rr.z - a * q.z);
+}
+
+// p = z + beta p, beta = rz_new / rz_old
+__global__ void k_cg_dir(int n, const double *__restrict__ scal, const double3 *__restrict__ z,
+                         double3 *__restrict__ p) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double beta = scal[S_RZ] / scal[S_RZOLD];
+    double3 zz = z[i], pp = p[i];
+    p[i] = make_double3(zz.x + beta * pp.x, zz.y + beta * pp.y, zz.z + beta * pp.z);
+}
+
+__global__ void k_copy_slot(double *scal, int from, int to) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) scal[to] = scal[from];
+}
+
+// ---------------------------------------------------------------- integrators
+// prop_velocity_verlet first half (src/integration.c:33-38)
+__global__ void k_vv1(int n, double dt, double dtsq2, const double *__restrict__ invm, double4 *__restrict__ r,
+                      const double3 *__restrict__ v, const double3 *__restrict__ f, double3 *__restrict__ fs) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double4 x = r[i];
+    double3 vv = v[i], ff = f[i];
+    double im = invm[i];
+    fs[i] = ff;
+    x.x += vv.x * dt + (ff.x * dtsq2) * im;
+    x.y += vv.y * dt + (ff.y * dtsq2) * im;
+    x.z += vv.z * dt + (ff.z * dtsq2) * im;
+    r[i] = x;
+}
+
+// prop_velocity_verlet second half (src/integration.c:47-57) + kinetic partials
+__global__ void k_vv2(int n, double dt2, const double *__restrict__ invm, const double *__restrict__ mass,
+                      double3 *__restrict__ v, const double3 *__restrict__ f, const double3 *__restrict__ fs,
+                      double *part, int stride) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double k[1] = {0.0};
+    if (i < n) {
+        double3 vv = v[i], ff = f[i], f0 = fs[i];
+        double im = invm[i];
+        vv.x += (f0.x + ff.x) * dt2 * im;
+        vv.y += (f0.y + ff.y) * dt2 * im;
+        vv.z += (f0.z + ff.z) * dt2 * im;
+        v[i] = vv;
+        k[0] = (vv.x * vv.x + vv.y * vv.y + vv.z * vv.z) * mass[i];
+    }
+    block_sum_to_part<1>(k, part, S_KIN, stride);
+}
+
+// prop_pos_vel_verlet (src/integration.c:66-90): half kick + drift ...
+__global__ void k_pv1(int n, double dt, double dt2, const double *__restrict__ invm, double4 *__restrict__ r,
+                      double3 *__restrict__ v, const double3 *__restrict__ f) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double4 x = r[i];
+    double3 vv = v[i], ff = f[i];
+    double im = invm[i];
+    vv.x += ff.x * dt2 * im;
+    vv.y += ff.y * dt2 * im;
+    vv.z += ff.z * dt2 * im;
+    x.x += vv.x * dt;
+    x.y += vv.y * dt;
+    x.z += vv.z * dt;
+    v[i] = vv;
+    r[i] = x;
+}
+
+// ... and the second half kick + kinetic partials
+__global__ void k_pv2(int n, double dt2, const double *__restrict__ invm, const double *__restrict__ mass,
+                      double3 *__restrict__ v, const double3 *__restrict__ f, double *part, int stride) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double k[1] = {0.0};
+    if (i < n) {
+        double3 vv = v[i], ff = f[i];
+        double im = invm[i];
+        vv.x += ff.x * dt2 * im;
+        vv.y += ff.y * dt2 * im;
+        vv.z += ff.z * dt2 * im;
+        v[i] = vv;
+        k[0] = (vv.x * vv.x + vv.y * vv.y + vv.z * vv.z) * mass[i];
+    }
+    block_sum_to_part<1>(k, part, S_KIN, stride);
+}
+
+// kinetic partials, optionally after scaling v by the NHC factor s (src/integration.c:281-287)
+__global__ void k_scale_kin(int n, const DevScalars *__restrict__ out, int scale, const double *__restrict__ mass,
+                            double3 *__restrict__ v, double *part, int stride) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double k[1] = {0.0};
+    if (i < n) {
+        double3 vv = v[i];
+        if (scale) {
+            double s = out->nhc_s;
+            vv.x *= s;
+            vv.y *= s;
+            vv.z *= s;
+            v[i] = vv;
+        }
+        k[0] = (vv.x * vv.x + vv.y * vv.y + vv.z * vv.z) * mass[i];
+    }
+    block_sum_to_part<1>(k, part, S_KIN, stride);
+}
+
+// leap-frog (src/integration.c:93-137)
+__global__ void k_lf(int n, double dtsq, double idt, const double *__restrict__ invm, const double *__restrict__ mass,
+                     double4 *__restrict__ r, double3 *__restrict__ rs, double3 *__restrict__ v,
+                     const double3 *__restrict__ f, double *part, int stride) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double k[1] = {0.0};
+    if (i < n) {
+        double4 x = r[i];
+        double3 o = rs[i], ff = f[i];
+        double im = invm[i];
+        double ux = 2.0 * x.x - o.x + ff.x * dtsq * im;
+        double uy = 2.0 * x.y - o.y + ff.y * dtsq * im;
+        double uz = 2.0 * x.z - o.z + ff.z * dtsq * im;
+        double3 vv = make_double3(idt * (ux - o.x), idt * (uy - o.y), idt * (uz - o.z));
+        v[i] = vv;
+        k[0] = (vv.x * vv.x + vv.y * vv.y + vv.z * vv.z) * mass[i];
+        rs[i] = make_double3(x.x, x.y, x.z);
+        r[i] = make_double4(ux, uy, uz, x.w);
+    }
+    block_sum_to_part<1>(k, part, S_KIN, stride);
+}
+
+// chain_nhcn (src/integration.c:189-294) on one thread: thermostat variables in
+// d_nhc (xi[16], vxi[16]); kin from the S_KIN slot (sum m v^2); writes s.  The
+// second sweep stops at nhc_n-2 as in the reference (src/integration.c:269).
+struct NhcArgs {
+    int nn, yo, mults;
+    double dt, temp, L, w[7];
+};
+__global__ void k_nhc_chain(NhcArgs a, double *__restrict__ nhc, const double *__restrict__ scal, DevScalars *out) {
+    if (threadIdx.x || blockIdx.x) return;
+    double *xi = nhc, *vxi = nhc + 16, *Q = nhc + 32;
+    double kin = 0.5 * scal[S_KIN];
+    double G[16];
+    for (int k = 0; k < 16; k++) G[k] = 0.0;
+    double dty[7];
+    for (int k = 0; k < 7; k++) dty[k] = a.w[k] * a.dt / ((double)a.mults);
+    double s = 1.0;
+    int nn = a.nn;
+    G[0] = 2.0 * kin - a.L * a.temp;
+    for (int k = 0; k < a.mults; k++) {
+        for (int j = 0; j < a.yo && j < 7; j++) {
+            double dts = dty[j], dts2 = dts * 0.5, dts4 = dts2 * 0.5, dts8 = dts4 * 0.5;
+            G[nn - 1] = (vxi[nn - 2] * vxi[nn - 2] / Q[nn - 2] - a.temp);
+            vxi[nn - 1] += G[nn - 1] * dts4;
+            for (int inh = nn - 2; inh > -1; inh--) {
+                vxi[inh] *= exp(-vxi[inh + 1] * dts8 / Q[inh + 1]);
+                vxi[inh] += G[inh] * dts4;
+                vxi[inh] *= exp(-vxi[inh + 1] * dts8 / Q[inh + 1]);
+            }
+            s *= exp(-vxi[0] * dts2 / Q[0]);
+            for (int i = 0; i < nn; i++) xi[i] += vxi[i] * dts2 / Q[i];
+            G[0] = 2.0 * kin * s * s - a.L * a.temp;
+            for (int inh = 0; inh < nn - 2; inh++) {
+                vxi[inh] *= exp(-vxi[inh + 1] * dts8 / Q[inh + 1]);
+                vxi[inh] += G[inh] * dts4;
+                vxi[inh] *= exp(-vxi[inh + 1] * dts8 / Q[inh + 1]);
+                G[inh + 1] = (vxi[inh] * vxi[inh] / Q[inh] - a.temp);
+            }
+            vxi[nn - 1] += G[nn - 1] * dts4;
+        }
+    }
+    out->nhc_s = s;
+}
+
+// e_kin and the NHC conserved-quantity term e_nvt (src/integration.c:156-176)
+__global__ void k_nhc_energy(int nn, double L, double temp, const double *__restrict__ nhc,
+                             const double *__restrict__ scal, DevScalars *out) {
+    if (threadIdx.x || blockIdx.x) return;
+    const double *xi = nhc, *vxi = nhc + 16, *Q = nhc + 32;
+    out->e_kin = 0.5 * scal[S_KIN];
+    double nvt1 = L * temp * xi[0], nvt2 = vxi[0] * vxi[0] * 0.5 / Q[0], nvt3 = 0.0, nvt4 = 0.0;
+    for (int i = 1; i < nn; i++) {
+        nvt3 += vxi[i] * vxi[i] * 0.5 / Q[i];
+        nvt4 += temp * xi[i];
+    }
+    out->e_nvt = nvt1 + nvt2 + nvt3 + nvt4;
+    for (int i = 0; i < 16; i++) {
+        out->xi[i] = xi[i];
+        out->vxi[i] = vxi[i];
+    }
+}
+
+__global__ void k_set_ekin(const double *__restrict__ scal, DevScalars *out) {
+    if (threadIdx.x || blockIdx.x) return;
+    out->e_kin = 0.5 * scal[S_KIN];
+}
+
+// non-finite guard on positions and forces (status word)
+__global__ void k_check_finite(int n, const double4 *__restrict__ r, const double3 *__restrict__ f, unsigned *status) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double4 x = r[i];
+    double3 g = f[i];
+    if (!isfinite(x.x + x.y + x.z + g.x + g.y + g.z)) atomicOr(status, ST_NONFINITE);
+}
+
+}  // namespace mdffgpu

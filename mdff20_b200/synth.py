@@ -127,13 +127,35 @@ def random_sequential_addition(types: np.ndarray, L: float, dmin: np.ndarray, rn
     return pos
 
 
+def cristobalite(ncell: int, density: float = 2.20, jitter: float = 0.0,
+                 rng: Optional[np.random.Generator] = None):
+    """Ideal beta-cristobalite supercell (ncell^3 cubic cells of 8 SiO2), scaled to the
+    given density: Si on a diamond lattice, O halfway along every Si-Si bond.  Returns
+    (positions grouped O then Si, box edge); `jitter` adds seeded Gaussian displacements."""
+    fcc = np.array([[0, 0, 0], [0, .5, .5], [.5, 0, .5], [.5, .5, 0]])
+    bonds = np.array([[.25, .25, .25], [.25, -.25, -.25], [-.25, .25, -.25], [-.25, -.25, .25]])
+    si_cell = np.concatenate([fcc, fcc + 0.25])
+    o_cell = (fcc[:, None, :] + bonds[None, :, :] * 0.5).reshape(-1, 3)
+    g = np.stack(np.meshgrid(*[np.arange(ncell)] * 3, indexing="ij"), -1).reshape(-1, 1, 3)
+    si = (g + si_cell[None]).reshape(-1, 3)
+    o = (g + o_cell[None]).reshape(-1, 3)
+    L = box_length(si.shape[0], o.shape[0], density)
+    a = L / ncell
+    pos = np.concatenate([o, si]) * a
+    if jitter > 0.0:
+        pos = pos + rng.standard_normal(pos.shape) * jitter
+    pos -= L * np.round(pos / L)
+    return pos, L
+
+
 def silica(n_si: int, seed: int, density: float = 2.20, dmin=1.4,
            polarizable: bool = False, rc_sr: float = 7.0, rc_lr: float = 10.0,
            alpha: float = 0.32, kmax: int = 12, skin: float = 1.0,
            integrator: str = "nvt-nhcn", temp: float = 3000.0, dt: float = 0.001,
            npas: int = 1000, nhc_n: int = 3, timesca_thermo: float = 0.1,
            conv_tol: float = 1e-6, extrapolate_order: int = 0,
-           damping: bool = True, velocities: bool = True, L: Optional[float] = None) -> System:
+           damping: bool = True, velocities: bool = True, L: Optional[float] = None,
+           structure: str = "random", jitter: float = 0.05) -> System:
     """Configs 2, 3 and 5: silica with Buckingham short range and Ewald electrostatics.
 
     Buckingham (BHMFT without damping, D=0) Si-O A=18003.7572 eV, B=4.87318 1/Å,
@@ -141,21 +163,29 @@ def silica(n_si: int, seed: int, density: float = 2.20, dmin=1.4,
     q_O=-1.2.  With ``polarizable``, alpha_O = 1 Å^3 (isotropic), alpha_Si = 0 and the
     charge->dipole field on O is Tang-Toennies damped, f_4(b r) with b=2, c=1.
     ``dmin`` is one minimum separation for all pairs or a (2,2) table by type.
+    ``structure`` "random": random sequential addition; "cristobalite": beta-cristobalite
+    supercell (n_si = 8 m^3) with seeded Gaussian displacements of rms `jitter` Å.
     """
     n_o = 2 * n_si
     n = n_si + n_o
-    if L is None:
-        L = box_length(n_si, n_o, density)
     rng = np.random.Generator(np.random.PCG64(seed))
-    types = np.array([O] * n_o + [SI] * n_si)
-    dm = np.full((2, 2), float(dmin)) if np.isscalar(dmin) else np.asarray(dmin, float)
-    # placement order alternates the species in runs of 64 ions so neither fills the box first
-    order = np.concatenate([np.concatenate([np.arange(n_o)[k * 128:(k + 1) * 128],
-                                            n_o + np.arange(n_si)[k * 64:(k + 1) * 64]])
-                            for k in range((n_si + 63) // 64)])
-    pos = np.empty((n, 3))
-    pos[order] = random_sequential_addition(types[order], L, dm, rng)
-    pos -= L * np.round(pos / L)      # centre on the origin like the reference's POSFF files
+    if structure == "cristobalite":
+        m = round((n_si / 8) ** (1.0 / 3.0))
+        if 8 * m ** 3 != n_si:
+            raise ValueError("cristobalite needs n_si = 8 m^3")
+        pos, L = cristobalite(m, density, jitter, rng)
+    else:
+        if L is None:
+            L = box_length(n_si, n_o, density)
+        types = np.array([O] * n_o + [SI] * n_si)
+        dm = np.full((2, 2), float(dmin)) if np.isscalar(dmin) else np.asarray(dmin, float)
+        # placement order alternates the species in runs of 64 ions so neither fills the box first
+        order = np.concatenate([np.concatenate([np.arange(n_o)[k * 128:(k + 1) * 128],
+                                                n_o + np.arange(n_si)[k * 64:(k + 1) * 64]])
+                                for k in range((n_si + 63) // 64)])
+        pos = np.empty((n, 3))
+        pos[order] = random_sequential_addition(types[order], L, dm, rng)
+        pos -= L * np.round(pos / L)      # centre on the origin like the reference's POSFF files
     masses = np.array([MASS_O] * n_o + [MASS_SI] * n_si)
     vel = maxwell_boltzmann(masses, temp * BOLTZ_UNIT, rng) if velocities else None
     A = np.zeros((2, 2)); B = np.zeros((2, 2)); C = np.zeros((2, 2)); D = np.zeros((2, 2))
@@ -205,6 +235,10 @@ def config3() -> System:
     return s
 
 
-def config5() -> System:
+def config5(structure: str = "cristobalite") -> System:
+    """N = 24000 polarisable silica, NHC (chain 3) at 2500 K, 1 Å skin, SCF to 1e-6 with
+    ASPC order 4.  MD starts from a 10^3 beta-cristobalite supercell at 2.20 g/cm^3
+    (L = 71.3 Å) with 0.05 Å seeded displacements: a random packing of these ions falls
+    into the Buckingham short-range divergence within tens of steps."""
     return silica(8000, seed=6, polarizable=True, kmax=14, temp=2500.0, npas=10000,
-                  conv_tol=1e-6, extrapolate_order=4, dmin=PIM_DMIN)
+                  conv_tol=1e-6, extrapolate_order=4, dmin=PIM_DMIN, structure=structure)

@@ -197,6 +197,14 @@ class Oracle:
         except Exception:
             pass
 
+    def set_positions(self, pos):
+        self._pos = np.ascontiguousarray(pos, float)
+        self.L.orc_set_positions(self.h, _dp(self._pos))
+
+    def set_velocities(self, vel):
+        v = np.ascontiguousarray(vel, float)
+        self.L.orc_set_velocities(self.h, _dp(v))
+
     # ---------------------------------------------------------------- lists
     def gen_verletlist(self):
         rc = self.L.orc_gen_verletlist(self.h)

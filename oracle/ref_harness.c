@@ -238,7 +238,11 @@ int main(int argc, char *argv[]) {
     } else if (strcmp(task, "md") == 0) {
         int nsteps = (argc > 3) ? atoi(argv[3]) : 1;
         int every = (argc > 4) ? atoi(argv[4]) : 0;
-        npas = nsteps;
+        /* first step index: istep drives the ASPC order (src/pim.c:324-334); starting
+           past extrapolate_order avoids the first-steps order switch, whose predictor
+           reads coefficients the reference never sets for ions >= 1 */
+        int first = (argc > 5) ? atoi(argv[5]) : 1;
+        npas = first - 1 + nsteps;
         put_xyz("r_in", rx, ry, rz);
         if (lverletL) force_rebuild();
         istep = 0;
@@ -270,11 +274,11 @@ int main(int argc, char *argv[]) {
         if (every > 0) REC_FRAME();
         double t0 = omp_get_wtime();
         /* the MD loop body of src/md.c:229-247 without its output */
-        for (istep = 1; istep < npas + 1; istep++) {
+        for (istep = first; istep < npas + 1; istep++) {
             prop_agate(istep);
             if (lverletL) check_verletlist();
             if ((rescale_allowed) && (istep < nequil) && (istep % nequilT == 0)) rescale_velocities(1);
-            REC_THERMO(istep);
+            REC_THERMO(istep - first + 1);
             if (every > 0 && istep % every == 0) REC_FRAME();
         }
         double t1 = omp_get_wtime();

@@ -1,0 +1,74 @@
+"""The systems behind the golden fixtures (shared by make_golden.py and the tests).
+
+Each case is a small seeded system the compiled reference runs in seconds.  The
+fixture stores the reference's own inputs (positions after read_config's wrap,
+velocities) next to its outputs, so a test rebuilds the System from here and feeds the
+stored positions.
+
+Single points use random packings; MD cases start from a jittered beta-cristobalite
+cell (a random packing of these ions collapses into the Buckingham short-range
+divergence within tens of steps, in the reference as in the engine).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from mdff20_b200 import synth
+
+
+def lj256():
+    return synth.lj_fcc(ncell=4)
+
+
+def silica96(polarizable: bool, **kw):
+    args = dict(rc_sr=4.5, rc_lr=5.0, skin=0.5, kmax=5, alpha=0.6, conv_tol=1e-10, extrapolate_order=0)
+    args.update(kw)
+    dmin = synth.PIM_DMIN if polarizable else 1.4
+    return synth.silica(32, seed=11, polarizable=polarizable, dmin=dmin, **args)
+
+
+def silica450(polarizable: bool, **kw):
+    # L = 18.9 A, list cut 6 A: three cells per edge, so the cell-list path is used
+    args = dict(rc_sr=5.0, rc_lr=5.5, skin=0.5, kmax=6, alpha=0.55, conv_tol=1e-10, extrapolate_order=0)
+    args.update(kw)
+    dmin = synth.PIM_DMIN if polarizable else 1.4
+    return synth.silica(150, seed=12, polarizable=polarizable, dmin=dmin, **args)
+
+
+def crist192(polarizable: bool, **kw):
+    # 2x2x2 beta-cristobalite (64 SiO2), L = 14.26 A
+    args = dict(rc_sr=5.0, rc_lr=6.0, skin=0.5, kmax=6, alpha=0.5, conv_tol=1e-10, extrapolate_order=0,
+                structure="cristobalite", jitter=0.05)
+    args.update(kw)
+    return synth.silica(64, seed=13, polarizable=polarizable, **args)
+
+
+def es_inputs(s, seed: int = 0):
+    """Charges and random dipoles for multipole_ES flag tests."""
+    rng = np.random.default_rng(seed)
+    q = np.repeat(np.array([-1.2, 2.4]), s.nionit)
+    mu = rng.normal(size=(s.nion, 3)) * 0.1
+    return q, mu
+
+
+# flags lq ld ldamp do_forces do_stress do_ef do_efg do_dir do_rec
+ES_FLAG_SETS = [
+    (1, 1, 1, 1, 1, 1, 1, 1, 1),
+    (0, 1, 0, 0, 0, 1, 0, 1, 1),
+    (1, 1, 0, 1, 1, 1, 1, 1, 0),
+    (1, 0, 0, 1, 1, 1, 1, 0, 1),
+    (1, 0, 1, 0, 0, 1, 0, 1, 1),
+    (1, 1, 1, 1, 1, 0, 0, 1, 1),
+]
+ES_FLAG_NAMES = ["lq", "ld", "ldamp", "do_forces", "do_stress", "do_ef", "do_efg", "do_dir", "do_rec"]
+
+CASES = {
+    "lj256": lambda: lj256(),
+    "silica96_rigid": lambda: silica96(False),
+    "silica96_pim": lambda: silica96(True),
+    "silica450_pim": lambda: silica450(True),
+    "crist192_nhc": lambda: crist192(False, integrator="nvt-nhcn", temp=3000.0),
+    "crist192_pim_nhc": lambda: crist192(True, integrator="nvt-nhcn", temp=2500.0),
+    "crist192_pim_vv": lambda: crist192(True, integrator="nve-vv", temp=2500.0),
+}
+MD_CASES = (("lj256", 50), ("crist192_nhc", 30), ("crist192_pim_nhc", 10), ("crist192_pim_vv", 10))
