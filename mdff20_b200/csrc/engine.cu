@@ -856,12 +856,13 @@ void Engine::multipole_es_dev(const double *d_qv, const double3 *d_muv, double a
     MDFF_CK(cudaMemsetAsync(fd, 0, sizeof(double3) * n, stream));
     MDFF_CK(cudaMemsetAsync(egd, 0, sizeof(double) * 9 * n, stream));
     if (dir) {
-        launch_dir(*this, d_qv, d_muv, alpha, lq, ld, damp, fo || st, ef, want_efg_dir, efg, efd, egd, fd);
+        launch_dir(*this, d_qv, d_muv, alpha, lq, ld, damp, fo || st, ef, want_efg_dir, efg, ef ? efd : nullptr,
+                   want_efg_dir ? egd : nullptr, fd);
         reduce(S_DIR_U, 7, ceil_div(n, 8));
     }
     if (rec) {
         RecOut o;
-        o.ef = d_ef_out;
+        o.ef = ef ? d_ef_out : nullptr;   // without do_ef the field is the self term only
         o.ef_dir = efd;
         o.self2 = self2;
         o.f = fo ? d_f_out : nullptr;
@@ -872,6 +873,7 @@ void Engine::multipole_es_dev(const double *d_qv, const double3 *d_muv, double a
         o.self_q = d_qv;
         o.self_mu = d_muv;
         launch_rec(*this, d_qv, d_muv, lq, ld, o);
+        if (!ef) MDFF_LAUNCH(*this, k_self_plus_dir, nb, 256, 0, n, self2, d_muv, efd, d_ef_out);
         if (d_efg_out && !ef) MDFF_LAUNCH(*this, k_efg_self_dir, nb, 256, 0, n, self2, d_qv, egd, d_efg_out);
     } else {
         MDFF_LAUNCH(*this, k_self_plus_dir, nb, 256, 0, n, self2, d_muv, efd, d_ef_out);
