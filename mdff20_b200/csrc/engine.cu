@@ -198,6 +198,7 @@ Engine::~Engine() {
     cudaFree(d_row);
     cudaFree(d_rho_part);
     cudaFree(d_rho);
+    cudaFree(d_ion_part);
     cudaFree(d_out);
     cudaFree(d_status);
     if (h_out) cudaFreeHost(h_out);
@@ -457,8 +458,9 @@ void Engine::setup_kspace() {
     }
     nrow = (int)rows.size();
     nseg = (int)segs.size();
-    // ion-pass tiles: whole rows, at most 2048 k per tile (32 KB of shared memory)
-    const int TILEK = 2048;
+    // ion-pass k slices: whole rows, at most 512 k per slice (8 KB of shared memory);
+    // the slices are the second grid dimension of the ion pass
+    const int TILEK = 512;
     h_tile_row.clear();
     h_tile_k.clear();
     int r = 0;
@@ -492,16 +494,20 @@ void Engine::setup_kspace() {
     MDFF_CK(cudaMemcpy(d_seg, segs.data(), sizeof(KSeg) * nseg, cudaMemcpyHostToDevice));
     MDFF_CK(cudaMemcpy(d_tile_row, h_tile_row.data(), sizeof(int) * (ntile + 1), cudaMemcpyHostToDevice));
     MDFF_CK(cudaMemcpy(d_tile_k, h_tile_k.data(), sizeof(int) * (ntile + 1), cudaMemcpyHostToDevice));
-    // rho pass grid: segment blocks x ion chunks, about two waves of the SMs
+    // rho pass grid: segment blocks x ion chunks filling `waves` full waves of
+    // RHO_MIN_BLOCKS resident blocks per SM (MDFFGPU_RHO_WAVES overrides, default 1)
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
     int segblocks = ceil_div(nseg, 128);
-    int chunks = std::max(1, ceil_div(2 * nsm, segblocks));
+    double waves = 1.0;
+    if (const char *w = getenv("MDFFGPU_RHO_WAVES")) waves = std::max(0.1, atof(w));
+    int chunks = std::max(1, (int)(waves * RHO_MIN_BLOCKS * nsm) / segblocks);
     chunks = std::min(chunks, std::max(1, ceil_div(n, 32)));
     rho_chunk = ceil_div(n, chunks);
     rho_chunks = ceil_div(n, rho_chunk);
     d_rho_part = dalloc<double2>((size_t)rho_chunks * nk);
     d_rho = dalloc<double2>(nk);
+    d_ion_part = dalloc<double>((size_t)ntile * n * 12);
 }
 
 void Engine::setup_cells() {
@@ -542,7 +548,10 @@ void Engine::alloc_lists(int cnb, int cco) {
     d_nbn = dalloc<int>(n);
     d_co = dalloc<int>((size_t)n * cap_co);
     d_con = dalloc<int>(n);
+    dfree(d_coef);
+    if (p.lcoulombic && lpol) d_coef = dalloc<double2>((size_t)n * cap_co);
     list_ready = false;
+    coef_ready = false;
 }
 
 // ---------------------------------------------------------------- state
@@ -676,7 +685,10 @@ static double self2_of(double alpha) {
 // electric field of (q, mu): self + direct + reciprocal, as multipole_ES with
 // do_ef only (src/ewald.c:75-348); no energy, no forces
 void Engine::field_of(const double *d_qv, const double3 *d_muv, bool lq, bool ld, bool damp, double3 *d_ef_out) {
-    launch_dir(*this, d_qv, d_muv, p.alphaES, lq, ld, damp, false, true, false, false, d_tmp3, nullptr, nullptr);
+    if (!lq && ld && !damp && coef_ready)
+        launch_dir_field_cached(*this, d_muv, d_tmp3);
+    else
+        launch_dir(*this, d_qv, d_muv, p.alphaES, lq, ld, damp, false, true, false, false, d_tmp3, nullptr, nullptr);
     RecOut o;
     o.ef = d_ef_out;
     o.ef_dir = d_tmp3;
@@ -783,11 +795,93 @@ void Engine::pim_cg() {
     MDFF_CK(cudaStreamSynchronize(stream));
 }
 
+// get_rmsd_mu (src/pim.c:431-449) of (mu, ef); also returns sum mu.invpol.mu
+double Engine::rmsd_of(const double3 *d_mu, const double3 *d_ef, double *upol_sum) {
+    int nb = ceil_div(n, 256);
+    MDFF_LAUNCH(*this, k_pim_sums, nb, 256, 0, n, d_polar, d_pol, d_invpol, d_mu, d_ef, d_part, part_stride);
+    reduce(S_UPOL, 2, nb);
+    double sc[2];
+    MDFF_CK(cudaMemcpyAsync(sc, d_scal + S_UPOL, sizeof(double) * 2, cudaMemcpyDeviceToHost, stream));
+    MDFF_CK(cudaStreamSynchronize(stream));
+    if (upol_sum) *upol_sum = sc[0];
+    double r = std::sqrt(sc[1] / (double)std::max(npol, 1));
+    if (!std::isfinite(r)) throw Error(MDFFGPU_ERR_NONFINITE, "induced dipoles diverged");
+    return r;
+}
+
+// induced_moment_inner_kO (src/pim.c:647-748): real-space-only relaxation of the
+// dipole increment with alpha_Ewald = 0.001 (src/pim.c:694) and omegakO mixing
+void Engine::ko_inner(double3 *d_dmu, const double3 *d_find) {
+    int nb = ceil_div(n, 256);
+    const double ak = 0.001, om = p.omegakO;
+    double rmsd_ext = rmsd_of(d_muzero, d_find, nullptr);
+    MDFF_LAUNCH(*this, k_induced, nb, 256, 0, n, d_polar, d_pol, d_find, d_dmu);
+    MDFF_LAUNCH(*this, k_scale_add3, nb, 256, 0, n, 0.0, d_dmu, om, d_dmu);
+    int it = 0;
+    double rmsd_in = 1.0e300;
+    while ((it <= 20) && (rmsd_in > 0.1 * rmsd_ext)) {
+        it++;
+        MDFF_CK(cudaMemcpyAsync(d_mu_save, d_dmu, sizeof(double3) * n, cudaMemcpyDeviceToDevice, stream));
+        launch_dir(*this, d_qzero, d_dmu, ak, false, true, false, false, true, false, false, d_tmp3, nullptr,
+                   nullptr);
+        MDFF_LAUNCH(*this, k_self_plus_dir, nb, 256, 0, n, self2_of(ak), d_dmu, d_tmp3, d_ef_ind);
+        MDFF_LAUNCH(*this, k_add3, nb, 256, 0, n, d_find, d_ef_ind, d_ef_ind);   // ef_tot = ef_ext + ef_ind
+        rmsd_in = rmsd_of(d_dmu, d_ef_ind, nullptr);
+        MDFF_LAUNCH(*this, k_induced, nb, 256, 0, n, d_polar, d_pol, d_ef_ind, d_dmu);
+        MDFF_LAUNCH(*this, k_scale_add3, nb, 256, 0, n, 1.0 - om, d_mu_save, om, d_dmu);
+    }
+}
+
+// momentpolaSCFkO (src/pim.c:457-603)
+void Engine::pim_ko() {
+    int nb = ceil_div(n, 256);
+    field_of(d_q, d_mu_static, lqch != 0, ldip != 0, ldmp != 0, d_ef_stat);
+    MDFF_CK(cudaMemcpyAsync(d_ef, d_ef_stat, sizeof(double3) * n, cudaMemcpyDeviceToDevice, stream));
+    MDFF_CK(cudaMemcpyAsync(d_cg_r, d_ef_stat, sizeof(double3) * n, cudaMemcpyDeviceToDevice, stream));  // f_ind
+    MDFF_CK(cudaMemsetAsync(d_mu_ind, 0, sizeof(double3) * n, stream));
+    MDFF_CK(cudaMemsetAsync(d_cg_p, 0, sizeof(double3) * n, stream));   // dmu_ind
+    int ord = p.extrapolate_order;
+    if (ord < 0 || ord > 5) throw Error(MDFFGPU_ERR_ARG, "extrapolate_order must be 0..5");
+    int e = (istep >= ord + 1) ? ord : (!istep ? 0 : istep - 1);
+    int es = (e != ord) ? e + 1 : e;
+    static const double Wt[6] = {0.0, 2.0 / 3.0, 0.6, 4.0 / 7.0, 5.0 / 9.0, 6.0 / 11.0};
+    int iscf = 0;
+    double rmsd = 1.0e300, upol = 0.0;
+    while (((iscf < p.max_scf_pim_iter) && (rmsd > p.conv_tol_ind)) || (iscf < p.min_scf_pim_iter)) {
+        if ((!iscf) && (istep > 1)) {
+            MDFF_LAUNCH(*this, k_aspc_predict, nb, 256, 0, n, e, es, d_hist, d_mu_ind);
+        } else {
+            ko_inner(d_cg_p, d_cg_r);
+            MDFF_LAUNCH(*this, k_scale_add3, nb, 256, 0, n, 1.0, d_cg_p, 1.0, d_mu_ind);
+        }
+        rmsd_of(d_mu_ind, d_ef, &upol);   // u_pol of these dipoles (src/pim.c:539)
+        field_of(d_qzero, d_mu_ind, false, true, false, d_ef_ind);
+        MDFF_LAUNCH(*this, k_add3, nb, 256, 0, n, d_ef_stat, d_ef_ind, d_ef);
+        if (!iscf) MDFF_LAUNCH(*this, k_aspc_correct, nb, 256, 0, n, Wt[e], d_polar, d_pol, d_ef, d_mu_ind);
+        rmsd = rmsd_of(d_mu_ind, d_ef, nullptr);
+        MDFF_LAUNCH(*this, k_ko_find, nb, 256, 0, n, d_polar, d_invpol, d_ef, d_mu_ind, d_cg_r);
+        iscf++;
+    }
+    MDFF_LAUNCH(*this, k_hist_store, nb, 256, 0, n, d_mu_ind, d_hist);
+    last_scf_iter = iscf;
+    last_rmsd = rmsd;
+    double v = 0.5 * upol * coul_unit;
+    MDFF_CK(cudaMemcpyAsync(&d_out->u_pol, &v, sizeof(double), cudaMemcpyHostToDevice, stream));
+    MDFF_CK(cudaStreamSynchronize(stream));
+}
+
 // get_dipoles (src/coulombic.c:67-130): mu = static + induced
 void Engine::get_dipoles() {
     if (lpol) {
+        // positions are fixed through the solve: cache the dipole-field pair factors
+        struct CoefScope {
+            bool &flag;
+            ~CoefScope() { flag = false; }
+        } scope{coef_ready};
+        launch_dir_prep(*this, p.alphaES);
+        coef_ready = true;
         if (pim_solver == MDFFGPU_PIM_CG) pim_cg();
-        else if (p.algo_pim == 1) throw Error(MDFFGPU_ERR_ARG, "algo_pim scfkO runs through the reference solver");
+        else if (p.algo_pim == 1) pim_ko();
         else pim_reference();
         int nb = ceil_div(n, 256);
         MDFF_LAUNCH(*this, k_add3, nb, 256, 0, n, d_mu_static, d_mu_ind, d_mu_tot);

@@ -24,6 +24,7 @@ struct PairDamp {
 
 // one k-space row segment: up to KSEG consecutive nz values at fixed (nx, ny)
 constexpr int KSEG = 16;
+constexpr int RHO_MIN_BLOCKS = 4;   // resident k_rho blocks per SM (caps registers at 128)
 struct KSeg {
     int nx, ny, z0, cnt;
     int koff, pad0, pad1, pad2;
@@ -74,6 +75,10 @@ void launch_sr(Engine &e, bool lj);            // adds forces into e.d_f, partia
 // out_ef; efg: EFG into out_efg (efg_q adds the charge part, src/ewald.c:724-729).
 void launch_dir(Engine &e, const double *q, const double3 *mu, double alpha, bool lq, bool ld, bool damp,
                 bool forces, bool ef, bool efg, bool efg_q, double3 *out_ef, double *out_efg, double3 *out_f);
+// per list entry (F1/d^3, 3 F2/d^5) for the current positions, then the dipole-only
+// field from them (the induced-dipole iterations of one force evaluation)
+void launch_dir_prep(Engine &e, double alpha);
+void launch_dir_field_cached(Engine &e, const double3 *mu, double3 *out_ef);
 // kspace.cu
 struct RecOut {
     double3 *ef = nullptr;            // self2*mu + ef_dir + E_rec
@@ -141,6 +146,8 @@ struct Engine {
     // ---- neighbour lists (full lists, row-major [n][cap])
     int cap_nb = 0, cap_co = 0;
     int *d_nb = nullptr, *d_nbn = nullptr, *d_co = nullptr, *d_con = nullptr;
+    double2 *d_coef = nullptr;   // [n][cap_co] cached dipole-field pair factors
+    bool coef_ready = false;     // d_coef matches the current positions
     double4 *d_svl = nullptr;    // fractional positions at the last build
     int nc[3] = {1, 1, 1}, ncell = 1, cell_cap = 4096;
     int *d_cell_of = nullptr, *d_cell_cnt = nullptr, *d_cell_start = nullptr, *d_cell_cur = nullptr,
@@ -159,6 +166,7 @@ struct Engine {
     int *d_tile_row = nullptr, *d_tile_k = nullptr;
     int ntile = 0, tile_kmax = 0;
     double2 *d_rho_part = nullptr, *d_rho = nullptr;   // partial per ion chunk, total (Ak-scaled)
+    double *d_ion_part = nullptr;                       // ion-pass partial sums [ntile][n][12]
     int rho_chunks = 0, rho_chunk = 0;
 
     // ---- reductions
@@ -214,6 +222,9 @@ struct Engine {
     void get_dipoles();
     void pim_reference();
     void pim_cg();
+    void pim_ko();
+    void ko_inner(double3 *d_dmu, const double3 *d_find);
+    double rmsd_of(const double3 *d_mu, const double3 *d_ef, double *upol_sum);
     void prop_agate(int step);
     void md_steps(int first, int nsteps, double *thermo);
     void sync_scalars();

@@ -9,10 +9,14 @@
 // complex recurrence.  Two passes:
 //   k_rho     : rho(k) = sum_i (q_i + i k.mu_i) exp(i k.r_i); threads own k-row
 //               segments of up to KSEG values of nz, ions stream through shared memory
-//               in tiles; per-ion-chunk partial sums, reduced in a fixed order;
-//   k_rec_ion : per ion, the k sums for field, force and EFG, threads own ions, the
-//               Ak-scaled rho(k) streams through shared memory in row-aligned tiles;
-//               sums are kept in n-space and mapped to Cartesian k once per ion.
+//               in tiles; per-ion-chunk partial sums, reduced in a fixed order.  With
+//               b = E0[nx] E1[ny] and k.mu = c0 + nz c1 the summand is
+//               (B1 + nz B2) E2[nz], B1 = (q + i c0) b, B2 = i c1 b: 6 FP64 ops per k.
+//   k_rec_ion : per (ion, k-slice) the k sums for field, force and EFG; threads own
+//               ions, blockIdx.y a row-aligned slice of k whose Ak*rho(k) sits in
+//               shared memory; two independent phase recurrences (even and odd nz);
+//               sums kept in n-space, combined over slices and mapped to Cartesian k
+//               once per ion by k_rec_combine.
 #include "engine.cuh"
 
 namespace mdffgpu {
@@ -20,6 +24,7 @@ namespace mdffgpu {
 constexpr int RHO_THREADS = 128;
 constexpr int RHO_TI = 32;          // ions per shared-memory tile
 constexpr int ION_THREADS = 128;
+constexpr int ION_NV = 12;          // per (ion, slice) partial sums: S[3] P[3] H[6]
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
     return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -42,7 +47,7 @@ __device__ __forceinline__ double3 phase_coord(const Cell &c, double x, double y
 
 // ---------------------------------------------------------------- pass 1: rho(k)
 template <bool LQ, bool LD>
-__global__ void __launch_bounds__(RHO_THREADS) k_rho(int n, int chunk, Cell c, int K0, int K1, int K2,
+__global__ void __launch_bounds__(RHO_THREADS, RHO_MIN_BLOCKS) k_rho(int n, int chunk, Cell c, int K0, int K1, int K2,
                                                     const double4 *__restrict__ r, const double *__restrict__ q,
                                                     const double3 *__restrict__ mu, int nseg,
                                                     const KSeg *__restrict__ seg, double2 *__restrict__ part,
@@ -87,9 +92,9 @@ __global__ void __launch_bounds__(RHO_THREADS) k_rho(int n, int chunk, Cell c, i
                     if (LD) {
                         double3 m3 = mu[ia];
                         double3 mm = phase_coord(c, m3.x, m3.y, m3.z);
-                        ms[3 * slot] = mm.x;
-                        ms[3 * slot + 1] = mm.y;
-                        ms[3 * slot + 2] = mm.z;
+                        ms[3 * slot] = tpi * mm.x;
+                        ms[3 * slot + 1] = tpi * mm.y;
+                        ms[3 * slot + 2] = tpi * mm.z;
                     }
                 }
             }
@@ -100,25 +105,27 @@ __global__ void __launch_bounds__(RHO_THREADS) k_rho(int n, int chunk, Cell c, i
                 const double2 *T = E + a * WT;
                 double2 b = cmul(T[S.nx], T[W0 + K1 + S.ny]);
                 const double2 *Z = T + W0 + W1 + K2 + S.z0;
+                // B1 = (q + i c0) b, B2 = i c1 b; summand (B1 + nz B2) E2[nz]
                 double qa = LQ ? qs[a] : 0.0;
                 double c0 = 0.0, c1 = 0.0;
                 if (LD) {
-                    c0 = tpi * ((double)S.nx * ms[3 * a] + (double)S.ny * ms[3 * a + 1]);
-                    c1 = tpi * ms[3 * a + 2];
+                    c0 = (double)S.nx * ms[3 * a] + (double)S.ny * ms[3 * a + 1];
+                    c1 = ms[3 * a + 2];
                 }
+                double2 B1 = make_double2(qa * b.x - c0 * b.y, qa * b.y + c0 * b.x);
+                double2 B2 = make_double2(-c1 * b.y, c1 * b.x);
+                double zf = (double)S.z0;
 #pragma unroll
                 for (int z = 0; z < KSEG; z++) {
                     if (z < S.cnt) {
-                        double2 ph = cmul(b, Z[z]);
-                        if (LQ) {
-                            acc[z].x += qa * ph.x;
-                            acc[z].y += qa * ph.y;
-                        }
+                        double2 C = B1;
                         if (LD) {
-                            double kmu = c0 + (double)(S.z0 + z) * c1;
-                            acc[z].x -= kmu * ph.y;
-                            acc[z].y += kmu * ph.x;
+                            C.x = B1.x + (zf + (double)z) * B2.x;
+                            C.y = B1.y + (zf + (double)z) * B2.y;
                         }
+                        double2 e = Z[z];
+                        acc[z].x += C.x * e.x - C.y * e.y;
+                        acc[z].y += C.x * e.y + C.y * e.x;
                     }
                 }
             }
@@ -184,6 +191,7 @@ struct IonArgs {
     const int *tile_row, *tile_k;
     int ntile;
     const double2 *rho_s;
+    double *part;           // [ntile][n][ION_NV]
     double tfpiV, self2;    // 8 pi / V, 2*selfa2 (self field coefficient)
     int ld, want_ef, want_f, want_efg;
     const double3 *ef_dir;  // added to the result when not null
@@ -197,93 +205,151 @@ struct IonArgs {
     const double3 *muself;
 };
 
+// one slice of rows: S = sum_k n recarg, P = sum_k n (n.m) recarg2, H = sum_k n n^T recarg2
 template <bool WF, bool WEFG>
 __global__ void __launch_bounds__(ION_THREADS) k_rec_ion(IonArgs a) {
     extern __shared__ double2 rk[];
     int i = blockIdx.x * ION_THREADS + threadIdx.x;
+    int tl = blockIdx.y;
     bool act = i < a.n;
+    int r0 = a.tile_row[tl], r1 = a.tile_row[tl + 1];
+    int k0 = a.tile_k[tl], k1 = a.tile_k[tl + 1];
+    for (int k = k0 + threadIdx.x; k < k1; k += ION_THREADS) rk[k - k0] = a.rho_s[k];
     double3 t = make_double3(0, 0, 0), m = make_double3(0, 0, 0);
-    double qi = 0.0;
     if (act) {
         double4 ri = a.r[i];
         t = phase_coord(a.c, ri.x, ri.y, ri.z);
-        qi = a.q ? a.q[i] : 0.0;
         if (WF && a.ld) {
             double3 mu = a.mu[i];
             m = phase_coord(a.c, mu.x, mu.y, mu.z);
         }
     }
+    __syncthreads();
     double2 e1 = cis2pi(t.y), e2 = cis2pi(t.z);
+    double2 e22 = cmul(e2, e2);
     double2 e2m = cis2pi(-(double)a.K2 * t.z);
-    double S0 = 0, S1 = 0, S2 = 0;              // sum n recarg
-    double P0 = 0, P1 = 0, P2 = 0;              // sum n (n.m) recarg2
-    double H[6] = {0, 0, 0, 0, 0, 0};           // sum n n^T recarg2
+    double S0 = 0, S1 = 0, S2 = 0, P0 = 0, P1 = 0, P2 = 0;
+    double H[6] = {0, 0, 0, 0, 0, 0};
     double2 base = make_double2(1.0, 0.0);
     int cur_nx = -1, last_ny = 0;
-    for (int tl = 0; tl < a.ntile; tl++) {
-        int r0 = a.tile_row[tl], r1 = a.tile_row[tl + 1];
-        int k0 = a.tile_k[tl], k1 = a.tile_k[tl + 1];
-        for (int k = k0 + threadIdx.x; k < k1; k += ION_THREADS) rk[k - k0] = a.rho_s[k];
-        __syncthreads();
-        for (int rr = r0; rr < r1; rr++) {
-            KRow R = a.row[rr];
-            if (R.nx != cur_nx) {
-                cur_nx = R.nx;
-                base = cis2pi((double)R.nx * t.x + (double)R.ny * t.y);
-            } else {
-                for (int s = last_ny; s < R.ny; s++) base = cmul(base, e1);
+    for (int rr = r0; rr < r1; rr++) {
+        KRow R = a.row[rr];
+        if (R.nx != cur_nx) {
+            cur_nx = R.nx;
+            base = cis2pi((double)R.nx * t.x + (double)R.ny * t.y);
+        } else {
+            for (int s = last_ny; s < R.ny; s++) base = cmul(base, e1);
+        }
+        last_ny = R.ny;
+        // two independent chains: even offsets from ph0, odd from ph1, both stepping e2^2
+        double2 ph0 = (R.z0 == 1) ? cmul(base, e2) : cmul(base, e2m);
+        double2 ph1 = cmul(ph0, e2);
+        const double2 *rho = rk + (R.koff - k0);
+        double R1a = 0, Rza = 0, T1a = 0, Tza = 0, Q0a = 0, Q1a = 0, Q2a = 0;
+        double R1b = 0, Rzb = 0, T1b = 0, Tzb = 0, Q0b = 0, Q1b = 0, Q2b = 0;
+        double za = (double)R.z0, zb = za + 1.0;
+        double c0 = (double)R.nx * m.x + (double)R.ny * m.y;
+        int cnt = R.cnt;
+        for (int kz = 0; kz < cnt; kz += 2) {
+            double2 ra = rho[kz];
+            double rca = ra.y * ph0.x - ra.x * ph0.y;
+            R1a += rca;
+            Rza += za * rca;
+            if (WF || WEFG) {
+                double rc2 = ra.x * ph0.x + ra.y * ph0.y;
+                if (WF) {
+                    double tq = (c0 + za * m.z) * rc2;
+                    T1a += tq;
+                    Tza += za * tq;
+                }
+                if (WEFG) {
+                    Q0a += rc2;
+                    Q1a += za * rc2;
+                    Q2a += za * za * rc2;
+                }
             }
-            last_ny = R.ny;
-            double2 ph = (R.z0 == 1) ? cmul(base, e2) : cmul(base, e2m);
-            const double2 *rho = rk + (R.koff - k0);
-            double R1 = 0, Rz = 0, T1 = 0, Tz = 0, Q0 = 0, Q1 = 0, Q2 = 0;
-            double z = (double)R.z0;
-            double c0 = (double)R.nx * m.x + (double)R.ny * m.y;
-            for (int kz = 0; kz < R.cnt; kz++) {
-                double2 rh = rho[kz];
-                double recarg = rh.y * ph.x - rh.x * ph.y;
-                R1 += recarg;
-                Rz += z * recarg;
+            if (kz + 1 < cnt) {
+                double2 rb = rho[kz + 1];
+                double rcb = rb.y * ph1.x - rb.x * ph1.y;
+                R1b += rcb;
+                Rzb += zb * rcb;
                 if (WF || WEFG) {
-                    double recarg2 = rh.x * ph.x + rh.y * ph.y;
+                    double rc2 = rb.x * ph1.x + rb.y * ph1.y;
                     if (WF) {
-                        double tq = (c0 + z * m.z) * recarg2;
-                        T1 += tq;
-                        Tz += z * tq;
+                        double tq = (c0 + zb * m.z) * rc2;
+                        T1b += tq;
+                        Tzb += zb * tq;
                     }
                     if (WEFG) {
-                        Q0 += recarg2;
-                        Q1 += z * recarg2;
-                        Q2 += z * z * recarg2;
+                        Q0b += rc2;
+                        Q1b += zb * rc2;
+                        Q2b += zb * zb * rc2;
                     }
                 }
-                ph = cmul(ph, e2);
-                z += 1.0;
             }
-            double nx = (double)R.nx, ny = (double)R.ny;
-            S0 += nx * R1;
-            S1 += ny * R1;
-            S2 += Rz;
-            if (WF) {
-                P0 += nx * T1;
-                P1 += ny * T1;
-                P2 += Tz;
-            }
-            if (WEFG) {
-                H[0] += nx * nx * Q0;
-                H[1] += nx * ny * Q0;
-                H[2] += nx * Q1;
-                H[3] += ny * ny * Q0;
-                H[4] += ny * Q1;
-                H[5] += Q2;
-            }
+            ph0 = cmul(ph0, e22);
+            ph1 = cmul(ph1, e22);
+            za += 2.0;
+            zb += 2.0;
         }
-        __syncthreads();
+        double nx = (double)R.nx, ny = (double)R.ny;
+        double R1 = R1a + R1b, Rz = Rza + Rzb;
+        S0 += nx * R1;
+        S1 += ny * R1;
+        S2 += Rz;
+        if (WF) {
+            double T1 = T1a + T1b, Tz = Tza + Tzb;
+            P0 += nx * T1;
+            P1 += ny * T1;
+            P2 += Tz;
+        }
+        if (WEFG) {
+            double Q0 = Q0a + Q0b, Q1 = Q1a + Q1b, Q2 = Q2a + Q2b;
+            H[0] += nx * nx * Q0;
+            H[1] += nx * ny * Q0;
+            H[2] += nx * Q1;
+            H[3] += ny * ny * Q0;
+            H[4] += ny * Q1;
+            H[5] += Q2;
+        }
     }
     if (!act) return;
+    double *o = a.part + ((size_t)tl * a.n + i) * ION_NV;
+    o[0] = S0;
+    o[1] = S1;
+    o[2] = S2;
+    if (WF) {
+        o[3] = P0;
+        o[4] = P1;
+        o[5] = P2;
+    }
+    if (WEFG)
+        for (int k = 0; k < 6; k++) o[6 + k] = H[k];
+}
+
+// sum the slices of each ion (fixed order) and write field, force and EFG
+template <bool WF, bool WEFG>
+__global__ void k_rec_combine(IonArgs a) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    double S0 = 0, S1 = 0, S2 = 0, P0 = 0, P1 = 0, P2 = 0, H[6] = {0, 0, 0, 0, 0, 0};
+    for (int tl = 0; tl < a.ntile; tl++) {
+        const double *o = a.part + ((size_t)tl * a.n + i) * ION_NV;
+        S0 += o[0];
+        S1 += o[1];
+        S2 += o[2];
+        if (WF) {
+            P0 += o[3];
+            P1 += o[4];
+            P2 += o[5];
+        }
+        if (WEFG)
+            for (int k = 0; k < 6; k++) H[k] += o[6 + k];
+    }
     const Cell &c = a.c;
     const double tpi = TPI_D;
-    // B S: sum_k k recarg = 2 pi B S
+    double qi = a.q ? a.q[i] : 0.0;
+    // sum_k k recarg = 2 pi B S ; sum_k k (k.mu) recarg2 = (2 pi)^2 B P
     double gS[3], gP[3];
     for (int q = 0; q < 3; q++) {
         gS[q] = tpi * (c.B[q][0] * S0 + c.B[q][1] * S1 + c.B[q][2] * S2);
@@ -333,23 +399,23 @@ __global__ void __launch_bounds__(ION_THREADS) k_rec_ion(IonArgs a) {
 }
 
 // ---------------------------------------------------------------- launcher
-// rho pass + reduction + ion pass.  `o` says where the per-ion results go:
-//   o.ef  = self2*mu + o.ef_dir + E_rec          (when o.ef)
-//   o.f   = o.f + o.f_dir*coul + F_rec*coul      (when o.f)
-//   o.efg = self + o.efg_dir + EFG_rec (upper)   (when o.efg)
 // Algorithmic flops per (ion, k) pair, counted from the loop bodies (FMA = 2 flops):
-//   k_rho     : phase b*E2 6, charge term 4, dipole term (k.mu 2 + 4) 6
-//   k_rec_ion : phase recurrence 6, recarg 3, R sums 3, z += 1 1           (field: 13)
-//               + recarg2 3, (n.m) recarg2 3, P sums 3                      (force: 22)
-//               + Q sums 7                                                  (EFG:   29)
-double rho_flops_per_pair(bool lq, bool ld) { return (lq ? 4.0 : 0.0) + (ld ? 6.0 : 0.0) + 6.0; }
-double ion_flops_per_pair(bool f, bool efg) { return 13.0 + (f ? 9.0 : 0.0) + (efg ? 7.0 : 0.0); }
+//   k_rho     : (B1 + nz B2) 4 when dipoles, complex multiply-accumulate 8
+//   k_rec_ion : phase recurrence 6, recarg 3, R sums 4                     (field: 13)
+//               + recarg2 3, (c0 + nz m) recarg2 3, T sums 4                (force: 23)
+//               + Q sums 7                                                  (EFG:   30)
+double rho_flops_per_pair(bool lq, bool ld) { return 8.0 + (ld ? 4.0 : 0.0) + (lq ? 0.0 : 0.0); }
+double ion_flops_per_pair(bool f, bool efg) { return 13.0 + (f ? 10.0 : 0.0) + (efg ? 7.0 : 0.0); }
 
 template <typename K>
 static void allow_smem(K kernel, size_t bytes) {
     if (bytes > 48 * 1024) MDFF_CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
 }
 
+// rho pass + reduction + ion pass.  `o` says where the per-ion results go:
+//   o.ef  = self2*mu + o.ef_dir + E_rec          (when o.ef)
+//   o.f   = o.f + o.f_dir*coul + F_rec*coul      (when o.f)
+//   o.efg = self + o.efg_dir + EFG_rec (upper)   (when o.efg)
 void launch_rec(Engine &e, const double *q, const double3 *mu, bool lq, bool ld, const RecOut &o) {
     int segblocks = ceil_div(e.nseg, RHO_THREADS);
     dim3 grid(segblocks, e.rho_chunks);
@@ -392,6 +458,7 @@ void launch_rec(Engine &e, const double *q, const double3 *mu, bool lq, bool ld,
     a.tile_k = e.d_tile_k;
     a.ntile = e.ntile;
     a.rho_s = e.d_rho;
+    a.part = e.d_ion_part;
     a.tfpiV = 2.0 * 2.0 * TPI_D * e.cell.inveOmega;
     a.self2 = o.self2;
     a.qself = o.self_q;
@@ -409,16 +476,23 @@ void launch_rec(Engine &e, const double *q, const double3 *mu, bool lq, bool ld,
     a.efg_dir = o.efg_dir;
     if (!a.want_ef && !a.want_f && !a.want_efg) return;
     size_t smem2 = sizeof(double2) * e.tile_kmax;
-    int nb = ceil_div(e.n, ION_THREADS);
+    dim3 g2(ceil_div(e.n, ION_THREADS), e.ntile);
+    int nb = ceil_div(e.n, 256);
     int pi = -1;
     e.prof_begin("k_rec_ion", &pi);
     if (a.want_efg)
-        MDFF_LAUNCH(e, (k_rec_ion<true, true>), nb, ION_THREADS, smem2, a);
+        MDFF_LAUNCH(e, (k_rec_ion<true, true>), g2, ION_THREADS, smem2, a);
     else if (a.want_f)
-        MDFF_LAUNCH(e, (k_rec_ion<true, false>), nb, ION_THREADS, smem2, a);
+        MDFF_LAUNCH(e, (k_rec_ion<true, false>), g2, ION_THREADS, smem2, a);
     else
-        MDFF_LAUNCH(e, (k_rec_ion<false, false>), nb, ION_THREADS, smem2, a);
+        MDFF_LAUNCH(e, (k_rec_ion<false, false>), g2, ION_THREADS, smem2, a);
     e.prof_end("k_rec_ion", pi, ion_flops_per_pair(a.want_f || a.want_efg, a.want_efg) * (double)e.n * e.nk);
+    if (a.want_efg)
+        MDFF_LAUNCH(e, (k_rec_combine<true, true>), nb, 256, 0, a);
+    else if (a.want_f)
+        MDFF_LAUNCH(e, (k_rec_combine<true, false>), nb, 256, 0, a);
+    else
+        MDFF_LAUNCH(e, (k_rec_combine<false, false>), nb, 256, 0, a);
 }
 
 }  // namespace mdffgpu

@@ -374,4 +374,94 @@ void launch_dir(Engine &e, const double *q, const double3 *mu, double alpha, boo
         MDFF_LAUNCH(e, (k_dir<false, true, false>), nb, PAIR_WARPS * 32, 0, a);
 }
 
+// ---------------------------------------------------------------- cached dipole field
+// Within one force evaluation the positions are fixed while the induced dipoles are
+// iterated (src/pim.c:236-278), so the screened pair factors F1/d^3 and 3 F2/d^5 of
+// the dipole field (the T2 tensor, src/ewald.c:581-603) are computed once per list
+// entry and reused by every iteration: the iteration kernel then does no erfc/exp.
+__global__ void __launch_bounds__(PAIR_WARPS * 32) k_dir_prep(int n, Cell c, const double4 *__restrict__ s,
+                                                             const int *__restrict__ col,
+                                                             const int *__restrict__ con, int cap, double lrcutsq,
+                                                             double alpha, double2 *__restrict__ coef) {
+    int i = blockIdx.x * PAIR_WARPS + (threadIdx.x >> 5);
+    int lane = threadIdx.x & 31;
+    if (i >= n) return;
+    const double rpi = 1.7724538509055160273;
+    const double alpha2 = alpha * alpha, alpha3 = alpha2 * alpha;
+    double4 si = s[i];
+    int m = min(con[i], cap);
+    const int *L = col + (size_t)i * cap;
+    double2 *C = coef + (size_t)i * cap;
+    for (int k = lane; k < m; k += 32) {
+        double4 sj = s[L[k]];
+        double3 r = pbc_frac(c, dsub(si.x, sj.x), dsub(si.y, sj.y), dsub(si.z, sj.z));
+        double d2 = norm2_exact(r);
+        double2 out = make_double2(0.0, 0.0);
+        if (!(d2 > lrcutsq)) {
+            double d = sqrt(d2), d3 = d2 * d;
+            double dm1 = 1.0 / d, dm3 = dm1 / d2, dm5 = dm3 / d2;
+            double expon = exp(-alpha2 * d2) / rpi;
+            double F0 = erfc(alpha * d);
+            double F1 = F0 + 2.0 * alpha * d * expon;
+            double F2 = F1 + 4.0 * alpha3 * d3 * expon / 3.0;
+            out = make_double2(F1 * dm3, 3.0 * F2 * dm5);
+        }
+        C[k] = out;
+    }
+}
+
+// field of the dipoles mu from the cached factors: E_i = sum_j (3F2/d^5 (r.mu_j) r - F1/d^3 mu_j),
+// only when mu_i and mu_j are non-zero (src/ewald.c:737-749)
+__global__ void __launch_bounds__(PAIR_WARPS * 32) k_dir_field_cached(int n, Cell c, const double4 *__restrict__ s,
+                                                                     const int *__restrict__ col,
+                                                                     const int *__restrict__ con, int cap,
+                                                                     const double2 *__restrict__ coef,
+                                                                     const double3 *__restrict__ mu,
+                                                                     double3 *__restrict__ ef) {
+    int i = blockIdx.x * PAIR_WARPS + (threadIdx.x >> 5);
+    int lane = threadIdx.x & 31;
+    if (i >= n) return;
+    double3 mi = mu[i];
+    bool dip_i = (mi.x != 0.0) || (mi.y != 0.0) || (mi.z != 0.0);
+    double ex = 0.0, ey = 0.0, ez = 0.0;
+    if (dip_i) {
+        double4 si = s[i];
+        int m = min(con[i], cap);
+        const int *L = col + (size_t)i * cap;
+        const double2 *C = coef + (size_t)i * cap;
+        for (int k = lane; k < m; k += 32) {
+            double2 cf = C[k];
+            if (cf.x == 0.0 && cf.y == 0.0) continue;
+            int j = L[k];
+            double3 mj = mu[j];
+            if (mj.x == 0.0 && mj.y == 0.0 && mj.z == 0.0) continue;
+            double4 sj = s[j];
+            double3 r = pbc_frac(c, dsub(si.x, sj.x), dsub(si.y, sj.y), dsub(si.z, sj.z));
+            double rmj = r.x * mj.x + r.y * mj.y + r.z * mj.z;
+            ex += cf.y * rmj * r.x - cf.x * mj.x;
+            ey += cf.y * rmj * r.y - cf.x * mj.y;
+            ez += cf.y * rmj * r.z - cf.x * mj.z;
+        }
+    }
+    ex = warp_sum(ex);
+    ey = warp_sum(ey);
+    ez = warp_sum(ez);
+    if (lane == 0) ef[i] = make_double3(ex, ey, ez);
+}
+
+void launch_dir_prep(Engine &e, double alpha) {
+    int nb = ceil_div(e.n, PAIR_WARPS);
+    MDFF_LAUNCH(e, k_dir_prep, nb, PAIR_WARPS * 32, 0, e.n, e.cell, e.d_s, e.d_co, e.d_con, e.cap_co, e.lrcutsq,
+                alpha, e.d_coef);
+}
+
+void launch_dir_field_cached(Engine &e, const double3 *mu, double3 *out_ef) {
+    int nb = ceil_div(e.n, PAIR_WARPS);
+    int pd = -1;
+    e.prof_begin("k_dir", &pd);
+    MDFF_LAUNCH(e, k_dir_field_cached, nb, PAIR_WARPS * 32, 0, e.n, e.cell, e.d_s, e.d_co, e.d_con, e.cap_co,
+                e.d_coef, mu, out_ef);
+    e.prof_end("k_dir", pd, 0.0);
+}
+
 }  // namespace mdffgpu

@@ -72,3 +72,15 @@ CASES = {
     "crist192_pim_vv": lambda: crist192(True, integrator="nve-vv", temp=2500.0),
 }
 MD_CASES = (("lj256", 50), ("crist192_nhc", 30), ("crist192_pim_nhc", 10), ("crist192_pim_vv", 10))
+
+
+def silica96_ko():
+    """algo_pim scfkO (momentpolaSCFkO, src/pim.c:457-603) with omegakO 0.8."""
+    s = silica96(True)
+    s.algo_pim = "scfkO"
+    s.omegakO = 0.8
+    s.conv_tol_ind = 1e-9
+    return s
+
+
+CASES["silica96_ko"] = silica96_ko

@@ -35,7 +35,7 @@ def main():
     m = ref.run(s, "md", 50, 0)
     out["lj256"].update(md_thermo=m["thermo"], md_r=m["r"], md_v=m["v"], md_f=m["f"])
 
-    for name in ("silica96_rigid", "silica96_pim", "silica450_pim"):
+    for name in ("silica96_rigid", "silica96_pim", "silica450_pim", "silica96_ko"):
         s = cases.CASES[name]()
         r = ref.run(s, "list")
         d = dict(r_in=r["r_in"], nb_point=r["nb_point"], nb_list=r["nb_list"], coul_point=r["coul_point"],

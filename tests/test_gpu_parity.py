@@ -16,7 +16,7 @@ from tests.helpers import load_golden, rel_err
 
 pytestmark = pytest.mark.gpu
 
-SINGLE = ["lj256", "silica96_rigid", "silica96_pim", "silica450_pim"]
+SINGLE = ["lj256", "silica96_rigid", "silica96_pim", "silica450_pim", "silica96_ko"]
 
 
 def _engine_for(name, **kw):

@@ -27,7 +27,7 @@ def _oracle_for(name, wrap_from_golden=True):
     return Oracle(s, wrap=False), g, s
 
 
-@pytest.mark.parametrize("name", ["lj256", "silica96_rigid", "silica96_pim", "silica450_pim"])
+@pytest.mark.parametrize("name", ["lj256", "silica96_rigid", "silica96_pim", "silica450_pim", "silica96_ko"])
 def test_lists_bit_exact(name):
     o, g, s = _oracle_for(name)
     o.gen_verletlist()
@@ -37,7 +37,7 @@ def test_lists_bit_exact(name):
         assert np.array_equal(lst, g[f"{key}_list"])
 
 
-@pytest.mark.parametrize("name", ["lj256", "silica96_rigid", "silica96_pim", "silica450_pim"])
+@pytest.mark.parametrize("name", ["lj256", "silica96_rigid", "silica96_pim", "silica450_pim", "silica96_ko"])
 def test_engforce_vs_reference(name):
     o, g, s = _oracle_for(name)
     o.gen_verletlist()
