@@ -170,6 +170,28 @@ int mdffgpu_prop_agate(mdffgpu_ctx *ctx, int istep);
  * pvir_bhmftd pvir_coul nlist_builds scf_iter scf_rmsd. */
 int mdffgpu_md_steps(mdffgpu_ctx *ctx, int first, int nsteps, double *thermo);
 
+/* Neighbour-list build that allocates no memory.  No counterpart in the reference; it
+ * is for callers that cannot allocate device memory (an application that owns all GPU
+ * memory through its own pool and forbids allocations after start-up, or one that
+ * records its MD step into a CUDA graph).  It runs the kernels of
+ * mdffgpu_gen_verletlist without a context: d_pos is the caller's device array
+ * [n][4] (x, y, z, unused; 32-byte aligned), cell the lattice rows [3][3] on the host,
+ * cut_nb/cut_co the two list radii (rc + skin); the FULL lists go to the caller's
+ * device buffers d_nb[n][cap_nb], d_nbn[n], d_co[n][cap_co], d_con[n] (each ion's
+ * neighbours, both directions of every pair).  Scratch is a static device array of
+ * about 5 MB, shared by every call on a device and holding the last call's data:
+ * limits n <= 65536, at most 32768 cells, at most 4096 ions per cell (so n <= 4096 when
+ * the cell is too small for a cell grid); larger inputs return MDFFGPU_ERR_ARG or
+ * MDFFGPU_ERR_CELL.  Calls that overlap on the GPU (other streams, other threads) race
+ * on that array.  The first call on a device looks up the array's device address (with
+ * that device current); make that first call before any stream capture.  Runs on
+ * `stream` (NULL: the default stream) and synchronises it; *status_out (may be NULL)
+ * receives the kernels' status bits; a list longer than its capacity returns
+ * MDFFGPU_ERR_LIST_OVERFLOW with the true counts in d_nbn/d_con. */
+int mdffgpu_build_lists_noalloc(const double *d_pos, int n, const double *cell, double cut_nb, double cut_co,
+                                int cap_nb, int *d_nb, int *d_nbn, int cap_co, int *d_co, int *d_con,
+                                void *stream, int *status_out);
+
 /* Number of kernel launches the engine made so far (for accounting).  No counterpart
  * in the reference. */
 long long mdffgpu_launch_count(const mdffgpu_ctx *ctx);

@@ -155,6 +155,7 @@ EXPORTS = (
     "mdffgpu_engforce", "mdffgpu_engforce_nmlj", "mdffgpu_engforce_bhmftd", "mdffgpu_multipole_es",
     "mdffgpu_get_dipoles", "mdffgpu_prop_agate", "mdffgpu_md_steps", "mdffgpu_launch_count",
     "mdffgpu_stream", "mdffgpu_fma_peak", "mdffgpu_profile", "mdffgpu_profile_result",
+    "mdffgpu_build_lists_noalloc",
 )
 
 _lib = None
@@ -210,6 +211,8 @@ def load_library(path: str = LIB_PATH):
     L.mdffgpu_profile.restype = C.c_int
     L.mdffgpu_profile_result.argtypes = [vp, dp, C.POINTER(C.c_longlong), dp]
     L.mdffgpu_profile_result.restype = C.c_int
+    L.mdffgpu_build_lists_noalloc.argtypes = [vp, I, dp, D, D, I, vp, vp, I, vp, vp, vp, ip]
+    L.mdffgpu_build_lists_noalloc.restype = C.c_int
     _lib = L
     return L
 
