@@ -186,6 +186,15 @@ def run_ours(args):
     eng = Engine(s, positions=pos, device=dev, precision=prec, pim_solver=solver)
     eng.gen_verletlist()
     eng.engforce()                                    # forces at t=0 (src/md.c:209)
+    force_err = None
+    if prec == MIXED:
+        # relative RMS force error of the mixed path against the FP64 path at t=0
+        ref = Engine(s, positions=pos, device=dev, precision=FP64, pim_solver=solver)
+        ref.gen_verletlist()
+        ref.engforce()
+        f64, f32 = ref.forces(), eng.forces()
+        force_err = float(np.sqrt(np.mean(np.sum((f32 - f64) ** 2, 1)) / np.mean(np.sum(f64 ** 2, 1))))
+        ref.close()
     istep = 1
     if args.warmup > 0:
         eng.md_steps(istep, args.warmup)
@@ -282,6 +291,7 @@ def run_ours(args):
                          "share_of_step": (kms / total_ms) if world == 1 else None},
             "clocks": clk,
             "gpu_launches": launches,
+            "force_rms_rel_err_vs_fp64": force_err,
             "scf_iter_mean": float(th[:, 10].mean()),
             "list_rebuilds": int(th[-1, 9] - th[0, 9]) + 1,
             "finite": bool(np.isfinite(th).all()),

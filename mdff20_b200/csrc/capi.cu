@@ -81,6 +81,7 @@ int mdffgpu_set_precision(mdffgpu_ctx *ctx, int precision) {
         if (precision == MDFFGPU_MIXED && !mdffgpu::mixed_available())
             throw Error(MDFFGPU_ERR_ARG, "mixed precision kernels are not built in this library");
         e.precision = precision;
+        e.use32 = (precision == MDFFGPU_MIXED);
     });
 }
 
@@ -282,6 +283,7 @@ int mdffgpu_get_dipoles(mdffgpu_ctx *ctx, double *mu, double *upol) {
         if (!e.p.lcoulombic) throw Error(MDFFGPU_ERR_STATE, "lcoulombic is not set");
         e.ensure_lists();
         mdffgpu::launch_kardir(e, e.d_r, e.d_s);
+        if (e.use32) mdffgpu::launch_coords32(e);
         e.get_dipoles();
         e.sync_scalars();
         if (mu) download(e, mu, e.d_mu_tot, sizeof(double3) * e.n);

@@ -145,6 +145,8 @@ Engine::Engine(const mdffgpu_params &prm, int dev) : p(prm) {
     d_qzero = dalloc<double>(n);
     d_muzero = dalloc<double3>(n);
     d_svl = dalloc<double4>(n);
+    d_s32 = dalloc<float4>(n);
+    d_t32 = dalloc<float4>(n);
     d_rebuild = dalloc<int>(1);
     d_status = dalloc<unsigned>(1);
     d_scal = dalloc<double>(NSLOT);
@@ -199,6 +201,10 @@ Engine::~Engine() {
     cudaFree(d_rho_part);
     cudaFree(d_rho);
     cudaFree(d_ion_part);
+    cudaFree(d_coef);
+    cudaFree(d_coef32);
+    cudaFree(d_s32);
+    cudaFree(d_t32);
     cudaFree(d_out);
     cudaFree(d_status);
     if (h_out) cudaFreeHost(h_out);
@@ -549,7 +555,11 @@ void Engine::alloc_lists(int cnb, int cco) {
     d_co = dalloc<int>((size_t)n * cap_co);
     d_con = dalloc<int>(n);
     dfree(d_coef);
-    if (p.lcoulombic && lpol) d_coef = dalloc<double2>((size_t)n * cap_co);
+    dfree(d_coef32);
+    if (p.lcoulombic && lpol) {
+        d_coef = dalloc<double2>((size_t)n * cap_co);
+        d_coef32 = dalloc<float2>((size_t)n * cap_co);
+    }
     list_ready = false;
     coef_ready = false;
 }
@@ -685,10 +695,14 @@ static double self2_of(double alpha) {
 // electric field of (q, mu): self + direct + reciprocal, as multipole_ES with
 // do_ef only (src/ewald.c:75-348); no energy, no forces
 void Engine::field_of(const double *d_qv, const double3 *d_muv, bool lq, bool ld, bool damp, double3 *d_ef_out) {
-    if (!lq && ld && !damp && coef_ready)
-        launch_dir_field_cached(*this, d_muv, d_tmp3);
-    else
+    if (!lq && ld && !damp && coef_ready) {
+        if (use32) launch_dir_field_cached32(*this, d_muv, d_tmp3);
+        else launch_dir_field_cached(*this, d_muv, d_tmp3);
+    } else if (use32) {
+        launch_dir32(*this, d_qv, d_muv, p.alphaES, lq, ld, damp, false, true, d_tmp3, nullptr);
+    } else {
         launch_dir(*this, d_qv, d_muv, p.alphaES, lq, ld, damp, false, true, false, false, d_tmp3, nullptr, nullptr);
+    }
     RecOut o;
     o.ef = d_ef_out;
     o.ef_dir = d_tmp3;
@@ -878,7 +892,8 @@ void Engine::get_dipoles() {
             bool &flag;
             ~CoefScope() { flag = false; }
         } scope{coef_ready};
-        launch_dir_prep(*this, p.alphaES);
+        if (use32) launch_dir_prep32(*this, p.alphaES);
+        else launch_dir_prep(*this, p.alphaES);
         coef_ready = true;
         if (pim_solver == MDFFGPU_PIM_CG) pim_cg();
         else if (p.algo_pim == 1) pim_ko();
@@ -907,14 +922,18 @@ void Engine::engforce() {
     ensure_lists();
     MDFF_CK(cudaMemsetAsync(d_f, 0, sizeof(double3) * n, stream));
     launch_kardir(*this, d_r, d_s);
+    if (use32) launch_coords32(*this);
     if (p.lnmlj) sr_forces(true, nullptr, nullptr, nullptr);
     if (p.lbhmft || p.lbhmftd) sr_forces(false, nullptr, nullptr, nullptr);
     if (p.lcoulombic) {
         get_dipoles();
         bool ld = (ldip || lpol);
         // direct space: forces, energy, virial (do_forces, do_stress; src/field.c:381-383)
-        launch_dir(*this, d_q, d_mu_tot, p.alphaES, lqch != 0, ld, ldmp != 0, true, false, false, false, nullptr,
-                   nullptr, d_tmp3);
+        if (use32)
+            launch_dir32(*this, d_q, d_mu_tot, p.alphaES, lqch != 0, ld, ldmp != 0, true, false, nullptr, d_tmp3);
+        else
+            launch_dir(*this, d_q, d_mu_tot, p.alphaES, lqch != 0, ld, ldmp != 0, true, false, false, false,
+                       nullptr, nullptr, d_tmp3);
         reduce(S_DIR_U, 7, ceil_div(n, 8));
         RecOut o;
         o.f = d_f;

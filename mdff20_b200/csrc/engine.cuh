@@ -96,7 +96,13 @@ void launch_rec(Engine &e, const double *q, const double3 *mu, bool lq, bool ld,
 // integrate.cu
 void launch_reduce_slots(Engine &e, int first_slot, int nslots, int nparts);
 // true once the FP32 pair/k-space kernels exist in this build
-inline bool mixed_available() { return false; }
+inline bool mixed_available() { return true; }
+// mixed.cu: FP32 coordinates, real-space and cached-field kernels
+void launch_coords32(Engine &e);
+void launch_dir32(Engine &e, const double *q, const double3 *mu, double alpha, bool lq, bool ld, bool damp,
+                  bool forces, bool ef, double3 *out_ef, double3 *out_f);
+void launch_dir_prep32(Engine &e, double alpha);
+void launch_dir_field_cached32(Engine &e, const double3 *mu, double3 *out_ef);
 
 // ---------------------------------------------------------------- engine state
 struct Engine {
@@ -147,6 +153,9 @@ struct Engine {
     int cap_nb = 0, cap_co = 0;
     int *d_nb = nullptr, *d_nbn = nullptr, *d_co = nullptr, *d_con = nullptr;
     double2 *d_coef = nullptr;   // [n][cap_co] cached dipole-field pair factors
+    float2 *d_coef32 = nullptr;  // same, mixed precision
+    float4 *d_s32 = nullptr, *d_t32 = nullptr;   // wrapped fractional / phase coordinates, FP32
+    bool use32 = false;          // mixed precision: FP32 Ewald kernels
     bool coef_ready = false;     // d_coef matches the current positions
     double4 *d_svl = nullptr;    // fractional positions at the last build
     int nc[3] = {1, 1, 1}, ncell = 1, cell_cap = 4096;

@@ -416,14 +416,21 @@ static void allow_smem(K kernel, size_t bytes) {
 //   o.ef  = self2*mu + o.ef_dir + E_rec          (when o.ef)
 //   o.f   = o.f + o.f_dir*coul + F_rec*coul      (when o.f)
 //   o.efg = self + o.efg_dir + EFG_rec (upper)   (when o.efg)
+void launch_rho32(Engine &e, const double *q, const double3 *mu, bool lq, bool ld);
+void launch_ion32(Engine &e, const double3 *mu, bool ld, bool want_f);
+
 void launch_rec(Engine &e, const double *q, const double3 *mu, bool lq, bool ld, const RecOut &o) {
+    // FP32 passes in mixed precision (no FP32 EFG: EFG requests run in FP64)
+    bool fp32 = e.use32 && o.efg == nullptr;
     int segblocks = ceil_div(e.nseg, RHO_THREADS);
     dim3 grid(segblocks, e.rho_chunks);
     int WT = (e.kmax[0] + 1) + (2 * e.kmax[1] + 1) + (2 * e.kmax[2] + 1);
     size_t smem = sizeof(double2) * RHO_TI * WT + sizeof(double) * RHO_TI * 4;
     int ps = -1;
-    e.prof_begin("k_rho", &ps);
-    if (lq && ld) {
+    if (!fp32) e.prof_begin("k_rho", &ps);
+    if (fp32) {
+        launch_rho32(e, q, mu, lq, ld);
+    } else if (lq && ld) {
         allow_smem(k_rho<true, true>, smem);
         MDFF_LAUNCH(e, (k_rho<true, true>), grid, RHO_THREADS, smem, e.n, e.rho_chunk, e.cell, e.kmax[0], e.kmax[1],
                     e.kmax[2], e.d_r, q, mu, e.nseg, e.d_seg, e.d_rho_part, e.nk);
@@ -438,7 +445,7 @@ void launch_rec(Engine &e, const double *q, const double3 *mu, bool lq, bool ld,
     } else {
         MDFF_CK(cudaMemsetAsync(e.d_rho_part, 0, sizeof(double2) * (size_t)e.nk * e.rho_chunks, e.stream));
     }
-    e.prof_end("k_rho", ps, (lq || ld) ? rho_flops_per_pair(lq, ld) * (double)e.n * e.nk : 0.0);
+    if (!fp32) e.prof_end("k_rho", ps, (lq || ld) ? rho_flops_per_pair(lq, ld) * (double)e.n * e.nk : 0.0);
     int nbr = ceil_div(e.nk, 256);
     MDFF_LAUNCH(e, k_rho_reduce, nbr, 256, 0, e.nk, e.rho_chunks, e.d_rho_part, e.d_Ak, e.d_kcoe, e.d_kvec,
                 e.d_rho, e.d_part, (int)S_REC_U, e.part_stride);
@@ -479,14 +486,18 @@ void launch_rec(Engine &e, const double *q, const double3 *mu, bool lq, bool ld,
     dim3 g2(ceil_div(e.n, ION_THREADS), e.ntile);
     int nb = ceil_div(e.n, 256);
     int pi = -1;
-    e.prof_begin("k_rec_ion", &pi);
-    if (a.want_efg)
-        MDFF_LAUNCH(e, (k_rec_ion<true, true>), g2, ION_THREADS, smem2, a);
-    else if (a.want_f)
-        MDFF_LAUNCH(e, (k_rec_ion<true, false>), g2, ION_THREADS, smem2, a);
-    else
-        MDFF_LAUNCH(e, (k_rec_ion<false, false>), g2, ION_THREADS, smem2, a);
-    e.prof_end("k_rec_ion", pi, ion_flops_per_pair(a.want_f || a.want_efg, a.want_efg) * (double)e.n * e.nk);
+    if (fp32) {
+        launch_ion32(e, mu, ld, a.want_f);
+    } else {
+        e.prof_begin("k_rec_ion", &pi);
+        if (a.want_efg)
+            MDFF_LAUNCH(e, (k_rec_ion<true, true>), g2, ION_THREADS, smem2, a);
+        else if (a.want_f)
+            MDFF_LAUNCH(e, (k_rec_ion<true, false>), g2, ION_THREADS, smem2, a);
+        else
+            MDFF_LAUNCH(e, (k_rec_ion<false, false>), g2, ION_THREADS, smem2, a);
+        e.prof_end("k_rec_ion", pi, ion_flops_per_pair(a.want_f || a.want_efg, a.want_efg) * (double)e.n * e.nk);
+    }
     if (a.want_efg)
         MDFF_LAUNCH(e, (k_rec_combine<true, true>), nb, 256, 0, a);
     else if (a.want_f)

@@ -221,3 +221,43 @@ def test_list_capacity_grows():
         p1, l1 = o.verletlist(which)
         p2, l2 = e.verletlist(which)
         assert np.array_equal(p1, p2) and np.array_equal(l1, l2)
+
+
+# ---------------------------------------------------------------------------- mixed precision
+def _rms_rel(a, b):
+    return float(np.sqrt(np.mean(np.sum((a - b) ** 2, axis=1))) / np.sqrt(np.mean(np.sum(b ** 2, axis=1))))
+
+
+@pytest.mark.parametrize("name", ["silica450_pim", "silica96_rigid"])
+def test_mixed_precision_force_error_small(name):
+    """Mixed FP32/FP64 forces within 1e-5 relative RMS of the reference's FP64 forces."""
+    from mdff20_b200.engine import MIXED
+    e, g, s = _engine_for(name, precision=MIXED)
+    e.gen_verletlist()
+    e.engforce()
+    fr = g["f"].reshape(-1, 3)
+    assert _rms_rel(e.forces(), fr) < 1e-5
+    th = e.thermo()
+    assert abs(th["u_coul"] - float(g["u_coul"][0])) < 1e-6 * abs(float(g["u_coul"][0]))
+
+
+def test_mixed_precision_force_error_full_size():
+    """N=24000 PIM silica (the bench system): mixed vs FP64 engine, same solver."""
+    from mdff20_b200.engine import MIXED
+    s = synth.config5()
+    pos = wrapped_positions(s)
+    ref = Engine(s, positions=pos, pim_solver=PIM_CG)
+    ref.gen_verletlist()
+    ref.engforce()
+    mix = Engine(s, positions=pos, pim_solver=PIM_CG, precision=MIXED)
+    mix.gen_verletlist()
+    mix.engforce()
+    err = _rms_rel(mix.forces(), ref.forces())
+    assert err < 1e-5, err
+    a, b = mix.thermo(), ref.thermo()
+    # energies: same 1e-5 relative bar as the forces (u_pol carries the SCF
+    # convergence tolerance on top of the FP32 field error)
+    for k in ("u_coul", "u_pol", "u_bhmftd"):
+        assert abs(a[k] - b[k]) < 1e-5 * max(1.0, abs(b[k])), k
+    th = mix.md_steps(1, 3)
+    assert np.isfinite(th).all()
