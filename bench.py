@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
-    ap.add_argument("--solver", choices=["cg", "reference"], default="cg")
+    ap.add_argument("--solver", choices=["cg", "fused", "reference"], default="cg")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--roof-kernel", default="k_rho")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -173,7 +173,7 @@ def run_ours(args):
     import torch
 
     from mdff20_b200 import synth
-    from mdff20_b200.engine import FP64, MIXED, PIM_CG, PIM_REFERENCE, Engine, fma_peak_tflops
+    from mdff20_b200.engine import FP64, MIXED, PIM_CG, PIM_CG_FUSED, PIM_REFERENCE, Engine, fma_peak_tflops
     from mdff20_b200.cellmath import wrap_positions
 
     world, rank, local, pg = dist_setup(args)
@@ -182,7 +182,7 @@ def run_ours(args):
     s = synth.config5()
     pos = wrap_positions(s.cell, s.pos)
     prec = MIXED if args.precision == "mixed" else FP64
-    solver = PIM_CG if args.solver == "cg" else PIM_REFERENCE
+    solver = {"cg": PIM_CG, "fused": PIM_CG_FUSED, "reference": PIM_REFERENCE}[args.solver]
     eng = Engine(s, positions=pos, device=dev, precision=prec, pim_solver=solver)
     eng.gen_verletlist()
     eng.engforce()                                    # forces at t=0 (src/md.c:209)

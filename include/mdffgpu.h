@@ -47,6 +47,8 @@ extern "C" {
 /* induced-dipole solver */
 #define MDFFGPU_PIM_REFERENCE 0 /* the reference's algo_pim (scf: Jacobi + ASPC, scfkO) */
 #define MDFFGPU_PIM_CG 1        /* preconditioned conjugate gradient on (alpha^-1 - T) mu = E_stat */
+#define MDFFGPU_PIM_CG_FUSED 2  /* CG with E_stat and the first residual from one Ewald pass, and
+                                   rho(k) carried along the iterates for the force pass */
 
 /* Parameter block: the values the reference's parsers leave in its globals, in
  * control-file units (read_global src/global.c:13-60, read_md src/md.c:29-98,

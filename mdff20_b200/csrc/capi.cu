@@ -87,7 +87,8 @@ int mdffgpu_set_precision(mdffgpu_ctx *ctx, int precision) {
 
 int mdffgpu_set_pim_solver(mdffgpu_ctx *ctx, int solver) {
     return guarded(ctx, [&](Engine &e) {
-        if (solver != MDFFGPU_PIM_REFERENCE && solver != MDFFGPU_PIM_CG) throw Error(MDFFGPU_ERR_ARG, "bad solver");
+        if (solver != MDFFGPU_PIM_REFERENCE && solver != MDFFGPU_PIM_CG && solver != MDFFGPU_PIM_CG_FUSED)
+            throw Error(MDFFGPU_ERR_ARG, "bad solver");
         e.pim_solver = solver;
     });
 }

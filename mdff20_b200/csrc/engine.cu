@@ -156,7 +156,7 @@ Engine::Engine(const mdffgpu_params &prm, int dev) : p(prm) {
     MDFF_CK(cudaMallocHost((void **)&h_stage, sizeof(double) * 10 * (size_t)n));
     memset(h_out, 0, sizeof(DevScalars));
     if (p.lcoulombic) setup_kspace();
-    int nkb = nk > 0 ? ceil_div(nk, 256) : 1;
+    int nkb = nk > 0 ? ceil_div(nk, RHOR_K) : 1;
     part_stride = std::max(ceil_div(n, 8), nkb) + 8;
     d_part = dalloc<double>((size_t)NSLOT * part_stride);
     // neighbour lists: initial capacities from the number density
@@ -200,6 +200,8 @@ Engine::~Engine() {
     cudaFree(d_row);
     cudaFree(d_rho_part);
     cudaFree(d_rho);
+    cudaFree(d_rho_acc);
+    cudaFree(d_rho_it);
     cudaFree(d_ion_part);
     cudaFree(d_coef);
     cudaFree(d_coef32);
@@ -513,6 +515,8 @@ void Engine::setup_kspace() {
     rho_chunks = ceil_div(n, rho_chunk);
     d_rho_part = dalloc<double2>((size_t)rho_chunks * nk);
     d_rho = dalloc<double2>(nk);
+    d_rho_acc = dalloc<double2>(nk);
+    d_rho_it = dalloc<double2>(nk);
     d_ion_part = dalloc<double>((size_t)ntile * n * 12);
 }
 
@@ -694,7 +698,8 @@ static double self2_of(double alpha) {
 
 // electric field of (q, mu): self + direct + reciprocal, as multipole_ES with
 // do_ef only (src/ewald.c:75-348); no energy, no forces
-void Engine::field_of(const double *d_qv, const double3 *d_muv, bool lq, bool ld, bool damp, double3 *d_ef_out) {
+void Engine::field_of(const double *d_qv, const double3 *d_muv, bool lq, bool ld, bool damp, double3 *d_ef_out,
+                      double2 *rho_raw) {
     if (!lq && ld && !damp && coef_ready) {
         if (use32) launch_dir_field_cached32(*this, d_muv, d_tmp3);
         else launch_dir_field_cached(*this, d_muv, d_tmp3);
@@ -708,6 +713,7 @@ void Engine::field_of(const double *d_qv, const double3 *d_muv, bool lq, bool ld
     o.ef_dir = d_tmp3;
     o.self2 = self2_of(p.alphaES);
     o.self_mu = d_muv;
+    o.rho_raw = rho_raw;
     launch_rec(*this, d_qv, d_muv, lq, ld, o);
 }
 
@@ -760,16 +766,38 @@ void Engine::pim_reference() {
 // preconditioned conjugate gradient on (alpha^-1 - T) mu = E_stat, polarisable ions;
 // initial guess from the ASPC predictor; stops when the reference's residual measure
 // sqrt(sum (mu/alpha - E)^2 / npol) (src/pim.c:431-449) is below conv_tol_ind
-void Engine::pim_cg() {
+// fused: E_stat + T mu0 is one Ewald evaluation of (q, mu_static + mu0) (the residual
+// needs only their sum), and rho(k) of (q, mu_static + mu) follows the iterates
+// (rho is linear in mu: rho(x + a p) = rho(x) + a rho(p)), so the force evaluation
+// that follows skips its rho pass (rho_acc_ready).
+void Engine::pim_cg(bool fused) {
     int nb = ceil_div(n, 256);
-    field_of(d_q, d_mu_static, lqch != 0, ldip != 0, ldmp != 0, d_ef_stat);
     int ord = p.extrapolate_order;
     if (ord < 0 || ord > 5) throw Error(MDFFGPU_ERR_ARG, "extrapolate_order must be 0..5");
     int e = (istep >= ord + 1) ? ord : (!istep ? 0 : istep - 1);
     int es = (e != ord) ? e + 1 : e;
-    MDFF_LAUNCH(*this, k_aspc_predict, nb, 256, 0, n, e, es, d_hist, d_mu_ind);
-    field_of(d_qzero, d_mu_ind, false, true, false, d_ef_ind);
-    MDFF_LAUNCH(*this, k_cg_residual, nb, 256, 0, n, d_polar, d_invpol, d_ef_stat, d_ef_ind, d_mu_ind, d_cg_r);
+    if (fused) {
+        MDFF_LAUNCH(*this, k_aspc_predict, nb, 256, 0, n, e, es, d_hist, d_mu_ind);
+        MDFF_LAUNCH(*this, k_add3, nb, 256, 0, n, d_mu_static, d_mu_ind, d_mu_tot);
+        if (use32)
+            launch_dir32(*this, d_q, d_mu_tot, p.alphaES, lqch != 0, true, ldmp != 0, false, true, d_tmp3, nullptr);
+        else
+            launch_dir(*this, d_q, d_mu_tot, p.alphaES, lqch != 0, true, ldmp != 0, false, true, false, false,
+                       d_tmp3, nullptr, nullptr);
+        RecOut o;
+        o.ef = d_ef_ind;
+        o.ef_dir = d_tmp3;
+        o.self2 = self2_of(p.alphaES);
+        o.self_mu = d_mu_tot;
+        o.rho_raw = d_rho_acc;
+        launch_rec(*this, d_q, d_mu_tot, lqch != 0, true, o);
+        MDFF_LAUNCH(*this, k_cg_residual, nb, 256, 0, n, d_polar, d_invpol, d_muzero, d_ef_ind, d_mu_ind, d_cg_r);
+    } else {
+        field_of(d_q, d_mu_static, lqch != 0, ldip != 0, ldmp != 0, d_ef_stat);
+        MDFF_LAUNCH(*this, k_aspc_predict, nb, 256, 0, n, e, es, d_hist, d_mu_ind);
+        field_of(d_qzero, d_mu_ind, false, true, false, d_ef_ind);
+        MDFF_LAUNCH(*this, k_cg_residual, nb, 256, 0, n, d_polar, d_invpol, d_ef_stat, d_ef_ind, d_mu_ind, d_cg_r);
+    }
     MDFF_LAUNCH(*this, k_cg_rz, nb, 256, 0, n, d_polar, d_pol, d_cg_r, d_mu_save, d_part, part_stride);
     reduce(S_RZ, 2, nb);
     MDFF_CK(cudaMemcpyAsync(d_cg_p, d_mu_save, sizeof(double3) * n, cudaMemcpyDeviceToDevice, stream));
@@ -780,11 +808,12 @@ void Engine::pim_cg() {
     int it = 0;
     int maxit = std::max(p.max_scf_pim_iter, 1);
     while (rmsd > p.conv_tol_ind && it < maxit) {
-        field_of(d_qzero, d_cg_p, false, true, false, d_ef_ind);     // T p
+        field_of(d_qzero, d_cg_p, false, true, false, d_ef_ind, fused ? d_rho_it : nullptr);   // T p
         MDFF_LAUNCH(*this, k_cg_ap, nb, 256, 0, n, d_polar, d_invpol, d_cg_p, d_ef_ind, d_cg_ap, d_part, part_stride);
         reduce(S_PAP, 1, nb);
         MDFF_LAUNCH(*this, k_copy_slot, 1, 1, 0, d_scal, (int)S_RZ, (int)S_RZOLD);
         MDFF_LAUNCH(*this, k_cg_update, nb, 256, 0, n, d_scal, d_cg_p, d_cg_ap, d_mu_ind, d_cg_r);
+        if (fused) launch_rho_axpy(*this, S_RZOLD, S_PAP, d_rho_it, d_rho_acc);
         MDFF_LAUNCH(*this, k_cg_rz, nb, 256, 0, n, d_polar, d_pol, d_cg_r, d_mu_save, d_part, part_stride);
         reduce(S_RZ, 2, nb);
         MDFF_CK(cudaMemcpyAsync(&rr, d_scal + S_RR, sizeof(double), cudaMemcpyDeviceToHost, stream));
@@ -804,6 +833,7 @@ void Engine::pim_cg() {
     MDFF_LAUNCH(*this, k_hist_store, nb, 256, 0, n, d_mu_ind, d_hist);
     last_scf_iter = it;
     last_rmsd = rmsd;
+    rho_acc_ready = fused;
     double v = 0.5 * up * coul_unit;
     MDFF_CK(cudaMemcpyAsync(&d_out->u_pol, &v, sizeof(double), cudaMemcpyHostToDevice, stream));
     MDFF_CK(cudaStreamSynchronize(stream));
@@ -895,7 +925,8 @@ void Engine::get_dipoles() {
         if (use32) launch_dir_prep32(*this, p.alphaES);
         else launch_dir_prep(*this, p.alphaES);
         coef_ready = true;
-        if (pim_solver == MDFFGPU_PIM_CG) pim_cg();
+        if (pim_solver == MDFFGPU_PIM_CG || pim_solver == MDFFGPU_PIM_CG_FUSED)
+            pim_cg(pim_solver == MDFFGPU_PIM_CG_FUSED);
         else if (p.algo_pim == 1) pim_ko();
         else pim_reference();
         int nb = ceil_div(n, 256);
@@ -926,6 +957,7 @@ void Engine::engforce() {
     if (p.lnmlj) sr_forces(true, nullptr, nullptr, nullptr);
     if (p.lbhmft || p.lbhmftd) sr_forces(false, nullptr, nullptr, nullptr);
     if (p.lcoulombic) {
+        rho_acc_ready = false;
         get_dipoles();
         bool ld = (ldip || lpol);
         // direct space: forces, energy, virial (do_forces, do_stress; src/field.c:381-383)
@@ -939,6 +971,8 @@ void Engine::engforce() {
         o.f = d_f;
         o.f_dir = d_tmp3;
         o.coul = coul_unit;
+        if (rho_acc_ready) o.rho_acc = d_rho_acc;   // rho(k) of (q, mu_tot) from the fused CG
+        rho_acc_ready = false;
         launch_rec(*this, d_q, d_mu_tot, lqch != 0, ld, o);
         int nb = ceil_div(n, 256);
         MDFF_LAUNCH(*this, k_self_sums, nb, 256, 0, n, d_q, d_mu_tot, d_part, part_stride);

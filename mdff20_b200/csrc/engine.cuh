@@ -25,6 +25,7 @@ struct PairDamp {
 // one k-space row segment: up to KSEG consecutive nz values at fixed (nx, ny)
 constexpr int KSEG = 16;
 constexpr int RHO_MIN_BLOCKS = 4;   // resident k_rho blocks per SM (caps registers at 128)
+constexpr int RHOR_K = 32;          // k per k_rho_reduce block
 struct KSeg {
     int nx, ny, z0, cnt;
     int koff, pad0, pad1, pad2;
@@ -91,8 +92,12 @@ struct RecOut {
     double coul = 1.0;
     double *efg = nullptr;            // self + efg_dir + EFG_rec (upper triangle)
     const double *efg_dir = nullptr;
+    double2 *rho_raw = nullptr;       // receives rho(k) of (q, mu) when set
+    const double2 *rho_acc = nullptr; // rho(k) of (q, mu) given: the rho pass is skipped
 };
 void launch_rec(Engine &e, const double *q, const double3 *mu, bool lq, bool ld, const RecOut &o);
+// acc += (scal[num_slot] / scal[den_slot]) x over the k-vectors
+void launch_rho_axpy(Engine &e, int num_slot, int den_slot, const double2 *x, double2 *acc);
 // integrate.cu
 void launch_reduce_slots(Engine &e, int first_slot, int nslots, int nparts);
 // true once the FP32 pair/k-space kernels exist in this build
@@ -175,6 +180,8 @@ struct Engine {
     int *d_tile_row = nullptr, *d_tile_k = nullptr;
     int ntile = 0, tile_kmax = 0;
     double2 *d_rho_part = nullptr, *d_rho = nullptr;   // partial per ion chunk, total (Ak-scaled)
+    double2 *d_rho_acc = nullptr, *d_rho_it = nullptr; // rho(k) of (q, mu) along the fused CG; of its p
+    bool rho_acc_ready = false;                         // d_rho_acc holds rho(k) of (q, mu_tot)
     double *d_ion_part = nullptr;                       // ion-pass partial sums [ntile][n][12]
     int rho_chunks = 0, rho_chunk = 0;
 
@@ -227,10 +234,11 @@ struct Engine {
     void sr_forces(bool lj, double *u, double *pvir, double *tau);
     void multipole_es_dev(const double *d_qv, const double3 *d_muv, double alpha, int flags, double3 *d_ef_out,
                           double *d_efg_out, double3 *d_f_out);
-    void field_of(const double *d_qv, const double3 *d_muv, bool lq, bool ld, bool damp, double3 *d_ef_out);
+    void field_of(const double *d_qv, const double3 *d_muv, bool lq, bool ld, bool damp, double3 *d_ef_out,
+                  double2 *rho_raw = nullptr);
     void get_dipoles();
     void pim_reference();
-    void pim_cg();
+    void pim_cg(bool fused);
     void pim_ko();
     void ko_inner(double3 *d_dmu, const double3 *d_find);
     double rmsd_of(const double3 *d_mu, const double3 *d_ef, double *upol_sum);

@@ -140,20 +140,15 @@ __global__ void __launch_bounds__(RHO_THREADS, RHO_MIN_BLOCKS) k_rho(int n, int 
     }
 }
 
-// sum the ion-chunk partials of rho(k) in a fixed order; store Ak*rho(k); block
-// partials of u_rec = sum Ak|rho|^2 and of the k-space virial (src/ewald.c:945-1006)
-__global__ void k_rho_reduce(int nk, int nchunks, const double2 *__restrict__ part, const double *__restrict__ Ak,
-                             const double *__restrict__ kcoe, const double3 *__restrict__ kv,
-                             double2 *__restrict__ rho_s, double *__restrict__ ppart, int slot, int stride) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
+// one warp, one k per lane: store Ak*rho(k); warp partials of u_rec = sum Ak|rho|^2 and
+// of the k-space virial (src/ewald.c:945-1006) into ppart[slot..slot+6][blockIdx.x]
+__device__ __forceinline__ void rho_finish(int k, int nk, double2 rho, const double *__restrict__ Ak,
+                                           const double *__restrict__ kcoe, const double3 *__restrict__ kv,
+                                           double2 *__restrict__ rho_s, double *__restrict__ ppart, int slot,
+                                           int stride) {
+    int l = threadIdx.x & 31;
     double v[7] = {0, 0, 0, 0, 0, 0, 0};
     if (k < nk) {
-        double2 rho = make_double2(0.0, 0.0);
-        for (int c = 0; c < nchunks; c++) {
-            double2 p = part[(size_t)c * nk + k];
-            rho.x += p.x;
-            rho.y += p.y;
-        }
         double ak = Ak[k], co = kcoe[k];
         double3 kk = kv[k];
         double str = (rho.x * rho.x + rho.y * rho.y) * ak;
@@ -166,18 +161,70 @@ __global__ void k_rho_reduce(int nk, int nchunks, const double2 *__restrict__ pa
         v[5] = -co * kk.y * kk.z * str;
         v[6] = (1.0 - co * kk.z * kk.z) * str;
     }
-    __shared__ double sh[8][7];
-    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
 #pragma unroll
     for (int q = 0; q < 7; q++) v[q] = warp_sum(v[q]);
-    if (l == 0)
-        for (int q = 0; q < 7; q++) sh[w][q] = v[q];
-    __syncthreads();
-    if (threadIdx.x < 7) {
-        double a = 0.0;
-        for (int q = 0; q < (int)(blockDim.x >> 5); q++) a += sh[q][threadIdx.x];
-        ppart[(size_t)(slot + threadIdx.x) * stride + blockIdx.x] = a;
+    if (l < 7) {
+        double a = v[0];
+#pragma unroll
+        for (int q = 1; q < 7; q++)
+            if (l == q) a = v[q];
+        ppart[(size_t)(slot + l) * stride + blockIdx.x] = a;
     }
+}
+
+// sum the ion-chunk partials of rho(k) in a fixed order, then rho_finish. A block owns
+// RHOR_K consecutive k (one per lane); its 8 warps take every 8th chunk and warp 0 adds
+// the 8 warp sums in warp order. rho_raw (optional) receives rho(k) itself.
+__global__ void __launch_bounds__(256) k_rho_reduce(int nk, int nchunks, const double2 *__restrict__ part,
+                                                    const double *__restrict__ Ak, const double *__restrict__ kcoe,
+                                                    const double3 *__restrict__ kv, double2 *__restrict__ rho_s,
+                                                    double2 *__restrict__ rho_raw, double *__restrict__ ppart,
+                                                    int slot, int stride) {
+    __shared__ double2 ws[8][RHOR_K];
+    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    int k = blockIdx.x * RHOR_K + l;
+    double2 acc = make_double2(0.0, 0.0);
+    if (k < nk)
+        for (int c = w; c < nchunks; c += 8) {
+            double2 p = part[(size_t)c * nk + k];
+            acc.x += p.x;
+            acc.y += p.y;
+        }
+    ws[w][l] = acc;
+    __syncthreads();
+    if (w) return;
+    double2 rho = ws[0][l];
+#pragma unroll
+    for (int q = 1; q < 8; q++) {
+        rho.x += ws[q][l].x;
+        rho.y += ws[q][l].y;
+    }
+    if (rho_raw && k < nk) rho_raw[k] = rho;
+    rho_finish(k, nk, rho, Ak, kcoe, kv, rho_s, ppart, slot, stride);
+}
+
+// rho_finish on a rho(k) assembled elsewhere (one warp per RHOR_K k)
+__global__ void __launch_bounds__(32) k_rho_from_acc(int nk, const double2 *__restrict__ acc,
+                                                     const double *__restrict__ Ak, const double *__restrict__ kcoe,
+                                                     const double3 *__restrict__ kv, double2 *__restrict__ rho_s,
+                                                     double *__restrict__ ppart, int slot, int stride) {
+    int k = blockIdx.x * RHOR_K + threadIdx.x;
+    double2 rho = k < nk ? acc[k] : make_double2(0.0, 0.0);
+    rho_finish(k, nk, rho, Ak, kcoe, kv, rho_s, ppart, slot, stride);
+}
+
+// acc += (scal[num] / scal[den]) x: rho(k) of a CG iterate follows its update x += a p
+__global__ void k_rho_axpy(int nk, const double *__restrict__ scal, int num, int den, const double2 *__restrict__ x,
+                           double2 *__restrict__ acc) {
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nk) return;
+    double a = scal[num] / scal[den];
+    double2 v = x[k], s = acc[k];
+    acc[k] = make_double2(s.x + a * v.x, s.y + a * v.y);
+}
+
+void launch_rho_axpy(Engine &e, int num_slot, int den_slot, const double2 *x, double2 *acc) {
+    MDFF_LAUNCH(e, k_rho_axpy, ceil_div(e.nk, 256), 256, 0, e.nk, e.d_scal, num_slot, den_slot, x, acc);
 }
 
 // ---------------------------------------------------------------- pass 2: per ion
@@ -427,8 +474,15 @@ void launch_rec(Engine &e, const double *q, const double3 *mu, bool lq, bool ld,
     int WT = (e.kmax[0] + 1) + (2 * e.kmax[1] + 1) + (2 * e.kmax[2] + 1);
     size_t smem = sizeof(double2) * RHO_TI * WT + sizeof(double) * RHO_TI * 4;
     int ps = -1;
-    if (!fp32) e.prof_begin("k_rho", &ps);
-    if (fp32) {
+    int nbr = ceil_div(e.nk, RHOR_K);
+    if (o.rho_acc) {   // rho(k) already known (linear in q and mu): no ion x k pass
+        MDFF_LAUNCH(e, k_rho_from_acc, nbr, 32, 0, e.nk, o.rho_acc, e.d_Ak, e.d_kcoe, e.d_kvec, e.d_rho, e.d_part,
+                    (int)S_REC_U, e.part_stride);
+        e.reduce(S_REC_U, 7, nbr);
+    }
+    if (!fp32 && !o.rho_acc) e.prof_begin("k_rho", &ps);
+    if (o.rho_acc) {
+    } else if (fp32) {
         launch_rho32(e, q, mu, lq, ld);
     } else if (lq && ld) {
         allow_smem(k_rho<true, true>, smem);
@@ -445,11 +499,12 @@ void launch_rec(Engine &e, const double *q, const double3 *mu, bool lq, bool ld,
     } else {
         MDFF_CK(cudaMemsetAsync(e.d_rho_part, 0, sizeof(double2) * (size_t)e.nk * e.rho_chunks, e.stream));
     }
-    if (!fp32) e.prof_end("k_rho", ps, (lq || ld) ? rho_flops_per_pair(lq, ld) * (double)e.n * e.nk : 0.0);
-    int nbr = ceil_div(e.nk, 256);
-    MDFF_LAUNCH(e, k_rho_reduce, nbr, 256, 0, e.nk, e.rho_chunks, e.d_rho_part, e.d_Ak, e.d_kcoe, e.d_kvec,
-                e.d_rho, e.d_part, (int)S_REC_U, e.part_stride);
-    e.reduce(S_REC_U, 7, nbr);
+    if (!o.rho_acc) {
+        if (!fp32) e.prof_end("k_rho", ps, (lq || ld) ? rho_flops_per_pair(lq, ld) * (double)e.n * e.nk : 0.0);
+        MDFF_LAUNCH(e, k_rho_reduce, nbr, 256, 0, e.nk, e.rho_chunks, e.d_rho_part, e.d_Ak, e.d_kcoe, e.d_kvec,
+                    e.d_rho, o.rho_raw, e.d_part, (int)S_REC_U, e.part_stride);
+        e.reduce(S_REC_U, 7, nbr);
+    }
 
     IonArgs a;
     a.n = e.n;

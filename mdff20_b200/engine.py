@@ -28,7 +28,7 @@ STATUS = {
     6: "ERR_STATE", 7: "ERR_NOMEM", 8: "ERR_CELL", 9: "ERR_TIMEOUT",
 }
 FP64, MIXED = 0, 1
-PIM_REFERENCE, PIM_CG = 0, 1
+PIM_REFERENCE, PIM_CG, PIM_CG_FUSED = 0, 1, 2
 ES_FLAGS = dict(lq=1, ld=2, ldamp=4, do_forces=8, do_stress=16, do_ef=32, do_efg=64, do_dir=128, do_rec=256)
 
 

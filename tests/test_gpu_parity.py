@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from mdff20_b200 import synth
-from mdff20_b200.engine import PIM_CG, Engine, MdffgpuError
+from mdff20_b200.engine import PIM_CG, PIM_CG_FUSED, Engine, MdffgpuError
 from oracle.oracle import Oracle, wrapped_positions
 from tests.golden import cases
 from tests.helpers import load_golden, rel_err
@@ -124,6 +124,37 @@ def test_cg_solver_converges_to_reference_fixed_point():
     assert rel_err(e.dipole_history()[:, 0, :], g["mu_ind"].reshape(-1, 3)) < 1e-8
     assert rel_err(e.forces(), g["f"].reshape(-1, 3)) < 1e-9
     assert abs(th["u_coul"] - float(g["u_coul"][0])) < 1e-8 * abs(float(g["u_coul"][0]))
+
+
+def test_fused_cg_matches_cg():
+    """PIM_CG_FUSED (one Ewald pass for E_stat + T mu0, rho(k) carried along the CG
+    iterates for the force pass) is the same CG: reference fixed point, and over MD
+    steps the same trajectory as PIM_CG to rounding."""
+    g = load_golden("silica450_pim")
+    s = cases.CASES["silica450_pim"]()
+    pos = g["r_in"].reshape(-1, 3)
+    e = Engine(s, positions=pos, pim_solver=PIM_CG_FUSED)
+    e.gen_verletlist()
+    e.engforce()
+    th = e.thermo()
+    assert th["scf_rmsd"] <= s.conv_tol_ind
+    assert rel_err(e.forces(), g["f"].reshape(-1, 3)) < 1e-9
+    assert abs(th["u_coul"] - float(g["u_coul"][0])) < 1e-8 * abs(float(g["u_coul"][0]))
+    assert abs(th["u_pol"] - float(g["u_pol"][0])) < 1e-8 * abs(float(g["u_pol"][0]))
+    g2 = load_golden("crist192_pim_nhc")
+    s2 = cases.CASES["crist192_pim_nhc"]()
+    s2.vel = g2["vel"].reshape(-1, 3)
+    p2 = g2["r_in"].reshape(-1, 3)
+    a = Engine(s2, positions=p2, pim_solver=PIM_CG)
+    b = Engine(s2, positions=p2, pim_solver=PIM_CG_FUSED)
+    for x in (a, b):
+        x.gen_verletlist()
+        x.engforce()
+    ta, tb = a.md_steps(1, 8), b.md_steps(1, 8)
+    # both stop at the SCF tolerance (1e-9): agreement to well below it
+    assert np.allclose(ta, tb, rtol=1e-8, atol=1e-8)
+    assert rel_err(b.forces(), a.forces()) < 1e-8
+    assert rel_err(b.state()[0], a.state()[0]) < 1e-12
 
 
 def test_random_systems_vs_oracle():
@@ -242,14 +273,15 @@ def test_mixed_precision_force_error_small(name):
 
 
 def test_mixed_precision_force_error_full_size():
-    """N=24000 PIM silica (the bench system): mixed vs FP64 engine, same solver."""
+    """N=24000 PIM silica (the bench system): mixed with the fused CG (the bench's
+    mixed configuration) vs the FP64 engine with the plain CG."""
     from mdff20_b200.engine import MIXED
     s = synth.config5()
     pos = wrapped_positions(s)
     ref = Engine(s, positions=pos, pim_solver=PIM_CG)
     ref.gen_verletlist()
     ref.engforce()
-    mix = Engine(s, positions=pos, pim_solver=PIM_CG, precision=MIXED)
+    mix = Engine(s, positions=pos, pim_solver=PIM_CG_FUSED, precision=MIXED)
     mix.gen_verletlist()
     mix.engforce()
     err = _rms_rel(mix.forces(), ref.forces())
