@@ -193,7 +193,7 @@ def run_ours(args):
         ref.gen_verletlist()
         ref.engforce()
         f64, f32 = ref.forces(), eng.forces()
-        force_err = float(np.sqrt(np.mean(np.sum((f32 - f64) ** 2, 1)) / np.mean(np.sum(f64 ** 2, 1))))
+        force_err = float(np.sqrt(np.mean(np.sum((f32 - f64) ** 2, 1))) / np.sqrt(np.mean(np.sum(f64 ** 2, 1))))
         ref.close()
     istep = 1
     if args.warmup > 0:

@@ -82,6 +82,12 @@ int mdffgpu_set_precision(mdffgpu_ctx *ctx, int precision) {
             throw Error(MDFFGPU_ERR_ARG, "mixed precision kernels are not built in this library");
         e.precision = precision;
         e.use32 = (precision == MDFFGPU_MIXED);
+        e.real32 = e.rec32 = e.subset32 = true;
+        if (const char *v = getenv("MDFFGPU_MIXED_PARTS")) {
+            e.real32 = strstr(v, "real") != nullptr;
+            e.rec32 = strstr(v, "rec") != nullptr;
+        }
+        if (const char *v = getenv("MDFFGPU_PIM_SUBSET")) e.subset32 = atoi(v) != 0;
     });
 }
 

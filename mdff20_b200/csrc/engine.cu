@@ -68,15 +68,6 @@ __global__ void k_sort_cells(int ncell, int cell_cap, const int *start, const in
                              const int *rebuild);
 
 template <typename T>
-static T *dalloc(size_t count) {
-    T *p = nullptr;
-    if (count == 0) count = 1;
-    cudaError_t e = cudaMalloc((void **)&p, sizeof(T) * count);
-    if (e != cudaSuccess) throw Error(MDFFGPU_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
-    cudaMemset(p, 0, sizeof(T) * count);
-    return p;
-}
-template <typename T>
 static void dfree(T *&p) {
     if (p) cudaFree(p);
     p = nullptr;
@@ -145,8 +136,6 @@ Engine::Engine(const mdffgpu_params &prm, int dev) : p(prm) {
     d_qzero = dalloc<double>(n);
     d_muzero = dalloc<double3>(n);
     d_svl = dalloc<double4>(n);
-    d_s32 = dalloc<float4>(n);
-    d_t32 = dalloc<float4>(n);
     d_rebuild = dalloc<int>(1);
     d_status = dalloc<unsigned>(1);
     d_scal = dalloc<double>(NSLOT);
@@ -202,11 +191,14 @@ Engine::~Engine() {
     cudaFree(d_rho);
     cudaFree(d_rho_acc);
     cudaFree(d_rho_it);
+    cudaFree(d_seg32);
+    cudaFree(d_tab32);
+    cudaFree(d_rho_part32);
+    cudaFree(d_ion_part32);
+    cudaFree(d_pidx);
     cudaFree(d_ion_part);
     cudaFree(d_coef);
-    cudaFree(d_coef32);
-    cudaFree(d_s32);
-    cudaFree(d_t32);
+    dfree32();
     cudaFree(d_out);
     cudaFree(d_status);
     if (h_out) cudaFreeHost(h_out);
@@ -316,7 +308,14 @@ void Engine::setup_types() {
         }
     }
     npol = 0;
-    for (int i = 0; i < n; i++) npol += polar[i];
+    std::vector<int> pidx;
+    for (int i = 0; i < n; i++)
+        if (polar[i]) pidx.push_back(i);
+    npol = (int)pidx.size();
+    if (npol) {
+        d_pidx = dalloc<int>(npol);
+        MDFF_CK(cudaMemcpy(d_pidx, pidx.data(), sizeof(int) * npol, cudaMemcpyHostToDevice));
+    }
     h_q = q;
     d_typ = dalloc<int>(n);
     d_mass = dalloc<double>(n);
@@ -518,6 +517,7 @@ void Engine::setup_kspace() {
     d_rho_acc = dalloc<double2>(nk);
     d_rho_it = dalloc<double2>(nk);
     d_ion_part = dalloc<double>((size_t)ntile * n * 12);
+    setup_kspace32(*this, rows);
 }
 
 void Engine::setup_cells() {
@@ -559,11 +559,7 @@ void Engine::alloc_lists(int cnb, int cco) {
     d_co = dalloc<int>((size_t)n * cap_co);
     d_con = dalloc<int>(n);
     dfree(d_coef);
-    dfree(d_coef32);
-    if (p.lcoulombic && lpol) {
-        d_coef = dalloc<double2>((size_t)n * cap_co);
-        d_coef32 = dalloc<float2>((size_t)n * cap_co);
-    }
+    if (p.lcoulombic && lpol) d_coef = dalloc<double2>((size_t)n * cap_co);
     list_ready = false;
     coef_ready = false;
 }
@@ -701,9 +697,10 @@ static double self2_of(double alpha) {
 void Engine::field_of(const double *d_qv, const double3 *d_muv, bool lq, bool ld, bool damp, double3 *d_ef_out,
                       double2 *rho_raw) {
     if (!lq && ld && !damp && coef_ready) {
-        if (use32) launch_dir_field_cached32(*this, d_muv, d_tmp3);
+        // induced dipoles: nonzero at polarisable ions only, field needed there only
+        if (use32 && real32) launch_pol_field32(*this, d_muv, d_tmp3);
         else launch_dir_field_cached(*this, d_muv, d_tmp3);
-    } else if (use32) {
+    } else if (use32 && real32) {
         launch_dir32(*this, d_qv, d_muv, p.alphaES, lq, ld, damp, false, true, d_tmp3, nullptr);
     } else {
         launch_dir(*this, d_qv, d_muv, p.alphaES, lq, ld, damp, false, true, false, false, d_tmp3, nullptr, nullptr);
@@ -715,6 +712,22 @@ void Engine::field_of(const double *d_qv, const double3 *d_muv, bool lq, bool ld
     o.self_mu = d_muv;
     o.rho_raw = rho_raw;
     launch_rec(*this, d_qv, d_muv, lq, ld, o);
+}
+
+// field of a CG search direction p, which vanishes off the polarisable ions: the
+// k-space passes run over those ions only and the field is written there only
+void Engine::field_pol(const double3 *d_p, double3 *d_out, double2 *rho_raw) {
+    if (real32) launch_pol_field32(*this, d_p, d_tmp3);
+    else launch_dir_field_cached(*this, d_p, d_tmp3);
+    RecOut o;
+    o.ef = d_out;
+    o.ef_dir = d_tmp3;
+    o.self2 = self2_of(p.alphaES);
+    o.self_mu = d_p;
+    o.rho_raw = rho_raw;
+    o.idx = d_pidx;
+    o.cnt = npol;
+    launch_rec(*this, d_qzero, d_p, false, true, o);
 }
 
 // momentpolaSCF (src/pim.c:177-306) with extrapolate_dipole_aspc (src/pim.c:314-424)
@@ -779,7 +792,7 @@ void Engine::pim_cg(bool fused) {
     if (fused) {
         MDFF_LAUNCH(*this, k_aspc_predict, nb, 256, 0, n, e, es, d_hist, d_mu_ind);
         MDFF_LAUNCH(*this, k_add3, nb, 256, 0, n, d_mu_static, d_mu_ind, d_mu_tot);
-        if (use32)
+        if (use32 && real32)
             launch_dir32(*this, d_q, d_mu_tot, p.alphaES, lqch != 0, true, ldmp != 0, false, true, d_tmp3, nullptr);
         else
             launch_dir(*this, d_q, d_mu_tot, p.alphaES, lqch != 0, true, ldmp != 0, false, true, false, false,
@@ -808,7 +821,8 @@ void Engine::pim_cg(bool fused) {
     int it = 0;
     int maxit = std::max(p.max_scf_pim_iter, 1);
     while (rmsd > p.conv_tol_ind && it < maxit) {
-        field_of(d_qzero, d_cg_p, false, true, false, d_ef_ind, fused ? d_rho_it : nullptr);   // T p
+        if (fused && use32 && rec32 && subset32 && npol > 0) field_pol(d_cg_p, d_ef_ind, d_rho_it);              // T p
+        else field_of(d_qzero, d_cg_p, false, true, false, d_ef_ind, fused ? d_rho_it : nullptr);
         MDFF_LAUNCH(*this, k_cg_ap, nb, 256, 0, n, d_polar, d_invpol, d_cg_p, d_ef_ind, d_cg_ap, d_part, part_stride);
         reduce(S_PAP, 1, nb);
         MDFF_LAUNCH(*this, k_copy_slot, 1, 1, 0, d_scal, (int)S_RZ, (int)S_RZOLD);
@@ -916,14 +930,16 @@ void Engine::pim_ko() {
 
 // get_dipoles (src/coulombic.c:67-130): mu = static + induced
 void Engine::get_dipoles() {
+    // mixed precision: in-cutoff list and dipole-field records of these positions (the
+    // real-space kernels of this force evaluation read them)
+    if (use32 && real32) launch_pair_prep32(*this);
     if (lpol) {
         // positions are fixed through the solve: cache the dipole-field pair factors
         struct CoefScope {
             bool &flag;
             ~CoefScope() { flag = false; }
         } scope{coef_ready};
-        if (use32) launch_dir_prep32(*this, p.alphaES);
-        else launch_dir_prep(*this, p.alphaES);
+        if (!(use32 && real32)) launch_dir_prep(*this, p.alphaES);
         coef_ready = true;
         if (pim_solver == MDFFGPU_PIM_CG || pim_solver == MDFFGPU_PIM_CG_FUSED)
             pim_cg(pim_solver == MDFFGPU_PIM_CG_FUSED);
@@ -961,7 +977,7 @@ void Engine::engforce() {
         get_dipoles();
         bool ld = (ldip || lpol);
         // direct space: forces, energy, virial (do_forces, do_stress; src/field.c:381-383)
-        if (use32)
+        if (use32 && real32)
             launch_dir32(*this, d_q, d_mu_tot, p.alphaES, lqch != 0, ld, ldmp != 0, true, false, nullptr, d_tmp3);
         else
             launch_dir(*this, d_q, d_mu_tot, p.alphaES, lqch != 0, ld, ldmp != 0, true, false, false, false,
@@ -990,6 +1006,7 @@ void Engine::multipole_es_dev(const double *d_qv, const double3 *d_muv, double a
     bool efg = flags & MDFFGPU_ES_EFG, dir = flags & MDFFGPU_ES_DIR, rec = flags & MDFFGPU_ES_REC;
     ensure_lists();
     launch_kardir(*this, d_r, d_s);
+    if (use32) launch_coords32(*this);
     int nb = ceil_div(n, 256);
     double self2 = self2_of(alpha);
     // efg_dir accumulates the charge part when do_efg and the dipole part when do_efg

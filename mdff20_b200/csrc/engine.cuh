@@ -64,6 +64,21 @@ struct DevScalars {
 
 struct Engine;
 
+// zero-initialised device allocation; MDFFGPU_ERR_NOMEM on failure.  The zeroing runs on
+// the legacy stream, which the engine's non-blocking stream does not wait for, so it is
+// completed here before the buffer is handed out.
+template <typename T>
+inline T *dalloc(size_t count) {
+    T *p = nullptr;
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc((void **)&p, sizeof(T) * count);
+    if (e != cudaSuccess) throw Error(MDFFGPU_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    e = cudaMemset(p, 0, sizeof(T) * count);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+    if (e != cudaSuccess) throw Error(MDFFGPU_ERR_CUDA, std::string("cudaMemset: ") + cudaGetErrorString(e));
+    return p;
+}
+
 // ---------------------------------------------------------------- launchers
 // lists.cu
 void launch_kardir(Engine &e, const double4 *r, double4 *s);
@@ -94,6 +109,8 @@ struct RecOut {
     const double *efg_dir = nullptr;
     double2 *rho_raw = nullptr;       // receives rho(k) of (q, mu) when set
     const double2 *rho_acc = nullptr; // rho(k) of (q, mu) given: the rho pass is skipped
+    const int *idx = nullptr;         // mixed precision: only these ions (q, mu zero elsewhere;
+    int cnt = -1;                     // outputs written at these ions only), cnt of them
 };
 void launch_rec(Engine &e, const double *q, const double3 *mu, bool lq, bool ld, const RecOut &o);
 // acc += (scal[num_slot] / scal[den_slot]) x over the k-vectors
@@ -102,12 +119,21 @@ void launch_rho_axpy(Engine &e, int num_slot, int den_slot, const double2 *x, do
 void launch_reduce_slots(Engine &e, int first_slot, int nslots, int nparts);
 // true once the FP32 pair/k-space kernels exist in this build
 inline bool mixed_available() { return true; }
-// mixed.cu: FP32 coordinates, real-space and cached-field kernels
-void launch_coords32(Engine &e);
+// real32.cu: mixed-precision real space.  launch_pair_prep32 once per force evaluation
+// (in-cutoff list and dipole-field records); launch_dir32 as launch_dir (charges from
+// the fractional coordinates' w); launch_pol_field32: T mu at the polarisable ions from
+// the dipole-field records (zero at the others)
+void launch_pair_prep32(Engine &e);
 void launch_dir32(Engine &e, const double *q, const double3 *mu, double alpha, bool lq, bool ld, bool damp,
                   bool forces, bool ef, double3 *out_ef, double3 *out_f);
-void launch_dir_prep32(Engine &e, double alpha);
-void launch_dir_field_cached32(Engine &e, const double3 *mu, double3 *out_ef);
+void launch_pol_field32(Engine &e, const double3 *p, double3 *out_ef);
+// kspace32.cu: per force evaluation, the phase tables of the current positions
+void launch_coords32(Engine &e);
+// kspace32.cu: FP32 phase tables and k-space passes (idx: optional ion subset of cnt ions)
+void setup_kspace32(Engine &e, const std::vector<KRow> &rows);
+void launch_phase32(Engine &e);
+void launch_rho32(Engine &e, const double *q, const double3 *mu, bool lq, bool ld, const int *idx, int cnt);
+void launch_ion32(Engine &e, const double *q, const double3 *mu, bool ld, const RecOut &o, const int *idx, int cnt);
 
 // ---------------------------------------------------------------- engine state
 struct Engine {
@@ -158,9 +184,16 @@ struct Engine {
     int cap_nb = 0, cap_co = 0;
     int *d_nb = nullptr, *d_nbn = nullptr, *d_co = nullptr, *d_con = nullptr;
     double2 *d_coef = nullptr;   // [n][cap_co] cached dipole-field pair factors
-    float2 *d_coef32 = nullptr;  // same, mixed precision
-    float4 *d_s32 = nullptr, *d_t32 = nullptr;   // wrapped fractional / phase coordinates, FP32
     bool use32 = false;          // mixed precision: FP32 Ewald kernels
+    // parts of the mixed path (all on by default; MDFFGPU_MIXED_PARTS=real|rec keeps
+    // only that part in FP32, MDFFGPU_PIM_SUBSET=0 runs the CG field over all ions)
+    bool real32 = true, rec32 = true, subset32 = true;
+    // mixed-precision real space (real32.cu), sized like the Coulomb list
+    int *d_nl32 = nullptr, *d_nln32 = nullptr;   // in-cutoff neighbours [n][cap32]
+    int *d_pl32 = nullptr, *d_pln32 = nullptr;   // polarisable neighbours of polarisable ions
+    float4 *d_pu32 = nullptr;                    // their dipole-field records (u, c1)
+    float4 *d_qm32 = nullptr;                    // per-ion dipole (FP32), w = type
+    int cap32 = 0;
     bool coef_ready = false;     // d_coef matches the current positions
     double4 *d_svl = nullptr;    // fractional positions at the last build
     int nc[3] = {1, 1, 1}, ncell = 1, cell_cap = 4096;
@@ -181,6 +214,15 @@ struct Engine {
     int ntile = 0, tile_kmax = 0;
     double2 *d_rho_part = nullptr, *d_rho = nullptr;   // partial per ion chunk, total (Ak-scaled)
     double2 *d_rho_acc = nullptr, *d_rho_it = nullptr; // rho(k) of (q, mu) along the fused CG; of its p
+    // mixed precision k space (kspace32.cu)
+    KSeg *d_seg32 = nullptr;                            // (row, z block) segments, pad0 = block
+    int nseg32 = 0, tab_w = 0;
+    float2 *d_tab32 = nullptr;                          // phase table rows [n][tab_w]
+    int rho32_chunks = 0;
+    float2 *d_rho_part32 = nullptr;                     // [rho32_chunks][nk]
+    int ion32_rows = 0, ion32_slices = 0;
+    double *d_ion_part32 = nullptr;                     // [slices][n][6]
+    int *d_pidx = nullptr;                              // polarisable ions, ascending
     bool rho_acc_ready = false;                         // d_rho_acc holds rho(k) of (q, mu_tot)
     double *d_ion_part = nullptr;                       // ion-pass partial sums [ntile][n][12]
     int rho_chunks = 0, rho_chunk = 0;
@@ -236,6 +278,9 @@ struct Engine {
                           double *d_efg_out, double3 *d_f_out);
     void field_of(const double *d_qv, const double3 *d_muv, bool lq, bool ld, bool damp, double3 *d_ef_out,
                   double2 *rho_raw = nullptr);
+    void field_pol(const double3 *d_p, double3 *d_out, double2 *rho_raw);
+    void ensure_real32();
+    void dfree32();
     void get_dipoles();
     void pim_reference();
     void pim_cg(bool fused);

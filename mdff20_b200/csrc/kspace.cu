@@ -174,8 +174,10 @@ __device__ __forceinline__ void rho_finish(int k, int nk, double2 rho, const dou
 
 // sum the ion-chunk partials of rho(k) in a fixed order, then rho_finish. A block owns
 // RHOR_K consecutive k (one per lane); its 8 warps take every 8th chunk and warp 0 adds
-// the 8 warp sums in warp order. rho_raw (optional) receives rho(k) itself.
-__global__ void __launch_bounds__(256) k_rho_reduce(int nk, int nchunks, const double2 *__restrict__ part,
+// the 8 warp sums in warp order. rho_raw (optional) receives rho(k) itself.  Partials
+// are FP64 (kspace.cu) or FP32 (kspace32.cu: sums over one chunk of ions), added in FP64.
+template <typename PT>
+__global__ void __launch_bounds__(256) k_rho_reduce(int nk, int nchunks, const PT *__restrict__ part,
                                                     const double *__restrict__ Ak, const double *__restrict__ kcoe,
                                                     const double3 *__restrict__ kv, double2 *__restrict__ rho_s,
                                                     double2 *__restrict__ rho_raw, double *__restrict__ ppart,
@@ -186,9 +188,9 @@ __global__ void __launch_bounds__(256) k_rho_reduce(int nk, int nchunks, const d
     double2 acc = make_double2(0.0, 0.0);
     if (k < nk)
         for (int c = w; c < nchunks; c += 8) {
-            double2 p = part[(size_t)c * nk + k];
-            acc.x += p.x;
-            acc.y += p.y;
+            PT p = part[(size_t)c * nk + k];
+            acc.x += (double)p.x;
+            acc.y += (double)p.y;
         }
     ws[w][l] = acc;
     __syncthreads();
@@ -463,12 +465,30 @@ static void allow_smem(K kernel, size_t bytes) {
 //   o.ef  = self2*mu + o.ef_dir + E_rec          (when o.ef)
 //   o.f   = o.f + o.f_dir*coul + F_rec*coul      (when o.f)
 //   o.efg = self + o.efg_dir + EFG_rec (upper)   (when o.efg)
-void launch_rho32(Engine &e, const double *q, const double3 *mu, bool lq, bool ld);
-void launch_ion32(Engine &e, const double3 *mu, bool ld, bool want_f);
+// mixed precision: kspace32.cu passes, FP64 reduction of the FP32 chunk partials
+static void launch_rec32(Engine &e, const double *q, const double3 *mu, bool lq, bool ld, const RecOut &o) {
+    int nbr = ceil_div(e.nk, RHOR_K);
+    int cnt = o.idx ? o.cnt : e.n;
+    if (o.rho_acc) {
+        MDFF_LAUNCH(e, k_rho_from_acc, nbr, 32, 0, e.nk, o.rho_acc, e.d_Ak, e.d_kcoe, e.d_kvec, e.d_rho, e.d_part,
+                    (int)S_REC_U, e.part_stride);
+    } else {
+        launch_rho32(e, q, mu, lq, ld, o.idx, cnt);
+        MDFF_LAUNCH(e, k_rho_reduce<float2>, nbr, 256, 0, e.nk, e.rho32_chunks, e.d_rho_part32, e.d_Ak, e.d_kcoe,
+                    e.d_kvec, e.d_rho, o.rho_raw, e.d_part, (int)S_REC_U, e.part_stride);
+    }
+    e.reduce(S_REC_U, 7, nbr);
+    if (!o.ef && !o.f) return;
+    launch_ion32(e, lq ? q : nullptr, mu, ld, o, o.idx, cnt);
+}
 
 void launch_rec(Engine &e, const double *q, const double3 *mu, bool lq, bool ld, const RecOut &o) {
     // FP32 passes in mixed precision (no FP32 EFG: EFG requests run in FP64)
-    bool fp32 = e.use32 && o.efg == nullptr;
+    if (e.use32 && e.rec32 && o.efg == nullptr) {
+        launch_rec32(e, q, mu, lq, ld, o);
+        return;
+    }
+    if (o.idx) throw Error(MDFFGPU_ERR_STATE, "ion subsets are a mixed-precision k-space feature");
     int segblocks = ceil_div(e.nseg, RHO_THREADS);
     dim3 grid(segblocks, e.rho_chunks);
     int WT = (e.kmax[0] + 1) + (2 * e.kmax[1] + 1) + (2 * e.kmax[2] + 1);
@@ -480,10 +500,8 @@ void launch_rec(Engine &e, const double *q, const double3 *mu, bool lq, bool ld,
                     (int)S_REC_U, e.part_stride);
         e.reduce(S_REC_U, 7, nbr);
     }
-    if (!fp32 && !o.rho_acc) e.prof_begin("k_rho", &ps);
+    if (!o.rho_acc) e.prof_begin("k_rho", &ps);
     if (o.rho_acc) {
-    } else if (fp32) {
-        launch_rho32(e, q, mu, lq, ld);
     } else if (lq && ld) {
         allow_smem(k_rho<true, true>, smem);
         MDFF_LAUNCH(e, (k_rho<true, true>), grid, RHO_THREADS, smem, e.n, e.rho_chunk, e.cell, e.kmax[0], e.kmax[1],
@@ -500,8 +518,8 @@ void launch_rec(Engine &e, const double *q, const double3 *mu, bool lq, bool ld,
         MDFF_CK(cudaMemsetAsync(e.d_rho_part, 0, sizeof(double2) * (size_t)e.nk * e.rho_chunks, e.stream));
     }
     if (!o.rho_acc) {
-        if (!fp32) e.prof_end("k_rho", ps, (lq || ld) ? rho_flops_per_pair(lq, ld) * (double)e.n * e.nk : 0.0);
-        MDFF_LAUNCH(e, k_rho_reduce, nbr, 256, 0, e.nk, e.rho_chunks, e.d_rho_part, e.d_Ak, e.d_kcoe, e.d_kvec,
+        e.prof_end("k_rho", ps, (lq || ld) ? rho_flops_per_pair(lq, ld) * (double)e.n * e.nk : 0.0);
+        MDFF_LAUNCH(e, k_rho_reduce<double2>, nbr, 256, 0, e.nk, e.rho_chunks, e.d_rho_part, e.d_Ak, e.d_kcoe, e.d_kvec,
                     e.d_rho, o.rho_raw, e.d_part, (int)S_REC_U, e.part_stride);
         e.reduce(S_REC_U, 7, nbr);
     }
@@ -541,18 +559,14 @@ void launch_rec(Engine &e, const double *q, const double3 *mu, bool lq, bool ld,
     dim3 g2(ceil_div(e.n, ION_THREADS), e.ntile);
     int nb = ceil_div(e.n, 256);
     int pi = -1;
-    if (fp32) {
-        launch_ion32(e, mu, ld, a.want_f);
-    } else {
-        e.prof_begin("k_rec_ion", &pi);
-        if (a.want_efg)
-            MDFF_LAUNCH(e, (k_rec_ion<true, true>), g2, ION_THREADS, smem2, a);
-        else if (a.want_f)
-            MDFF_LAUNCH(e, (k_rec_ion<true, false>), g2, ION_THREADS, smem2, a);
-        else
-            MDFF_LAUNCH(e, (k_rec_ion<false, false>), g2, ION_THREADS, smem2, a);
-        e.prof_end("k_rec_ion", pi, ion_flops_per_pair(a.want_f || a.want_efg, a.want_efg) * (double)e.n * e.nk);
-    }
+    e.prof_begin("k_rec_ion", &pi);
+    if (a.want_efg)
+        MDFF_LAUNCH(e, (k_rec_ion<true, true>), g2, ION_THREADS, smem2, a);
+    else if (a.want_f)
+        MDFF_LAUNCH(e, (k_rec_ion<true, false>), g2, ION_THREADS, smem2, a);
+    else
+        MDFF_LAUNCH(e, (k_rec_ion<false, false>), g2, ION_THREADS, smem2, a);
+    e.prof_end("k_rec_ion", pi, ion_flops_per_pair(a.want_f || a.want_efg, a.want_efg) * (double)e.n * e.nk);
     if (a.want_efg)
         MDFF_LAUNCH(e, (k_rec_combine<true, true>), nb, 256, 0, a);
     else if (a.want_f)

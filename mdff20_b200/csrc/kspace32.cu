@@ -1,0 +1,508 @@
+// Reciprocal-space Ewald sum in mixed precision (MDFFGPU_MIXED): the sums of kspace.cu
+// with FP32 arithmetic per (ion, k) and FP64 wherever a sum spans many terms.
+//
+// Phase tables.  With k = 2 pi B n the phase of ion i factorises into
+// E0[nx] E1[ny] E2[nz], E_d[m] = exp(2 pi i m t_d), t = B^T r (kspace.cu).  k_phase32
+// writes, once per force evaluation (positions are fixed through the induced-dipole
+// solve), one row of FP32 complex values per ion:
+//     [ E0[0..K0] | E1[-K1..K1] | pad | Z blocks of ZB values of E2 ]
+// every entry from its own FP64-reduced argument m t_d - rint(m t_d) (no recurrence,
+// so each value carries one rounding).  The z range of a k-row is cut into blocks of
+// ZB consecutive nz (negative half -K2..0 and positive half 1..K2 separately, zero
+// padded), so that a thread owns one block of one row and reads it with 16-byte loads.
+//
+// k_rho32   : rho(k) = sum_i (q_i + i k.mu_i) E0 E1 E2.  Thread = one (row, z block)
+//             segment, ions stream through shared memory in tiles of table rows; the
+//             summand (B1' + j B2) E2[z0 + j] costs 6 FMA (4 without dipoles), j an
+//             unrolled constant.  FP32 sums over one block's ion chunk, chunk partials
+//             summed in FP64 in a fixed order (k_rho_reduce32).
+// k_ion32   : per ion and k-slice the n-space sums of field (and force) terms.  Thread
+//             = ion; Ak rho(k) of the slice sits in shared memory as (rho_z, rho_-z)
+//             pairs; per row the phase base exp(2 pi i (nx tx + ny ty)) is reduced in
+//             FP64, E2[z] (z = 1..KZ) sits in registers, and the phases of +z and -z come
+//             from one product each (6 ops per pair of k).  Row sums FP32, rows FP64.
+// Both passes take an optional ion index list (the polarisable ions of an induced-
+// dipole iteration, whose search directions vanish elsewhere).
+#include "engine.cuh"
+
+namespace mdffgpu {
+
+constexpr int ZB = 16;              // nz per segment block (two complex per 16-byte load)
+constexpr int RHO32_THREADS = 128;
+constexpr int RHO32_TI = 32;        // ions per shared-memory tile
+constexpr int RHO32_MIN_BLOCKS = 8;
+constexpr int ION32_THREADS = 128;
+constexpr int ION32_MIN_BLOCKS = 6;
+
+__device__ __forceinline__ float2 cmul32(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// exp(2 pi i x) for an FP64 argument: exact reduction to [-1/2, 1/2], FP32 sincospi
+__device__ __forceinline__ float2 cis2pi32(double x) {
+    x -= rint(x);
+    float sn, cs;
+    sincospif((float)(2.0 * x), &sn, &cs);
+    return make_float2(cs, sn);
+}
+
+// ---------------------------------------------------------------- phase tables
+struct TabLayout {
+    int K0, K1, K2, nzb_neg, nzb, e1, z, w;   // offsets in float2 units
+};
+
+// one thread per (ion, table entry)
+__global__ void k_phase32(int n, Cell c, const double4 *__restrict__ r, TabLayout L, float2 *__restrict__ tab) {
+    long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= (long long)n * L.w) return;
+    int i = (int)(g / L.w), e = (int)(g - (long long)i * L.w);
+    int d = -1, m = 0;
+    if (e < L.K0 + 1) {
+        d = 0;
+        m = e;
+    } else if (e < L.e1 + 2 * L.K1 + 1) {
+        d = 1;
+        m = e - L.e1 - L.K1;
+    } else if (e >= L.z) {
+        int b = (e - L.z) / ZB, j = (e - L.z) - b * ZB;
+        if (b < L.nzb_neg) {
+            m = -L.K2 + ZB * b + j;
+            if (m <= 0) d = 2;
+        } else {
+            m = 1 + ZB * (b - L.nzb_neg) + j;
+            if (m <= L.K2) d = 2;
+        }
+    }
+    float2 v = make_float2(0.f, 0.f);
+    if (d >= 0) {
+        double4 ri = r[i];
+        double t = c.B[0][d] * ri.x + c.B[1][d] * ri.y + c.B[2][d] * ri.z;
+        v = cis2pi32((double)m * t);
+    }
+    tab[g] = v;
+}
+
+// ---------------------------------------------------------------- pass 1: rho(k)
+template <bool LQ, bool LD>
+__global__ void __launch_bounds__(RHO32_THREADS, RHO32_MIN_BLOCKS)
+    k_rho32(int cnt, const int *__restrict__ idx, int chunk, TabLayout L, const float2 *__restrict__ tab,
+            Cell c, const double *__restrict__ q, const double3 *__restrict__ mu, int nseg,
+            const KSeg *__restrict__ seg, float2 *__restrict__ part, int nk) {
+    extern __shared__ float4 sm4[];
+    float2 *T = (float2 *)sm4;                          // [RHO32_TI][L.w]
+    float4 *QM = sm4 + RHO32_TI * (L.w / 2);            // [RHO32_TI] (q, 2 pi m)
+    const int hw = L.w / 2;
+    int sid = blockIdx.x * RHO32_THREADS + threadIdx.x;
+    KSeg S;
+    if (sid < nseg) S = seg[sid];
+    else S.nx = S.ny = S.z0 = S.cnt = S.koff = S.pad0 = 0;
+    const float fnx = (float)S.nx, fny = (float)S.ny, fz0 = (float)S.z0;
+    const int o0 = S.nx, o1 = L.e1 + L.K1 + S.ny, oz = (L.z + ZB * S.pad0) / 2;
+    float2 acc[ZB];
+#pragma unroll
+    for (int z = 0; z < ZB; z++) acc[z] = make_float2(0.f, 0.f);
+    int a0 = blockIdx.y * chunk, a1 = min(cnt, a0 + chunk);
+    int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const double tpi = TPI_D;
+    for (int t0 = a0; t0 < a1; t0 += RHO32_TI) {
+        int nt = min(RHO32_TI, a1 - t0);
+        // table rows: warp w copies rows w, w+4, ...
+        for (int a = w; a < nt; a += RHO32_THREADS / 32) {
+            int ion = idx ? idx[t0 + a] : t0 + a;
+            const float4 *src = (const float4 *)(tab + (size_t)ion * L.w);
+            for (int j = lane; j < hw; j += 32) sm4[a * hw + j] = src[j];
+        }
+        if (threadIdx.x < nt) {
+            int ion = idx ? idx[t0 + threadIdx.x] : t0 + threadIdx.x;
+            float4 v = make_float4(LQ ? (float)q[ion] : 0.f, 0.f, 0.f, 0.f);
+            if (LD) {
+                double3 m3 = mu[ion];
+                v.y = (float)(tpi * (c.B[0][0] * m3.x + c.B[1][0] * m3.y + c.B[2][0] * m3.z));
+                v.z = (float)(tpi * (c.B[0][1] * m3.x + c.B[1][1] * m3.y + c.B[2][1] * m3.z));
+                v.w = (float)(tpi * (c.B[0][2] * m3.x + c.B[1][2] * m3.y + c.B[2][2] * m3.z));
+            }
+            QM[threadIdx.x] = v;
+        }
+        __syncthreads();
+        if (sid < nseg) {
+            for (int a = 0; a < nt; a++) {
+                const float2 *R = T + a * L.w;
+                float2 b = cmul32(R[o0], R[o1]);
+                float4 qm = QM[a];
+                const float4 *Z = sm4 + a * hw + oz;
+                if (LD) {
+                    // k.mu = c0 + nz c1; B1 = (q + i c0) b, B2 = i c1 b, summand (B1 + nz B2) E2
+                    float c0 = fnx * qm.y + fny * qm.z, c1 = qm.w;
+                    float2 B1 = make_float2(qm.x * b.x - c0 * b.y, qm.x * b.y + c0 * b.x);
+                    float2 B2 = make_float2(-c1 * b.y, c1 * b.x);
+                    B1.x += fz0 * B2.x;
+                    B1.y += fz0 * B2.y;
+#pragma unroll
+                    for (int h = 0; h < ZB / 2; h++) {
+                        float4 ee = Z[h];
+                        float2 C0 = make_float2(B1.x + (float)(2 * h) * B2.x, B1.y + (float)(2 * h) * B2.y);
+                        float2 C1 = make_float2(B1.x + (float)(2 * h + 1) * B2.x, B1.y + (float)(2 * h + 1) * B2.y);
+                        acc[2 * h].x += C0.x * ee.x - C0.y * ee.y;
+                        acc[2 * h].y += C0.x * ee.y + C0.y * ee.x;
+                        acc[2 * h + 1].x += C1.x * ee.z - C1.y * ee.w;
+                        acc[2 * h + 1].y += C1.x * ee.w + C1.y * ee.z;
+                    }
+                } else {
+                    float2 C = make_float2(qm.x * b.x, qm.x * b.y);
+#pragma unroll
+                    for (int h = 0; h < ZB / 2; h++) {
+                        float4 ee = Z[h];
+                        acc[2 * h].x += C.x * ee.x - C.y * ee.y;
+                        acc[2 * h].y += C.x * ee.y + C.y * ee.x;
+                        acc[2 * h + 1].x += C.x * ee.z - C.y * ee.w;
+                        acc[2 * h + 1].y += C.x * ee.w + C.y * ee.z;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (sid < nseg) {
+        float2 *P = part + (size_t)blockIdx.y * nk + S.koff;
+#pragma unroll
+        for (int z = 0; z < ZB; z++)
+            if (z < S.cnt) P[z] = acc[z];
+    }
+}
+
+// ---------------------------------------------------------------- pass 2: per ion
+struct Ion32Args {
+    int cnt, nrow, rows_per_slice, nk;
+    const int *idx;
+    Cell c;
+    const double4 *r;
+    const double3 *mu;
+    const KRow *row;
+    const double2 *rho_s;
+    double *part;          // [slice][cnt][nv]
+    int ld;
+};
+
+template <int KZ, bool WF>
+__global__ void __launch_bounds__(ION32_THREADS, ION32_MIN_BLOCKS) k_ion32(Ion32Args a) {
+    extern __shared__ float4 rk4[];          // [rows of the slice][KZ + 1]: (rho_z, rho_-z)
+    int li = blockIdx.x * ION32_THREADS + threadIdx.x;
+    int sl = blockIdx.y;
+    int r0 = sl * a.rows_per_slice, r1 = min(a.nrow, r0 + a.rows_per_slice);
+    // Ak rho(k) of the slice's rows, padded to z = -KZ..KZ
+    int nrs = r1 - r0;
+    for (int e = threadIdx.x; e < nrs * (KZ + 1); e += ION32_THREADS) {
+        int rr = e / (KZ + 1), zz = e - rr * (KZ + 1);
+        KRow R = a.row[r0 + rr];
+        int zlo = R.z0, zhi = R.z0 + R.cnt - 1;
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (zz >= zlo && zz <= zhi) {
+            double2 p = a.rho_s[R.koff + zz - zlo];
+            v.x = (float)p.x;
+            v.y = (float)p.y;
+        }
+        if (zz > 0 && -zz >= zlo && -zz <= zhi) {
+            double2 p = a.rho_s[R.koff - zz - zlo];
+            v.z = (float)p.x;
+            v.w = (float)p.y;
+        }
+        rk4[e] = v;
+    }
+    bool act = li < a.cnt;
+    int ion = act ? (a.idx ? a.idx[li] : li) : 0;
+    double4 ri = a.r[ion];
+    const Cell &c = a.c;
+    double tx = c.B[0][0] * ri.x + c.B[1][0] * ri.y + c.B[2][0] * ri.z;
+    double ty = c.B[0][1] * ri.x + c.B[1][1] * ri.y + c.B[2][1] * ri.z;
+    double tz = c.B[0][2] * ri.x + c.B[1][2] * ri.y + c.B[2][2] * ri.z;
+    float2 E[KZ];
+#pragma unroll
+    for (int z = 0; z < KZ; z++) E[z] = cis2pi32((double)(z + 1) * tz);
+    float mz = 0.f;
+    double mx = 0.0, my = 0.0;
+    if (WF && a.ld) {
+        double3 m3 = a.mu[ion];
+        mx = c.B[0][0] * m3.x + c.B[1][0] * m3.y + c.B[2][0] * m3.z;
+        my = c.B[0][1] * m3.x + c.B[1][1] * m3.y + c.B[2][1] * m3.z;
+        mz = (float)(c.B[0][2] * m3.x + c.B[1][2] * m3.y + c.B[2][2] * m3.z);
+    }
+    __syncthreads();
+    double S0 = 0, S1 = 0, S2 = 0, P0 = 0, P1 = 0, P2 = 0;
+    for (int rr = 0; rr < nrs; rr++) {
+        KRow R = a.row[r0 + rr];
+        float2 w = cis2pi32((double)R.nx * tx + (double)R.ny * ty);
+        const float4 *rho = rk4 + rr * (KZ + 1);
+        float4 r00 = rho[0];
+        // z = 0: phase w
+        float R1 = r00.y * w.x - r00.x * w.y, Rz = 0.f;
+        float Q0 = 0.f, Q1 = 0.f, Q2 = 0.f;
+        if (WF) Q0 = r00.x * w.x + r00.y * w.y;
+#pragma unroll
+        for (int z = 1; z <= KZ; z++) {
+            float4 rp = rho[z];
+            float2 e = E[z - 1];
+            // w e = (p, s), w conj(e) = (p', s')
+            float u1 = w.y * e.y, u2 = w.y * e.x;
+            float p = w.x * e.x - u1, pp = w.x * e.x + u1;
+            float s = w.x * e.y + u2, sp = u2 - w.x * e.y;
+            // rho.y ph.x - rho.x ph.y (the sign convention of k_rec_ion) for +z and -z
+            float xp = rp.y * p - rp.x * s, xm = rp.w * pp - rp.z * sp;
+            R1 += xp + xm;
+            Rz += (float)z * (xp - xm);
+            if (WF) {
+                float cp = rp.x * p + rp.y * s, cm = rp.z * pp + rp.w * sp;
+                Q0 += cp + cm;
+                Q1 += (float)z * (cp - cm);
+                Q2 += (float)(z * z) * (cp + cm);
+            }
+        }
+        double fx = (double)R.nx, fy = (double)R.ny;
+        S0 += fx * (double)R1;
+        S1 += fy * (double)R1;
+        S2 += (double)Rz;
+        if (WF) {
+            // sum_k (n.m) Re(conj(rho) ph) per component weight n: c0 = nx mx + ny my
+            double c0 = fx * mx + fy * my;
+            double T1 = c0 * (double)Q0 + (double)mz * (double)Q1;
+            double Tz = c0 * (double)Q1 + (double)mz * (double)Q2;
+            P0 += fx * T1;
+            P1 += fy * T1;
+            P2 += Tz;
+        }
+    }
+    if (!act) return;
+    const int nv = WF ? 6 : 3;
+    double *o = a.part + ((size_t)sl * a.cnt + li) * nv;
+    o[0] = S0;
+    o[1] = S1;
+    o[2] = S2;
+    if (WF) {
+        o[3] = P0;
+        o[4] = P1;
+        o[5] = P2;
+    }
+}
+
+// slices summed in a fixed order; field / force / self terms as k_rec_combine (kspace.cu)
+struct Comb32Args {
+    int cnt, nslice;
+    const int *idx;
+    Cell c;
+    const double *part;
+    double tfpiV, self2, coul;
+    int ld;
+    const double *q;
+    const double3 *muself;
+    const double3 *ef_dir;
+    double3 *ef;
+    const double3 *f_dir;
+    double3 *f;
+};
+
+template <bool WF>
+__global__ void k_combine32(Comb32Args a) {
+    int li = blockIdx.x * blockDim.x + threadIdx.x;
+    if (li >= a.cnt) return;
+    int i = a.idx ? a.idx[li] : li;
+    const int nv = WF ? 6 : 3;
+    double S[3] = {0, 0, 0}, P[3] = {0, 0, 0};
+    for (int s = 0; s < a.nslice; s++) {
+        const double *o = a.part + ((size_t)s * a.cnt + li) * nv;
+        for (int k = 0; k < 3; k++) S[k] += o[k];
+        if (WF)
+            for (int k = 0; k < 3; k++) P[k] += o[3 + k];
+    }
+    const Cell &c = a.c;
+    const double tpi = TPI_D;
+    double gS[3], gP[3];
+    for (int k = 0; k < 3; k++) {
+        gS[k] = tpi * (c.B[k][0] * S[0] + c.B[k][1] * S[1] + c.B[k][2] * S[2]);
+        gP[k] = tpi * tpi * (c.B[k][0] * P[0] + c.B[k][1] * P[1] + c.B[k][2] * P[2]);
+    }
+    if (a.ef) {
+        double3 mu = a.muself ? a.muself[i] : make_double3(0, 0, 0);
+        double3 b = make_double3(a.self2 * mu.x, a.self2 * mu.y, a.self2 * mu.z);
+        if (a.ef_dir) {
+            double3 d = a.ef_dir[i];
+            b.x += d.x;
+            b.y += d.y;
+            b.z += d.z;
+        }
+        a.ef[i] = make_double3(b.x + (-a.tfpiV * gS[0]), b.y + (-a.tfpiV * gS[1]), b.z + (-a.tfpiV * gS[2]));
+    }
+    if (WF && a.f) {
+        double qi = a.q ? a.q[i] : 0.0;
+        double3 fo = a.f[i];
+        if (a.f_dir) {
+            double3 d = a.f_dir[i];
+            fo.x += d.x * a.coul;
+            fo.y += d.y * a.coul;
+            fo.z += d.z * a.coul;
+        }
+        double fr[3];
+        for (int k = 0; k < 3; k++) fr[k] = a.tfpiV * (-qi * gS[k] + (a.ld ? gP[k] : 0.0));
+        a.f[i] = make_double3(fo.x + fr[0] * a.coul, fo.y + fr[1] * a.coul, fo.z + fr[2] * a.coul);
+    }
+}
+
+// ---------------------------------------------------------------- set-up and launchers
+static TabLayout layout_of(const Engine &e) {
+    TabLayout L;
+    L.K0 = e.kmax[0];
+    L.K1 = e.kmax[1];
+    L.K2 = e.kmax[2];
+    L.nzb_neg = ceil_div(L.K2 + 1, ZB);
+    L.nzb = L.nzb_neg + ceil_div(L.K2, ZB);
+    L.e1 = L.K0 + 1;
+    L.z = L.e1 + 2 * L.K1 + 1;
+    L.z += L.z & 1;
+    L.w = L.z + ZB * L.nzb;
+    return L;
+}
+
+static int kz_of(int K2) { return K2 <= 8 ? 8 : (K2 <= 14 ? 14 : (K2 <= 16 ? 16 : 32)); }
+
+void setup_kspace32(Engine &e, const std::vector<KRow> &rows) {
+    TabLayout L = layout_of(e);
+    if (kz_of(L.K2) < L.K2) throw Error(MDFFGPU_ERR_ARG, "mixed precision k-space supports kmax_z <= 32");
+    std::vector<KSeg> segs;
+    for (const KRow &R : rows) {
+        int zlo = R.z0, zhi = R.z0 + R.cnt - 1;
+        for (int b = 0; b < L.nzb; b++) {
+            int z0 = (b < L.nzb_neg) ? -L.K2 + ZB * b : 1 + ZB * (b - L.nzb_neg);
+            int z1 = (b < L.nzb_neg) ? std::min(z0 + ZB - 1, 0) : std::min(z0 + ZB - 1, L.K2);
+            int lo = std::max(z0, zlo), hi = std::min(z1, zhi);
+            if (lo > hi) continue;
+            if (lo != z0) throw Error(MDFFGPU_ERR_ARG, "k row does not start on a z block");
+            KSeg S;
+            S.nx = R.nx;
+            S.ny = R.ny;
+            S.z0 = z0;
+            S.cnt = hi - lo + 1;
+            S.koff = R.koff + (lo - zlo);
+            S.pad0 = b;
+            S.pad1 = S.pad2 = 0;
+            segs.push_back(S);
+        }
+    }
+    e.nseg32 = (int)segs.size();
+    e.d_seg32 = dalloc<KSeg>(e.nseg32);
+    MDFF_CK(cudaMemcpy(e.d_seg32, segs.data(), sizeof(KSeg) * e.nseg32, cudaMemcpyHostToDevice));
+    e.tab_w = L.w;
+    e.d_tab32 = dalloc<float2>((size_t)e.n * L.w);
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, e.device);
+    int segblocks = ceil_div(e.nseg32, RHO32_THREADS);
+    int chunks = std::max(1, RHO32_MIN_BLOCKS * nsm / segblocks);
+    chunks = std::min(chunks, std::max(1, ceil_div(e.n, RHO32_TI)));
+    e.rho32_chunks = chunks;
+    e.d_rho_part32 = dalloc<float2>((size_t)chunks * e.nk);
+    // ion-pass slices: enough to fill one wave of the full-ion grid
+    int iblocks = ceil_div(e.n, ION32_THREADS);
+    int ns = std::max(1, std::min(e.nrow, ION32_MIN_BLOCKS * nsm / std::max(1, iblocks)));
+    int maxrows = std::max(1, (48 * 1024) / ((kz_of(L.K2) + 1) * (int)sizeof(float4)));
+    ns = std::max(ns, ceil_div(e.nrow, maxrows));
+    e.ion32_rows = ceil_div(e.nrow, ns);
+    e.ion32_slices = ceil_div(e.nrow, e.ion32_rows);
+    e.d_ion_part32 = dalloc<double>((size_t)e.ion32_slices * e.n * 6);
+}
+
+void launch_phase32(Engine &e) {
+    TabLayout L = layout_of(e);
+    long long tot = (long long)e.n * L.w;
+    MDFF_LAUNCH(e, k_phase32, (unsigned)((tot + 255) / 256), 256, 0, e.n, e.cell, e.d_r, L, e.d_tab32);
+}
+
+void launch_coords32(Engine &e) {
+    if (e.d_tab32) launch_phase32(e);
+}
+
+double rho_flops_per_pair(bool lq, bool ld);
+double ion_flops_per_pair(bool f, bool efg);
+void launch_rho_reduce32(Engine &e, const float2 *part, int nchunks, double2 *rho_raw);
+
+template <bool LQ, bool LD>
+static void rho32_launch(Engine &e, dim3 grid, size_t smem, int cnt, const int *idx, int chunk, const TabLayout &L,
+                         const double *q, const double3 *mu) {
+    if (smem > 48 * 1024)
+        MDFF_CK(cudaFuncSetAttribute(k_rho32<LQ, LD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    MDFF_LAUNCH(e, (k_rho32<LQ, LD>), grid, RHO32_THREADS, smem, cnt, idx, chunk, L, e.d_tab32, e.cell, q, mu,
+                e.nseg32, e.d_seg32, e.d_rho_part32, e.nk);
+}
+
+// rho(k) of (q, mu) over `cnt` ions (all when idx is null) into e.d_rho_part32 partials
+void launch_rho32(Engine &e, const double *q, const double3 *mu, bool lq, bool ld, const int *idx, int cnt) {
+    TabLayout L = layout_of(e);
+    int segblocks = ceil_div(e.nseg32, RHO32_THREADS);
+    int chunk = ceil_div(std::max(cnt, 1), e.rho32_chunks);
+    chunk = ceil_div(chunk, 4) * 4;
+    dim3 grid(segblocks, e.rho32_chunks);
+    size_t smem = sizeof(float2) * RHO32_TI * L.w + sizeof(float4) * RHO32_TI;
+    int ps = -1;
+    e.prof_begin("k_rho", &ps);
+    if (lq && ld) rho32_launch<true, true>(e, grid, smem, cnt, idx, chunk, L, q, mu);
+    else if (lq) rho32_launch<true, false>(e, grid, smem, cnt, idx, chunk, L, q, mu);
+    else if (ld) rho32_launch<false, true>(e, grid, smem, cnt, idx, chunk, L, q, mu);
+    else MDFF_CK(cudaMemsetAsync(e.d_rho_part32, 0, sizeof(float2) * (size_t)e.nk * e.rho32_chunks, e.stream));
+    e.prof_end("k_rho", ps, (lq || ld) ? rho_flops_per_pair(lq, ld) * (double)cnt * e.nk : 0.0);
+}
+
+template <int KZ, bool WF>
+static void ion32_launch(Engine &e, dim3 g, size_t smem, const Ion32Args &a) {
+    MDFF_LAUNCH(e, (k_ion32<KZ, WF>), g, ION32_THREADS, smem, a);
+}
+
+template <int KZ>
+static void ion32_dispatch(Engine &e, dim3 g, size_t smem, const Ion32Args &a, bool wf) {
+    if (wf) ion32_launch<KZ, true>(e, g, smem, a);
+    else ion32_launch<KZ, false>(e, g, smem, a);
+}
+
+// field (and force) terms of Ak rho(k) (e.d_rho) at `cnt` ions, then slice sums + self/direct terms
+void launch_ion32(Engine &e, const double *q, const double3 *mu, bool ld, const RecOut &o, const int *idx, int cnt) {
+    bool wf = o.f != nullptr;
+    Ion32Args a;
+    a.cnt = cnt;
+    a.nrow = e.nrow;
+    a.rows_per_slice = e.ion32_rows;
+    a.nk = e.nk;
+    a.idx = idx;
+    a.c = e.cell;
+    a.r = e.d_r;
+    a.mu = mu;
+    a.row = e.d_row;
+    a.rho_s = e.d_rho;
+    a.part = e.d_ion_part32;
+    a.ld = ld;
+    int KZ = kz_of(e.kmax[2]);
+    size_t smem = sizeof(float4) * e.ion32_rows * (KZ + 1);
+    dim3 g(ceil_div(std::max(cnt, 1), ION32_THREADS), e.ion32_slices);
+    int pi = -1;
+    e.prof_begin("k_rec_ion", &pi);
+    if (KZ == 8) ion32_dispatch<8>(e, g, smem, a, wf);
+    else if (KZ == 14) ion32_dispatch<14>(e, g, smem, a, wf);
+    else if (KZ == 16) ion32_dispatch<16>(e, g, smem, a, wf);
+    else ion32_dispatch<32>(e, g, smem, a, wf);
+    e.prof_end("k_rec_ion", pi, ion_flops_per_pair(wf, false) * (double)cnt * e.nk);
+    Comb32Args b;
+    b.cnt = cnt;
+    b.nslice = e.ion32_slices;
+    b.idx = idx;
+    b.c = e.cell;
+    b.part = e.d_ion_part32;
+    b.tfpiV = 2.0 * 2.0 * TPI_D * e.cell.inveOmega;
+    b.self2 = o.self2;
+    b.coul = o.coul;
+    b.ld = ld;
+    b.q = q;
+    b.muself = o.self_mu;
+    b.ef_dir = o.ef_dir;
+    b.ef = o.ef;
+    b.f_dir = o.f_dir;
+    b.f = o.f;
+    int nb = ceil_div(std::max(cnt, 1), 256);
+    if (wf) MDFF_LAUNCH(e, k_combine32<true>, nb, 256, 0, b);
+    else MDFF_LAUNCH(e, k_combine32<false>, nb, 256, 0, b);
+}
+
+}  // namespace mdffgpu
