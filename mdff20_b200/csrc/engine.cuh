@@ -220,7 +220,7 @@ struct Engine {
     float2 *d_tab32 = nullptr;                          // phase table rows [n][tab_w]
     int rho32_chunks = 0;
     float2 *d_rho_part32 = nullptr;                     // [rho32_chunks][nk]
-    int ion32_rows = 0, ion32_slices = 0;
+    int ion32_slices = 0, nsm = 148;                    // most ion-pass slices; SMs
     double *d_ion_part32 = nullptr;                     // [slices][n][6]
     int *d_pidx = nullptr;                              // polarisable ions, ascending
     bool rho_acc_ready = false;                         // d_rho_acc holds rho(k) of (q, mu_tot)

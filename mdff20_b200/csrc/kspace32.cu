@@ -137,25 +137,27 @@ __global__ void __launch_bounds__(RHO32_THREADS, RHO32_MIN_BLOCKS)
                     float2 B2 = make_float2(-c1 * b.y, c1 * b.x);
                     B1.x += fz0 * B2.x;
                     B1.y += fz0 * B2.y;
+                    // explicit FMA chains: acc += C e as four FMA per complex term
 #pragma unroll
                     for (int h = 0; h < ZB / 2; h++) {
                         float4 ee = Z[h];
-                        float2 C0 = make_float2(B1.x + (float)(2 * h) * B2.x, B1.y + (float)(2 * h) * B2.y);
-                        float2 C1 = make_float2(B1.x + (float)(2 * h + 1) * B2.x, B1.y + (float)(2 * h + 1) * B2.y);
-                        acc[2 * h].x += C0.x * ee.x - C0.y * ee.y;
-                        acc[2 * h].y += C0.x * ee.y + C0.y * ee.x;
-                        acc[2 * h + 1].x += C1.x * ee.z - C1.y * ee.w;
-                        acc[2 * h + 1].y += C1.x * ee.w + C1.y * ee.z;
+                        float2 C0 = make_float2(fmaf((float)(2 * h), B2.x, B1.x), fmaf((float)(2 * h), B2.y, B1.y));
+                        float2 C1 = make_float2(fmaf((float)(2 * h + 1), B2.x, B1.x),
+                                                fmaf((float)(2 * h + 1), B2.y, B1.y));
+                        acc[2 * h].x = fmaf(-C0.y, ee.y, fmaf(C0.x, ee.x, acc[2 * h].x));
+                        acc[2 * h].y = fmaf(C0.y, ee.x, fmaf(C0.x, ee.y, acc[2 * h].y));
+                        acc[2 * h + 1].x = fmaf(-C1.y, ee.w, fmaf(C1.x, ee.z, acc[2 * h + 1].x));
+                        acc[2 * h + 1].y = fmaf(C1.y, ee.z, fmaf(C1.x, ee.w, acc[2 * h + 1].y));
                     }
                 } else {
                     float2 C = make_float2(qm.x * b.x, qm.x * b.y);
 #pragma unroll
                     for (int h = 0; h < ZB / 2; h++) {
                         float4 ee = Z[h];
-                        acc[2 * h].x += C.x * ee.x - C.y * ee.y;
-                        acc[2 * h].y += C.x * ee.y + C.y * ee.x;
-                        acc[2 * h + 1].x += C.x * ee.z - C.y * ee.w;
-                        acc[2 * h + 1].y += C.x * ee.w + C.y * ee.z;
+                        acc[2 * h].x = fmaf(-C.y, ee.y, fmaf(C.x, ee.x, acc[2 * h].x));
+                        acc[2 * h].y = fmaf(C.y, ee.x, fmaf(C.x, ee.y, acc[2 * h].y));
+                        acc[2 * h + 1].x = fmaf(-C.y, ee.w, fmaf(C.x, ee.z, acc[2 * h + 1].x));
+                        acc[2 * h + 1].y = fmaf(C.y, ee.z, fmaf(C.x, ee.w, acc[2 * h + 1].y));
                     }
                 }
             }
@@ -397,14 +399,24 @@ void setup_kspace32(Engine &e, const std::vector<KRow> &rows) {
     chunks = std::min(chunks, std::max(1, ceil_div(e.n, RHO32_TI)));
     e.rho32_chunks = chunks;
     e.d_rho_part32 = dalloc<float2>((size_t)chunks * e.nk);
-    // ion-pass slices: enough to fill one wave of the full-ion grid
-    int iblocks = ceil_div(e.n, ION32_THREADS);
-    int ns = std::max(1, std::min(e.nrow, ION32_MIN_BLOCKS * nsm / std::max(1, iblocks)));
+    // ion-pass slices are chosen per launch (ion32_slicing); room for the largest count
+    e.nsm = nsm;
     int maxrows = std::max(1, (48 * 1024) / ((kz_of(L.K2) + 1) * (int)sizeof(float4)));
-    ns = std::max(ns, ceil_div(e.nrow, maxrows));
-    e.ion32_rows = ceil_div(e.nrow, ns);
-    e.ion32_slices = ceil_div(e.nrow, e.ion32_rows);
+    e.ion32_slices = std::max(std::min(32, e.nrow), ceil_div(e.nrow, maxrows));
     e.d_ion_part32 = dalloc<double>((size_t)e.ion32_slices * e.n * 6);
+}
+
+// k-row slices of one ion pass over `cnt` ions: about two full waves of resident blocks,
+// at most e.ion32_slices, each slice's Ak rho(k) within 48 KB of shared memory
+static void ion32_slicing(const Engine &e, int cnt, int &rows, int &slices) {
+    int KZ = kz_of(e.kmax[2]);
+    int iblocks = ceil_div(std::max(cnt, 1), ION32_THREADS);
+    int s = std::max(1, 2 * ION32_MIN_BLOCKS * e.nsm / iblocks);
+    s = std::min(s, std::min(e.nrow, e.ion32_slices));
+    int maxrows = std::max(1, (48 * 1024) / ((KZ + 1) * (int)sizeof(float4)));
+    s = std::max(s, ceil_div(e.nrow, maxrows));
+    rows = ceil_div(e.nrow, s);
+    slices = ceil_div(e.nrow, rows);
 }
 
 void launch_phase32(Engine &e) {
@@ -461,10 +473,12 @@ static void ion32_dispatch(Engine &e, dim3 g, size_t smem, const Ion32Args &a, b
 // field (and force) terms of Ak rho(k) (e.d_rho) at `cnt` ions, then slice sums + self/direct terms
 void launch_ion32(Engine &e, const double *q, const double3 *mu, bool ld, const RecOut &o, const int *idx, int cnt) {
     bool wf = o.f != nullptr;
+    int rows = 1, slices = 1;
+    ion32_slicing(e, cnt, rows, slices);
     Ion32Args a;
     a.cnt = cnt;
     a.nrow = e.nrow;
-    a.rows_per_slice = e.ion32_rows;
+    a.rows_per_slice = rows;
     a.nk = e.nk;
     a.idx = idx;
     a.c = e.cell;
@@ -475,8 +489,8 @@ void launch_ion32(Engine &e, const double *q, const double3 *mu, bool ld, const 
     a.part = e.d_ion_part32;
     a.ld = ld;
     int KZ = kz_of(e.kmax[2]);
-    size_t smem = sizeof(float4) * e.ion32_rows * (KZ + 1);
-    dim3 g(ceil_div(std::max(cnt, 1), ION32_THREADS), e.ion32_slices);
+    size_t smem = sizeof(float4) * rows * (KZ + 1);
+    dim3 g(ceil_div(std::max(cnt, 1), ION32_THREADS), slices);
     int pi = -1;
     e.prof_begin("k_rec_ion", &pi);
     if (KZ == 8) ion32_dispatch<8>(e, g, smem, a, wf);
@@ -486,7 +500,7 @@ void launch_ion32(Engine &e, const double *q, const double3 *mu, bool ld, const 
     e.prof_end("k_rec_ion", pi, ion_flops_per_pair(wf, false) * (double)cnt * e.nk);
     Comb32Args b;
     b.cnt = cnt;
-    b.nslice = e.ion32_slices;
+    b.nslice = slices;
     b.idx = idx;
     b.c = e.cell;
     b.part = e.d_ion_part32;

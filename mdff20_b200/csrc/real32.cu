@@ -394,17 +394,16 @@ void launch_pol_field32(Engine &e, const double3 *p, double3 *out_ef) {
     e.prof_end("k_dir", pd, 0.0);
 }
 
-// uniform Tang-Toennies order of the damped pairs (0 when mixed or none)
+// 4 when every Tang-Toennies function the pair kernel evaluates has order 4 or c = 0
+// (then f = 1 and f' = 0 whatever the order), else 0 (order read per pair)
 static int uniform_tt_order(const Engine &e) {
-    int k = -1;
     for (int a = 0; a < e.nt; a++)
         for (int b = 0; b < e.nt; b++) {
             if (!(e.p.lpoldamping[a][a][b] || e.p.lpoldamping[b][a][b])) continue;
-            int k1 = e.p.pol_damp_k[a][a][b], k2 = e.p.pol_damp_k[b][a][b];
-            if (k < 0) k = k1;
-            if (k1 != k || k2 != k) return 0;
+            if (e.p.pol_damp_c[a][a][b] != 0.0 && e.p.pol_damp_k[a][a][b] != 4) return 0;
+            if (e.p.pol_damp_c[b][a][b] != 0.0 && e.p.pol_damp_k[b][a][b] != 4) return 0;
         }
-    return k == 4 ? 4 : 0;
+    return 4;
 }
 
 template <bool FORCES, bool EF>
