@@ -106,6 +106,11 @@ int mdffgpu_destroy(mdffgpu_ctx *ctx);
 const char *mdffgpu_last_error(const mdffgpu_ctx *ctx);
 int mdffgpu_set_precision(mdffgpu_ctx *ctx, int precision);
 int mdffgpu_set_pim_solver(mdffgpu_ctx *ctx, int solver);
+/* No reference counterpart.  on != 0 (the default): mdffgpu_md_steps replays each MD
+ * step as one CUDA graph (the CG loop a device-controlled while node) whenever the step
+ * needs no host decision (Verlet lists on, a CG solver, the ASPC order at its final
+ * value); 0: every step is issued kernel by kernel.  Results are the same either way. */
+int mdffgpu_set_graph(mdffgpu_ctx *ctx, int on);
 
 /* State transfer (the reference's rx..fz globals, src/config.h:38-40). */
 int mdffgpu_set_positions(mdffgpu_ctx *ctx, const double *rx, const double *ry, const double *rz);

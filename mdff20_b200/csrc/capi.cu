@@ -82,6 +82,7 @@ int mdffgpu_set_precision(mdffgpu_ctx *ctx, int precision) {
             throw Error(MDFFGPU_ERR_ARG, "mixed precision kernels are not built in this library");
         e.precision = precision;
         e.use32 = (precision == MDFFGPU_MIXED);
+        e.gen++;
         e.real32 = e.rec32 = e.subset32 = true;
         if (const char *v = getenv("MDFFGPU_MIXED_PARTS")) {
             e.real32 = strstr(v, "real") != nullptr;
@@ -96,6 +97,14 @@ int mdffgpu_set_pim_solver(mdffgpu_ctx *ctx, int solver) {
         if (solver != MDFFGPU_PIM_REFERENCE && solver != MDFFGPU_PIM_CG && solver != MDFFGPU_PIM_CG_FUSED)
             throw Error(MDFFGPU_ERR_ARG, "bad solver");
         e.pim_solver = solver;
+        e.gen++;
+    });
+}
+
+int mdffgpu_set_graph(mdffgpu_ctx *ctx, int on) {
+    return guarded(ctx, [&](Engine &e) {
+        e.graph_on = on != 0;
+        if (!e.graph_on) e.drop_graph();
     });
 }
 

@@ -44,6 +44,9 @@ __global__ void k_cg_rz(int n, const int *polar, const double *pol, const double
 __global__ void k_cg_update(int n, const double *scal, const double3 *p, const double3 *ap, double3 *x, double3 *r);
 __global__ void k_cg_dir(int n, const double *scal, const double3 *z, double3 *p);
 __global__ void k_copy_slot(double *scal, int from, int to);
+__global__ void k_cg_check(cudaGraphConditionalHandle h, int first, const double *scal, DevScalars *out, int npol,
+                           double tol, int maxit, unsigned *status);
+__global__ void k_upol_final(const double *scal, double coul, DevScalars *out);
 __global__ void k_vv1(int n, double dt, double dtsq2, const double *invm, double4 *r, const double3 *v,
                       const double3 *f, double3 *fs);
 __global__ void k_vv2(int n, double dt2, const double *invm, const double *mass, double3 *v, const double3 *f,
@@ -112,6 +115,7 @@ Engine::Engine(const mdffgpu_params &prm, int dev) : p(prm) {
     if (dev >= 0) MDFF_CK(cudaSetDevice(dev));
     MDFF_CK(cudaGetDevice(&device));
     MDFF_CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    MDFF_CK(cudaStreamCreateWithFlags(&body_stream, cudaStreamNonBlocking));
     setup_units_and_cell();
     setup_types();
     // device buffers
@@ -203,6 +207,8 @@ Engine::~Engine() {
     cudaFree(d_status);
     if (h_out) cudaFreeHost(h_out);
     if (h_stage) cudaFreeHost(h_stage);
+    if (step_exec) cudaGraphExecDestroy(step_exec);
+    if (body_stream) cudaStreamDestroy(body_stream);
     if (stream) cudaStreamDestroy(stream);
 }
 
@@ -554,6 +560,7 @@ void Engine::alloc_lists(int cnb, int cco) {
     dfree(d_con);
     cap_nb = cnb;
     cap_co = cco;
+    gen++;
     d_nb = dalloc<int>((size_t)n * cap_nb);
     d_nbn = dalloc<int>(n);
     d_co = dalloc<int>((size_t)n * cap_co);
@@ -641,15 +648,16 @@ void Engine::gen_verletlist() {
     throw Error(MDFFGPU_ERR_LIST_OVERFLOW, "neighbour list capacity could not be grown");
 }
 
-int Engine::check_verletlist() {
+int Engine::check_verletlist(bool reset_status) {
     if (!list_ready) {
         gen_verletlist();
         return 1;
     }
-    MDFF_CK(cudaMemsetAsync(d_status, 0, sizeof(unsigned), stream));
+    if (reset_status) MDFF_CK(cudaMemsetAsync(d_status, 0, sizeof(unsigned), stream));
     launch_kardir(*this, d_r, d_s);
     launch_check_list(*this);
     launch_build_lists(*this, false);
+    if (capturing) return 0;   // the host reads the rebuild flag and status after the step
     int rb = 0;
     unsigned st = 0;
     MDFF_CK(cudaMemcpyAsync(&rb, d_rebuild, sizeof(int), cudaMemcpyDeviceToHost, stream));
@@ -814,14 +822,10 @@ void Engine::pim_cg(bool fused) {
     MDFF_LAUNCH(*this, k_cg_rz, nb, 256, 0, n, d_polar, d_pol, d_cg_r, d_mu_save, d_part, part_stride);
     reduce(S_RZ, 2, nb);
     MDFF_CK(cudaMemcpyAsync(d_cg_p, d_mu_save, sizeof(double3) * n, cudaMemcpyDeviceToDevice, stream));
-    double rr = 0.0;
-    MDFF_CK(cudaMemcpyAsync(&rr, d_scal + S_RR, sizeof(double), cudaMemcpyDeviceToHost, stream));
-    MDFF_CK(cudaStreamSynchronize(stream));
-    double rmsd = std::sqrt(rr / (double)std::max(npol, 1));
-    int it = 0;
     int maxit = std::max(p.max_scf_pim_iter, 1);
-    while (rmsd > p.conv_tol_ind && it < maxit) {
-        if (fused && use32 && rec32 && subset32 && npol > 0) field_pol(d_cg_p, d_ef_ind, d_rho_it);              // T p
+    // one CG iteration up to the new residual norm (p <- z + beta p follows the test)
+    auto iteration = [&]() {
+        if (fused && use32 && rec32 && subset32 && npol > 0) field_pol(d_cg_p, d_ef_ind, d_rho_it);   // T p
         else field_of(d_qzero, d_cg_p, false, true, false, d_ef_ind, fused ? d_rho_it : nullptr);
         MDFF_LAUNCH(*this, k_cg_ap, nb, 256, 0, n, d_polar, d_invpol, d_cg_p, d_ef_ind, d_cg_ap, d_part, part_stride);
         reduce(S_PAP, 1, nb);
@@ -830,27 +834,70 @@ void Engine::pim_cg(bool fused) {
         if (fused) launch_rho_axpy(*this, S_RZOLD, S_PAP, d_rho_it, d_rho_acc);
         MDFF_LAUNCH(*this, k_cg_rz, nb, 256, 0, n, d_polar, d_pol, d_cg_r, d_mu_save, d_part, part_stride);
         reduce(S_RZ, 2, nb);
+    };
+    if (capturing) {
+        // graph: the loop is a while node whose condition the device test sets
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t cgraph = nullptr;
+        const cudaGraphNode_t *deps = nullptr;
+        size_t ndeps = 0;
+        MDFF_CK(cudaStreamGetCaptureInfo(stream, &cs, nullptr, &cgraph, nullptr, nullptr));
+        MDFF_CK(cudaGraphConditionalHandleCreate(&cg_handle, cgraph, 0, 0));
+        MDFF_LAUNCH(*this, k_cg_check, 1, 32, 0, cg_handle, 1, d_scal, d_out, npol, p.conv_tol_ind, maxit, d_status);
+        MDFF_CK(cudaStreamGetCaptureInfo(stream, &cs, nullptr, &cgraph, &deps, &ndeps));
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = cg_handle;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        MDFF_CK(cudaGraphAddNode(&node, cgraph, deps, ndeps, &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        MDFF_CK(cudaStreamUpdateCaptureDependencies(stream, &node, 1, cudaStreamSetCaptureDependencies));
+        cudaStream_t outer = stream;
+        stream = body_stream;
+        MDFF_CK(cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        try {
+            long long b0 = launches;
+            iteration();
+            MDFF_LAUNCH(*this, k_cg_check, 1, 32, 0, cg_handle, 0, d_scal, d_out, npol, p.conv_tol_ind, maxit,
+                        d_status);
+            MDFF_LAUNCH(*this, k_cg_dir, nb, 256, 0, n, d_scal, d_mu_save, d_cg_p);
+            body_count = launches - b0;
+        } catch (...) {
+            cudaGraph_t g2 = nullptr;
+            cudaStreamEndCapture(stream, &g2);
+            stream = outer;
+            throw;
+        }
+        cudaGraph_t g2 = nullptr;
+        MDFF_CK(cudaStreamEndCapture(stream, &g2));
+        stream = outer;
+    } else {
+        double rr = 0.0;
         MDFF_CK(cudaMemcpyAsync(&rr, d_scal + S_RR, sizeof(double), cudaMemcpyDeviceToHost, stream));
         MDFF_CK(cudaStreamSynchronize(stream));
-        rmsd = std::sqrt(rr / (double)std::max(npol, 1));
-        if (!std::isfinite(rmsd)) throw Error(MDFFGPU_ERR_NONFINITE, "CG diverged");
-        it++;
-        if (rmsd <= p.conv_tol_ind) break;
-        MDFF_LAUNCH(*this, k_cg_dir, nb, 256, 0, n, d_scal, d_mu_save, d_cg_p);
+        double rmsd = std::sqrt(rr / (double)std::max(npol, 1));
+        int it = 0;
+        while (rmsd > p.conv_tol_ind && it < maxit) {
+            iteration();
+            MDFF_CK(cudaMemcpyAsync(&rr, d_scal + S_RR, sizeof(double), cudaMemcpyDeviceToHost, stream));
+            MDFF_CK(cudaStreamSynchronize(stream));
+            rmsd = std::sqrt(rr / (double)std::max(npol, 1));
+            if (!std::isfinite(rmsd)) throw Error(MDFFGPU_ERR_NONFINITE, "CG diverged");
+            it++;
+            if (rmsd <= p.conv_tol_ind) break;
+            MDFF_LAUNCH(*this, k_cg_dir, nb, 256, 0, n, d_scal, d_mu_save, d_cg_p);
+        }
+        if (rmsd > p.conv_tol_ind) throw Error(MDFFGPU_ERR_SCF, "CG did not converge in max_scf_pim_iter");
+        last_scf_iter = it;
+        last_rmsd = rmsd;
     }
-    if (rmsd > p.conv_tol_ind) throw Error(MDFFGPU_ERR_SCF, "CG did not converge in max_scf_pim_iter");
     MDFF_LAUNCH(*this, k_pim_sums, nb, 256, 0, n, d_polar, d_pol, d_invpol, d_mu_ind, d_ef_stat, d_part, part_stride);
     reduce(S_UPOL, 1, nb);
-    double up = 0.0;
-    MDFF_CK(cudaMemcpyAsync(&up, d_scal + S_UPOL, sizeof(double), cudaMemcpyDeviceToHost, stream));
-    MDFF_CK(cudaStreamSynchronize(stream));
+    MDFF_LAUNCH(*this, k_upol_final, 1, 32, 0, d_scal, coul_unit, d_out);
     MDFF_LAUNCH(*this, k_hist_store, nb, 256, 0, n, d_mu_ind, d_hist);
-    last_scf_iter = it;
-    last_rmsd = rmsd;
     rho_acc_ready = fused;
-    double v = 0.5 * up * coul_unit;
-    MDFF_CK(cudaMemcpyAsync(&d_out->u_pol, &v, sizeof(double), cudaMemcpyHostToDevice, stream));
-    MDFF_CK(cudaStreamSynchronize(stream));
 }
 
 // get_rmsd_mu (src/pim.c:431-449) of (mu, ef); also returns sum mu.invpol.mu
@@ -1170,14 +1217,84 @@ void Engine::prop_agate(int step) {
     }
 }
 
+// a step can be replayed from a graph once nothing in it needs the host: Verlet lists
+// (rebuilt on the device when due), a CG solver, the ASPC order at its final value
+bool Engine::graph_ok(int step) const {
+    if (!graph_on || !p.lverletL || !prof_name.empty()) return false;
+    if (p.lcoulombic && lpol) {
+        if (pim_solver != MDFFGPU_PIM_CG && pim_solver != MDFFGPU_PIM_CG_FUSED) return false;
+        if (step < p.extrapolate_order + 1) return false;
+    }
+    return true;
+}
+
+void Engine::drop_graph() {
+    if (step_exec) cudaGraphExecDestroy(step_exec);
+    step_exec = nullptr;
+    graph_gen = -1;
+}
+
+// record prop_agate + check_verletlist of one step (src/md.c:237-241) as a graph
+void Engine::capture_step(int step) {
+    drop_graph();
+    if (use32 && real32 && p.lcoulombic) ensure_real32();   // no allocation while recording
+    MDFF_CK(cudaStreamSynchronize(stream));
+    long long l0 = launches;
+    body_count = 0;
+    MDFF_CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    capturing = true;
+    cudaGraph_t graph = nullptr;
+    try {
+        MDFF_CK(cudaMemsetAsync(d_status, 0, sizeof(unsigned), stream));
+        prop_agate(step);
+        check_verletlist(false);
+    } catch (...) {
+        capturing = false;
+        cudaStreamEndCapture(stream, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        launches = l0;
+        throw;
+    }
+    capturing = false;
+    MDFF_CK(cudaStreamEndCapture(stream, &graph));
+    cudaError_t err = cudaGraphInstantiate(&step_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (err != cudaSuccess) {
+        step_exec = nullptr;
+        MDFF_CK(err);
+    }
+    graph_body = body_count;
+    graph_outer = launches - l0 - body_count;
+    launches = l0;
+    graph_gen = gen;
+}
+
 // run_md's loop body (src/md.c:229-241)
 void Engine::md_steps(int first, int nsteps, double *thermo) {
     if (p.lverletL && !list_ready) gen_verletlist();
     for (int s = 0; s < nsteps; s++) {
-        MDFF_CK(cudaMemsetAsync(d_status, 0, sizeof(unsigned), stream));
-        prop_agate(first + s);
-        if (p.lverletL) check_verletlist();
+        int step = first + s;
+        bool graphed = graph_ok(step);
+        if (graphed) {
+            if (!step_exec || graph_gen != gen) capture_step(step);
+            istep = step;
+            MDFF_CK(cudaGraphLaunch(step_exec, stream));
+        } else {
+            MDFF_CK(cudaMemsetAsync(d_status, 0, sizeof(unsigned), stream));
+            prop_agate(step);
+            if (p.lverletL) check_verletlist(false);
+        }
         sync_scalars();
+        if (graphed) {
+            launches += graph_outer + graph_body * std::max(h_out->scf_iter, 0);
+            if (p.lcoulombic && lpol) {
+                last_scf_iter = h_out->scf_iter;
+                last_rmsd = h_out->scf_rmsd;
+            }
+            unsigned st = (unsigned)h_out->status;
+            if (st & ST_SCF) throw Error(MDFFGPU_ERR_SCF, "CG did not converge in max_scf_pim_iter");
+            if (st & ST_LIST_OVERFLOW) gen_verletlist();   // positions unchanged: rebuild larger
+        }
         check_status();
         if (thermo) {
             double *t = thermo + 12 * (size_t)s;

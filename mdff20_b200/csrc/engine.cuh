@@ -252,6 +252,16 @@ struct Engine {
     double last_rmsd = 0.0;
     int nbuilds = 0;
 
+    // one MD step as a CUDA graph (md_steps): the induced-dipole CG loop is a while node
+    // whose condition a device kernel sets, so a step needs no host round trip
+    bool graph_on = true;
+    bool capturing = false;                 // launches are being recorded
+    cudaGraphConditionalHandle cg_handle = 0;
+    cudaStream_t body_stream = nullptr;     // records the CG loop body
+    cudaGraphExec_t step_exec = nullptr;
+    long long gen = 0, graph_gen = -1;      // gen: bumped when buffers or modes change
+    long long graph_outer = 0, graph_body = 0, body_count = 0;   // kernels per replay / per CG iteration
+
     explicit Engine(const mdffgpu_params &prm, int dev);
     ~Engine();
     Engine(const Engine &) = delete;
@@ -270,7 +280,7 @@ struct Engine {
     void get_state(double *rx, double *ry, double *rz, double *vx, double *vy, double *vz, double *fx,
                    double *fy, double *fz);
     void gen_verletlist();
-    int check_verletlist();
+    int check_verletlist(bool reset_status = true);
     void ensure_lists();
     void engforce();
     void sr_forces(bool lj, double *u, double *pvir, double *tau);
@@ -289,6 +299,9 @@ struct Engine {
     double rmsd_of(const double3 *d_mu, const double3 *d_ef, double *upol_sum);
     void prop_agate(int step);
     void md_steps(int first, int nsteps, double *thermo);
+    bool graph_ok(int step) const;
+    void capture_step(int step);
+    void drop_graph();
     void sync_scalars();
     void check_status();
     void finalize_coul(bool stress);

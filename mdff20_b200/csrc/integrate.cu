@@ -340,6 +340,33 @@ __global__ void k_copy_slot(double *scal, int from, int to) {
     if (threadIdx.x == 0 && blockIdx.x == 0) scal[to] = scal[from];
 }
 
+// CG stopping test on the device (graph-captured steps): rmsd = sqrt(r.r / npol), the
+// reference's residual measure (src/pim.c:431-449).  first: before the iterations
+// (iteration count 0); otherwise after one.  Sets the while-loop condition: continue
+// while rmsd > tol and fewer than maxit iterations; non-finite residuals and
+// non-convergence raise status bits read by the host after the step.
+__global__ void k_cg_check(cudaGraphConditionalHandle h, int first, const double *scal, DevScalars *out, int npol,
+                           double tol, int maxit, unsigned *status) {
+    if (threadIdx.x || blockIdx.x) return;
+    double rmsd = sqrt(scal[S_RR] / (double)(npol > 1 ? npol : 1));
+    int it = first ? 0 : out->scf_iter + 1;
+    out->scf_iter = it;
+    out->scf_rmsd = rmsd;
+    unsigned go = 0;
+    if (!isfinite(rmsd)) atomicOr(status, (unsigned)ST_NONFINITE);
+    else if (rmsd > tol) {
+        if (it < maxit) go = 1;
+        else atomicOr(status, (unsigned)ST_SCF);
+    }
+    cudaGraphSetConditional(h, go);
+}
+
+// u_pol = 1/2 sum mu.alpha^-1.mu in energy units
+__global__ void k_upol_final(const double *scal, double coul, DevScalars *out) {
+    if (threadIdx.x || blockIdx.x) return;
+    out->u_pol = 0.5 * scal[S_UPOL] * coul;
+}
+
 // ---------------------------------------------------------------- integrators
 // prop_velocity_verlet first half (src/integration.c:33-38)
 __global__ void k_vv1(int n, double dt, double dtsq2, const double *__restrict__ invm, double4 *__restrict__ r,

@@ -353,8 +353,10 @@ static CellF3 cellf3(const Cell &c) {
 
 void Engine::ensure_real32() {
     if (d_nl32 && cap32 == cap_co) return;
+    if (capturing) throw Error(MDFFGPU_ERR_STATE, "mixed-precision pair buffers allocated while recording");
     dfree32();
     cap32 = cap_co;
+    gen++;
     d_nl32 = dalloc<int>((size_t)n * cap_co);
     d_nln32 = dalloc<int>(n);
     d_qm32 = dalloc<float4>(n);

@@ -149,7 +149,8 @@ def params_from_system(s: System) -> Params:
 
 EXPORTS = (
     "mdffgpu_create", "mdffgpu_destroy", "mdffgpu_last_error", "mdffgpu_set_precision",
-    "mdffgpu_set_pim_solver", "mdffgpu_set_positions", "mdffgpu_set_velocities", "mdffgpu_get_state",
+    "mdffgpu_set_pim_solver", "mdffgpu_set_graph", "mdffgpu_set_positions", "mdffgpu_set_velocities",
+    "mdffgpu_get_state",
     "mdffgpu_set_dipole_history", "mdffgpu_get_dipole_history", "mdffgpu_set_nhc", "mdffgpu_get_nhc",
     "mdffgpu_get_thermo", "mdffgpu_gen_verletlist", "mdffgpu_check_verletlist", "mdffgpu_get_verletlist",
     "mdffgpu_engforce", "mdffgpu_engforce_nmlj", "mdffgpu_engforce_bhmftd", "mdffgpu_multipole_es",
@@ -176,6 +177,7 @@ def load_library(path: str = LIB_PATH):
         "mdffgpu_destroy": [vp],
         "mdffgpu_set_precision": [vp, I],
         "mdffgpu_set_pim_solver": [vp, I],
+        "mdffgpu_set_graph": [vp, I],
         "mdffgpu_set_positions": [vp, dp, dp, dp],
         "mdffgpu_set_velocities": [vp, dp, dp, dp],
         "mdffgpu_get_state": [vp, dp, dp, dp, dp, dp, dp, dp, dp, dp],
@@ -264,6 +266,10 @@ class Engine:
         self.h = h
         self._check(self.L.mdffgpu_set_precision(self.h, precision))
         self._check(self.L.mdffgpu_set_pim_solver(self.h, pim_solver))
+
+    def set_graph(self, on: bool):
+        """Replay MD steps as CUDA graphs (default on); off issues every kernel."""
+        self._check(self.L.mdffgpu_set_graph(self.h, 1 if on else 0))
 
     def close(self):
         if getattr(self, "h", None):

@@ -157,6 +157,47 @@ def test_fused_cg_matches_cg():
     assert rel_err(b.state()[0], a.state()[0]) < 1e-12
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_graph_steps_match_eager(precision):
+    """MD steps replayed as CUDA graphs (device-side CG loop) give exactly the results of
+    the kernel-by-kernel steps, in both precisions."""
+    g = load_golden("crist192_pim_nhc")
+    s = cases.CASES["crist192_pim_nhc"]()
+    s.vel = g["vel"].reshape(-1, 3)
+    p0 = g["r_in"].reshape(-1, 3)
+    runs = []
+    for graph in (False, True):
+        e = Engine(s, positions=p0, pim_solver=PIM_CG_FUSED, precision=precision)
+        e.set_graph(graph)
+        e.gen_verletlist()
+        e.engforce()
+        l0 = e.launch_count()
+        th = e.md_steps(1, 12)
+        runs.append((th, e.state(), e.launch_count() - l0))
+        e.close()
+    (ta, sa, la), (tb, sb, lb) = runs
+    assert np.array_equal(ta, tb)
+    for a, b in zip(sa, sb):
+        assert np.array_equal(a, b)
+    # the graph counts what it replays: the device-side CG tests (one per iteration and
+    # one before) and the search-direction update after the last iteration come on top
+    assert la < lb <= la + 12 * 16
+
+
+def test_graph_scf_nonconvergence_reported():
+    """A CG iteration cap that cannot be met is reported as ERR_SCF from a graph step."""
+    g = load_golden("crist192_pim_nhc")
+    s = cases.CASES["crist192_pim_nhc"]()
+    s.vel = g["vel"].reshape(-1, 3)
+    s.max_scf_pim_iter = 1
+    s.conv_tol_ind = 1e-14
+    e = Engine(s, positions=g["r_in"].reshape(-1, 3), pim_solver=PIM_CG_FUSED)
+    e.gen_verletlist()
+    with pytest.raises(MdffgpuError) as ex:
+        e.md_steps(1, 3)
+    assert ex.value.code == 4   # MDFFGPU_ERR_SCF
+
+
 def test_random_systems_vs_oracle():
     """Fresh seeds (not in the fixtures), engine vs oracle, several flag paths."""
     for seed in (201, 202):
