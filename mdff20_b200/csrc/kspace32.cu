@@ -5,11 +5,13 @@
 // E0[nx] E1[ny] E2[nz], E_d[m] = exp(2 pi i m t_d), t = B^T r (kspace.cu).  k_phase32
 // writes, once per force evaluation (positions are fixed through the induced-dipole
 // solve), one row of FP32 complex values per ion:
-//     [ E0[0..K0] | E1[-K1..K1] | pad | Z blocks of ZB values of E2 ]
+//     [ E0[0..K0] | E1[-K1..K1] | pad | Z blocks of ZB values of E2, stride ZS ]
 // every entry from its own FP64-reduced argument m t_d - rint(m t_d) (no recurrence,
 // so each value carries one rounding).  The z range of a k-row is cut into blocks of
 // ZB consecutive nz (negative half -K2..0 and positive half 1..K2 separately, zero
-// padded), so that a thread owns one block of one row and reads it with 16-byte loads.
+// padded), so that a thread owns one block of one row and reads it with 16-byte loads;
+// the two extra entries per block put neighbouring blocks in different shared-memory
+// banks (the lanes of a warp read two blocks of the same ion at once).
 //
 // k_rho32   : rho(k) = sum_i (q_i + i k.mu_i) E0 E1 E2.  Thread = one (row, z block)
 //             segment, ions stream through shared memory in tiles of table rows; the
@@ -28,14 +30,26 @@
 namespace mdffgpu {
 
 constexpr int ZB = 16;              // nz per segment block (two complex per 16-byte load)
+constexpr int ZS = ZB + 2;          // block stride: consecutive blocks start 4 banks apart
 constexpr int RHO32_THREADS = 128;
-constexpr int RHO32_TI = 32;        // ions per shared-memory tile
+constexpr int RHO32_TI = 16;        // ions per shared-memory tile (two tiles in flight)
 constexpr int RHO32_MIN_BLOCKS = 8;
 constexpr int ION32_THREADS = 128;
 constexpr int ION32_MIN_BLOCKS = 6;
 
 __device__ __forceinline__ float2 cmul32(float2 a, float2 b) {
     return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// asynchronous global -> shared copy of 16 bytes (both addresses 16-byte aligned)
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
 // exp(2 pi i x) for an FP64 argument: exact reduction to [-1/2, 1/2], FP32 sincospi
@@ -64,8 +78,9 @@ __global__ void k_phase32(int n, Cell c, const double4 *__restrict__ r, TabLayou
         d = 1;
         m = e - L.e1 - L.K1;
     } else if (e >= L.z) {
-        int b = (e - L.z) / ZB, j = (e - L.z) - b * ZB;
-        if (b < L.nzb_neg) {
+        int b = (e - L.z) / ZS, j = (e - L.z) - b * ZS;
+        if (j >= ZB) {
+        } else if (b < L.nzb_neg) {
             m = -L.K2 + ZB * b + j;
             if (m <= 0) d = 2;
         } else {
@@ -89,29 +104,44 @@ __global__ void __launch_bounds__(RHO32_THREADS, RHO32_MIN_BLOCKS)
             Cell c, const double *__restrict__ q, const double3 *__restrict__ mu, int nseg,
             const KSeg *__restrict__ seg, float2 *__restrict__ part, int nk) {
     extern __shared__ float4 sm4[];
-    float2 *T = (float2 *)sm4;                          // [RHO32_TI][L.w]
-    float4 *QM = sm4 + RHO32_TI * (L.w / 2);            // [RHO32_TI] (q, 2 pi m)
-    const int hw = L.w / 2;
+    const int hw = L.w / 2;                              // table row in 16-byte units
+    // two stages: [2][RHO32_TI][hw] table rows, then [2][RHO32_TI] (q, 2 pi m)
+    float4 *QMs = sm4 + 2 * RHO32_TI * hw;
     int sid = blockIdx.x * RHO32_THREADS + threadIdx.x;
     KSeg S;
     if (sid < nseg) S = seg[sid];
     else S.nx = S.ny = S.z0 = S.cnt = S.koff = S.pad0 = 0;
     const float fnx = (float)S.nx, fny = (float)S.ny, fz0 = (float)S.z0;
-    const int o0 = S.nx, o1 = L.e1 + L.K1 + S.ny, oz = (L.z + ZB * S.pad0) / 2;
+    const int o0 = S.nx, o1 = L.e1 + L.K1 + S.ny, oz = (L.z + ZS * S.pad0) / 2;
     float2 acc[ZB];
 #pragma unroll
     for (int z = 0; z < ZB; z++) acc[z] = make_float2(0.f, 0.f);
     int a0 = blockIdx.y * chunk, a1 = min(cnt, a0 + chunk);
     int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const double tpi = TPI_D;
-    for (int t0 = a0; t0 < a1; t0 += RHO32_TI) {
+    // table rows of the tile at t0 into stage buffer `st` by asynchronous 16-byte copies
+    // (warp w copies rows w, w+4, ...); every thread commits one group per tile
+    auto issue = [&](int t0, int st) {
         int nt = min(RHO32_TI, a1 - t0);
-        // table rows: warp w copies rows w, w+4, ...
+        float4 *dst = sm4 + st * RHO32_TI * hw;
         for (int a = w; a < nt; a += RHO32_THREADS / 32) {
             int ion = idx ? idx[t0 + a] : t0 + a;
             const float4 *src = (const float4 *)(tab + (size_t)ion * L.w);
-            for (int j = lane; j < hw; j += 32) sm4[a * hw + j] = src[j];
+            for (int j = lane; j < hw; j += 32) cp_async16(dst + a * hw + j, src + j);
         }
+        cp_async_commit();
+    };
+    int ntiles = a1 > a0 ? (a1 - a0 + RHO32_TI - 1) / RHO32_TI : 0;
+    if (ntiles > 0) issue(a0, 0);
+    for (int t = 0; t < ntiles; t++) {
+        int t0 = a0 + t * RHO32_TI, nt = min(RHO32_TI, a1 - t0), st = t & 1;
+        if (t + 1 < ntiles) {
+            issue(t0 + RHO32_TI, st ^ 1);   // overlaps this tile's arithmetic
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        float4 *QM = QMs + st * RHO32_TI;
         if (threadIdx.x < nt) {
             int ion = idx ? idx[t0 + threadIdx.x] : t0 + threadIdx.x;
             float4 v = make_float4(LQ ? (float)q[ion] : 0.f, 0.f, 0.f, 0.f);
@@ -124,12 +154,13 @@ __global__ void __launch_bounds__(RHO32_THREADS, RHO32_MIN_BLOCKS)
             QM[threadIdx.x] = v;
         }
         __syncthreads();
+        const float4 *cur = sm4 + st * RHO32_TI * hw;
         if (sid < nseg) {
             for (int a = 0; a < nt; a++) {
-                const float2 *R = T + a * L.w;
+                const float2 *R = (const float2 *)(cur + a * hw);
                 float2 b = cmul32(R[o0], R[o1]);
                 float4 qm = QM[a];
-                const float4 *Z = sm4 + a * hw + oz;
+                const float4 *Z = cur + a * hw + oz;
                 if (LD) {
                     // k.mu = c0 + nz c1; B1 = (q + i c0) b, B2 = i c1 b, summand (B1 + nz B2) E2
                     float c0 = fnx * qm.y + fny * qm.z, c1 = qm.w;
@@ -188,11 +219,16 @@ struct Ion32Args {
 template <int KZ, bool WF>
 __global__ void __launch_bounds__(ION32_THREADS, ION32_MIN_BLOCKS) k_ion32(Ion32Args a) {
     extern __shared__ float4 rk4[];          // [rows of the slice][KZ + 1]: (rho_z, rho_-z)
+    int2 *rnxy = (int2 *)(rk4 + a.rows_per_slice * (KZ + 1));   // (nx, ny) of the slice's rows
     int li = blockIdx.x * ION32_THREADS + threadIdx.x;
     int sl = blockIdx.y;
     int r0 = sl * a.rows_per_slice, r1 = min(a.nrow, r0 + a.rows_per_slice);
     // Ak rho(k) of the slice's rows, padded to z = -KZ..KZ
     int nrs = r1 - r0;
+    for (int e = threadIdx.x; e < nrs; e += ION32_THREADS) {
+        KRow R = a.row[r0 + e];
+        rnxy[e] = make_int2(R.nx, R.ny);
+    }
     for (int e = threadIdx.x; e < nrs * (KZ + 1); e += ION32_THREADS) {
         int rr = e / (KZ + 1), zz = e - rr * (KZ + 1);
         KRow R = a.row[r0 + rr];
@@ -231,34 +267,38 @@ __global__ void __launch_bounds__(ION32_THREADS, ION32_MIN_BLOCKS) k_ion32(Ion32
     __syncthreads();
     double S0 = 0, S1 = 0, S2 = 0, P0 = 0, P1 = 0, P2 = 0;
     for (int rr = 0; rr < nrs; rr++) {
-        KRow R = a.row[r0 + rr];
-        float2 w = cis2pi32((double)R.nx * tx + (double)R.ny * ty);
+        int2 R = rnxy[rr];
+        float2 w = cis2pi32((double)R.x * tx + (double)R.y * ty);
         const float4 *rho = rk4 + rr * (KZ + 1);
         float4 r00 = rho[0];
-        // z = 0: phase w
-        float R1 = r00.y * w.x - r00.x * w.y, Rz = 0.f;
-        float Q0 = 0.f, Q1 = 0.f, Q2 = 0.f;
-        if (WF) Q0 = r00.x * w.x + r00.y * w.y;
+        // z = 0: phase w.  Even and odd z accumulate separately (shorter dependence chains)
+        float R1a = r00.y * w.x - r00.x * w.y, Rza = 0.f, R1b = 0.f, Rzb = 0.f;
+        float Q0a = 0.f, Q1a = 0.f, Q2a = 0.f, Q0b = 0.f, Q1b = 0.f, Q2b = 0.f;
+        if (WF) Q0a = r00.x * w.x + r00.y * w.y;
 #pragma unroll
         for (int z = 1; z <= KZ; z++) {
             float4 rp = rho[z];
             float2 e = E[z - 1];
             // w e = (p, s), w conj(e) = (p', s')
             float u1 = w.y * e.y, u2 = w.y * e.x;
-            float p = w.x * e.x - u1, pp = w.x * e.x + u1;
-            float s = w.x * e.y + u2, sp = u2 - w.x * e.y;
+            float p = fmaf(w.x, e.x, -u1), pp = fmaf(w.x, e.x, u1);
+            float s = fmaf(w.x, e.y, u2), sp = fmaf(-w.x, e.y, u2);
             // rho.y ph.x - rho.x ph.y (the sign convention of k_rec_ion) for +z and -z
-            float xp = rp.y * p - rp.x * s, xm = rp.w * pp - rp.z * sp;
+            float xp = fmaf(rp.y, p, -rp.x * s), xm = fmaf(rp.w, pp, -rp.z * sp);
+            float &R1 = (z & 1) ? R1a : R1b, &Rz = (z & 1) ? Rza : Rzb;
             R1 += xp + xm;
-            Rz += (float)z * (xp - xm);
+            Rz = fmaf((float)z, xp - xm, Rz);
             if (WF) {
-                float cp = rp.x * p + rp.y * s, cm = rp.z * pp + rp.w * sp;
+                float cp = fmaf(rp.x, p, rp.y * s), cm = fmaf(rp.z, pp, rp.w * sp);
+                float &Q0 = (z & 1) ? Q0a : Q0b, &Q1 = (z & 1) ? Q1a : Q1b, &Q2 = (z & 1) ? Q2a : Q2b;
                 Q0 += cp + cm;
-                Q1 += (float)z * (cp - cm);
-                Q2 += (float)(z * z) * (cp + cm);
+                Q1 = fmaf((float)z, cp - cm, Q1);
+                Q2 = fmaf((float)(z * z), cp + cm, Q2);
             }
         }
-        double fx = (double)R.nx, fy = (double)R.ny;
+        float R1 = R1a + R1b, Rz = Rza + Rzb;
+        float Q0 = Q0a + Q0b, Q1 = Q1a + Q1b, Q2 = Q2a + Q2b;
+        double fx = (double)R.x, fy = (double)R.y;
         S0 += fx * (double)R1;
         S1 += fy * (double)R1;
         S2 += (double)Rz;
@@ -358,7 +398,7 @@ static TabLayout layout_of(const Engine &e) {
     L.e1 = L.K0 + 1;
     L.z = L.e1 + 2 * L.K1 + 1;
     L.z += L.z & 1;
-    L.w = L.z + ZB * L.nzb;
+    L.w = L.z + ZS * L.nzb;
     return L;
 }
 
@@ -401,7 +441,7 @@ void setup_kspace32(Engine &e, const std::vector<KRow> &rows) {
     e.d_rho_part32 = dalloc<float2>((size_t)chunks * e.nk);
     // ion-pass slices are chosen per launch (ion32_slicing); room for the largest count
     e.nsm = nsm;
-    int maxrows = std::max(1, (48 * 1024) / ((kz_of(L.K2) + 1) * (int)sizeof(float4)));
+    int maxrows = std::max(1, (48 * 1024) / ((kz_of(L.K2) + 1) * (int)sizeof(float4) + (int)sizeof(int2)));
     e.ion32_slices = std::max(std::min(32, e.nrow), ceil_div(e.nrow, maxrows));
     e.d_ion_part32 = dalloc<double>((size_t)e.ion32_slices * e.n * 6);
 }
@@ -413,7 +453,7 @@ static void ion32_slicing(const Engine &e, int cnt, int &rows, int &slices) {
     int iblocks = ceil_div(std::max(cnt, 1), ION32_THREADS);
     int s = std::max(1, 2 * ION32_MIN_BLOCKS * e.nsm / iblocks);
     s = std::min(s, std::min(e.nrow, e.ion32_slices));
-    int maxrows = std::max(1, (48 * 1024) / ((KZ + 1) * (int)sizeof(float4)));
+    int maxrows = std::max(1, (48 * 1024) / ((KZ + 1) * (int)sizeof(float4) + (int)sizeof(int2)));
     s = std::max(s, ceil_div(e.nrow, maxrows));
     rows = ceil_div(e.nrow, s);
     slices = ceil_div(e.nrow, rows);
@@ -449,7 +489,7 @@ void launch_rho32(Engine &e, const double *q, const double3 *mu, bool lq, bool l
     int chunk = ceil_div(std::max(cnt, 1), e.rho32_chunks);
     chunk = ceil_div(chunk, 4) * 4;
     dim3 grid(segblocks, e.rho32_chunks);
-    size_t smem = sizeof(float2) * RHO32_TI * L.w + sizeof(float4) * RHO32_TI;
+    size_t smem = 2 * (sizeof(float2) * RHO32_TI * L.w + sizeof(float4) * RHO32_TI);
     int ps = -1;
     e.prof_begin("k_rho", &ps);
     if (lq && ld) rho32_launch<true, true>(e, grid, smem, cnt, idx, chunk, L, q, mu);
@@ -489,7 +529,7 @@ void launch_ion32(Engine &e, const double *q, const double3 *mu, bool ld, const 
     a.part = e.d_ion_part32;
     a.ld = ld;
     int KZ = kz_of(e.kmax[2]);
-    size_t smem = sizeof(float4) * rows * (KZ + 1);
+    size_t smem = sizeof(float4) * rows * (KZ + 1) + sizeof(int2) * rows;
     dim3 g(ceil_div(std::max(cnt, 1), ION32_THREADS), slices);
     int pi = -1;
     e.prof_begin("k_rec_ion", &pi);
