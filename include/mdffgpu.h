@@ -216,6 +216,26 @@ int mdffgpu_profile_result(mdffgpu_ctx *ctx, double *ms, long long *count, doubl
  * k-space kernels.  No counterpart in the reference. */
 int mdffgpu_fma_peak(int device, int precision, double *tflops);
 
+/* Force matching with adjoint gradients (no counterpart in the reference; the fit tools
+ * of the reference's bin/ call its executable on perturbed inputs).  The parameter
+ * vector of the polarisable silica model, types tSi and tO of the context:
+ *   theta = { A, B, C (Si-O), A, B, C (O-O), q_Si (q_O = -q_Si/2), alpha_O (isotropic,
+ *             A^3), b, c (Tang-Toennies damping of every declared charge-dipole
+ *             damping) }
+ * mdffgpu_fit_set_params writes theta into the context's tables.  mdffgpu_force_match
+ * evaluates the forces F at the converged induced dipoles (a CG solver must be set),
+ * res[0] = sum_i |F_i - F_t,i|^2 and res[1..10] = dL/dtheta of L = scale/2 res[0],
+ * from one adjoint induced-dipole solve (FP64 adjoint arithmetic). */
+#define MDFFGPU_FIT_NPARAM 10
+int mdffgpu_fit_set_params(mdffgpu_ctx *ctx, int tSi, int tO, const double *theta);
+int mdffgpu_force_match(mdffgpu_ctx *ctx, int tSi, int tO, const double *fx_t, const double *fy_t,
+                        const double *fz_t, double scale, double *res);
+/* The same over nconf contexts (independent configurations, one GPU): theta set on all,
+ * targets[c] the AoS (x y z per ion) target forces of context c, res = the sums over
+ * the configurations.  nthreads host threads drive the contexts' streams concurrently. */
+int mdffgpu_fit_batch(mdffgpu_ctx **ctx, int nconf, int tSi, int tO, const double *theta,
+                      const double *const *targets, double scale, int nthreads, double *res);
+
 #ifdef __cplusplus
 }
 #endif

@@ -2,6 +2,7 @@
 // checks, host<->device transfer and conversion of engine exceptions to status codes.
 #include <algorithm>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "engine.cuh"
@@ -339,6 +340,65 @@ int mdffgpu_profile(mdffgpu_ctx *ctx, const char *kernel) {
 int mdffgpu_profile_result(mdffgpu_ctx *ctx, double *ms, long long *count, double *flops) {
     if (!ms || !count || !flops) return MDFFGPU_ERR_ARG;
     return guarded(ctx, [&](Engine &e) { e.prof_result(ms, count, flops); });
+}
+
+int mdffgpu_fit_set_params(mdffgpu_ctx *ctx, int tSi, int tO, const double *theta) {
+    if (!theta) return MDFFGPU_ERR_ARG;
+    return guarded(ctx, [&](Engine &e) { e.set_fit_params(tSi, tO, theta); });
+}
+
+namespace {
+// target forces (AoS) onto the device, then the force-matching evaluation
+void force_match_aos(Engine &e, int tSi, int tO, const double *ft_aos, double scale, double *res) {
+    if (!e.d_ft) e.d_ft = mdffgpu::dalloc<double3>(e.n);
+    MDFF_CK(cudaMemcpyAsync(e.d_ft, ft_aos, sizeof(double3) * e.n, cudaMemcpyHostToDevice, e.stream));
+    e.force_match(e.d_ft, scale, res, tSi, tO);
+}
+}  // namespace
+
+int mdffgpu_force_match(mdffgpu_ctx *ctx, int tSi, int tO, const double *fx_t, const double *fy_t,
+                        const double *fz_t, double scale, double *res) {
+    if (!fx_t || !fy_t || !fz_t || !res) return MDFFGPU_ERR_ARG;
+    return guarded(ctx, [&](Engine &e) {
+        std::vector<double> a((size_t)3 * e.n);
+        for (int i = 0; i < e.n; i++) {
+            a[3 * i] = fx_t[i];
+            a[3 * i + 1] = fy_t[i];
+            a[3 * i + 2] = fz_t[i];
+        }
+        force_match_aos(e, tSi, tO, a.data(), scale, res);
+    });
+}
+
+int mdffgpu_fit_batch(mdffgpu_ctx **ctx, int nconf, int tSi, int tO, const double *theta,
+                      const double *const *targets, double scale, int nthreads, double *res) {
+    if (!ctx || nconf <= 0 || !theta || !targets || !res) return MDFFGPU_ERR_ARG;
+    for (int c = 0; c < nconf; c++)
+        if (!ctx[c] || !ctx[c]->e || !targets[c]) return MDFFGPU_ERR_ARG;
+    int nt = std::max(1, std::min(nthreads, nconf));
+    std::vector<std::vector<double>> part(nconf, std::vector<double>(1 + MDFFGPU_FIT_NPARAM, 0.0));
+    std::vector<int> rc(nconf, MDFFGPU_OK);
+    int device = ctx[0]->e->device;
+    auto work = [&](int t) {
+        cudaSetDevice(device);
+        for (int c = t; c < nconf; c += nt) {
+            rc[c] = guarded(ctx[c], [&](Engine &e) {
+                e.set_fit_params(tSi, tO, theta);
+                force_match_aos(e, tSi, tO, targets[c], scale, part[c].data());
+            });
+            if (rc[c] != MDFFGPU_OK) return;
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; t++) pool.emplace_back(work, t);
+    work(0);
+    for (auto &th : pool) th.join();
+    for (int k = 0; k <= MDFFGPU_FIT_NPARAM; k++) res[k] = 0.0;
+    for (int c = 0; c < nconf; c++) {
+        if (rc[c] != MDFFGPU_OK) return rc[c];
+        for (int k = 0; k <= MDFFGPU_FIT_NPARAM; k++) res[k] += part[c][k];   // configuration order
+    }
+    return MDFFGPU_OK;
 }
 
 }  // extern "C"

@@ -203,6 +203,10 @@ Engine::~Engine() {
     cudaFree(d_ion_part);
     cudaFree(d_coef);
     dfree32();
+    for (void *x : {(void *)d_fpart, (void *)d_fscal, (void *)d_w, (void *)d_lam, (void *)d_sv, (void *)d_fa,
+                    (void *)d_fb, (void *)d_fc, (void *)d_qw, (void *)d_efg_rec, (void *)d_muw, (void *)d_rw,
+                    (void *)d_ft})
+        cudaFree(x);
     cudaFree(d_out);
     cudaFree(d_status);
     if (h_out) cudaFreeHost(h_out);
@@ -400,6 +404,7 @@ void Engine::setup_types() {
     }
     d_pair = dalloc<PairSR>((size_t)nt * nt);
     MDFF_CK(cudaMemcpy(d_pair, pr.data(), sizeof(PairSR) * nt * nt, cudaMemcpyHostToDevice));
+    h_pair = pr;
     std::vector<PairDamp> dm((size_t)nt * nt);
     for (int a = 0; a < nt; a++)
         for (int b = 0; b < nt; b++) {
@@ -411,10 +416,12 @@ void Engine::setup_types() {
             D.b2 = p.pol_damp_b[b][a][b];
             D.c2 = p.pol_damp_c[b][a][b];
             D.k2 = p.pol_damp_k[b][a][b];
-            D.pad = 0;
+            // which of the two directions is a declared damping (parameter updates)
+            D.pad = (p.lpoldamping[a][a][b] ? 1 : 0) | (p.lpoldamping[b][a][b] ? 2 : 0);
         }
     d_damp = dalloc<PairDamp>((size_t)nt * nt);
     MDFF_CK(cudaMemcpy(d_damp, dm.data(), sizeof(PairDamp) * nt * nt, cudaMemcpyHostToDevice));
+    h_damp = dm;
 }
 
 // k-vectors in the reference's generation order (set_param_kmesh, src/kspace.c:64-102),

@@ -178,6 +178,8 @@ struct Engine {
     double3 *d_muzero = nullptr;
     // pair tables
     PairSR *d_pair = nullptr;
+    std::vector<PairSR> h_pair;      // host copies (parameter updates of the force-matching fit)
+    std::vector<PairDamp> h_damp;
     PairDamp *d_damp = nullptr;
 
     // ---- neighbour lists (full lists, row-major [n][cap])
@@ -252,6 +254,15 @@ struct Engine {
     double last_rmsd = 0.0;
     int nbuilds = 0;
 
+    // force matching (fit.cu)
+    double *d_fpart = nullptr, *d_fscal = nullptr;
+    double3 *d_w = nullptr, *d_lam = nullptr, *d_sv = nullptr, *d_fa = nullptr, *d_fb = nullptr, *d_fc = nullptr;
+    double *d_qw = nullptr, *d_efg_rec = nullptr;
+    double3 *d_muw = nullptr;
+    double2 *d_rw = nullptr;
+    double3 *d_ft = nullptr;         // target forces
+    int last_adj_iter = 0;
+
     // one MD step as a CUDA graph (md_steps): the induced-dipole CG loop is a while node
     // whose condition a device kernel sets, so a step needs no host round trip
     bool graph_on = true;
@@ -299,6 +310,14 @@ struct Engine {
     double rmsd_of(const double3 *d_mu, const double3 *d_ef, double *upol_sum);
     void prop_agate(int step);
     void md_steps(int first, int nsteps, double *thermo);
+    // force matching: theta = (A, B, C of Si-O, A, B, C of O-O, q_Si, alpha_O, b, c);
+    // force_match: res[0] = sum |F - F_t|^2, res[1..10] = dL/dtheta for
+    // L = scale/2 sum |F - F_t|^2 (w = scale (F - F_t))
+    void set_fit_params(int tSi, int tO, const double *theta);
+    void force_match(const double3 *d_ft, double scale, double *res, int tSi, int tO);
+    void solve_pim(const double3 *d_b, double3 *d_x, double rtol, int maxit);
+    void fit_reduce(int first, int cnt, int nparts);
+    void coul_forces(const double *d_qv, const double3 *d_muv, bool lq, bool ld, double3 *out);
     bool graph_ok(int step) const;
     void capture_step(int step);
     void drop_graph();

@@ -156,8 +156,9 @@ EXPORTS = (
     "mdffgpu_engforce", "mdffgpu_engforce_nmlj", "mdffgpu_engforce_bhmftd", "mdffgpu_multipole_es",
     "mdffgpu_get_dipoles", "mdffgpu_prop_agate", "mdffgpu_md_steps", "mdffgpu_launch_count",
     "mdffgpu_stream", "mdffgpu_fma_peak", "mdffgpu_profile", "mdffgpu_profile_result",
-    "mdffgpu_build_lists_noalloc",
+    "mdffgpu_build_lists_noalloc", "mdffgpu_fit_set_params", "mdffgpu_force_match", "mdffgpu_fit_batch",
 )
+FIT_NPARAM = 10
 
 _lib = None
 
@@ -196,6 +197,9 @@ def load_library(path: str = LIB_PATH):
         "mdffgpu_get_dipoles": [vp, dp, dp],
         "mdffgpu_prop_agate": [vp, I],
         "mdffgpu_md_steps": [vp, I, I, dp],
+        "mdffgpu_fit_set_params": [vp, I, I, dp],
+        "mdffgpu_force_match": [vp, I, I, dp, dp, dp, D, dp],
+        "mdffgpu_fit_batch": [vpp, I, I, I, dp, C.POINTER(dp), D, I, dp],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -406,3 +410,16 @@ class Engine:
     def stream_handle(self) -> int:
         """The cudaStream_t of this context (for CUDA events around calls)."""
         return int(self.L.mdffgpu_stream(self.h) or 0)
+
+    # ---------------------------------------------------------------- force matching
+    def fit_set_params(self, tSi: int, tO: int, theta):
+        th = np.ascontiguousarray(np.asarray(theta, float))
+        assert th.shape == (FIT_NPARAM,)
+        self._check(self.L.mdffgpu_fit_set_params(self.h, tSi, tO, _dp(th)))
+
+    def force_match(self, tSi: int, tO: int, f_target, scale: float):
+        """(sum |F - F_t|^2, dL/dtheta) for L = scale/2 sum |F - F_t|^2 at the current parameters."""
+        fx, fy, fz = _soa(np.asarray(f_target, float))
+        res = np.zeros(1 + FIT_NPARAM)
+        self._check(self.L.mdffgpu_force_match(self.h, tSi, tO, _dp(fx), _dp(fy), _dp(fz), scale, _dp(res)))
+        return float(res[0]), res[1:].copy()

@@ -1,0 +1,233 @@
+"""Batched force matching of the polarisable silica model with adjoint gradients.
+
+The workload of the fit tools of the reference (bin/ drives the mdff20 executable on
+perturbed inputs and compares forces): many independent configurations, one force-
+matching loss and its gradient with respect to the force-field parameters
+
+    theta = (A, B, C of Si-O, A, B, C of O-O, q_Si (q_O = -q_Si/2), alpha_O, b, c)
+
+with L(theta) = sum_c sum_i |F_i(theta) - F_i^target|^2 / (3 N_total).  The forces come
+from the CUDA engine at the converged induced dipoles; the gradient from one adjoint
+induced-dipole solve per configuration (mdffgpu_force_match, mdffgpu_fit_batch).
+
+* ``ewald_tune``: the Ewald splitting alpha, the real-space cutoff and kmax of each
+  configuration, chosen for a fixed accuracy at the lowest estimated cost.
+* ``config4``: the seeded set of configurations (ion counts uniform over 96..1536 in
+  steps of 96, Si:O = 1:2, 2.2 g/cm^3) with their tuned Ewald parameters.
+* ``ForceMatchBatch``: engines for a set of configurations, loss and gradient at theta.
+* ``ForceMatchLoss``: torch.autograd.Function over ForceMatchBatch.
+"""
+from __future__ import annotations
+
+import copy
+import ctypes as C
+import math
+from dataclasses import dataclass
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import synth
+from .system import System
+
+PARAM_NAMES = ("A_SiO", "B_SiO", "C_SiO", "A_OO", "B_OO", "C_OO", "q_Si", "alpha_O", "b", "c")
+NPARAM = len(PARAM_NAMES)
+O_TYPE, SI_TYPE = synth.O, synth.SI
+NUMBER_DENSITY = 0.066151   # silica ions per A^3 at 2.2 g/cm^3
+
+
+# ---------------------------------------------------------------------------- parameters
+def theta_of(s: System) -> np.ndarray:
+    """The parameter vector of a polarisable silica System (types O = 0, Si = 1)."""
+    o, si = O_TYPE, SI_TYPE
+    damp = [d for d in s.poldamp]
+    b = damp[0][3] if damp else 0.0
+    c = damp[0][4] if damp else 0.0
+    return np.array([s.Abhmftd[si, o], s.Bbhmftd[si, o], s.Cbhmftd[si, o],
+                     s.Abhmftd[o, o], s.Bbhmftd[o, o], s.Cbhmftd[o, o],
+                     s.qit[si], s.polit[o][0, 0], b, c], float)
+
+
+def with_theta(s: System, theta) -> System:
+    """A copy of `s` carrying the parameters `theta` (host side, e.g. for the oracle)."""
+    t = np.asarray(theta, float)
+    o, si = O_TYPE, SI_TYPE
+    s2 = copy.deepcopy(s)
+    for arr, k in ((s2.Abhmftd, 0), (s2.Bbhmftd, 1), (s2.Cbhmftd, 2)):
+        arr[si, o] = arr[o, si] = t[k]
+        arr[o, o] = t[3 + k]
+    s2.qit = list(s2.qit)
+    s2.qit[si] = t[6]
+    s2.qit[o] = -0.5 * t[6]
+    s2.polit = np.array(s2.polit, float)
+    s2.polit[o] = np.eye(3) * t[7]
+    s2.poldamp = [(d[0], d[1], d[2], t[8], t[9], d[5]) for d in s2.poldamp]
+    return s2
+
+
+def perturbed_theta(theta0, seed: int = 5, frac: float = 0.05) -> np.ndarray:
+    """theta0 with every component scaled by 1 + frac or 1 - frac (seeded signs)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    sign = rng.choice([-1.0, 1.0], size=len(theta0))
+    return np.asarray(theta0, float) * (1.0 + frac * sign)
+
+
+# ---------------------------------------------------------------------------- autotuner
+@dataclass
+class EwaldChoice:
+    alpha: float
+    rc: float        # real-space cutoff, A
+    kmax: int
+    cost: float      # estimated flops per force evaluation
+
+
+def _erfc_root(eps: float) -> float:
+    """x with erfc(x) = eps (bisection)."""
+    lo, hi = 0.0, 10.0
+    for _ in range(80):
+        mid = 0.5 * (lo + hi)
+        if math.erfc(mid) > eps:
+            lo = mid
+        else:
+            hi = mid
+    return 0.5 * (lo + hi)
+
+
+def ewald_tune(L: float, n: int, eps: float = 1e-6, rc_max: float = 10.0, skin: float = 0.5,
+               pair_flops: float = 300.0, kspace_flops: float = 35.0) -> EwaldChoice:
+    """Ewald parameters of a cubic box of side L holding n ions at accuracy eps.
+
+    For a real-space cutoff rc the splitting parameter makes the real-space truncation
+    erfc(alpha rc) = eps, and kmax is the smallest integer with
+    exp(-(pi kmax / (alpha L))^2) <= eps (the reciprocal-space truncation).  The
+    estimated cost of one force evaluation, pair_flops per real-space pair within rc
+    plus kspace_flops per (ion, k) of the half k-box, is minimised over rc in
+    [3 A, min(rc_max, L/2 - skin)] (minimum image)."""
+    rho = n / L ** 3
+    xr = _erfc_root(eps)
+    xk = math.sqrt(-math.log(eps))
+    rc_hi = min(rc_max, 0.5 * L - skin)
+    if rc_hi < 3.0:
+        raise ValueError("box too small for the minimum-image real-space sum")
+    best = None
+    for rc in np.arange(3.0, rc_hi + 1e-9, 0.05):
+        alpha = xr / rc
+        kmax = max(1, math.ceil(alpha * L * xk / math.pi))
+        nk = kmax + kmax * (2 * kmax + 1) + kmax * (2 * kmax + 1) ** 2
+        cost = n * (pair_flops * 0.5 * rho * 4.0 / 3.0 * math.pi * rc ** 3 + kspace_flops * nk)
+        if best is None or cost < best.cost:
+            best = EwaldChoice(alpha=float(alpha), rc=float(rc), kmax=int(kmax), cost=float(cost))
+    return best
+
+
+# ---------------------------------------------------------------------------- config 4
+def config4_sizes(nconf: int = 512, seed: int = 4) -> List[int]:
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return [96 * int(k) for k in rng.integers(1, 17, size=nconf)]
+
+
+def config4(nconf: int = 512, seed: int = 4, eps: float = 1e-6, conv_tol: float = 1e-8,
+            sizes: Optional[Sequence[int]] = None) -> List[System]:
+    """The batched force-matching set: polarisable silica configurations (config 3's
+    model) of seeded sizes, random sequential placement with the PIM minimum
+    separations, each with its tuned Ewald parameters (single points, skin 0.5 A)."""
+    sizes = list(sizes) if sizes is not None else config4_sizes(nconf, seed)
+    out = []
+    for c, n in enumerate(sizes):
+        n_si = n // 3
+        L = (n / NUMBER_DENSITY) ** (1.0 / 3.0)
+        ch = ewald_tune(L, n, eps=eps)
+        rc_sr = min(7.0, ch.rc)
+        s = synth.silica(n_si, seed=seed * 100003 + c, polarizable=True, rc_sr=rc_sr, rc_lr=ch.rc, skin=0.5,
+                         alpha=ch.alpha, kmax=ch.kmax, integrator="nve-vv", temp=0.0, velocities=False,
+                         conv_tol=conv_tol, dmin=synth.PIM_DMIN, L=L)
+        s.lstatic = True
+        s.name = f"fit{c}_{n}"
+        out.append(s)
+    return out
+
+
+# ---------------------------------------------------------------------------- batch
+class ForceMatchBatch:
+    """Engines for a list of configurations; loss and adjoint gradient at theta."""
+
+    def __init__(self, systems: Sequence[System], targets: Sequence[np.ndarray], device: int = -1,
+                 precision: int = 0, threads: int = 8):
+        from .engine import PIM_CG, Engine, load_library
+        from .cellmath import wrap_positions
+        self.L = load_library()
+        self.systems = list(systems)
+        self.engines = []
+        for s in self.systems:
+            e = Engine(s, positions=wrap_positions(s.cell, s.pos), device=device, precision=precision,
+                       pim_solver=PIM_CG)
+            e.gen_verletlist()
+            self.engines.append(e)
+        self.targets = [np.ascontiguousarray(np.asarray(t, float).reshape(-1, 3)) for t in targets]
+        self.ntot = sum(s.nion for s in self.systems)
+        self.scale = 2.0 / (3.0 * self.ntot)
+        self.threads = threads
+        n = len(self.engines)
+        self._ctx = (C.c_void_p * n)(*[e.h.value for e in self.engines])
+        self._tgt = (C.POINTER(C.c_double) * n)(*[t.ctypes.data_as(C.POINTER(C.c_double))
+                                                  for t in self.targets])
+
+    def loss_grad(self, theta) -> tuple:
+        """(L, dL/dtheta) of L = sum |F - F_t|^2 / (3 N_total)."""
+        th = np.ascontiguousarray(np.asarray(theta, float))
+        res = np.zeros(1 + NPARAM)
+        rc = self.L.mdffgpu_fit_batch(self._ctx, len(self.engines), SI_TYPE, O_TYPE,
+                                      th.ctypes.data_as(C.POINTER(C.c_double)), self._tgt, self.scale,
+                                      self.threads, res.ctypes.data_as(C.POINTER(C.c_double)))
+        if rc != 0:
+            from .engine import MdffgpuError
+            raise MdffgpuError(rc, "mdffgpu_fit_batch failed")
+        return 0.5 * self.scale * res[0], res[1:].copy()
+
+    def forces(self, theta) -> List[np.ndarray]:
+        out = []
+        for e in self.engines:
+            e.fit_set_params(SI_TYPE, O_TYPE, theta)
+            e.engforce()
+            out.append(e.forces())
+        return out
+
+    def close(self):
+        for e in self.engines:
+            e.close()
+        self.engines = []
+
+
+def target_forces(systems: Sequence[System], theta_t, device: int = -1) -> List[np.ndarray]:
+    """FP64 forces of every configuration at the parameters theta_t (the fit targets)."""
+    from .engine import PIM_CG, Engine
+    from .cellmath import wrap_positions
+    out = []
+    for s in systems:
+        e = Engine(s, positions=wrap_positions(s.cell, s.pos), device=device, pim_solver=PIM_CG)
+        e.gen_verletlist()
+        e.fit_set_params(SI_TYPE, O_TYPE, theta_t)
+        e.engforce()
+        out.append(e.forces())
+        e.close()
+    return out
+
+
+try:
+    import torch
+
+    class ForceMatchLoss(torch.autograd.Function):
+        """L(theta) of a ForceMatchBatch; backward returns the adjoint gradient."""
+
+        @staticmethod
+        def forward(ctx, theta, batch: ForceMatchBatch):
+            loss, grad = batch.loss_grad(theta.detach().cpu().double().numpy())
+            ctx.save_for_backward(torch.as_tensor(grad, dtype=theta.dtype, device=theta.device))
+            return torch.as_tensor(loss, dtype=theta.dtype, device=theta.device)
+
+        @staticmethod
+        def backward(ctx, gout):
+            (grad,) = ctx.saved_tensors
+            return gout * grad, None
+except ImportError:   # torch is optional for the C-ABI users
+    ForceMatchLoss = None
