@@ -50,7 +50,7 @@ def theta_of(s: System) -> np.ndarray:
 
 def with_theta(s: System, theta) -> System:
     """A copy of `s` carrying the parameters `theta` (host side, e.g. for the oracle)."""
-    t = np.asarray(theta, float)
+    t = [float(x) for x in np.asarray(theta, float)]
     o, si = O_TYPE, SI_TYPE
     s2 = copy.deepcopy(s)
     for arr, k in ((s2.Abhmftd, 0), (s2.Bbhmftd, 1), (s2.Cbhmftd, 2)):
@@ -147,12 +147,39 @@ def config4(nconf: int = 512, seed: int = 4, eps: float = 1e-6, conv_tol: float 
     return out
 
 
+# ---------------------------------------------------------------------------- sharding
+def shard(sizes: Sequence[int], world: int) -> List[List[int]]:
+    """Configuration indices per rank: size-balanced greedy bins (largest first to the
+    least-loaded rank; cost ~ ions), each bin in ascending order."""
+    load = [0.0] * world
+    bins: List[List[int]] = [[] for _ in range(world)]
+    for c in sorted(range(len(sizes)), key=lambda k: (-sizes[k], k)):
+        r = min(range(world), key=lambda k: (load[k], k))
+        bins[r].append(c)
+        load[r] += sizes[c]
+    return [sorted(b) for b in bins]
+
+
+def allreduce_loss_grad(loss: float, grad, group=None):
+    """Sum (loss, grad) over the ranks of a torch.distributed group (one all-reduce of
+    1 + NPARAM doubles: the only exchange of the sharded fit)."""
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend(group) == "nccl" else "cpu"
+    t = torch.tensor([loss] + list(np.asarray(grad, float)), dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    v = t.cpu().numpy()
+    return float(v[0]), v[1:].copy()
+
+
 # ---------------------------------------------------------------------------- batch
 class ForceMatchBatch:
     """Engines for a list of configurations; loss and adjoint gradient at theta."""
 
     def __init__(self, systems: Sequence[System], targets: Sequence[np.ndarray], device: int = -1,
-                 precision: int = 0, threads: int = 8):
+                 precision: int = 0, threads: int = 8, ntot: Optional[int] = None):
+        """ntot: ions of the whole fit when these systems are one shard of it (the loss is
+        normalised by 3 ntot), default the ions of these systems."""
         from .engine import PIM_CG, Engine, load_library
         from .cellmath import wrap_positions
         self.L = load_library()
@@ -164,7 +191,7 @@ class ForceMatchBatch:
             e.gen_verletlist()
             self.engines.append(e)
         self.targets = [np.ascontiguousarray(np.asarray(t, float).reshape(-1, 3)) for t in targets]
-        self.ntot = sum(s.nion for s in self.systems)
+        self.ntot = ntot if ntot is not None else sum(s.nion for s in self.systems)
         self.scale = 2.0 / (3.0 * self.ntot)
         self.threads = threads
         n = len(self.engines)

@@ -1,0 +1,98 @@
+"""Force-matching loss and adjoint gradient on the GPU (through the C ABI) against the
+reference's FP64 forces and finite-difference gradient (tests/golden/fit96.npz), against
+finite differences of the GPU loss itself, batched vs single evaluations, the
+torch.autograd wrapper and the mixed-precision engine."""
+import numpy as np
+import pytest
+
+from mdff20_b200 import fit
+from mdff20_b200.engine import MIXED, PIM_CG, Engine
+from tests.helpers import load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    return float(np.max(np.abs(np.asarray(a) - np.asarray(b)) / np.maximum(np.abs(b), 1e-30)))
+
+
+def test_gradient_vs_reference_finite_differences():
+    g = load_golden("fit96")
+    s = fit.config4(sizes=[96], conv_tol=1e-11)[0]
+    pos = g["r_in"].reshape(-1, 3)
+    e = Engine(s, positions=pos, pim_solver=PIM_CG)
+    e.gen_verletlist()
+    e.fit_set_params(fit.SI_TYPE, fit.O_TYPE, g["theta0"])
+    scale = 2.0 / (3.0 * s.nion)
+    sq, grad = e.force_match(fit.SI_TYPE, fit.O_TYPE, g["f_t"].reshape(-1, 3), scale)
+    assert np.abs(e.forces() - g["f0"].reshape(-1, 3)).max() < 1e-8
+    loss = 0.5 * scale * sq
+    assert abs(loss - float(g["loss0"][0])) < 1e-8 * float(g["loss0"][0])
+    # the reference gradient is a central difference (step 1e-5 relative): 1e-4 bar
+    assert _rel(grad, g["grad_fd"]) < 1e-4, (grad, g["grad_fd"])
+    e.close()
+
+
+def test_gradient_vs_gpu_finite_differences():
+    systems = fit.config4(sizes=[96, 192], conv_tol=1e-11)
+    th0 = fit.theta_of(systems[0])
+    targets = fit.target_forces(systems, fit.perturbed_theta(th0))
+    b = fit.ForceMatchBatch(systems, targets, threads=2)
+    _, grad = b.loss_grad(th0)
+    for k in range(fit.NPARAM):
+        h = 1e-5 * abs(th0[k])
+        tp, tm = th0.copy(), th0.copy()
+        tp[k] += h
+        tm[k] -= h
+        gfd = (b.loss_grad(tp)[0] - b.loss_grad(tm)[0]) / (2.0 * h)
+        assert abs(grad[k] - gfd) <= 1e-4 * abs(gfd), (fit.PARAM_NAMES[k], grad[k], gfd)
+    b.close()
+
+
+def test_batch_is_the_sum_of_single_evaluations():
+    systems = fit.config4(sizes=[96, 288, 192])
+    th0 = fit.theta_of(systems[0])
+    targets = fit.target_forces(systems, fit.perturbed_theta(th0, seed=9))
+    b = fit.ForceMatchBatch(systems, targets, threads=3)
+    loss, grad = b.loss_grad(th0)
+    sq, gs = 0.0, np.zeros(fit.NPARAM)
+    for e, t in zip(b.engines, targets):
+        e.fit_set_params(fit.SI_TYPE, fit.O_TYPE, th0)
+        a, g = e.force_match(fit.SI_TYPE, fit.O_TYPE, t, b.scale)
+        sq += a
+        gs += g
+    assert abs(loss - 0.5 * b.scale * sq) <= 1e-12 * loss
+    assert _rel(grad, gs) < 1e-10
+    b.close()
+
+
+def test_torch_autograd_wrapper():
+    import torch
+    systems = fit.config4(sizes=[96, 192], conv_tol=1e-10)
+    th0 = fit.theta_of(systems[0])
+    targets = fit.target_forces(systems, fit.perturbed_theta(th0))
+    b = fit.ForceMatchBatch(systems, targets, threads=2)
+    theta = torch.tensor(th0, dtype=torch.float64, requires_grad=True)
+    loss = fit.ForceMatchLoss.apply(theta, b)
+    loss.backward()
+    _, grad = b.loss_grad(th0)
+    assert np.allclose(theta.grad.numpy(), grad, rtol=1e-12, atol=0.0)
+    # directional derivative along a mixed direction against a central difference
+    v = np.array([1.0, 1e-4, 1.0, 1.0, 1e-4, 1.0, 1e-4, 1e-4, 1e-4, 1e-4]) * th0 * 1e-5
+    d_fd = (b.loss_grad(th0 + v)[0] - b.loss_grad(th0 - v)[0]) / 2.0
+    assert abs(float(np.dot(grad, v)) - d_fd) <= 1e-4 * abs(d_fd)
+    b.close()
+
+
+def test_mixed_precision_gradient_close_to_fp64():
+    systems = fit.config4(sizes=[192, 480], conv_tol=1e-8)
+    th0 = fit.theta_of(systems[0])
+    targets = fit.target_forces(systems, fit.perturbed_theta(th0))
+    ref = fit.ForceMatchBatch(systems, targets, threads=2)
+    mix = fit.ForceMatchBatch(systems, targets, threads=2, precision=MIXED)
+    l64, g64 = ref.loss_grad(th0)
+    l32, g32 = mix.loss_grad(th0)
+    assert abs(l32 - l64) < 1e-4 * l64
+    assert np.max(np.abs(g32 - g64)) < 1e-4 * np.max(np.abs(g64))
+    ref.close()
+    mix.close()
