@@ -31,6 +31,7 @@ import subprocess
 import sys
 import threading
 import time
+from typing import Optional
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
@@ -52,6 +53,9 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--roof-kernel", default="k_rho")
     ap.add_argument("--profile-steps", type=int, default=3)
+    ap.add_argument("--fit-configs", type=int, default=512, help="batched fit configurations (0: skip)")
+    ap.add_argument("--fit-evals", type=int, default=3)
+    ap.add_argument("--fit-threads", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -146,6 +150,90 @@ def dist_setup(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
         pg = dist
     return world, rank, local, pg
+
+
+def fit_cpu_baseline(sizes, sample: int = 4) -> dict:
+    """The reference's own code computing force-matching gradients the only way it can:
+    central finite differences, 2 x 10 + 1 force evaluations per configuration, on a
+    sample of the configurations (every len/sample-th), all host cores."""
+    from mdff20_b200 import fit
+    from oracle import ref
+    threads = os.cpu_count() or 1
+    idx = list(range(0, len(sizes), max(1, len(sizes) // sample)))[:sample]
+    if not ref.available("tim"):
+        return {"value": None, "unit": "config-gradients/s", "error": "compiled reference not built"}
+    t0 = time.perf_counter()
+    for c in idx:
+        s = fit.config4_one(c, sizes[c])
+        th0 = fit.theta_of(s)
+        for k in range(2 * fit.NPARAM + 1):
+            th = th0.copy()
+            if k:
+                th[(k - 1) // 2] *= 1.0 + (1e-5 if k % 2 else -1e-5)
+            ref.run(fit.with_theta(s, th), "engforce", variant="tim", threads=threads, timeout=600)
+    wall = time.perf_counter() - t0
+    return {"value": len(idx) / wall, "unit": "config-gradients/s", "cores": threads, "kind": "reference",
+            "sample": f"configurations {idx} (ions {[sizes[c] for c in idx]}) of the set, each gradient by "
+                      f"{2 * fit.NPARAM + 1} reference force evaluations (central differences), "
+                      f"mdff20 -O3 -Ofast -fopenmp, OMP_NUM_THREADS={threads}, {wall:.1f} s"}
+
+
+def run_fit(args, world, rank, dev, pg) -> Optional[dict]:
+    """Batched force matching (config 4): loss + adjoint gradient over all configurations
+    per evaluation, FP64 and mixed engines; configurations sharded over the ranks, one
+    all-reduce of (loss, gradient) per evaluation."""
+    import numpy as np
+    import torch
+
+    from mdff20_b200 import fit
+    from mdff20_b200.engine import FP64, MIXED
+    sizes = fit.config4_sizes(args.fit_configs)
+    mine = fit.shard(sizes, world)[rank]
+    t0 = time.perf_counter()
+    systems = fit.config4(sizes=sizes, indices=mine, workers=min(16, os.cpu_count() or 1))
+    gen_s = time.perf_counter() - t0
+    th0 = fit.theta_of(systems[0])
+    tht = fit.perturbed_theta(th0)
+    b = fit.ForceMatchBatch(systems, None, device=dev, precision=FP64, threads=args.fit_threads, ntot=sum(sizes))
+    b.set_targets(b.forces(tht))   # FP64 forces at the perturbed parameters
+    res = {}
+    for label, prec in (("fp64", FP64), ("mixed", MIXED)):
+        b.set_precision(prec)
+        b.loss_grad(th0)                       # warm-up (first CG solves, allocations)
+        if pg is not None:
+            pg.barrier()
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        for _ in range(args.fit_evals):
+            loss, grad = b.loss_grad(th0)      # synchronous: every configuration's stream done
+            if pg is not None:
+                loss, grad = fit.allreduce_loss_grad(loss, grad)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t
+        if pg is not None:
+            tt = torch.tensor([dt], device=f"cuda:{dev}", dtype=torch.float64)
+            pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+            dt = float(tt.item())
+        res[label] = {"value": len(sizes) * args.fit_evals / dt, "ms_per_eval": 1000.0 * dt / args.fit_evals,
+                      "loss": loss, "grad": [float(x) for x in grad]}
+    b.close()
+    g64, g32 = np.array(res["fp64"]["grad"]), np.array(res["mixed"]["grad"])
+    out = {"metric": "batched fit-gradients/s", "unit": "config-gradients/s", "value": res["mixed"]["value"],
+           "fp64": res["fp64"]["value"], "configs": len(sizes), "ions": int(sum(sizes)), "evals": args.fit_evals,
+           "ms_per_eval_mixed": res["mixed"]["ms_per_eval"], "ms_per_eval_fp64": res["fp64"]["ms_per_eval"],
+           "grad_max_rel_err_mixed_vs_fp64": float(np.max(np.abs(g32 - g64)) / np.max(np.abs(g64))),
+           "loss_rel_err_mixed_vs_fp64": abs(res["mixed"]["loss"] - res["fp64"]["loss"]) / res["fp64"]["loss"],
+           "params": list(fit.PARAM_NAMES), "host_threads": args.fit_threads, "setup_s": round(gen_s, 1),
+           "timing": "host clock around the synchronous batched C-ABI call (host parameters in, host loss and "
+                     "gradient out, target forces uploaded per call), device synchronised on both sides, "
+                     "max over ranks",
+           "data": "synthetic: seeded random silica configurations, targets = FP64 forces at +-5% parameters"}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            out["cpu_baseline"] = fit_cpu_baseline(sizes)
+        except Exception as exc:  # reported, not fatal
+            out["cpu_baseline"] = {"value": None, "error": str(exc)[:200]}
+    return out
 
 
 def run_reference(args):
@@ -311,8 +399,12 @@ def run_ours(args):
                 line["cpu_baseline"] = cpu_baseline(s, 2)
             except Exception as exc:  # reported, not fatal
                 line["cpu_baseline"] = {"value": None, "error": str(exc)[:200]}
-        print(json.dumps(line), flush=True)
     eng.close()
+    fit_line = run_fit(args, world, rank, dev, pg) if args.fit_configs > 0 else None
+    if rank == 0:
+        if fit_line is not None:
+            line["fit"] = fit_line
+        print(json.dumps(line), flush=True)
     if pg is not None:
         pg.barrier()
         pg.destroy_process_group()

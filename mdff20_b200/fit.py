@@ -126,25 +126,41 @@ def config4_sizes(nconf: int = 512, seed: int = 4) -> List[int]:
     return [96 * int(k) for k in rng.integers(1, 17, size=nconf)]
 
 
+def config4_one(c: int, n: int, seed: int = 4, eps: float = 1e-6, conv_tol: float = 1e-8) -> System:
+    """Configuration number c (n ions) of the batched force-matching set."""
+    n_si = n // 3
+    L = (n / NUMBER_DENSITY) ** (1.0 / 3.0)
+    ch = ewald_tune(L, n, eps=eps)
+    rc_sr = min(7.0, ch.rc)
+    s = synth.silica(n_si, seed=seed * 100003 + c, polarizable=True, rc_sr=rc_sr, rc_lr=ch.rc, skin=0.5,
+                     alpha=ch.alpha, kmax=ch.kmax, integrator="nve-vv", temp=0.0, velocities=False,
+                     conv_tol=conv_tol, dmin=synth.PIM_DMIN, L=L)
+    s.lstatic = True
+    s.name = f"fit{c}_{n}"
+    return s
+
+
+def _one(args):
+    return config4_one(*args)
+
+
 def config4(nconf: int = 512, seed: int = 4, eps: float = 1e-6, conv_tol: float = 1e-8,
-            sizes: Optional[Sequence[int]] = None) -> List[System]:
+            sizes: Optional[Sequence[int]] = None, indices: Optional[Sequence[int]] = None,
+            workers: int = 1) -> List[System]:
     """The batched force-matching set: polarisable silica configurations (config 3's
     model) of seeded sizes, random sequential placement with the PIM minimum
-    separations, each with its tuned Ewald parameters (single points, skin 0.5 A)."""
+    separations, each with its tuned Ewald parameters (single points, skin 0.5 A).
+    indices: which configurations of the set (default all); workers > 1 builds them in
+    that many spawned processes."""
     sizes = list(sizes) if sizes is not None else config4_sizes(nconf, seed)
-    out = []
-    for c, n in enumerate(sizes):
-        n_si = n // 3
-        L = (n / NUMBER_DENSITY) ** (1.0 / 3.0)
-        ch = ewald_tune(L, n, eps=eps)
-        rc_sr = min(7.0, ch.rc)
-        s = synth.silica(n_si, seed=seed * 100003 + c, polarizable=True, rc_sr=rc_sr, rc_lr=ch.rc, skin=0.5,
-                         alpha=ch.alpha, kmax=ch.kmax, integrator="nve-vv", temp=0.0, velocities=False,
-                         conv_tol=conv_tol, dmin=synth.PIM_DMIN, L=L)
-        s.lstatic = True
-        s.name = f"fit{c}_{n}"
-        out.append(s)
-    return out
+    idx = list(indices) if indices is not None else list(range(len(sizes)))
+    jobs = [(c, sizes[c], seed, eps, conv_tol) for c in idx]
+    if workers > 1 and len(jobs) > 1:
+        import concurrent.futures as cf
+        import multiprocessing as mp
+        with cf.ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+            return list(ex.map(_one, jobs, chunksize=max(1, len(jobs) // (4 * workers))))
+    return [_one(j) for j in jobs]
 
 
 # ---------------------------------------------------------------------------- sharding
@@ -176,7 +192,7 @@ def allreduce_loss_grad(loss: float, grad, group=None):
 class ForceMatchBatch:
     """Engines for a list of configurations; loss and adjoint gradient at theta."""
 
-    def __init__(self, systems: Sequence[System], targets: Sequence[np.ndarray], device: int = -1,
+    def __init__(self, systems: Sequence[System], targets: Optional[Sequence[np.ndarray]], device: int = -1,
                  precision: int = 0, threads: int = 8, ntot: Optional[int] = None):
         """ntot: ions of the whole fit when these systems are one shard of it (the loss is
         normalised by 3 ntot), default the ions of these systems."""
@@ -190,14 +206,18 @@ class ForceMatchBatch:
                        pim_solver=PIM_CG)
             e.gen_verletlist()
             self.engines.append(e)
-        self.targets = [np.ascontiguousarray(np.asarray(t, float).reshape(-1, 3)) for t in targets]
         self.ntot = ntot if ntot is not None else sum(s.nion for s in self.systems)
         self.scale = 2.0 / (3.0 * self.ntot)
         self.threads = threads
         n = len(self.engines)
         self._ctx = (C.c_void_p * n)(*[e.h.value for e in self.engines])
-        self._tgt = (C.POINTER(C.c_double) * n)(*[t.ctypes.data_as(C.POINTER(C.c_double))
-                                                  for t in self.targets])
+        if targets is None:   # set later (set_targets), e.g. from forces() of this batch
+            targets = [np.zeros((s.nion, 3)) for s in self.systems]
+        self.set_targets(targets)
+
+    def set_precision(self, precision: int):
+        for e in self.engines:
+            e._check(e.L.mdffgpu_set_precision(e.h, precision))
 
     def loss_grad(self, theta) -> tuple:
         """(L, dL/dtheta) of L = sum |F - F_t|^2 / (3 N_total)."""
@@ -210,6 +230,12 @@ class ForceMatchBatch:
             from .engine import MdffgpuError
             raise MdffgpuError(rc, "mdffgpu_fit_batch failed")
         return 0.5 * self.scale * res[0], res[1:].copy()
+
+    def set_targets(self, targets: Sequence[np.ndarray]):
+        self.targets = [np.ascontiguousarray(np.asarray(t, float).reshape(-1, 3)) for t in targets]
+        n = len(self.engines)
+        self._tgt = (C.POINTER(C.c_double) * n)(*[t.ctypes.data_as(C.POINTER(C.c_double))
+                                                  for t in self.targets])
 
     def forces(self, theta) -> List[np.ndarray]:
         out = []
