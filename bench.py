@@ -2,14 +2,18 @@
 """Benchmark: MD ion-steps/s of the N=24,000 polarisable silica Nose-Hoover-chain step.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--precision fp64|mixed] [--solver cg|reference]
+                    [--precision mixed|fp64] [--solver fused|cg|reference]
+                    [--fp64-steps K64] [--fit-configs C] [--fit-evals E]
 
-A step is one MD step (src/md.c:229-241: prop_agate = NHC half-step, velocity-Verlet
+MD: a step is one MD step (src/md.c:229-241: prop_agate = NHC half-step, velocity-Verlet
 drift, force evaluation with the induced-dipole solve, kick, NHC half-step; then
 check_verletlist) of the seeded 24,000-ion system (8000 Si + 16000 O, beta-cristobalite
 10^3 supercell with 0.05 Å displacements, 2.20 g/cm^3, L = 71.3 Å, MB velocities at
 2500 K), Buckingham rc 7 Å, Ewald alpha 0.32, rc 10 Å, kmax 14, skin 1 Å, PIM with
-ASPC order 4 and residual 1e-6.
+ASPC order 4 and residual 1e-6.  `value` is the mixed-precision step (fused CG, each
+step a CUDA graph); `fp64_plain` the FP64 step with the plain CG on the same system.
+Fit (`fit`): one evaluation = force-matching loss + adjoint gradient over the seeded
+set of 512 configurations (427k ions); metric config-gradients/s.
 
 ours      : state resident on the GPU; each timed step is bracketed by CUDA events on
             the engine stream, with a 256 MB L2 flush between steps (not timed).
@@ -18,8 +22,9 @@ ours      : state resident on the GPU; each timed step is bracketed by CUDA even
             forces downloaded, every step.
 reference : the reference's own CPU code (oracle/_ref, -O3 -Ofast -fopenmp) on all host
             cores, on a bounded sample of steps of the same system.
-N > 1 GPUs: one process per GPU (torchrun), an independent replica per rank (the path
-has no collective; weak scaling); time = max over ranks.
+N > 1 GPUs: one process per GPU (torchrun).  MD: an independent replica per rank (the
+path has no collective; weak scaling).  Fit: configurations sharded over the ranks,
+one all-reduce of (loss, gradient) per evaluation.  Times = max over ranks.
 """
 from __future__ import annotations
 
@@ -45,11 +50,13 @@ WORKLOAD = ("pim_silica_nvt_24000: 8000 Si + 16000 O, 2.20 g/cm^3, L=71.3 A, Buc
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
-    ap.add_argument("--solver", choices=["cg", "fused", "reference"], default="cg")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
+    ap.add_argument("--solver", choices=["cg", "fused", "reference"], default="fused")
+    ap.add_argument("--fp64-steps", type=int, default=100, help="steps of the plain FP64 path timed beside")
+    ap.add_argument("--force-check", type=int, default=1, help="mixed: force error against an FP64 evaluation")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--roof-kernel", default="k_rho")
     ap.add_argument("--profile-steps", type=int, default=3)
@@ -152,6 +159,17 @@ def dist_setup(args):
     return world, rank, local, pg
 
 
+def h_drift(th, nion: int) -> dict:
+    """Conserved-quantity drift over recorded steps: H_tot = E_kin + U_lj + U_bh + U_coul
+    + U_pol + e_nvt (info_thermo, src/thermo.c:12-35), thermo columns 0-5 (eV)."""
+    import numpy as np
+    h = th[:, 0] + th[:, 1] + th[:, 2] + th[:, 3] + th[:, 4] + th[:, 5]
+    steps = max(1, len(h) - 1)
+    return {"h_start_ev": float(h[0]), "h_end_ev": float(h[-1]),
+            "ev_per_ion_per_step": float((h[-1] - h[0]) / (nion * steps)),
+            "rel": float((h[-1] - h[0]) / abs(h[0])), "steps": int(len(h))}
+
+
 def fit_cpu_baseline(sizes, sample: int = 4) -> dict:
     """The reference's own code computing force-matching gradients the only way it can:
     central finite differences, 2 x 10 + 1 force evaluations per configuration, on a
@@ -251,6 +269,11 @@ def run_reference(args):
                 "cpu_baseline": cb,
                 "e2e": {"value": cb["value"], "unit": "ion-steps/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
+        if args.fit_configs > 0:
+            from mdff20_b200 import fit
+            fb = fit_cpu_baseline(fit.config4_sizes(args.fit_configs))
+            line["fit"] = {"metric": "batched fit-gradients/s", "unit": "config-gradients/s",
+                           "value": fb.get("value"), "cpu_baseline": fb}
         print(json.dumps(line), flush=True)
     if pg is not None:
         pg.barrier()
@@ -276,7 +299,7 @@ def run_ours(args):
     eng.gen_verletlist()
     eng.engforce()                                    # forces at t=0 (src/md.c:209)
     force_err = None
-    if prec == MIXED:
+    if prec == MIXED and args.force_check:
         # relative RMS force error of the mixed path against the FP64 path at t=0
         ref = Engine(s, positions=pos, device=dev, precision=FP64, pim_solver=solver)
         ref.gen_verletlist()
@@ -332,6 +355,39 @@ def run_ours(args):
         total_ms = float(t.item())
     th = np.array(thermo)
     value = world * s.nion * args.steps / (total_ms / 1000.0)
+
+    # ------------------------------------------------ the plain FP64 path (FP64, CG), same system
+    fp64_plain = None
+    if prec == MIXED and args.fp64_steps > 0:
+        e64 = Engine(s, positions=pos, device=dev, precision=FP64, pim_solver=PIM_CG)
+        e64.gen_verletlist()
+        e64.engforce()
+        if args.warmup > 0:
+            e64.md_steps(1, args.warmup)
+        st64 = torch.cuda.ExternalStream(e64.stream_handle(), device=dev)
+        ev64 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                for _ in range(args.fp64_steps)]
+        th64 = []
+        if pg is not None:
+            pg.barrier()
+        torch.cuda.synchronize()
+        for k in range(args.fp64_steps):
+            with torch.cuda.stream(st64):
+                flush.zero_()
+            ev64[k][0].record(st64)
+            th64.append(e64.md_steps(1 + args.warmup + k, 1)[0])
+            ev64[k][1].record(st64)
+        torch.cuda.synchronize()
+        ms64 = float(sum(a.elapsed_time(b) for a, b in ev64))
+        if pg is not None:
+            t = torch.tensor([ms64], device=f"cuda:{dev}", dtype=torch.float64)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            ms64 = float(t.item())
+        th64 = np.array(th64)
+        e64.close()
+        fp64_plain = {"value": world * s.nion * args.fp64_steps / (ms64 / 1000.0),
+                      "ms_per_step": ms64 / args.fp64_steps, "steps": args.fp64_steps, "precision": "fp64",
+                      "pim_solver": "cg", "graph": True, "h_tot_drift": h_drift(th64, s.nion)}
 
     # ------------------------------------------------ end to end through the C ABI
     nE = max(1, args.e2e_steps)
@@ -390,6 +446,8 @@ def run_ours(args):
             "clocks": clk,
             "gpu_launches": launches,
             "force_rms_rel_err_vs_fp64": force_err,
+            "h_tot_drift": h_drift(th, n),
+            "fp64_plain": fp64_plain,
             "scf_iter_mean": float(th[:, 10].mean()),
             "list_rebuilds": int(th[-1, 9] - th[0, 9]) + 1,
             "finite": bool(np.isfinite(th).all()),
