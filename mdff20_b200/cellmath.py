@@ -43,3 +43,27 @@ def wrap_positions(A: np.ndarray, pos: np.ndarray) -> np.ndarray:
     s = kardir(np.asarray(pos, float), B)
     s = s - np.rint(s)
     return np.ascontiguousarray(dirkar(s, A))
+
+
+def auto_es(A: np.ndarray, cutlongrange: float, epsw: float):
+    """set_autoES (src/ewald.c:48-71): (alphaES, kES, cutlongrange) from the cell and epsw.
+
+    The cutoff grows to half the smallest face distance when shorter; alpha takes the C
+    integer abs() of a logarithm (truncation toward zero), so it moves in steps of
+    sqrt(integer) / rc; kES = nearbyint(0.25 + |column k of A| alpha tol1 / pi).
+    """
+    import math
+
+    A = np.asarray(A, float)
+    _, _, w = lattice(A)
+    rc = float(cutlongrange)
+    half = 0.5 * float(min(w))
+    if rc < half:
+        rc = half
+    eps = min(abs(epsw), 0.5)
+    tol = math.sqrt(abs(math.log(eps * rc)))
+    alpha = math.sqrt(float(abs(int(math.log(eps * rc * tol))))) / rc
+    tol1 = math.sqrt(-math.log(eps * rc * (2.0 * tol * alpha) * (2.0 * tol * alpha)))
+    anorm = [math.sqrt(A[0, k] * A[0, k] + A[1, k] * A[1, k] + A[2, k] * A[2, k]) for k in range(3)]
+    kes = tuple(int(np.rint(0.25 + anorm[k] * alpha * tol1 / math.pi)) for k in range(3))
+    return alpha, kes, rc

@@ -252,6 +252,7 @@ void Engine::setup_units_and_cell() {
     // check_md, src/md.c:120-127
     tauT = p.tauTberendsen;
     if (p.nequil > 0 && tauT == 0.0) tauT = p.dt;
+    if (p.egrator == 0 && p.nequil > 0) p.egrator = 1;   // equilibration runs velocity Verlet
     temp = p.temp * boltz_unit;
     dt = p.dt * time_unit;
     tauT *= time_unit;

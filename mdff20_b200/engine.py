@@ -127,6 +127,12 @@ def params_from_system(s: System) -> Params:
     P.alphaES = s.alphaES
     for k in range(3):
         P.kES[k] = int(s.kES[k])
+    if s.lcoulombic and s.lautoES:   # init_field runs set_autoES (src/field.c:330-331)
+        from .cellmath import auto_es
+
+        P.alphaES, kes, P.cutlongrange = auto_es(s.cell, s.cutlongrange, s.epsw)
+        for k in range(3):
+            P.kES[k] = kes[k]
     P.algo_pim = ALGO_PIM.index(s.algo_pim)
     P.algo_extrapolate_dipole = ALGO_EXTRAPOLATE.index(s.algo_extrapolate_dipole)
     P.extrapolate_order = s.extrapolate_order

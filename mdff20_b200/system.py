@@ -100,6 +100,12 @@ class System:
     dt: float = 0.001
     temp: float = 0.0
     npas: int = 0
+    # output periods of run_md (src/md.c:242-281); tprint 0: no trajectory
+    nprint: int = 1000000
+    fprint: int = 1000000
+    cprint: int = 1000000
+    tprint: int = 0
+    tstart: int = 0
     nhc_n: int = 3
     nhc_mults: int = 1
     nhc_yosh_order: int = 1
@@ -160,7 +166,8 @@ class System:
               f"cutshortrange {self.cutshortrange!r}", f"cutlongrange {self.cutlongrange!r}",
               f"lstatic {b(self.lstatic)}", f"lreduced {b(self.lreduced)}", f"lpstress {b(self.lpstress)}"]
         L += [f"integrator {self.integrator}", f"dt {self.dt!r}", f"temp {self.temp!r}",
-              f"npas {self.npas}", "nprint 1000000", "fprint 1000000", "cprint 1000000", "tprint 0",
+              f"npas {self.npas}", f"nprint {self.nprint}", f"fprint {self.fprint}", f"cprint {self.cprint}",
+              f"tprint {self.tprint}", f"tstart {self.tstart}",
               f"nequil {self.nequil}", f"nequilT {self.nequilT}", f"tauTberendsen {self.tauTberendsen!r}",
               f"nhc_n {self.nhc_n}", f"nhc_mults {self.nhc_mults}", f"nhc_yosh_order {self.nhc_yosh_order}",
               f"timesca_thermo {self.timesca_thermo!r}"]

@@ -84,3 +84,37 @@ def silica96_ko():
 
 
 CASES["silica96_ko"] = silica96_ko
+
+
+# ---------------------------------------------------------------- C host (mdff20gpu.x)
+def _with(s, **kw):
+    for k, v in kw.items():
+        setattr(s, k, v)
+    return s
+
+
+def host_runs():
+    """Runs of the reference program mdff20.x whose output files (OSZIFF, CONTFF, TRAJFF,
+    the stdout thermodynamic blocks) pin the C host's: NHC with induced dipoles and ASPC,
+    velocity Verlet with velocity rescaling during equilibration, LJ in reduced units, a static run and a zero-step run (the initial velocities)."""
+    pim = dict(integrator="nvt-nhcn", temp=1500.0)
+    return {
+        "pim_nhc": _with(crist192(True, extrapolate_order=2, **pim),
+                         npas=6, nprint=3, fprint=1, cprint=4, tprint=3, tstart=1),
+        "rigid_equil": _with(crist192(False, integrator="nve-vv", temp=2000.0),
+                             npas=6, nequil=4, nequilT=2, nprint=2, fprint=2, cprint=6, tprint=6),
+        "lj_vv": _with(lj256(), tauTberendsen=0.005, npas=5, nprint=5, fprint=1, cprint=5, tprint=5, tstart=6),
+        "pim_static": _with(crist192(True), lstatic=True, lpstress=True),
+        "pim_init": _with(crist192(True, **pim), npas=0, nprint=1, fprint=1, cprint=1, tprint=1),
+    }
+
+
+def autoes_cases():
+    """Systems for set_autoES (src/ewald.c:48-71): cubic and triclinic cells, two epsw."""
+    a = _with(crist192(False), lautoES=True, epsw=1e-6)
+    b = _with(silica450(False), lautoES=True, epsw=1e-5, cutlongrange=12.0)
+    c = _with(crist192(False), lautoES=True, epsw=1e-3)
+    c.cell = c.cell.copy()
+    c.cell[1, 0] = 1.5
+    c.cell[2, 1] = -0.75
+    return {"crist192_1e-6": a, "silica450_1e-5": b, "crist192_tri_1e-3": c}
