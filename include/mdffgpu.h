@@ -123,6 +123,18 @@ int mdffgpu_get_dipole_history(mdffgpu_ctx *ctx, double *hist);
 /* Nose-Hoover chain state xi, vxi (nhc_n values each, src/md.h:26) */
 int mdffgpu_set_nhc(mdffgpu_ctx *ctx, const double *xi, const double *vxi);
 int mdffgpu_get_nhc(mdffgpu_ctx *ctx, double *xi, double *vxi);
+/* Exact restart.  No counterpart in the reference, whose restart file CONTFF
+ * (write_config, src/config.c:291-345) keeps wrapped positions, velocities and forces
+ * at 12 decimals and drops the ASPC dipole history (src/config.h:48), the Nose-Hoover
+ * chain (src/md.h:26), the leap-frog r(t-dt) (src/config.h:39), the list-build
+ * positions (src/verlet.c:124-170) and the step count that sets the ASPC order.
+ * save_state writes the whole MD state after the last step run into buf (state_size
+ * bytes, plain little-endian words); load_state puts it into a context created from
+ * the same system and returns that step in *istep, so that
+ * mdffgpu_md_steps(ctx, *istep + 1, ...) continues the saved run bit for bit. */
+int mdffgpu_state_size(const mdffgpu_ctx *ctx, size_t *bytes);
+int mdffgpu_save_state(mdffgpu_ctx *ctx, void *buf, size_t bytes);
+int mdffgpu_load_state(mdffgpu_ctx *ctx, const void *buf, size_t bytes, int *istep);
 /* info_thermo's inputs (src/thermo.c:12-35) */
 int mdffgpu_get_thermo(mdffgpu_ctx *ctx, mdffgpu_thermo *t);
 

@@ -159,6 +159,29 @@ int mdffgpu_get_nhc(mdffgpu_ctx *ctx, double *xi, double *vxi) {
     });
 }
 
+int mdffgpu_state_size(const mdffgpu_ctx *ctx, size_t *bytes) {
+    if (!ctx || !ctx->e || !bytes) return MDFFGPU_ERR_ARG;
+    *bytes = ctx->e->state_bytes();
+    return MDFFGPU_OK;
+}
+
+int mdffgpu_save_state(mdffgpu_ctx *ctx, void *buf, size_t bytes) {
+    if (!ctx || !ctx->e || !buf) return MDFFGPU_ERR_ARG;
+    if (bytes < ctx->e->state_bytes()) {
+        ctx->err = "save_state: buffer smaller than mdffgpu_state_size";
+        return MDFFGPU_ERR_ARG;
+    }
+    return guarded(ctx, [&](Engine &e) { e.save_state((unsigned char *)buf); });
+}
+
+int mdffgpu_load_state(mdffgpu_ctx *ctx, const void *buf, size_t bytes, int *istep) {
+    if (!buf) return MDFFGPU_ERR_ARG;
+    return guarded(ctx, [&](Engine &e) {
+        int s = e.load_state((const unsigned char *)buf, bytes);
+        if (istep) *istep = s;
+    });
+}
+
 int mdffgpu_get_thermo(mdffgpu_ctx *ctx, mdffgpu_thermo *t) {
     if (!t) return MDFFGPU_ERR_ARG;
     return guarded(ctx, [&](Engine &e) {

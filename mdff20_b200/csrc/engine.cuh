@@ -318,6 +318,10 @@ struct Engine {
     void solve_pim(const double3 *d_b, double3 *d_x, double rtol, int maxit);
     void fit_reduce(int first, int cnt, int nparts);
     void coul_forces(const double *d_qv, const double3 *d_muv, bool lq, bool ld, double3 *out);
+    // exact restart (state.cu): the complete MD state as one byte block
+    size_t state_bytes() const;
+    void save_state(unsigned char *buf);
+    int load_state(const unsigned char *buf, size_t bytes);
     bool graph_ok(int step) const;
     void capture_step(int step);
     void drop_graph();

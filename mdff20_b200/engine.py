@@ -163,6 +163,7 @@ EXPORTS = (
     "mdffgpu_get_dipoles", "mdffgpu_prop_agate", "mdffgpu_md_steps", "mdffgpu_launch_count",
     "mdffgpu_stream", "mdffgpu_fma_peak", "mdffgpu_profile", "mdffgpu_profile_result",
     "mdffgpu_build_lists_noalloc", "mdffgpu_fit_set_params", "mdffgpu_force_match", "mdffgpu_fit_batch",
+    "mdffgpu_state_size", "mdffgpu_save_state", "mdffgpu_load_state",
 )
 FIT_NPARAM = 10
 
@@ -193,6 +194,9 @@ def load_library(path: str = LIB_PATH):
         "mdffgpu_set_nhc": [vp, dp, dp],
         "mdffgpu_get_nhc": [vp, dp, dp],
         "mdffgpu_get_thermo": [vp, C.POINTER(Thermo)],
+        "mdffgpu_state_size": [vp, C.POINTER(C.c_size_t)],
+        "mdffgpu_save_state": [vp, vp, C.c_size_t],
+        "mdffgpu_load_state": [vp, vp, C.c_size_t, ip],
         "mdffgpu_gen_verletlist": [vp],
         "mdffgpu_check_verletlist": [vp, ip],
         "mdffgpu_get_verletlist": [vp, I, ip, ip, I, ip],
@@ -342,6 +346,21 @@ class Engine:
         vxi = np.zeros(max(k, 1))
         self._check(self.L.mdffgpu_get_nhc(self.h, _dp(xi), _dp(vxi)))
         return xi[:k], vxi[:k]
+
+    def save_state(self) -> bytes:
+        """The complete MD state after the last step (mdffgpu_save_state)."""
+        nb = C.c_size_t(0)
+        self._check(self.L.mdffgpu_state_size(self.h, C.byref(nb)))
+        buf = C.create_string_buffer(nb.value)
+        self._check(self.L.mdffgpu_save_state(self.h, buf, nb))
+        return buf.raw
+
+    def load_state(self, blob: bytes) -> int:
+        """Restore a saved state; returns the step it was saved after."""
+        step = C.c_int(0)
+        buf = C.create_string_buffer(blob, len(blob))
+        self._check(self.L.mdffgpu_load_state(self.h, buf, C.c_size_t(len(blob)), C.byref(step)))
+        return step.value
 
     # ------------------------------------------------------------ lists
     def gen_verletlist(self):

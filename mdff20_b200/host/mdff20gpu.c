@@ -1,7 +1,7 @@
 /* mdff20gpu.x -- the reference's program (src/mdff20.c, run_md src/md.c:192-283) with
  * every force evaluation, neighbour list and MD step on the GPU through libmdffgpu.
  *
- *   mdff20gpu.x [-p fp64|mixed] [-s reference|cg|cg-fused] [-g 0|1] [-d device] <control>
+ *   mdff20gpu.x [-p fp64|mixed] [-s reference|cg|cg-fused] [-g 0|1] [-d device] [-r RESTART] <control>
  *
  * It reads the control file and ./POSFF like mdff20.x and writes the same files:
  * OSZIFF every fprint steps, CONTFF every cprint steps and at the end, TRAJFF every
@@ -10,6 +10,12 @@
  * -p mixed / -s cg-fused select the fast paths; -g 0 disables CUDA-graph replay.
  * Steps between two outputs that need the host run as one mdffgpu_md_steps call;
  * the per-step thermodynamic records of that call give the OSZIFF lines.
+ *
+ * Next to every CONTFF it writes RESTART: the engine's complete state
+ * (mdffgpu_save_state) behind a small header (step, OSZIFF record count, OSZIFF and
+ * TRAJFF lengths).  -r RESTART continues such a run up to npas: OSZIFF and TRAJFF are
+ * cut back to their lengths at the restart step and appended to, so the files end up
+ * as one uninterrupted run would have left them.
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -23,6 +29,10 @@
 #define SEP "============================================================="
 
 static mdffgpu_ctx *g_ctx;
+
+/* RESTART: "MDFFHRS1", int32 istep, int32 oszcall, int64 OSZIFF and TRAJFF sizes at
+ * that step, uint64 engine block size, the block */
+static const char RESTART_MAGIC[8] = {'M', 'D', 'F', 'F', 'H', 'R', 'S', '1'};
 
 static void die(const char *what, const char *msg) {
     fprintf(stderr, "ERROR: %s: %s\n", what, msg ? msg : "");
@@ -53,6 +63,62 @@ static void pull_state(mdffh_run *run) {
           "get_state");
 }
 
+static long long file_size(const char *path) {
+    FILE *fp = fopen(path, "rb");
+    if (!fp) return 0;
+    fseek(fp, 0, SEEK_END);
+    long long n = ftell(fp);
+    fclose(fp);
+    return n;
+}
+
+static void write_restart(mdffh_run *run, int istep, FILE *osz) {
+    size_t bytes = 0;
+    check(mdffgpu_state_size(g_ctx, &bytes), "state_size");
+    void *blob = malloc(bytes);
+    if (!blob) die("RESTART", "out of memory");
+    check(mdffgpu_save_state(g_ctx, blob, bytes), "save_state");
+    fflush(osz);
+    int head[2] = {istep, run->oszcall};
+    long long sizes[2] = {file_size("OSZIFF"), file_size("TRAJFF")};
+    unsigned long long nb = bytes;
+    FILE *fp = fopen("RESTART", "wb");
+    if (!fp) die("RESTART", "cannot open for writing");
+    int ok = fwrite(RESTART_MAGIC, 8, 1, fp) == 1 && fwrite(head, sizeof head, 1, fp) == 1 &&
+             fwrite(sizes, sizeof sizes, 1, fp) == 1 && fwrite(&nb, sizeof nb, 1, fp) == 1 &&
+             fwrite(blob, bytes, 1, fp) == 1;
+    if (fclose(fp) != 0 || !ok) die("RESTART", "write failed");
+    free(blob);
+}
+
+/* Loads a RESTART file into the context and cuts OSZIFF and TRAJFF back to their
+ * lengths at that step; returns the step. */
+static int read_restart(mdffh_run *run, const char *path) {
+    FILE *fp = fopen(path, "rb");
+    if (!fp) die(path, "cannot open restart file");
+    char magic[8];
+    int head[2];
+    long long sizes[2];
+    unsigned long long nb = 0;
+    if (fread(magic, 8, 1, fp) != 1 || memcmp(magic, RESTART_MAGIC, 8) != 0 || fread(head, sizeof head, 1, fp) != 1 ||
+        fread(sizes, sizeof sizes, 1, fp) != 1 || fread(&nb, sizeof nb, 1, fp) != 1)
+        die(path, "not a restart file");
+    void *blob = malloc(nb ? nb : 1);
+    if (!blob || fread(blob, nb, 1, fp) != 1) die(path, "truncated restart file");
+    fclose(fp);
+    int istep = 0;
+    check(mdffgpu_load_state(g_ctx, blob, nb, &istep), "load_state");
+    free(blob);
+    if (istep != head[0]) die(path, "inconsistent restart file");
+    run->oszcall = head[1];
+    const char *files[2] = {"OSZIFF", "TRAJFF"};
+    for (int k = 0; k < 2; k++) {
+        if (file_size(files[k]) < sizes[k]) die(files[k], "shorter than at the restart step");
+        if (access(files[k], F_OK) == 0 && truncate(files[k], sizes[k]) != 0) die(files[k], "cannot truncate");
+    }
+    return istep;
+}
+
 /* Does step s need the host (anything but an OSZIFF line)? */
 static int host_step(const mdffh_run *run, int s, int rescale_allowed) {
     const mdffgpu_params *p = &run->p;
@@ -62,25 +128,28 @@ static int host_step(const mdffh_run *run, int s, int rescale_allowed) {
            mdffh_iopsnode(s, run->npas, run->tprint, run->tstart);
 }
 
-static void run_md(mdffh_run *run) {
+/* run_md (src/md.c:192-283) from step first (1, or the step after a restart). */
+static void run_md(mdffh_run *run, int first) {
     const mdffgpu_params *p = &run->p;
     int egrator = (p->egrator == 0 && p->nequil > 0) ? 1 : p->egrator;   /* check_md, src/md.c:128-131 */
     int rescale_allowed = egrator == 1;
     mdffgpu_thermo t;
-    double e_kin = mdffh_calc_kin(run);
-    printf(SEP "\nproperties at t=0\n" SEP "\n\n");
-    check(mdffgpu_engforce(g_ctx), "engforce");
-    check(mdffgpu_get_thermo(g_ctx, &t), "get_thermo");
-    t.e_kin = e_kin;
-    t.e_nvt = 0.0;
-    mdffh_info_thermo(run, 0, stdout, 0, &t);
-    if (run->npas > 0) printf(SEP "\nstarting main MD loop\n" SEP "\n\n");
-    FILE *osz = fopen("OSZIFF", "w");
+    if (first == 1) {
+        double e_kin = mdffh_calc_kin(run);
+        printf(SEP "\nproperties at t=0\n" SEP "\n\n");
+        check(mdffgpu_engforce(g_ctx), "engforce");
+        check(mdffgpu_get_thermo(g_ctx, &t), "get_thermo");
+        t.e_kin = e_kin;
+        t.e_nvt = 0.0;
+        mdffh_info_thermo(run, 0, stdout, 0, &t);
+    }
+    if (run->npas >= first) printf(SEP "\nstarting main MD loop at step %d\n" SEP "\n\n", first);
+    FILE *osz = fopen("OSZIFF", first == 1 ? "w" : "a");
     if (!osz) die("opening OSZIFF file", "");
     double *rec = malloc(12 * sizeof(double) * (size_t)(run->npas > 0 ? run->npas : 1));
     struct timespec t0, t1;
     clock_gettime(CLOCK_MONOTONIC, &t0);
-    int istep = 1;
+    int istep = first;
     while (istep <= run->npas) {
         int last = istep;
         while (last < run->npas && !host_step(run, last, rescale_allowed)) last++;
@@ -109,26 +178,32 @@ static void run_md(mdffh_run *run) {
         if (mdffh_iopnode(s, run->npas, run->fprint)) mdffh_info_thermo(run, 1, osz, s, &t);
         if (need_state) {
             pull_state(run);
-            if (mdffh_iopnode(s, run->npas, run->cprint) && mdffh_write_config(run, "CONTFF", 'w')) die("CONTFF", run->err);
             if (mdffh_iopsnode(s, run->npas, run->tprint, run->tstart) && mdffh_write_config(run, "TRAJFF", 'a'))
                 die("TRAJFF", run->err);
+            if (mdffh_iopnode(s, run->npas, run->cprint)) {
+                if (mdffh_write_config(run, "CONTFF", 'w')) die("CONTFF", run->err);
+                write_restart(run, s, osz);
+            }
         }
         istep = last + 1;
     }
     free(rec);
     pull_state(run);
     if (mdffh_write_config(run, "CONTFF", 'w')) die("CONTFF", run->err);
+    write_restart(run, istep - 1, osz);
     fclose(osz);
 }
 
 static void usage(const char *prog) {
-    fprintf(stderr, "Usage : %s [-p fp64|mixed] [-s reference|cg|cg-fused] [-g 0|1] [-d device] <control>\n", prog);
+    fprintf(stderr, "Usage : %s [-p fp64|mixed] [-s reference|cg|cg-fused] [-g 0|1] [-d device] [-r RESTART] <control>\n",
+            prog);
     exit(-1);
 }
 
 int main(int argc, char **argv) {
     int precision = MDFFGPU_FP64, solver = MDFFGPU_PIM_REFERENCE, graph = 1, device = 0, opt;
-    while ((opt = getopt(argc, argv, "p:s:g:d:")) != -1) {
+    const char *restart = NULL;
+    while ((opt = getopt(argc, argv, "p:s:g:d:r:")) != -1) {
         if (opt == 'p')
             precision = strcmp(optarg, "mixed") == 0 ? MDFFGPU_MIXED : MDFFGPU_FP64;
         else if (opt == 's')
@@ -139,6 +214,8 @@ int main(int argc, char **argv) {
             graph = atoi(optarg);
         else if (opt == 'd')
             device = atoi(optarg);
+        else if (opt == 'r')
+            restart = optarg;
         else
             usage(argv[0]);
     }
@@ -157,8 +234,9 @@ int main(int argc, char **argv) {
     printf("precision %s, induced-dipole solver %s, graph %d\n" SEP "\n", precision ? "mixed" : "fp64",
            solver == MDFFGPU_PIM_REFERENCE ? "reference" : (solver == MDFFGPU_PIM_CG ? "cg" : "cg-fused"), graph);
     if (run.lrdf) die("lrdf", "the radial distribution mode is not handled by this host");
-    /* check_md (src/md.c:134-137): a requested trajectory starts from an empty file */
-    if (run.tprint > 0 && access("TRAJFF", F_OK) == 0) remove("TRAJFF");
+    /* check_md (src/md.c:134-137): a requested trajectory starts from an empty file
+     * (a restarted run appends to it) */
+    if (!restart && run.tprint > 0 && access("TRAJFF", F_OK) == 0) remove("TRAJFF");
 
     check(mdffgpu_create(p, run.rx, run.ry, run.rz, run.vx, run.vy, run.vz, device, &g_ctx), "create");
     check(mdffgpu_set_precision(g_ctx, precision), "set_precision");
@@ -167,9 +245,14 @@ int main(int argc, char **argv) {
     if (p->lverletL) check(mdffgpu_gen_verletlist(g_ctx), "gen_verletlist");
 
     if (!run.lstatic) {
-        mdffh_init_velocities(&run);
-        check(mdffgpu_set_velocities(g_ctx, run.vx, run.vy, run.vz), "set_velocities");
-        run_md(&run);
+        int first = 1;
+        if (restart) {
+            first = read_restart(&run, restart) + 1;
+        } else {
+            mdffh_init_velocities(&run);
+            check(mdffgpu_set_velocities(g_ctx, run.vx, run.vy, run.vz), "set_velocities");
+        }
+        run_md(&run, first);
     } else {
         mdffgpu_thermo t;
         double e_kin = mdffh_calc_kin(&run);

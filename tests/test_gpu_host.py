@@ -29,6 +29,8 @@ def layout(line: str) -> str:
     """The line with every floating-point field masked and mantissa signs blanked (a
     value near zero may change sign)."""
     return NUM.sub("#", MANTISSA_SIGN.sub(" ", line))
+
+
 CASES = ("pim_nhc", "rigid_equil", "lj_vv", "pim_static", "pim_init")
 
 
@@ -108,3 +110,27 @@ def test_host_program_rerun_overwrites(tmp_path):
     run_host("pim_nhc", str(tmp_path))
     for f, text in first.items():
         assert open(tmp_path / f).read() == text, f
+
+
+def test_host_program_restart_continues_exactly(tmp_path):
+    """npas 3, then -r RESTART up to npas 6, leaves the files of one 6-step run; a second
+    restart from the same step-3 RESTART cuts OSZIFF and TRAJFF back first."""
+    full = tmp_path / "full"
+    split = tmp_path / "split"
+    full.mkdir()
+    split.mkdir()
+    run_host("pim_nhc", str(full))
+    for f in ("control.s", "POSFF"):
+        shutil.copy(os.path.join(HOST_GOLDEN, "pim_nhc", f), split / f)
+    ctl = (split / "control.s").read_text()
+    assert "npas 6" in ctl
+    (split / "control.s").write_text(ctl.replace("npas 6", "npas 3"))
+    p = subprocess.run([EXE, "control.s"], cwd=split, capture_output=True, timeout=600)
+    assert p.returncode == 0, p.stderr.decode()[-2000:]
+    shutil.copy(split / "RESTART", split / "RESTART3")
+    (split / "control.s").write_text(ctl)
+    for attempt in range(2):
+        p = subprocess.run([EXE, "-r", "RESTART3", "control.s"], cwd=split, capture_output=True, timeout=600)
+        assert p.returncode == 0, p.stderr.decode()[-2000:]
+        for f in ("OSZIFF", "CONTFF", "TRAJFF"):
+            assert (split / f).read_bytes() == (full / f).read_bytes(), (attempt, f)

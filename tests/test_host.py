@@ -226,3 +226,32 @@ def test_posff_direct_and_rnn(lib, tmp_path):
         want = cellmath.wrap_positions(s.cell, cellmath.dirkar(frac, s.cell))
         np.testing.assert_array_equal(r, want)
         assert not inp.run.xyz("v").any()
+
+
+def test_host_library_exports_and_layout(lib, tmp_path):
+    """libmdffhost exports every function include/mdffhost.h declares, and mdffh_run has
+    the same layout in C and in the Python binding."""
+    import re
+    import subprocess
+    from tests.helpers import ROOT
+
+    header = os.path.join(ROOT, "include", "mdffhost.h")
+    names = sorted(set(re.findall(r"\b(mdffh_[a-z_0-9]+)\s*\(", open(header).read())))
+    assert len(names) >= 14
+    assert not [n for n in names if not hasattr(lib, n)]
+    src = r"""
+#include <stdio.h>
+#include <stddef.h>
+#include "mdffhost.h"
+int main(void) {
+  printf("%zu %zu %zu %zu %zu %zu\n", sizeof(mdffh_run), offsetof(mdffh_run, Fposff), offsetof(mdffh_run, B),
+         offsetof(mdffh_run, atypia), offsetof(mdffh_run, oszcall), offsetof(mdffh_run, err));
+  return 0;
+}
+"""
+    c, x = tmp_path / "t.c", tmp_path / "t.x"
+    c.write_text(src)
+    subprocess.run(["gcc", "-I", os.path.dirname(header), str(c), "-o", str(x)], check=True)
+    got = [int(v) for v in subprocess.run([str(x)], capture_output=True, text=True, check=True).stdout.split()]
+    H = host.HostRun
+    assert got == [C.sizeof(H), H.Fposff.offset, H.B.offset, H.atypia.offset, H.oszcall.offset, H.err.offset]
