@@ -211,6 +211,27 @@ int mdffgpu_build_lists_noalloc(const double *d_pos, int n, const double *cell, 
                                 int cap_nb, int *d_nb, int *d_nbn, int cap_co, int *d_co, int *d_con,
                                 void *stream, int *status_out);
 
+/* Radial distribution function: the pair histogram of get_gr
+ * (src/radial_distribution.c:180-230), accumulated over configurations on the GPU.
+ * An accumulator is independent of any context: nion ions in blocks of nionit per
+ * type (the order of POSFF), pairs closer than cutgr counted in bins of width resg,
+ * nbins of them.  rdf_add adds one configuration given as Cartesian host arrays and
+ * its cell rows [3][3] (read_next_traj + get_gr, src/radial_distribution.c:70-81);
+ * rdf_add_ctx adds a context's current positions without leaving the device (same
+ * ions and device).  rdf_counts returns the ordered-pair counts
+ * pairs[nbins][ntype][ntype] (bin of (int)(r/resg), both orders of every pair, as
+ * get_gr counts them; the reference additionally folds all pairs into its [0][0]
+ * entry) and the number of configurations added. */
+typedef struct mdffgpu_rdf mdffgpu_rdf;
+int mdffgpu_rdf_create(int nion, int ntype, const int *nionit, double cutgr, double resg, int nbins, int device,
+                       mdffgpu_rdf **out);
+int mdffgpu_rdf_destroy(mdffgpu_rdf *rdf);
+const char *mdffgpu_rdf_last_error(const mdffgpu_rdf *rdf);
+int mdffgpu_rdf_reset(mdffgpu_rdf *rdf);
+int mdffgpu_rdf_add(mdffgpu_rdf *rdf, const double *cell, const double *rx, const double *ry, const double *rz);
+int mdffgpu_rdf_add_ctx(mdffgpu_rdf *rdf, mdffgpu_ctx *ctx);
+int mdffgpu_rdf_counts(mdffgpu_rdf *rdf, long long *pairs, int *nconf);
+
 /* Number of kernel launches the engine made so far (for accounting).  No counterpart
  * in the reference. */
 long long mdffgpu_launch_count(const mdffgpu_ctx *ctx);

@@ -54,6 +54,10 @@ typedef struct mdffh_run {
     char atypit[MDFFGPU_NTMAX][MDFFH_NAMELEN];
     char (*atypia)[MDFFH_NAMELEN];     /* per-ion type name as read (written back by CONTFF) */
     double *rx, *ry, *rz, *vx, *vy, *vz, *fx, *fy, *fz;
+    /* radial distribution (src/radial_distribution.h): resolution, cut-off, bins,
+     * configurations to read from TRAJFF */
+    double resg, cutgr;
+    int nbins, nconf;
     /* output state */
     int oszcall;                       /* OSZIFF records written (src/io.c:58) */
     char err[256];
@@ -95,6 +99,23 @@ int mdffh_write_config(mdffh_run *run, const char *filename, char mode);
 void mdffh_info_thermo(mdffh_run *run, int key, FILE *fp, int istep, const mdffgpu_thermo *t);
 /* info_thermo key 1 appended to the file at path (opened and closed per record). */
 int mdffh_oszi_append(mdffh_run *run, const char *path, int istep, const mdffgpu_thermo *t);
+
+/* init_rdf's parameters (src/radial_distribution.c:14-41): resg (default 0.1) and nconf
+ * from the control file, cutgr = half the smallest face distance of the POSFF cell.
+ * The reference sizes its histogram from the default resg before it reads resg, so
+ * nbins = (int)(cutgr / 0.1) + 1 whenever resg >= 0.1; for resg < 0.1, where the
+ * reference writes past its histogram, nbins = (int)(cutgr / resg) + 1. */
+int mdffh_init_rdf(mdffh_run *run, const char *controlfn);
+/* read_next_traj (src/config.c:448-510): the next configuration of a TRAJFF stream into
+ * run (cell, positions, velocities, forces; Direct coordinates converted). */
+int mdffh_read_traj(mdffh_run *run, FILE *fp);
+/* write_rdf (src/radial_distribution.c:96-146) from the ordered-pair counts
+ * pairs[nbins][ntype][ntype] of nconf configurations: the all-pairs count added into
+ * [0][0] as get_gr does, normalised per type pair by nconf * 4 pi (resg r^2 + resg^3/12)
+ * / volume * nionit[a] * nionit[b], and written as lines of ntype(ntype+1)/2 (r, g)
+ * pairs taken in the order (0,0), (0,1), ... of the full type matrix, as the
+ * reference's loop leaves them.  The volume is that of the last configuration read. */
+int mdffh_write_rdf(mdffh_run *run, const long long *pairs, int nconf, const char *path);
 
 /* iopnode / iopsnode (src/io.c:62-69). */
 int mdffh_iopnode(int step, int npas, int every);

@@ -15,6 +15,8 @@ struct mdffgpu_ctx {
     std::string err;
 };
 
+mdffgpu::Engine *mdffgpu_engine_of(mdffgpu_ctx *ctx) { return ctx ? ctx->e : nullptr; }
+
 namespace {
 
 template <typename F>

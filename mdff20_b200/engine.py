@@ -164,6 +164,8 @@ EXPORTS = (
     "mdffgpu_stream", "mdffgpu_fma_peak", "mdffgpu_profile", "mdffgpu_profile_result",
     "mdffgpu_build_lists_noalloc", "mdffgpu_fit_set_params", "mdffgpu_force_match", "mdffgpu_fit_batch",
     "mdffgpu_state_size", "mdffgpu_save_state", "mdffgpu_load_state",
+    "mdffgpu_rdf_create", "mdffgpu_rdf_destroy", "mdffgpu_rdf_last_error", "mdffgpu_rdf_reset", "mdffgpu_rdf_add",
+    "mdffgpu_rdf_add_ctx", "mdffgpu_rdf_counts",
 )
 FIT_NPARAM = 10
 
@@ -197,6 +199,12 @@ def load_library(path: str = LIB_PATH):
         "mdffgpu_state_size": [vp, C.POINTER(C.c_size_t)],
         "mdffgpu_save_state": [vp, vp, C.c_size_t],
         "mdffgpu_load_state": [vp, vp, C.c_size_t, ip],
+        "mdffgpu_rdf_create": [I, I, ip, D, D, I, I, vpp],
+        "mdffgpu_rdf_destroy": [vp],
+        "mdffgpu_rdf_reset": [vp],
+        "mdffgpu_rdf_add": [vp, dp, dp, dp, dp],
+        "mdffgpu_rdf_add_ctx": [vp, vp],
+        "mdffgpu_rdf_counts": [vp, C.POINTER(C.c_longlong), ip],
         "mdffgpu_gen_verletlist": [vp],
         "mdffgpu_check_verletlist": [vp, ip],
         "mdffgpu_get_verletlist": [vp, I, ip, ip, I, ip],
@@ -229,6 +237,8 @@ def load_library(path: str = LIB_PATH):
     L.mdffgpu_profile_result.restype = C.c_int
     L.mdffgpu_build_lists_noalloc.argtypes = [vp, I, dp, D, D, I, vp, vp, I, vp, vp, vp, ip]
     L.mdffgpu_build_lists_noalloc.restype = C.c_int
+    L.mdffgpu_rdf_last_error.argtypes = [vp]
+    L.mdffgpu_rdf_last_error.restype = C.c_char_p
     _lib = L
     return L
 

@@ -39,6 +39,7 @@ class HostRun(C.Structure):
         ("rx", C.POINTER(D)), ("ry", C.POINTER(D)), ("rz", C.POINTER(D)),
         ("vx", C.POINTER(D)), ("vy", C.POINTER(D)), ("vz", C.POINTER(D)),
         ("fx", C.POINTER(D)), ("fy", C.POINTER(D)), ("fz", C.POINTER(D)),
+        ("resg", D), ("cutgr", D), ("nbins", I), ("nconf", I),
         ("oszcall", I), ("err", C.c_char * 256),
     ]
 
@@ -77,6 +78,9 @@ def load_library(path: str = LIB_PATH):
         "mdffh_iopnode": ([I, I, I], I),
         "mdffh_iopsnode": ([I, I, I, I], I),
         "mdffh_oszi_append": ([rp, C.c_char_p, I, C.POINTER(Thermo)], I),
+        "mdffh_init_rdf": ([rp, C.c_char_p], I),
+        "mdffh_read_traj": ([rp, C.c_void_p], I),
+        "mdffh_write_rdf": ([rp, C.POINTER(C.c_longlong), I, C.c_char_p], I),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -116,6 +120,39 @@ class Inputs:
     def init_velocities(self) -> np.ndarray:
         self.lib.mdffh_init_velocities(C.byref(self.run))
         return self.run.xyz("v")
+
+    def init_rdf(self, control: str) -> Tuple[float, float, int, int]:
+        """init_rdf's parameters: (resg, cutgr, nbins, nconf)."""
+        if self.lib.mdffh_init_rdf(C.byref(self.run), control.encode()) != 0:
+            raise ValueError(self.run.err.decode())
+        r = self.run
+        return r.resg, r.cutgr, r.nbins, r.nconf
+
+    def traj_frames(self, path: str, nconf: int):
+        """The first nconf configurations of a TRAJFF file (read_next_traj), as
+        [(cell (3,3), Cartesian positions (N,3))]."""
+        libc = C.CDLL(None)
+        libc.fopen.restype = C.c_void_p
+        libc.fopen.argtypes = [C.c_char_p, C.c_char_p]
+        libc.fclose.argtypes = [C.c_void_p]
+        fp = libc.fopen(path.encode(), b"r")
+        if not fp:
+            raise FileNotFoundError(path)
+        frames = []
+        try:
+            for _ in range(nconf):
+                if self.lib.mdffh_read_traj(C.byref(self.run), fp) != 0:
+                    raise ValueError(self.run.err.decode())
+                frames.append((np.array(self.run.p.cell[:], float).reshape(3, 3), self.run.xyz("r")))
+        finally:
+            libc.fclose(fp)
+        return frames
+
+    def write_rdf(self, pairs: np.ndarray, nconf: int, path: str) -> None:
+        pairs = np.ascontiguousarray(pairs, dtype=np.int64)
+        if self.lib.mdffh_write_rdf(C.byref(self.run), pairs.ctypes.data_as(C.POINTER(C.c_longlong)), int(nconf),
+                                    path.encode()) != 0:
+            raise OSError(self.run.err.decode())
 
     def write_config(self, path: str, mode: str = "w") -> None:
         if self.lib.mdffh_write_config(C.byref(self.run), path.encode(), mode.encode()) != 0:

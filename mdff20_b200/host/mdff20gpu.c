@@ -6,6 +6,8 @@
  * It reads the control file and ./POSFF like mdff20.x and writes the same files:
  * OSZIFF every fprint steps, CONTFF every cprint steps and at the end, TRAJFF every
  * tprint steps from tstart, and the thermodynamic block on stdout every nprint steps.
+ * With lrdf it reads nconf configurations of TRAJFF instead and writes RDFFF, the
+ * pair histogram accumulated on the GPU (mdffgpu_rdf_*).
  * Defaults reproduce the reference's numerics (FP64, the reference's algo_pim);
  * -p mixed / -s cg-fused select the fast paths; -g 0 disables CUDA-graph replay.
  * Steps between two outputs that need the host run as one mdffgpu_md_steps call;
@@ -194,6 +196,35 @@ static void run_md(mdffh_run *run, int first) {
     fclose(osz);
 }
 
+/* The lrdf branch of the reference's main (src/mdff20.c:108-110, init_rdf
+ * src/radial_distribution.c:147-163): nconf configurations of TRAJFF into the pair
+ * histogram on the GPU, then RDFFF. */
+static void run_rdf(mdffh_run *run, const char *controlfn, int device) {
+    mdffgpu_params *p = &run->p;
+    if (mdffh_init_rdf(run, controlfn)) die("rdf", run->err);
+    printf("radial distribution: resg = %.5f, nconf = %d, %d points in g(r), cutgr = %.5f\n", run->resg, run->nconf,
+           run->nbins, run->cutgr);
+    mdffgpu_rdf *acc = NULL;
+    if (mdffgpu_rdf_create(p->nion, p->ntype, p->nionit, run->cutgr, run->resg, run->nbins, device, &acc) != MDFFGPU_OK)
+        die("rdf_create", "bad sizes or no device");
+    FILE *fp = fopen("TRAJFF", "r");
+    if (!fp) die("TRAJFF", "not found");
+    for (int ic = 0; ic < run->nconf; ic++) {
+        if (mdffh_read_traj(run, fp)) die("TRAJFF", run->err);
+        if (mdffgpu_rdf_add(acc, &p->cell[0][0], run->rx, run->ry, run->rz) != MDFFGPU_OK)
+            die("rdf_add", mdffgpu_rdf_last_error(acc));
+    }
+    fclose(fp);
+    size_t nh = (size_t)run->nbins * p->ntype * p->ntype;
+    long long *pairs = malloc(sizeof(long long) * nh);
+    int nconf = 0;
+    if (!pairs || mdffgpu_rdf_counts(acc, pairs, &nconf) != MDFFGPU_OK) die("rdf_counts", mdffgpu_rdf_last_error(acc));
+    mdffgpu_rdf_destroy(acc);
+    if (mdffh_write_rdf(run, pairs, run->nconf, "RDFFF")) die("RDFFF", run->err);
+    free(pairs);
+    printf("write RDFFF\n");
+}
+
 static void usage(const char *prog) {
     fprintf(stderr, "Usage : %s [-p fp64|mixed] [-s reference|cg|cg-fused] [-g 0|1] [-d device] [-r RESTART] <control>\n",
             prog);
@@ -233,7 +264,11 @@ int main(int argc, char **argv) {
     if (p->lcoulombic) printf("alphaES = %f  kES = %d %d %d\n", p->alphaES, p->kES[0], p->kES[1], p->kES[2]);
     printf("precision %s, induced-dipole solver %s, graph %d\n" SEP "\n", precision ? "mixed" : "fp64",
            solver == MDFFGPU_PIM_REFERENCE ? "reference" : (solver == MDFFGPU_PIM_CG ? "cg" : "cg-fused"), graph);
-    if (run.lrdf) die("lrdf", "the radial distribution mode is not handled by this host");
+    if (run.lrdf) {   /* TRAJFF is input here: check_md keeps it (src/md.c:136) */
+        run_rdf(&run, controlfn, device);
+        mdffh_free(&run);
+        return 0;
+    }
     /* check_md (src/md.c:134-137): a requested trajectory starts from an empty file
      * (a restarted run appends to it) */
     if (!restart && run.tprint > 0 && access("TRAJFF", F_OK) == 0) remove("TRAJFF");

@@ -20,13 +20,15 @@
 #include "mdffhost.h"
 
 int mdffh_fail(mdffh_run *run, const char *fmt, ...);
+void mdffh_lattice(mdffh_run *run);
+void mdffh_to_cartesian(int n, double *x, double *y, double *z, const double A[3][3]);
 
 #define FF "%19.12f "
 
 /* lattice (src/cell.c:13-91): unnormalised reciprocal rows Bu_i = A_j x A_k, the volume
  * sum_i Bu_i[0] A_i[0], the face distances omega/|column i of Bu|, B = Bu/omega, and
  * the column norms Anorm[i] = |(A_0[i], A_1[i], A_2[i])|. */
-static void lattice(mdffh_run *run) {
+void mdffh_lattice(mdffh_run *run) {
     const double(*A)[3] = run->p.cell;
     double(*B)[3] = run->B;
     const int nx[3] = {1, 2, 0}, ny[3] = {2, 0, 1};
@@ -62,7 +64,7 @@ static void to_fractional(int n, double *x, double *y, double *z, const double B
     }
 }
 
-static void to_cartesian(int n, double *x, double *y, double *z, const double A[3][3]) {
+void mdffh_to_cartesian(int n, double *x, double *y, double *z, const double A[3][3]) {
     for (int i = 0; i < n; i++) {
         double a = x[i] * A[0][0] + y[i] * A[1][0] + z[i] * A[2][0];
         double b = x[i] * A[0][1] + y[i] * A[1][1] + z[i] * A[2][1];
@@ -78,7 +80,7 @@ static void wrap(const mdffh_run *run, int n, double *x, double *y, double *z) {
         y[i] -= nearbyint(y[i]);
         z[i] -= nearbyint(z[i]);
     }
-    to_cartesian(n, x, y, z, run->p.cell);
+    mdffh_to_cartesian(n, x, y, z, run->p.cell);
 }
 
 int mdffh_read_config(mdffh_run *run, const char *posff) {
@@ -93,7 +95,7 @@ int mdffh_read_config(mdffh_run *run, const char *posff) {
         fclose(fp);
         return mdffh_fail(run, "POSFF: bad header (nion, name, cell, ntype)");
     }
-    lattice(run);
+    mdffh_lattice(run);
     for (int t = 0; ok && t < p->ntype; t++) ok = fscanf(fp, "%80s", run->atypit[t]) == 1;
     int total = 0;
     for (int t = 0; ok && t < p->ntype; t++) {
@@ -118,7 +120,7 @@ int mdffh_read_config(mdffh_run *run, const char *posff) {
     fclose(fp);
     if (!ok) return mdffh_fail(run, "POSFF: truncated ion block (Fposff %d)", run->Fposff);
     if (strcmp(run->cpos, "Direct") == 0 || strcmp(run->cpos, "D") == 0)
-        to_cartesian(n, run->rx, run->ry, run->rz, p->cell);
+        mdffh_to_cartesian(n, run->rx, run->ry, run->rz, p->cell);
     wrap(run, n, run->rx, run->ry, run->rz);
     return 0;
 }

@@ -1210,3 +1210,36 @@ int orc_md(orc_ctx *c, int nsteps, double *thermo) {
     }
     return 0;
 }
+
+/* ------------------------------------------------------------------ g(r) */
+/* get_gr, src/radial_distribution.c:180-230, for one configuration: every ordered pair
+ * (ia, ja != ia) closer than cutgr adds 1 to hist[(int)(r/resg)][type ia][type ja].
+ * (The reference also tallies every pair into [0][0]; callers add that themselves.) */
+void orc_gr(int n, const double *cell9, const double *pos, const int *typ, int nt, double cutgr, double resg,
+            int nbins, long long *hist) {
+    orc_ctx *c = calloc(1, sizeof *c);
+    memcpy(c->A, cell9, 9 * sizeof(double));
+    c->press_unit = 1.0;
+    cell_setup(c);
+    double *s = malloc(3 * (size_t)n * sizeof(double));
+    for (int i = 0; i < n; i++) {
+        double x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
+        s[3 * i] = x * c->B[0][0] + y * c->B[0][1] + z * c->B[0][2];
+        s[3 * i + 1] = x * c->B[1][0] + y * c->B[1][1] + z * c->B[1][2];
+        s[3 * i + 2] = x * c->B[2][0] + y * c->B[2][1] + z * c->B[2][2];
+    }
+    double cut2 = cutgr * cutgr;
+    for (int ia = 0; ia < n; ia++)
+        for (int ja = 0; ja < n; ja++) {
+            if (ja == ia) continue;
+            double x = s[3 * ia] - s[3 * ja], y = s[3 * ia + 1] - s[3 * ja + 1], z = s[3 * ia + 2] - s[3 * ja + 2];
+            pbc(c, &x, &y, &z);
+            double rijsq = x * x + y * y + z * z;
+            if (rijsq < cut2) {
+                int igr = (int)(sqrt(rijsq) / resg);
+                if (igr >= 0 && igr < nbins) hist[((size_t)igr * nt + typ[ia]) * nt + typ[ja]]++;
+            }
+        }
+    free(s);
+    free(c);
+}

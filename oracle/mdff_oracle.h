@@ -109,6 +109,11 @@ int orc_md_step(orc_ctx *c, int istep);
  * u_coul u_pol e_nvt pvir_lj pvir_bhmftd pvir_coul nlist_builds scf_iter scf_rmsd */
 int orc_md(orc_ctx *c, int nsteps, double *thermo);
 
+/* get_gr (src/radial_distribution.c:180-230) of one configuration: pos (N,3) Cartesian,
+ * cell9 the rows of A, typ per ion; adds ordered-pair counts to hist[nbins][nt][nt]. */
+void orc_gr(int n, const double *cell9, const double *pos, const int *typ, int nt, double cutgr, double resg,
+            int nbins, long long *hist);
+
 #ifdef __cplusplus
 }
 #endif

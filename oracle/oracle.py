@@ -162,8 +162,26 @@ def lib():
                            ("orc_nk", [vp])]:
             getattr(L, name).argtypes = args
             getattr(L, name).restype = C.c_int
+        L.orc_gr.argtypes = [I, dp, dp, ip, I, D, D, I, C.POINTER(C.c_longlong)]
+        L.orc_gr.restype = None
         _lib = L
     return _lib
+
+
+def gr_counts(frames, nionit, cutgr: float, resg: float, nbins: int) -> np.ndarray:
+    """get_gr (src/radial_distribution.c:180-230) over frames [(cell (3,3), pos (N,3))]:
+    ordered-pair counts hist[nbins][nt][nt] (without the reference's all-pairs tally in
+    [0][0])."""
+    L = lib()
+    nt = len(nionit)
+    typ = np.ascontiguousarray(np.repeat(np.arange(nt, dtype=np.int32), nionit))
+    hist = np.zeros((nbins, nt, nt), dtype=np.int64)
+    for cell, pos in frames:
+        cell = np.ascontiguousarray(cell, float)
+        pos = np.ascontiguousarray(pos, float)
+        L.orc_gr(len(typ), _dp(cell), _dp(pos), typ.ctypes.data_as(C.POINTER(C.c_int)), nt, float(cutgr),
+                 float(resg), int(nbins), hist.ctypes.data_as(C.POINTER(C.c_longlong)))
+    return hist
 
 
 def _dp(a):

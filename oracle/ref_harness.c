@@ -15,6 +15,7 @@
  *   harness <control> md <nsteps> <record_positions_every>
  *   harness <control> engforce_timing <reps>
  *   harness <control> kmesh
+ *   harness <control> rdf [write]
  *
  * Parity deviations from src/mdff20.c, each required for a deterministic harness:
  *  - velocities come from POSFF (Fposff rvn/rvf, src/config.c:415-417) instead of
@@ -47,6 +48,7 @@
 #include "kinetic.h"
 #include "integration.h"
 #include "mpi_mdff.h"
+#include "radial_distribution.h"
 
 static FILE *g_out;
 
@@ -295,6 +297,35 @@ int main(int argc, char *argv[]) {
         put_thermo();
         free(th);
         free(traj);
+    } else if (strcmp(task, "rdf") == 0) {
+        /* init_rdf (src/radial_distribution.c:147-163) minus its sample_config prints:
+         * default_rdf, read_rdf, alloc_rdf, then read_next_traj + get_gr for each of
+         * the nconf TRAJFF configurations; dumps the integer histogram gr[bin][it][jt]
+         * of the types present, and with "write" also runs write_rdf (RDFFF) */
+        default_rdf();
+        read_rdf(controlfn);
+        alloc_rdf();
+        FILE *fp = fopen("TRAJFF", "r");
+        if (!fp) {
+            fprintf(stderr, "no TRAJFF\n");
+            return 2;
+        }
+        for (int ic = 0; ic < nconf; ic++) {
+            read_next_traj(fp);
+            get_gr();
+        }
+        fclose(fp);
+        int *h = malloc(sizeof(int) * (size_t)nbins * ntype * ntype);
+        for (int b = 0; b < nbins; b++)
+            for (int it = 0; it < ntype; it++)
+                for (int jt = 0; jt < ntype; jt++) h[(b * ntype + it) * ntype + jt] = gr[b][it][jt];
+        put_i("gr", h, (long long)nbins * ntype * ntype);
+        put_s("cutgr", cutgr);
+        put_s("resg", resg);
+        put_s("nbins", (double)nbins);
+        put_s("nconf", (double)nconf);
+        free(h);
+        if (argc > 3 && strcmp(argv[3], "write") == 0) write_rdf();
     } else {
         fprintf(stderr, "unknown task %s\n", task);
         return 2;
