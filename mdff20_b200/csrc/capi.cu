@@ -92,6 +92,8 @@ int mdffgpu_set_precision(mdffgpu_ctx *ctx, int precision) {
             e.rec32 = strstr(v, "rec") != nullptr;
         }
         if (const char *v = getenv("MDFFGPU_PIM_SUBSET")) e.subset32 = atoi(v) != 0;
+        e.rho_tc = false;   // MDFFGPU_KSPACE_TC=1: the rho pass on the tensor cores (kspace_tc.cu)
+        if (const char *v = getenv("MDFFGPU_KSPACE_TC")) e.rho_tc = atoi(v) != 0;
     });
 }
 

@@ -37,6 +37,7 @@ enum StatusBits : unsigned {
     ST_CELL_OVERFLOW = 2u,
     ST_NONFINITE = 4u,
     ST_SCF = 8u,
+    ST_TC_TIMEOUT = 16u,   // a tensor-core kernel gave up waiting on its MMAs
 };
 
 // ------------------------------------------------------------------ cell geometry

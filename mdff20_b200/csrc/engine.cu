@@ -200,6 +200,7 @@ Engine::~Engine() {
     cudaFree(d_rho_part32);
     cudaFree(d_ion_part32);
     cudaFree(d_pidx);
+    cudaFree(d_qm_tc);
     cudaFree(d_ion_part);
     cudaFree(d_coef);
     dfree32();
@@ -628,6 +629,7 @@ void Engine::check_status() {
     unsigned st = (unsigned)h_out->status;
     if (st & ST_CELL_OVERFLOW) throw Error(MDFFGPU_ERR_LIST_OVERFLOW, "a cell holds more ions than its capacity");
     if (st & ST_NONFINITE) throw Error(MDFFGPU_ERR_NONFINITE, "non-finite positions or forces");
+    if (st & ST_TC_TIMEOUT) throw Error(MDFFGPU_ERR_TIMEOUT, "tensor-core k-space pass timed out waiting on its MMAs");
 }
 
 // ---------------------------------------------------------------- lists

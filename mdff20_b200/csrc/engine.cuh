@@ -133,6 +133,9 @@ void launch_coords32(Engine &e);
 void setup_kspace32(Engine &e, const std::vector<KRow> &rows);
 void launch_phase32(Engine &e);
 void launch_rho32(Engine &e, const double *q, const double3 *mu, bool lq, bool ld, const int *idx, int cnt);
+// kspace_tc.cu: the same rho chunk partials from tcgen05 TF32 MMAs (false: k box out of range)
+bool launch_rho_tc(Engine &e, const double *q, const double3 *mu, bool lq, bool ld, const int *idx, int cnt,
+                   int tab_w, int z_off, int nzb_neg, int *chunks_used);
 void launch_ion32(Engine &e, const double *q, const double3 *mu, bool ld, const RecOut &o, const int *idx, int cnt);
 
 // ---------------------------------------------------------------- engine state
@@ -221,6 +224,9 @@ struct Engine {
     int nseg32 = 0, tab_w = 0;
     float2 *d_tab32 = nullptr;                          // phase table rows [n][tab_w]
     int rho32_chunks = 0;
+    int rho_chunks_used = 0;                            // chunk partials the last rho pass wrote
+    bool rho_tc = false;                                // rho pass on the tensor cores (kspace_tc.cu)
+    float4 *d_qm_tc = nullptr;                          // its per-ion (q, 2 pi B mu)
     float2 *d_rho_part32 = nullptr;                     // [rho32_chunks][nk]
     int ion32_slices = 0, nsm = 148;                    // most ion-pass slices; SMs
     double *d_ion_part32 = nullptr;                     // [slices][n][6]

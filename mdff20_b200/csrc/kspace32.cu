@@ -492,7 +492,11 @@ void launch_rho32(Engine &e, const double *q, const double3 *mu, bool lq, bool l
     size_t smem = 2 * (sizeof(float2) * RHO32_TI * L.w + sizeof(float4) * RHO32_TI);
     int ps = -1;
     e.prof_begin("k_rho", &ps);
-    if (lq && ld) rho32_launch<true, true>(e, grid, smem, cnt, idx, chunk, L, q, mu);
+    e.rho_chunks_used = e.rho32_chunks;
+    int used = 0;
+    if ((lq || ld) && e.rho_tc && launch_rho_tc(e, q, mu, lq, ld, idx, cnt, L.w, L.z, L.nzb_neg, &used)) {
+        e.rho_chunks_used = used;
+    } else if (lq && ld) rho32_launch<true, true>(e, grid, smem, cnt, idx, chunk, L, q, mu);
     else if (lq) rho32_launch<true, false>(e, grid, smem, cnt, idx, chunk, L, q, mu);
     else if (ld) rho32_launch<false, true>(e, grid, smem, cnt, idx, chunk, L, q, mu);
     else MDFF_CK(cudaMemsetAsync(e.d_rho_part32, 0, sizeof(float2) * (size_t)e.nk * e.rho32_chunks, e.stream));
