@@ -103,6 +103,8 @@ int mdffgpu_set_pim_solver(mdffgpu_ctx *ctx, int solver) {
             throw Error(MDFFGPU_ERR_ARG, "bad solver");
         e.pim_solver = solver;
         e.gen++;
+        e.cg_poly = true;   // MDFFGPU_CG_PREDICT=aspc: start the CG from the ASPC predictor instead
+        if (const char *v = getenv("MDFFGPU_CG_PREDICT")) e.cg_poly = strcmp(v, "aspc") != 0;
     });
 }
 

@@ -25,7 +25,7 @@ struct CoulFin {
 };
 __global__ void k_finalize_coul(const double *scal, CoulFin c, double *u, double *pvir, double *tau);
 __global__ void k_induced(int n, const int *polar, const double *pol, const double3 *ef, double3 *mu);
-__global__ void k_aspc_predict(int n, int e, int es, double *hist, double3 *mu);
+__global__ void k_aspc_predict(int n, int e, int es, double *hist, double3 *mu, int poly);
 __global__ void k_aspc_correct(int n, double W, const int *polar, const double *pol, const double3 *ef,
                                double3 *mu);
 __global__ void k_add3(int n, const double3 *a, const double3 *b, double3 *c);
@@ -763,7 +763,7 @@ void Engine::pim_reference() {
     double upol_pre = 0.0;
     while (((iscf < p.max_scf_pim_iter) && (rmsd > p.conv_tol_ind)) || (iscf < p.min_scf_pim_iter)) {
         MDFF_CK(cudaMemsetAsync(d_mu_ind, 0, sizeof(double3) * n, stream));
-        if (!iscf) MDFF_LAUNCH(*this, k_aspc_predict, nb, 256, 0, n, e, es, d_hist, d_mu_ind);
+        if (!iscf) MDFF_LAUNCH(*this, k_aspc_predict, nb, 256, 0, n, e, es, d_hist, d_mu_ind, 0);
         else MDFF_LAUNCH(*this, k_induced, nb, 256, 0, n, d_polar, d_pol, d_ef, d_mu_ind);
         if (!iscf) {  // u_pol of the predicted dipoles (src/pim.c:253), kept if the loop ends here
             MDFF_LAUNCH(*this, k_pim_sums, nb, 256, 0, n, d_polar, d_pol, d_invpol, d_mu_ind, d_ef, d_part,
@@ -795,7 +795,9 @@ void Engine::pim_reference() {
 }
 
 // preconditioned conjugate gradient on (alpha^-1 - T) mu = E_stat, polarisable ions;
-// initial guess from the ASPC predictor; stops when the reference's residual measure
+// initial guess extrapolated from the converged dipoles of the previous steps (the
+// polynomial through the last extrapolate_order + 1 of them: the CG needs no corrector,
+// so the more accurate predictor saves iterations; cg_poly false: ASPC coefficients); stops when the reference's residual measure
 // sqrt(sum (mu/alpha - E)^2 / npol) (src/pim.c:431-449) is below conv_tol_ind
 // fused: E_stat + T mu0 is one Ewald evaluation of (q, mu_static + mu0) (the residual
 // needs only their sum), and rho(k) of (q, mu_static + mu) follows the iterates
@@ -808,7 +810,7 @@ void Engine::pim_cg(bool fused) {
     int e = (istep >= ord + 1) ? ord : (!istep ? 0 : istep - 1);
     int es = (e != ord) ? e + 1 : e;
     if (fused) {
-        MDFF_LAUNCH(*this, k_aspc_predict, nb, 256, 0, n, e, es, d_hist, d_mu_ind);
+        MDFF_LAUNCH(*this, k_aspc_predict, nb, 256, 0, n, e, es, d_hist, d_mu_ind, cg_poly ? 1 : 0);
         MDFF_LAUNCH(*this, k_add3, nb, 256, 0, n, d_mu_static, d_mu_ind, d_mu_tot);
         if (use32 && real32)
             launch_dir32(*this, d_q, d_mu_tot, p.alphaES, lqch != 0, true, ldmp != 0, false, true, d_tmp3, nullptr);
@@ -825,7 +827,7 @@ void Engine::pim_cg(bool fused) {
         MDFF_LAUNCH(*this, k_cg_residual, nb, 256, 0, n, d_polar, d_invpol, d_muzero, d_ef_ind, d_mu_ind, d_cg_r);
     } else {
         field_of(d_q, d_mu_static, lqch != 0, ldip != 0, ldmp != 0, d_ef_stat);
-        MDFF_LAUNCH(*this, k_aspc_predict, nb, 256, 0, n, e, es, d_hist, d_mu_ind);
+        MDFF_LAUNCH(*this, k_aspc_predict, nb, 256, 0, n, e, es, d_hist, d_mu_ind, cg_poly ? 1 : 0);
         field_of(d_qzero, d_mu_ind, false, true, false, d_ef_ind);
         MDFF_LAUNCH(*this, k_cg_residual, nb, 256, 0, n, d_polar, d_invpol, d_ef_stat, d_ef_ind, d_mu_ind, d_cg_r);
     }
@@ -964,7 +966,7 @@ void Engine::pim_ko() {
     double rmsd = 1.0e300, upol = 0.0;
     while (((iscf < p.max_scf_pim_iter) && (rmsd > p.conv_tol_ind)) || (iscf < p.min_scf_pim_iter)) {
         if ((!iscf) && (istep > 1)) {
-            MDFF_LAUNCH(*this, k_aspc_predict, nb, 256, 0, n, e, es, d_hist, d_mu_ind);
+            MDFF_LAUNCH(*this, k_aspc_predict, nb, 256, 0, n, e, es, d_hist, d_mu_ind, 0);
         } else {
             ko_inner(d_cg_p, d_cg_r);
             MDFF_LAUNCH(*this, k_scale_add3, nb, 256, 0, n, 1.0, d_cg_p, 1.0, d_mu_ind);

@@ -226,6 +226,9 @@ struct Engine {
     int rho32_chunks = 0;
     int rho_chunks_used = 0;                            // chunk partials the last rho pass wrote
     bool rho_tc = false;                                // rho pass on the tensor cores (kspace_tc.cu)
+    // CG initial guess: polynomial extrapolation through the last extrapolate_order + 1
+    // converged dipoles (false: the reference's ASPC coefficients)
+    bool cg_poly = true;
     float4 *d_qm_tc = nullptr;                          // its per-ion (q, 2 pi B mu)
     float2 *d_rho_part32 = nullptr;                     // [rho32_chunks][nk]
     int ion32_slices = 0, nsm = 148;                    // most ion-pass slices; SMs

@@ -166,7 +166,7 @@ __global__ void k_induced(int n, const int *__restrict__ polar, const double *__
 
 // extrapolate_dipole_aspc predictor (src/pim.c:381-400) for order `e`, then the
 // history shift by `es` places
-__global__ void k_aspc_predict(int n, int e, int es, double *__restrict__ hist, double3 *__restrict__ mu) {
+__global__ void k_aspc_predict(int n, int e, int es, double *__restrict__ hist, double3 *__restrict__ mu, int poly) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double Bt[6][6] = {{1.0, 0, 0, 0, 0, 0},
@@ -175,10 +175,17 @@ __global__ void k_aspc_predict(int n, int e, int es, double *__restrict__ hist, 
                              {2.8, -2.8, 1.2, -0.2, 0, 0},
                              {3.0, -24.0 / 7.0, 27.0 / 14.0, -4.0 / 7.0, 1.0 / 14.0, 0},
                              {22.0 / 7.0, -55.0 / 14.0, 55.0 / 21.0, -22.0 / 21.0, 5.0 / 21.0, -1.0 / 42.0}};
+    // polynomial extrapolation through the last e + 1 values: (-1)^k C(e + 1, k + 1)
+    const double Pt[6][6] = {{1.0, 0, 0, 0, 0, 0},
+                             {2.0, -1.0, 0, 0, 0, 0},
+                             {3.0, -3.0, 1.0, 0, 0, 0},
+                             {4.0, -6.0, 4.0, -1.0, 0, 0},
+                             {5.0, -10.0, 10.0, -5.0, 1.0, 0},
+                             {6.0, -15.0, 20.0, -15.0, 6.0, -1.0}};
     double *h = hist + (size_t)i * ASPC_DEPTH * 3;
     double m[3] = {0.0, 0.0, 0.0};
     for (int k = 0; k < e + 1; k++)
-        for (int c = 0; c < 3; c++) m[c] += Bt[e][k] * h[3 * k + c];
+        for (int c = 0; c < 3; c++) m[c] += (poly ? Pt[e][k] : Bt[e][k]) * h[3 * k + c];
     for (int k = es; k > 0; k--)
         for (int c = 0; c < 3; c++) h[3 * k + c] = h[3 * (k - 1) + c];
     mu[i] = make_double3(m[0], m[1], m[2]);

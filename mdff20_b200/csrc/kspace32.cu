@@ -11,12 +11,15 @@
 // ZB consecutive nz (negative half -K2..0 and positive half 1..K2 separately, zero
 // padded), so that a thread owns one block of one row and reads it with 16-byte loads;
 // the two extra entries per block put neighbouring blocks in different shared-memory
-// banks (the lanes of a warp read two blocks of the same ion at once).
+// banks (the lanes of a warp read two blocks of the same ion at once).  Within a block
+// the values are stored as planar pairs, (Re E2[z], Re E2[z+1]) then (Im E2[z],
+// Im E2[z+1]), the operand layout of the packed FP32x2 FMA (FFMA2) of k_rho32.
 //
 // k_rho32   : rho(k) = sum_i (q_i + i k.mu_i) E0 E1 E2.  Thread = one (row, z block)
 //             segment, ions stream through shared memory in tiles of table rows; the
 //             summand (B1' + j B2) E2[z0 + j] costs 6 FMA (4 without dipoles), j an
-//             unrolled constant.  FP32 sums over one block's ion chunk, chunk partials
+//             unrolled constant, issued as packed FP32x2 FMAs over pairs of z (3 per z,
+//             2 without dipoles).  FP32 sums over one block's ion chunk, chunk partials
 //             summed in FP64 in a fixed order (k_rho_reduce32).
 // k_ion32   : per ion and k-slice the n-space sums of field (and force) terms.  Thread
 //             = ion; Ak rho(k) of the slice sits in shared memory as (rho_z, rho_-z)
@@ -35,7 +38,7 @@ constexpr int RHO32_THREADS = 128;
 constexpr int RHO32_TI = 16;        // ions per shared-memory tile (two tiles in flight)
 constexpr int RHO32_MIN_BLOCKS = 8;
 constexpr int ION32_THREADS = 128;
-constexpr int ION32_MIN_BLOCKS = 6;
+constexpr int ION32_MIN_BLOCKS = 5;
 
 __device__ __forceinline__ float2 cmul32(float2 a, float2 b) {
     return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -78,15 +81,22 @@ __global__ void k_phase32(int n, Cell c, const double4 *__restrict__ r, TabLayou
         d = 1;
         m = e - L.e1 - L.K1;
     } else if (e >= L.z) {
+        // z blocks hold planar pairs: entry 2p = (x of z_2p, x of z_2p+1), entry 2p + 1 =
+        // their y; the thread of entry 2p writes both
         int b = (e - L.z) / ZS, j = (e - L.z) - b * ZS;
         if (j >= ZB) {
-        } else if (b < L.nzb_neg) {
-            m = -L.K2 + ZB * b + j;
-            if (m <= 0) d = 2;
-        } else {
-            m = 1 + ZB * (b - L.nzb_neg) + j;
-            if (m <= L.K2) d = 2;
+            tab[g] = make_float2(0.f, 0.f);
+            return;
         }
+        if (j & 1) return;
+        int m0 = (b < L.nzb_neg) ? -L.K2 + ZB * b + j : 1 + ZB * (b - L.nzb_neg) + j;
+        bool ok0 = (b < L.nzb_neg) ? m0 <= 0 : m0 <= L.K2, ok1 = (b < L.nzb_neg) ? m0 + 1 <= 0 : m0 + 1 <= L.K2;
+        double4 ri = r[i];
+        double t = c.B[0][2] * ri.x + c.B[1][2] * ri.y + c.B[2][2] * ri.z;
+        float2 v0 = ok0 ? cis2pi32((double)m0 * t) : make_float2(0.f, 0.f);
+        float2 v1 = ok1 ? cis2pi32((double)(m0 + 1) * t) : make_float2(0.f, 0.f);
+        *(float4 *)(tab + g) = make_float4(v0.x, v1.x, v0.y, v1.y);
+        return;
     }
     float2 v = make_float2(0.f, 0.f);
     if (d >= 0) {
@@ -113,9 +123,10 @@ __global__ void __launch_bounds__(RHO32_THREADS, RHO32_MIN_BLOCKS)
     else S.nx = S.ny = S.z0 = S.cnt = S.koff = S.pad0 = 0;
     const float fnx = (float)S.nx, fny = (float)S.ny, fz0 = (float)S.z0;
     const int o0 = S.nx, o1 = L.e1 + L.K1 + S.ny, oz = (L.z + ZS * S.pad0) / 2;
-    float2 acc[ZB];
+    // accumulators of z pairs (2h, 2h + 1): real parts accX[h], imaginary parts accY[h]
+    float2 accX[ZB / 2], accY[ZB / 2];
 #pragma unroll
-    for (int z = 0; z < ZB; z++) acc[z] = make_float2(0.f, 0.f);
+    for (int h = 0; h < ZB / 2; h++) accX[h] = accY[h] = make_float2(0.f, 0.f);
     int a0 = blockIdx.y * chunk, a1 = min(cnt, a0 + chunk);
     int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const double tpi = TPI_D;
@@ -162,33 +173,34 @@ __global__ void __launch_bounds__(RHO32_THREADS, RHO32_MIN_BLOCKS)
                 float4 qm = QM[a];
                 const float4 *Z = cur + a * hw + oz;
                 if (LD) {
-                    // k.mu = c0 + nz c1; B1 = (q + i c0) b, B2 = i c1 b, summand (B1 + nz B2) E2
+                    // k.mu = c0 + nz c1; B1 = (q + i c0) b, B2 = i c1 b, summand (B1 + nz B2) E2;
+                    // packed FP32x2 FMAs over the z pair: C = B1 + (2h, 2h+1) B2, then
+                    // accX += Cx ex - Cy ey, accY += Cx ey + Cy ex
                     float c0 = fnx * qm.y + fny * qm.z, c1 = qm.w;
                     float2 B1 = make_float2(qm.x * b.x - c0 * b.y, qm.x * b.y + c0 * b.x);
                     float2 B2 = make_float2(-c1 * b.y, c1 * b.x);
                     B1.x += fz0 * B2.x;
                     B1.y += fz0 * B2.y;
-                    // explicit FMA chains: acc += C e as four FMA per complex term
+                    const float2 b1x = make_float2(B1.x, B1.x), b2x = make_float2(B2.x, B2.x);
+                    const float2 nb1y = make_float2(-B1.y, -B1.y), nb2y = make_float2(-B2.y, -B2.y);
 #pragma unroll
                     for (int h = 0; h < ZB / 2; h++) {
                         float4 ee = Z[h];
-                        float2 C0 = make_float2(fmaf((float)(2 * h), B2.x, B1.x), fmaf((float)(2 * h), B2.y, B1.y));
-                        float2 C1 = make_float2(fmaf((float)(2 * h + 1), B2.x, B1.x),
-                                                fmaf((float)(2 * h + 1), B2.y, B1.y));
-                        acc[2 * h].x = fmaf(-C0.y, ee.y, fmaf(C0.x, ee.x, acc[2 * h].x));
-                        acc[2 * h].y = fmaf(C0.y, ee.x, fmaf(C0.x, ee.y, acc[2 * h].y));
-                        acc[2 * h + 1].x = fmaf(-C1.y, ee.w, fmaf(C1.x, ee.z, acc[2 * h + 1].x));
-                        acc[2 * h + 1].y = fmaf(C1.y, ee.z, fmaf(C1.x, ee.w, acc[2 * h + 1].y));
+                        const float2 ex = make_float2(ee.x, ee.y), ey = make_float2(ee.z, ee.w);
+                        const float2 zp = make_float2((float)(2 * h), (float)(2 * h + 1));
+                        float2 Cx = __ffma2_rn(zp, b2x, b1x), nCy = __ffma2_rn(zp, nb2y, nb1y);
+                        accX[h] = __ffma2_rn(nCy, ey, __ffma2_rn(Cx, ex, accX[h]));
+                        accY[h] = __ffma2_rn(Cx, ey, __ffma2_rn(make_float2(-nCy.x, -nCy.y), ex, accY[h]));
                     }
                 } else {
-                    float2 C = make_float2(qm.x * b.x, qm.x * b.y);
+                    const float2 cx = make_float2(qm.x * b.x, qm.x * b.x), cy = make_float2(qm.x * b.y, qm.x * b.y);
+                    const float2 ncy = make_float2(-cy.x, -cy.y);
 #pragma unroll
                     for (int h = 0; h < ZB / 2; h++) {
                         float4 ee = Z[h];
-                        acc[2 * h].x = fmaf(-C.y, ee.y, fmaf(C.x, ee.x, acc[2 * h].x));
-                        acc[2 * h].y = fmaf(C.y, ee.x, fmaf(C.x, ee.y, acc[2 * h].y));
-                        acc[2 * h + 1].x = fmaf(-C.y, ee.w, fmaf(C.x, ee.z, acc[2 * h + 1].x));
-                        acc[2 * h + 1].y = fmaf(C.y, ee.z, fmaf(C.x, ee.w, acc[2 * h + 1].y));
+                        const float2 ex = make_float2(ee.x, ee.y), ey = make_float2(ee.z, ee.w);
+                        accX[h] = __ffma2_rn(ncy, ey, __ffma2_rn(cx, ex, accX[h]));
+                        accY[h] = __ffma2_rn(cy, ex, __ffma2_rn(cx, ey, accY[h]));
                     }
                 }
             }
@@ -198,8 +210,10 @@ __global__ void __launch_bounds__(RHO32_THREADS, RHO32_MIN_BLOCKS)
     if (sid < nseg) {
         float2 *P = part + (size_t)blockIdx.y * nk + S.koff;
 #pragma unroll
-        for (int z = 0; z < ZB; z++)
-            if (z < S.cnt) P[z] = acc[z];
+        for (int h = 0; h < ZB / 2; h++) {
+            if (2 * h < S.cnt) P[2 * h] = make_float2(accX[h].x, accY[h].x);
+            if (2 * h + 1 < S.cnt) P[2 * h + 1] = make_float2(accX[h].y, accY[h].y);
+        }
     }
 }
 
@@ -229,20 +243,32 @@ __global__ void __launch_bounds__(ION32_THREADS, ION32_MIN_BLOCKS) k_ion32(Ion32
         KRow R = a.row[r0 + e];
         rnxy[e] = make_int2(R.nx, R.ny);
     }
+    // per row: entry 0 = (rho_0, 0); then for each z pair (2p+1, 2p+2) two planar
+    // entries, +z: (Re rho_z, Re rho_z', Im rho_z, Im rho_z') and the same for -z
     for (int e = threadIdx.x; e < nrs * (KZ + 1); e += ION32_THREADS) {
         int rr = e / (KZ + 1), zz = e - rr * (KZ + 1);
         KRow R = a.row[r0 + rr];
         int zlo = R.z0, zhi = R.z0 + R.cnt - 1;
         float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (zz >= zlo && zz <= zhi) {
-            double2 p = a.rho_s[R.koff + zz - zlo];
-            v.x = (float)p.x;
-            v.y = (float)p.y;
-        }
-        if (zz > 0 && -zz >= zlo && -zz <= zhi) {
-            double2 p = a.rho_s[R.koff - zz - zlo];
-            v.z = (float)p.x;
-            v.w = (float)p.y;
+        if (zz == 0) {
+            if (0 >= zlo && 0 <= zhi) {
+                double2 p = a.rho_s[R.koff - zlo];
+                v.x = (float)p.x;
+                v.y = (float)p.y;
+            }
+        } else {
+            int pr = (zz - 1) >> 1, sg = ((zz - 1) & 1) ? -1 : 1;
+            int za = sg * (2 * pr + 1), zb = sg * (2 * pr + 2);
+            if (za >= zlo && za <= zhi) {
+                double2 p = a.rho_s[R.koff + za - zlo];
+                v.x = (float)p.x;
+                v.z = (float)p.y;
+            }
+            if (zb >= zlo && zb <= zhi) {
+                double2 p = a.rho_s[R.koff + zb - zlo];
+                v.y = (float)p.x;
+                v.w = (float)p.y;
+            }
         }
         rk4[e] = v;
     }
@@ -253,9 +279,14 @@ __global__ void __launch_bounds__(ION32_THREADS, ION32_MIN_BLOCKS) k_ion32(Ion32
     double tx = c.B[0][0] * ri.x + c.B[1][0] * ri.y + c.B[2][0] * ri.z;
     double ty = c.B[0][1] * ri.x + c.B[1][1] * ri.y + c.B[2][1] * ri.z;
     double tz = c.B[0][2] * ri.x + c.B[1][2] * ri.y + c.B[2][2] * ri.z;
-    float2 E[KZ];
+    // E2[z], z = 1..KZ, as planar pairs over (2p+1, 2p+2)
+    float2 Ex[KZ / 2], Ey[KZ / 2];
 #pragma unroll
-    for (int z = 0; z < KZ; z++) E[z] = cis2pi32((double)(z + 1) * tz);
+    for (int pr = 0; pr < KZ / 2; pr++) {
+        float2 ea = cis2pi32((double)(2 * pr + 1) * tz), eb = cis2pi32((double)(2 * pr + 2) * tz);
+        Ex[pr] = make_float2(ea.x, eb.x);
+        Ey[pr] = make_float2(ea.y, eb.y);
+    }
     float mz = 0.f;
     double mx = 0.0, my = 0.0;
     if (WF && a.ld) {
@@ -271,32 +302,39 @@ __global__ void __launch_bounds__(ION32_THREADS, ION32_MIN_BLOCKS) k_ion32(Ion32
         float2 w = cis2pi32((double)R.x * tx + (double)R.y * ty);
         const float4 *rho = rk4 + rr * (KZ + 1);
         float4 r00 = rho[0];
-        // z = 0: phase w.  Even and odd z accumulate separately (shorter dependence chains)
-        float R1a = r00.y * w.x - r00.x * w.y, Rza = 0.f, R1b = 0.f, Rzb = 0.f;
-        float Q0a = 0.f, Q1a = 0.f, Q2a = 0.f, Q0b = 0.f, Q1b = 0.f, Q2b = 0.f;
-        if (WF) Q0a = r00.x * w.x + r00.y * w.y;
+        // z = 0: phase w; z = 1..KZ in packed FP32x2 pairs (two z per lane pair)
+        const float2 wx = make_float2(w.x, w.x), wy = make_float2(w.y, w.y), nwx = make_float2(-w.x, -w.x);
+        float2 R1v = make_float2(r00.y * w.x - r00.x * w.y, 0.f), Rzv = make_float2(0.f, 0.f);
+        float2 Q0v = make_float2(0.f, 0.f), Q1v = Q0v, Q2v = Q0v;
+        if (WF) Q0v.x = r00.x * w.x + r00.y * w.y;
 #pragma unroll
-        for (int z = 1; z <= KZ; z++) {
-            float4 rp = rho[z];
-            float2 e = E[z - 1];
+        for (int pr = 0; pr < KZ / 2; pr++) {
+            const float4 A = rho[1 + 2 * pr], B = rho[2 + 2 * pr];
+            const float2 rpx = make_float2(A.x, A.y), rpy = make_float2(A.z, A.w);
+            const float2 rnx = make_float2(B.x, B.y), rny = make_float2(B.z, B.w);
+            const float2 ex = Ex[pr], ey = Ey[pr];
+            const float2 zq = make_float2((float)(2 * pr + 1), (float)(2 * pr + 2));
             // w e = (p, s), w conj(e) = (p', s')
-            float u1 = w.y * e.y, u2 = w.y * e.x;
-            float p = fmaf(w.x, e.x, -u1), pp = fmaf(w.x, e.x, u1);
-            float s = fmaf(w.x, e.y, u2), sp = fmaf(-w.x, e.y, u2);
+            float2 u1 = __fmul2_rn(wy, ey), u2 = __fmul2_rn(wy, ex);
+            float2 p = __ffma2_rn(wx, ex, make_float2(-u1.x, -u1.y)), pp = __ffma2_rn(wx, ex, u1);
+            float2 sv = __ffma2_rn(wx, ey, u2), sp = __ffma2_rn(nwx, ey, u2);
             // rho.y ph.x - rho.x ph.y (the sign convention of k_rec_ion) for +z and -z
-            float xp = fmaf(rp.y, p, -rp.x * s), xm = fmaf(rp.w, pp, -rp.z * sp);
-            float &R1 = (z & 1) ? R1a : R1b, &Rz = (z & 1) ? Rza : Rzb;
-            R1 += xp + xm;
-            Rz = fmaf((float)z, xp - xm, Rz);
+            float2 t1 = __fmul2_rn(rpx, sv), t2 = __fmul2_rn(rnx, sp);
+            float2 xp = __ffma2_rn(rpy, p, make_float2(-t1.x, -t1.y));
+            float2 xm = __ffma2_rn(rny, pp, make_float2(-t2.x, -t2.y));
+            R1v = __fadd2_rn(R1v, __fadd2_rn(xp, xm));
+            Rzv = __ffma2_rn(zq, __fadd2_rn(xp, make_float2(-xm.x, -xm.y)), Rzv);
             if (WF) {
-                float cp = fmaf(rp.x, p, rp.y * s), cm = fmaf(rp.z, pp, rp.w * sp);
-                float &Q0 = (z & 1) ? Q0a : Q0b, &Q1 = (z & 1) ? Q1a : Q1b, &Q2 = (z & 1) ? Q2a : Q2b;
-                Q0 += cp + cm;
-                Q1 = fmaf((float)z, cp - cm, Q1);
-                Q2 = fmaf((float)(z * z), cp + cm, Q2);
+                float2 cp = __ffma2_rn(rpx, p, __fmul2_rn(rpy, sv)), cm = __ffma2_rn(rnx, pp, __fmul2_rn(rny, sp));
+                float2 cs = __fadd2_rn(cp, cm);
+                Q0v = __fadd2_rn(Q0v, cs);
+                Q1v = __ffma2_rn(zq, __fadd2_rn(cp, make_float2(-cm.x, -cm.y)), Q1v);
+                Q2v = __ffma2_rn(__fmul2_rn(zq, zq), cs, Q2v);
             }
         }
-        float R1 = R1a + R1b, Rz = Rza + Rzb;
+        float R1a = R1v.x, R1b = R1v.y, Rza = Rzv.x, Rzb = Rzv.y;
+        float Q0a = Q0v.x, Q0b = Q0v.y, Q1a = Q1v.x, Q1b = Q1v.y, Q2a = Q2v.x, Q2b = Q2v.y;
+    float R1 = R1a + R1b, Rz = Rza + Rzb;
         float Q0 = Q0a + Q0b, Q1 = Q1a + Q1b, Q2 = Q2a + Q2b;
         double fx = (double)R.x, fy = (double)R.y;
         S0 += fx * (double)R1;

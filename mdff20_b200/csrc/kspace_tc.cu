@@ -280,7 +280,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_rho_tc(RhoTcArgs a) {
                         const int ion = a.idx ? __ldg(a.idx + t) : t;
                         const int slotz = z <= 0 ? (z + a.K2) / 16 * 18 + (z + a.K2) % 16
                                                  : (a.nzb_neg + (z - 1) / 16) * 18 + (z - 1) % 16;
-                        const float2 E = __ldg(a.tab + (size_t)ion * a.tab_w + a.z_off + slotz);
+                        // planar z pairs: entry 2p = (x, x'), entry 2p + 1 = (y, y')
+                        const float2 *zp = a.tab + (size_t)ion * a.tab_w + a.z_off + (slotz & ~1);
+                        const float2 px = __ldg(zp), py = __ldg(zp + 1);
+                        const float2 E = (slotz & 1) ? make_float2(px.y, py.y) : make_float2(px.x, py.x);
                         const float4 qm = __ldg(a.qm + t);
                         const float c2 = (float)z * qm.w;
                         // X = E (q + i nz m2), Y = i m0 E, Z = i m1 E
