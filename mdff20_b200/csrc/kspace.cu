@@ -185,13 +185,24 @@ __global__ void __launch_bounds__(256) k_rho_reduce(int nk, int nchunks, const P
     __shared__ double2 ws[8][RHOR_K];
     int w = threadIdx.x >> 5, l = threadIdx.x & 31;
     int k = blockIdx.x * RHOR_K + l;
-    double2 acc = make_double2(0.0, 0.0);
-    if (k < nk)
-        for (int c = w; c < nchunks; c += 8) {
-            PT p = part[(size_t)c * nk + k];
-            acc.x += (double)p.x;
-            acc.y += (double)p.y;
+    // chunks w, w + 8, ...: four loads in flight into four accumulators (fixed order)
+    double2 a0 = make_double2(0.0, 0.0), a1 = a0, a2 = a0, a3 = a0;
+    if (k < nk) {
+        int c = w;
+        for (; c + 24 < nchunks; c += 32) {
+            PT p0 = part[(size_t)c * nk + k], p1 = part[(size_t)(c + 8) * nk + k];
+            PT p2 = part[(size_t)(c + 16) * nk + k], p3 = part[(size_t)(c + 24) * nk + k];
+            a0.x += (double)p0.x, a0.y += (double)p0.y;
+            a1.x += (double)p1.x, a1.y += (double)p1.y;
+            a2.x += (double)p2.x, a2.y += (double)p2.y;
+            a3.x += (double)p3.x, a3.y += (double)p3.y;
         }
+        for (; c < nchunks; c += 8) {
+            PT p = part[(size_t)c * nk + k];
+            a0.x += (double)p.x, a0.y += (double)p.y;
+        }
+    }
+    double2 acc = make_double2((a0.x + a1.x) + (a2.x + a3.x), (a0.y + a1.y) + (a2.y + a3.y));
     ws[w][l] = acc;
     __syncthreads();
     if (w) return;
