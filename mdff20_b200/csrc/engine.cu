@@ -38,12 +38,11 @@ __global__ void k_scale_add3(int n, double a, const double3 *x, double b, double
 __global__ void k_cg_residual(int n, const int *polar, const double *invpol, const double3 *efs,
                               const double3 *tx, const double3 *x, double3 *r);
 __global__ void k_cg_ap(int n, const int *polar, const double *invpol, const double3 *p, const double3 *tp,
-                        double3 *ap, double *part, int stride);
+                        double3 *ap, double *part, int stride, double *scal, unsigned *ticket);
 __global__ void k_cg_rz(int n, const int *polar, const double *pol, const double3 *r, double3 *z, double *part,
-                        int stride);
-__global__ void k_cg_update(int n, const double *scal, const double3 *p, const double3 *ap, double3 *x, double3 *r);
+                        int stride, double *scal, unsigned *ticket);
+__global__ void k_cg_update(int n, double *scal, const double3 *p, const double3 *ap, double3 *x, double3 *r);
 __global__ void k_cg_dir(int n, const double *scal, const double3 *z, double3 *p);
-__global__ void k_copy_slot(double *scal, int from, int to);
 __global__ void k_cg_check(cudaGraphConditionalHandle h, int first, const double *scal, DevScalars *out, int npol,
                            double tol, int maxit, unsigned *status);
 __global__ void k_upol_final(const double *scal, double coul, DevScalars *out);
@@ -142,6 +141,7 @@ Engine::Engine(const mdffgpu_params &prm, int dev) : p(prm) {
     d_svl = dalloc<double4>(n);
     d_rebuild = dalloc<int>(1);
     d_status = dalloc<unsigned>(1);
+    d_ticket = dalloc<unsigned>(8);
     d_scal = dalloc<double>(NSLOT);
     d_out = dalloc<DevScalars>(1);
     d_nhc = dalloc<double>(48);
@@ -210,6 +210,7 @@ Engine::~Engine() {
         cudaFree(x);
     cudaFree(d_out);
     cudaFree(d_status);
+    cudaFree(d_ticket);
     if (h_out) cudaFreeHost(h_out);
     if (h_stage) cudaFreeHost(h_stage);
     if (step_exec) cudaGraphExecDestroy(step_exec);
@@ -745,6 +746,7 @@ void Engine::field_pol(const double3 *d_p, double3 *d_out, double2 *rho_raw) {
     o.rho_raw = rho_raw;
     o.idx = d_pidx;
     o.cnt = npol;
+    o.energy = false;   // the matrix-vector product needs the field only
     launch_rec(*this, d_qzero, d_p, false, true, o);
 }
 
@@ -831,21 +833,20 @@ void Engine::pim_cg(bool fused) {
         field_of(d_qzero, d_mu_ind, false, true, false, d_ef_ind);
         MDFF_LAUNCH(*this, k_cg_residual, nb, 256, 0, n, d_polar, d_invpol, d_ef_stat, d_ef_ind, d_mu_ind, d_cg_r);
     }
-    MDFF_LAUNCH(*this, k_cg_rz, nb, 256, 0, n, d_polar, d_pol, d_cg_r, d_mu_save, d_part, part_stride);
-    reduce(S_RZ, 2, nb);
+    MDFF_LAUNCH(*this, k_cg_rz, nb, 256, 0, n, d_polar, d_pol, d_cg_r, d_mu_save, d_part, part_stride, d_scal,
+                d_ticket + 1);
     MDFF_CK(cudaMemcpyAsync(d_cg_p, d_mu_save, sizeof(double3) * n, cudaMemcpyDeviceToDevice, stream));
     int maxit = std::max(p.max_scf_pim_iter, 1);
     // one CG iteration up to the new residual norm (p <- z + beta p follows the test)
     auto iteration = [&]() {
         if (fused && use32 && rec32 && subset32 && npol > 0) field_pol(d_cg_p, d_ef_ind, d_rho_it);   // T p
         else field_of(d_qzero, d_cg_p, false, true, false, d_ef_ind, fused ? d_rho_it : nullptr);
-        MDFF_LAUNCH(*this, k_cg_ap, nb, 256, 0, n, d_polar, d_invpol, d_cg_p, d_ef_ind, d_cg_ap, d_part, part_stride);
-        reduce(S_PAP, 1, nb);
-        MDFF_LAUNCH(*this, k_copy_slot, 1, 1, 0, d_scal, (int)S_RZ, (int)S_RZOLD);
+        MDFF_LAUNCH(*this, k_cg_ap, nb, 256, 0, n, d_polar, d_invpol, d_cg_p, d_ef_ind, d_cg_ap, d_part, part_stride,
+                    d_scal, d_ticket);
         MDFF_LAUNCH(*this, k_cg_update, nb, 256, 0, n, d_scal, d_cg_p, d_cg_ap, d_mu_ind, d_cg_r);
         if (fused) launch_rho_axpy(*this, S_RZOLD, S_PAP, d_rho_it, d_rho_acc);
-        MDFF_LAUNCH(*this, k_cg_rz, nb, 256, 0, n, d_polar, d_pol, d_cg_r, d_mu_save, d_part, part_stride);
-        reduce(S_RZ, 2, nb);
+        MDFF_LAUNCH(*this, k_cg_rz, nb, 256, 0, n, d_polar, d_pol, d_cg_r, d_mu_save, d_part, part_stride, d_scal,
+                    d_ticket + 1);
     };
     if (capturing) {
         // graph: the loop is a while node whose condition the device test sets

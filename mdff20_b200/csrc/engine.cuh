@@ -109,6 +109,7 @@ struct RecOut {
     const double *efg_dir = nullptr;
     double2 *rho_raw = nullptr;       // receives rho(k) of (q, mu) when set
     const double2 *rho_acc = nullptr; // rho(k) of (q, mu) given: the rho pass is skipped
+    bool energy = true;               // false: skip the energy/virial reduction (field-only passes)
     const int *idx = nullptr;         // mixed precision: only these ions (q, mu zero elsewhere;
     int cnt = -1;                     // outputs written at these ions only), cnt of them
 };
@@ -245,6 +246,7 @@ struct Engine {
     DevScalars *d_out = nullptr; // composed results
     DevScalars *h_out = nullptr; // pinned mirror
     unsigned *d_status = nullptr;
+    unsigned *d_ticket = nullptr;   // block-arrival counters of kernels that finish their own reductions
     double *d_nhc = nullptr;     // xi[16], vxi[16], Q[16]
 
     // per-kernel timing of one chosen kernel family (CUDA events on `stream`)

@@ -42,12 +42,11 @@ enum FitSlot : int {
 __global__ void k_reduce_slots(const double *part, int stride, int first, int nparts, double *scal);
 // preconditioned CG kernels of integrate.cu
 __global__ void k_cg_ap(int n, const int *polar, const double *invpol, const double3 *p, const double3 *tp,
-                        double3 *ap, double *part, int stride);
+                        double3 *ap, double *part, int stride, double *scal, unsigned *ticket);
 __global__ void k_cg_rz(int n, const int *polar, const double *pol, const double3 *r, double3 *z, double *part,
-                        int stride);
-__global__ void k_cg_update(int n, const double *scal, const double3 *p, const double3 *ap, double3 *x, double3 *r);
+                        int stride, double *scal, unsigned *ticket);
+__global__ void k_cg_update(int n, double *scal, const double3 *p, const double3 *ap, double3 *x, double3 *r);
 __global__ void k_cg_dir(int n, const double *scal, const double3 *z, double3 *p);
-__global__ void k_copy_slot(double *scal, int from, int to);
 
 struct TTd {
     double E[9];   // 1/k!
@@ -434,8 +433,8 @@ void Engine::solve_pim(const double3 *d_b, double3 *d_x, double rtol, int maxit)
     int nb = ceil_div(n, 256);
     MDFF_CK(cudaMemsetAsync(d_x, 0, sizeof(double3) * n, stream));
     MDFF_CK(cudaMemcpyAsync(d_cg_r, d_b, sizeof(double3) * n, cudaMemcpyDeviceToDevice, stream));
-    MDFF_LAUNCH(*this, k_cg_rz, nb, 256, 0, n, d_polar, d_pol, d_cg_r, d_mu_save, d_part, part_stride);
-    reduce(S_RZ, 2, nb);
+    MDFF_LAUNCH(*this, k_cg_rz, nb, 256, 0, n, d_polar, d_pol, d_cg_r, d_mu_save, d_part, part_stride, d_scal,
+                d_ticket + 1);
     MDFF_CK(cudaMemcpyAsync(d_cg_p, d_mu_save, sizeof(double3) * n, cudaMemcpyDeviceToDevice, stream));
     double rr0 = 0.0, rr = 0.0;
     MDFF_CK(cudaMemcpyAsync(&rr0, d_scal + S_RR, sizeof(double), cudaMemcpyDeviceToHost, stream));
@@ -444,12 +443,11 @@ void Engine::solve_pim(const double3 *d_b, double3 *d_x, double rtol, int maxit)
     int it = 0;
     while (rr > rtol * rtol * rr0 && rr > 0.0 && it < maxit) {
         field_of(d_qzero, d_cg_p, false, true, false, d_ef_ind);
-        MDFF_LAUNCH(*this, k_cg_ap, nb, 256, 0, n, d_polar, d_invpol, d_cg_p, d_ef_ind, d_cg_ap, d_part, part_stride);
-        reduce(S_PAP, 1, nb);
-        MDFF_LAUNCH(*this, k_copy_slot, 1, 1, 0, d_scal, (int)S_RZ, (int)S_RZOLD);
+        MDFF_LAUNCH(*this, k_cg_ap, nb, 256, 0, n, d_polar, d_invpol, d_cg_p, d_ef_ind, d_cg_ap, d_part, part_stride,
+                    d_scal, d_ticket);
         MDFF_LAUNCH(*this, k_cg_update, nb, 256, 0, n, d_scal, d_cg_p, d_cg_ap, d_x, d_cg_r);
-        MDFF_LAUNCH(*this, k_cg_rz, nb, 256, 0, n, d_polar, d_pol, d_cg_r, d_mu_save, d_part, part_stride);
-        reduce(S_RZ, 2, nb);
+        MDFF_LAUNCH(*this, k_cg_rz, nb, 256, 0, n, d_polar, d_pol, d_cg_r, d_mu_save, d_part, part_stride, d_scal,
+                    d_ticket + 1);
         MDFF_CK(cudaMemcpyAsync(&rr, d_scal + S_RR, sizeof(double), cudaMemcpyDeviceToHost, stream));
         MDFF_CK(cudaStreamSynchronize(stream));
         if (!std::isfinite(rr)) throw Error(MDFFGPU_ERR_NONFINITE, "adjoint CG diverged");

@@ -45,6 +45,37 @@ __device__ __forceinline__ void block_sum_to_part(double (&v)[NV], double *part,
     }
 }
 
+// The last block of a kernel to finish reduces the partials of slots first..first+nslots-1
+// exactly as k_reduce_slots does (same order), so the separate reduction launch is not
+// needed; ticket (zero between calls) counts the finished blocks.  The writers of the
+// partials fence their writes before arriving.
+__device__ __forceinline__ void last_block_slots(const double *part, int stride, int first, int nslots,
+                                                 double *scal, unsigned *ticket) {
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    __shared__ double sh[32];
+    for (int sl = first; sl < first + nslots; sl++) {
+        const volatile double *p = part + (size_t)sl * stride;
+        double a = 0.0;
+        for (int k = threadIdx.x; k < (int)gridDim.x; k += blockDim.x) a += p[k];
+        a = warp_sum(a);
+        if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = a;
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            double b = (threadIdx.x < (blockDim.x >> 5)) ? sh[threadIdx.x] : 0.0;
+            b = warp_sum(b);
+            if (threadIdx.x == 0) scal[sl] = b;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *ticket = 0u;
+}
+
 // ---------------------------------------------------------------- small helpers
 __global__ void k_fill3(int n, double3 *a, double3 v) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -284,7 +315,7 @@ __global__ void k_cg_residual(int n, const int *__restrict__ polar, const double
 // Ap = alpha^-1 p - T p ; partial sums of p.Ap
 __global__ void k_cg_ap(int n, const int *__restrict__ polar, const double *__restrict__ invpol,
                         const double3 *__restrict__ p, const double3 *__restrict__ tp, double3 *__restrict__ ap,
-                        double *part, int stride) {
+                        double *part, int stride, double *scal, unsigned *ticket) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double v[1] = {0.0};
     if (i < n) {
@@ -301,11 +332,13 @@ __global__ void k_cg_ap(int n, const int *__restrict__ polar, const double *__re
         }
     }
     block_sum_to_part<1>(v, part, S_PAP, stride);
+    last_block_slots(part, stride, S_PAP, 1, scal, ticket);
 }
 
 // z = alpha r ; partial sums of r.z and r.r
 __global__ void k_cg_rz(int n, const int *__restrict__ polar, const double *__restrict__ pol,
-                        const double3 *__restrict__ r, double3 *__restrict__ z, double *part, int stride) {
+                        const double3 *__restrict__ r, double3 *__restrict__ z, double *part, int stride,
+                        double *scal, unsigned *ticket) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double v[2] = {0.0, 0.0};
     if (i < n) {
@@ -320,14 +353,16 @@ __global__ void k_cg_rz(int n, const int *__restrict__ polar, const double *__re
         }
     }
     block_sum_to_part<2>(v, part, S_RZ, stride);  // r.z, r.r
+    last_block_slots(part, stride, S_RZ, 2, scal, ticket);
 }
 
-// x += a p ; r -= a Ap, with a = rz / pAp read on the device
-__global__ void k_cg_update(int n, const double *__restrict__ scal, const double3 *__restrict__ p,
+// x += a p ; r -= a Ap, with a = rz / pAp read on the device; rz is kept as rz_old
+__global__ void k_cg_update(int n, double *__restrict__ scal, const double3 *__restrict__ p,
                             const double3 *__restrict__ ap, double3 *__restrict__ x, double3 *__restrict__ r) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double a = scal[S_RZ] / scal[S_PAP];
+    if (i == 0) scal[S_RZOLD] = scal[S_RZ];
     if (i >= n) return;
-    double a = scal[S_RZOLD] / scal[S_PAP];
     double3 pp = p[i], q = ap[i], xx = x[i], rr = r[i];
     x[i] = make_double3(xx.x + a * pp.x, xx.y + a * pp.y, xx.z + a * pp.z);
     r[i] = make_double3(rr.x - a * q.x, rr.y - a * q.y, rr.z - a * q.z);
@@ -341,10 +376,6 @@ __global__ void k_cg_dir(int n, const double *__restrict__ scal, const double3 *
     double beta = scal[S_RZ] / scal[S_RZOLD];
     double3 zz = z[i], pp = p[i];
     p[i] = make_double3(zz.x + beta * pp.x, zz.y + beta * pp.y, zz.z + beta * pp.z);
-}
-
-__global__ void k_copy_slot(double *scal, int from, int to) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) scal[to] = scal[from];
 }
 
 // CG stopping test on the device (graph-captured steps): rmsd = sqrt(r.r / npol), the

@@ -488,7 +488,7 @@ static void launch_rec32(Engine &e, const double *q, const double3 *mu, bool lq,
         MDFF_LAUNCH(e, k_rho_reduce<float2>, nbr, 256, 0, e.nk, e.rho_chunks_used, e.d_rho_part32, e.d_Ak, e.d_kcoe,
                     e.d_kvec, e.d_rho, o.rho_raw, e.d_part, (int)S_REC_U, e.part_stride);
     }
-    e.reduce(S_REC_U, 7, nbr);
+    if (o.energy) e.reduce(S_REC_U, 7, nbr);
     if (!o.ef && !o.f) return;
     launch_ion32(e, lq ? q : nullptr, mu, ld, o, o.idx, cnt);
 }
