@@ -221,7 +221,7 @@ struct Engine {
     double2 *d_rho_part = nullptr, *d_rho = nullptr;   // partial per ion chunk, total (Ak-scaled)
     double2 *d_rho_acc = nullptr, *d_rho_it = nullptr; // rho(k) of (q, mu) along the fused CG; of its p
     // mixed precision k space (kspace32.cu)
-    KSeg *d_seg32 = nullptr;                            // (row, z block) segments, pad0 = block
+    KSeg *d_seg32 = nullptr;                            // rho segments: (row, block of |nz|), both signs
     int nseg32 = 0, tab_w = 0;
     float2 *d_tab32 = nullptr;                          // phase table rows [n][tab_w]
     int rho32_chunks = 0;

@@ -15,12 +15,13 @@
 // the values are stored as planar pairs, (Re E2[z], Re E2[z+1]) then (Im E2[z],
 // Im E2[z+1]), the operand layout of the packed FP32x2 FMA (FFMA2) of k_rho32.
 //
-// k_rho32   : rho(k) = sum_i (q_i + i k.mu_i) E0 E1 E2.  Thread = one (row, z block)
-//             segment, ions stream through shared memory in tiles of table rows; the
-//             summand (B1' + j B2) E2[z0 + j] costs 6 FMA (4 without dipoles), j an
-//             unrolled constant, issued as packed FP32x2 FMAs over pairs of z (3 per z,
-//             2 without dipoles).  FP32 sums over one block's ion chunk, chunk partials
-//             summed in FP64 in a fixed order (k_rho_reduce32).
+// k_rho32   : rho(k) = sum_i (q_i + i k.mu_i) E0 E1 E2.  Thread = one segment (a row
+//             and RZP values of |nz|, both signs: E2[-nz] = conj E2[nz]); ions stream
+//             through shared memory in tiles of table rows; eight weighted sums per
+//             |nz| give rho(+nz) and rho(-nz), 4 FMA per k-vector (2 without dipoles),
+//             issued as packed FP32x2 FMAs over pairs of |nz|.  FP32 sums over one
+//             block's ion chunk, chunk partials summed in FP64 in a fixed order
+//             (k_rho_reduce32).
 // k_ion32   : per ion and k-slice the n-space sums of field (and force) terms.  Thread
 //             = ion; Ak rho(k) of the slice sits in shared memory as (rho_z, rho_-z)
 //             pairs; per row the phase base exp(2 pi i (nx tx + ny ty)) is reduced in
@@ -34,9 +35,10 @@ namespace mdffgpu {
 
 constexpr int ZB = 16;              // nz per segment block (two complex per 16-byte load)
 constexpr int ZS = ZB + 2;          // block stride: consecutive blocks start 4 banks apart
+constexpr int RZP = 8;              // |nz| values per rho segment (each for +nz and -nz)
 constexpr int RHO32_THREADS = 128;
-constexpr int RHO32_TI = 16;        // ions per shared-memory tile (two tiles in flight)
-constexpr int RHO32_MIN_BLOCKS = 8;
+constexpr int RHO32_TI = 32;        // ions per shared-memory tile (two tiles in flight)
+constexpr int RHO32_MIN_BLOCKS = 5;
 constexpr int ION32_THREADS = 128;
 constexpr int ION32_MIN_BLOCKS = 5;
 
@@ -108,37 +110,50 @@ __global__ void k_phase32(int n, Cell c, const double4 *__restrict__ r, TabLayou
 }
 
 // ---------------------------------------------------------------- pass 1: rho(k)
+// The summand of k = (nx, ny, nz) is (B1 + nz B2) E2[nz] with B1 = (q + i c0) b,
+// B2 = i c1 b, b = E0[nx] E1[ny], c0 = 2 pi (nx m0 + ny m1), c1 = 2 pi m2 (m = B^T mu).
+// E2[-z] = conj E2[z], so with E2[z] = (c, d) the sums over ions of the eight products
+//     Sa = B1x c, Sb = B1y d, Sc = B1x d, Sd = B1y c,  Ta..Td the same with B2
+// give both rho(+z) and rho(-z):
+//     rho(+z) = (Sa - Sb + z (Ta - Tb),  Sc + Sd + z (Tc + Td))
+//     rho(-z) = (Sa + Sb - z (Ta + Tb),  Sd - Sc + z (Tc - Td))
+// 4 FMA per k-vector (2 without dipoles), issued as packed FP32x2 FMAs over the z pairs
+// of the table.  A thread owns one segment: a row (nx, ny) and RZP consecutive |nz|,
+// both signs, plus nz = 0 in the segment that starts at |nz| = 1.  Only the E0, E1 and
+// positive-z parts of a table row are staged in shared memory.
 template <bool LQ, bool LD>
 __global__ void __launch_bounds__(RHO32_THREADS, RHO32_MIN_BLOCKS)
     k_rho32(int cnt, const int *__restrict__ idx, int chunk, TabLayout L, const float2 *__restrict__ tab,
             Cell c, const double *__restrict__ q, const double3 *__restrict__ mu, int nseg,
             const KSeg *__restrict__ seg, float2 *__restrict__ part, int nk) {
+    constexpr int NP = RZP / 2;
     extern __shared__ float4 sm4[];
-    const int hw = L.w / 2;                              // table row in 16-byte units
-    // two stages: [2][RHO32_TI][hw] table rows, then [2][RHO32_TI] (q, 2 pi m)
-    float4 *QMs = sm4 + 2 * RHO32_TI * hw;
+    const int ha = L.z / 2, skip = (ZS / 2) * L.nzb_neg;   // 16-byte units
+    const int hw = L.w / 2, cw = hw - skip;               // staged row: E0 E1 | z > 0 blocks
+    // two stages: [2][RHO32_TI][cw] staged rows, then [2][RHO32_TI] (q, 2 pi m)
+    float4 *QMs = sm4 + 2 * RHO32_TI * cw;
     int sid = blockIdx.x * RHO32_THREADS + threadIdx.x;
     KSeg S;
     if (sid < nseg) S = seg[sid];
-    else S.nx = S.ny = S.z0 = S.cnt = S.koff = S.pad0 = 0;
-    const float fnx = (float)S.nx, fny = (float)S.ny, fz0 = (float)S.z0;
-    const int o0 = S.nx, o1 = L.e1 + L.K1 + S.ny, oz = (L.z + ZS * S.pad0) / 2;
-    // accumulators of z pairs (2h, 2h + 1): real parts accX[h], imaginary parts accY[h]
-    float2 accX[ZB / 2], accY[ZB / 2];
+    else S.nx = S.ny = S.z0 = S.cnt = S.koff = S.pad0 = S.pad1 = S.pad2 = 0;
+    const float fnx = (float)S.nx, fny = (float)S.ny;
+    const int o0 = S.nx, o1 = L.e1 + L.K1 + S.ny;
+    float2 Sa[NP], Sb[NP], Sc[NP], Sd[NP], Ta[NP], Tb[NP], Tc[NP], Td[NP];
 #pragma unroll
-    for (int h = 0; h < ZB / 2; h++) accX[h] = accY[h] = make_float2(0.f, 0.f);
+    for (int h = 0; h < NP; h++) Sa[h] = Sb[h] = Sc[h] = Sd[h] = Ta[h] = Tb[h] = Tc[h] = Td[h] = make_float2(0.f, 0.f);
+    float2 acc0 = make_float2(0.f, 0.f);
     int a0 = blockIdx.y * chunk, a1 = min(cnt, a0 + chunk);
     int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const double tpi = TPI_D;
-    // table rows of the tile at t0 into stage buffer `st` by asynchronous 16-byte copies
+    // staged rows of the tile at t0 into stage buffer `st` by asynchronous 16-byte copies
     // (warp w copies rows w, w+4, ...); every thread commits one group per tile
     auto issue = [&](int t0, int st) {
         int nt = min(RHO32_TI, a1 - t0);
-        float4 *dst = sm4 + st * RHO32_TI * hw;
+        float4 *dst = sm4 + st * RHO32_TI * cw;
         for (int a = w; a < nt; a += RHO32_THREADS / 32) {
             int ion = idx ? idx[t0 + a] : t0 + a;
             const float4 *src = (const float4 *)(tab + (size_t)ion * L.w);
-            for (int j = lane; j < hw; j += 32) cp_async16(dst + a * hw + j, src + j);
+            for (int j = lane; j < cw; j += 32) cp_async16(dst + a * cw + j, src + (j < ha ? j : j + skip));
         }
         cp_async_commit();
     };
@@ -165,42 +180,38 @@ __global__ void __launch_bounds__(RHO32_THREADS, RHO32_MIN_BLOCKS)
             QM[threadIdx.x] = v;
         }
         __syncthreads();
-        const float4 *cur = sm4 + st * RHO32_TI * hw;
+        const float4 *cur = sm4 + st * RHO32_TI * cw;
         if (sid < nseg) {
             for (int a = 0; a < nt; a++) {
-                const float2 *R = (const float2 *)(cur + a * hw);
+                const float2 *R = (const float2 *)(cur + a * cw);
                 float2 b = cmul32(R[o0], R[o1]);
                 float4 qm = QM[a];
-                const float4 *Z = cur + a * hw + oz;
+                float2 B1, B2 = make_float2(0.f, 0.f);
                 if (LD) {
-                    // k.mu = c0 + nz c1; B1 = (q + i c0) b, B2 = i c1 b, summand (B1 + nz B2) E2;
-                    // packed FP32x2 FMAs over the z pair: C = B1 + (2h, 2h+1) B2, then
-                    // accX += Cx ex - Cy ey, accY += Cx ey + Cy ex
                     float c0 = fnx * qm.y + fny * qm.z, c1 = qm.w;
-                    float2 B1 = make_float2(qm.x * b.x - c0 * b.y, qm.x * b.y + c0 * b.x);
-                    float2 B2 = make_float2(-c1 * b.y, c1 * b.x);
-                    B1.x += fz0 * B2.x;
-                    B1.y += fz0 * B2.y;
-                    const float2 b1x = make_float2(B1.x, B1.x), b2x = make_float2(B2.x, B2.x);
-                    const float2 nb1y = make_float2(-B1.y, -B1.y), nb2y = make_float2(-B2.y, -B2.y);
-#pragma unroll
-                    for (int h = 0; h < ZB / 2; h++) {
-                        float4 ee = Z[h];
-                        const float2 ex = make_float2(ee.x, ee.y), ey = make_float2(ee.z, ee.w);
-                        const float2 zp = make_float2((float)(2 * h), (float)(2 * h + 1));
-                        float2 Cx = __ffma2_rn(zp, b2x, b1x), nCy = __ffma2_rn(zp, nb2y, nb1y);
-                        accX[h] = __ffma2_rn(nCy, ey, __ffma2_rn(Cx, ex, accX[h]));
-                        accY[h] = __ffma2_rn(Cx, ey, __ffma2_rn(make_float2(-nCy.x, -nCy.y), ex, accY[h]));
-                    }
+                    B1 = LQ ? make_float2(qm.x * b.x - c0 * b.y, qm.x * b.y + c0 * b.x) : make_float2(-c0 * b.y, c0 * b.x);
+                    B2 = make_float2(-c1 * b.y, c1 * b.x);
                 } else {
-                    const float2 cx = make_float2(qm.x * b.x, qm.x * b.x), cy = make_float2(qm.x * b.y, qm.x * b.y);
-                    const float2 ncy = make_float2(-cy.x, -cy.y);
+                    B1 = make_float2(qm.x * b.x, qm.x * b.y);
+                }
+                acc0.x += B1.x;
+                acc0.y += B1.y;
+                const float2 b1x = make_float2(B1.x, B1.x), b1y = make_float2(B1.y, B1.y);
+                const float2 b2x = make_float2(B2.x, B2.x), b2y = make_float2(B2.y, B2.y);
+                const float4 *Z = cur + a * cw + S.pad0;
 #pragma unroll
-                    for (int h = 0; h < ZB / 2; h++) {
-                        float4 ee = Z[h];
-                        const float2 ex = make_float2(ee.x, ee.y), ey = make_float2(ee.z, ee.w);
-                        accX[h] = __ffma2_rn(ncy, ey, __ffma2_rn(cx, ex, accX[h]));
-                        accY[h] = __ffma2_rn(cy, ex, __ffma2_rn(cx, ey, accY[h]));
+                for (int h = 0; h < NP; h++) {
+                    const float4 ee = Z[h];
+                    const float2 cv = make_float2(ee.x, ee.y), dv = make_float2(ee.z, ee.w);
+                    Sa[h] = __ffma2_rn(b1x, cv, Sa[h]);
+                    Sb[h] = __ffma2_rn(b1y, dv, Sb[h]);
+                    Sc[h] = __ffma2_rn(b1x, dv, Sc[h]);
+                    Sd[h] = __ffma2_rn(b1y, cv, Sd[h]);
+                    if (LD) {
+                        Ta[h] = __ffma2_rn(b2x, cv, Ta[h]);
+                        Tb[h] = __ffma2_rn(b2y, dv, Tb[h]);
+                        Tc[h] = __ffma2_rn(b2x, dv, Tc[h]);
+                        Td[h] = __ffma2_rn(b2y, cv, Td[h]);
                     }
                 }
             }
@@ -208,11 +219,24 @@ __global__ void __launch_bounds__(RHO32_THREADS, RHO32_MIN_BLOCKS)
         __syncthreads();
     }
     if (sid < nseg) {
+        // k index of nz in this row: S.koff + nz
         float2 *P = part + (size_t)blockIdx.y * nk + S.koff;
+        const bool neg = S.pad1 & 1;
+        if (S.pad1 & 2) P[0] = acc0;
 #pragma unroll
-        for (int h = 0; h < ZB / 2; h++) {
-            if (2 * h < S.cnt) P[2 * h] = make_float2(accX[h].x, accY[h].x);
-            if (2 * h + 1 < S.cnt) P[2 * h + 1] = make_float2(accX[h].y, accY[h].y);
+        for (int h = 0; h < NP; h++) {
+#pragma unroll
+            for (int l = 0; l < 2; l++) {
+                if (2 * h + l >= S.cnt) continue;
+                const int z = S.z0 + 2 * h + l;
+                const float fz = (float)z;
+                const float sa = l ? Sa[h].y : Sa[h].x, sb = l ? Sb[h].y : Sb[h].x;
+                const float sc = l ? Sc[h].y : Sc[h].x, sd = l ? Sd[h].y : Sd[h].x;
+                const float ta = l ? Ta[h].y : Ta[h].x, tb = l ? Tb[h].y : Tb[h].x;
+                const float tc = l ? Tc[h].y : Tc[h].x, td = l ? Td[h].y : Td[h].x;
+                P[z] = make_float2(sa - sb + fz * (ta - tb), sc + sd + fz * (tc + td));
+                if (neg) P[-z] = make_float2(sa + sb - fz * (ta + tb), sd - sc + fz * (tc - td));
+            }
         }
     }
 }
@@ -432,7 +456,7 @@ static TabLayout layout_of(const Engine &e) {
     L.K1 = e.kmax[1];
     L.K2 = e.kmax[2];
     L.nzb_neg = ceil_div(L.K2 + 1, ZB);
-    L.nzb = L.nzb_neg + ceil_div(L.K2, ZB);
+    L.nzb = L.nzb_neg + std::max(1, ceil_div(L.K2, ZB));   // at least one z > 0 block
     L.e1 = L.K0 + 1;
     L.z = L.e1 + 2 * L.K1 + 1;
     L.z += L.z & 1;
@@ -445,23 +469,23 @@ static int kz_of(int K2) { return K2 <= 8 ? 8 : (K2 <= 14 ? 14 : (K2 <= 16 ? 16 
 void setup_kspace32(Engine &e, const std::vector<KRow> &rows) {
     TabLayout L = layout_of(e);
     if (kz_of(L.K2) < L.K2) throw Error(MDFFGPU_ERR_ARG, "mixed precision k-space supports kmax_z <= 32");
+    // rho segments: per row, |nz| blocks of RZP starting at 1; the row holds nz = -K2..K2,
+    // or nz = 1..K2 for (nx, ny) = (0, 0)
     std::vector<KSeg> segs;
     for (const KRow &R : rows) {
-        int zlo = R.z0, zhi = R.z0 + R.cnt - 1;
-        for (int b = 0; b < L.nzb; b++) {
-            int z0 = (b < L.nzb_neg) ? -L.K2 + ZB * b : 1 + ZB * (b - L.nzb_neg);
-            int z1 = (b < L.nzb_neg) ? std::min(z0 + ZB - 1, 0) : std::min(z0 + ZB - 1, L.K2);
-            int lo = std::max(z0, zlo), hi = std::min(z1, zhi);
-            if (lo > hi) continue;
-            if (lo != z0) throw Error(MDFFGPU_ERR_ARG, "k row does not start on a z block");
+        bool full = R.z0 == -L.K2;
+        if ((!full && R.z0 != 1) || R.z0 + R.cnt - 1 != L.K2) throw Error(MDFFGPU_ERR_ARG, "unexpected k row extent");
+        for (int z0 = 1; z0 <= std::max(L.K2, 1); z0 += RZP) {   // K2 = 0: one segment for nz = 0
             KSeg S;
             S.nx = R.nx;
             S.ny = R.ny;
             S.z0 = z0;
-            S.cnt = hi - lo + 1;
-            S.koff = R.koff + (lo - zlo);
-            S.pad0 = b;
-            S.pad1 = S.pad2 = 0;
+            S.cnt = std::max(0, std::min(RZP, L.K2 - z0 + 1));
+            S.koff = R.koff - R.z0;
+            // staged-row offset (16-byte units) of the pair (z0, z0 + 1) in the z > 0 blocks
+            S.pad0 = L.z / 2 + (ZS / 2) * ((z0 - 1) / ZB) + ((z0 - 1) % ZB) / 2;
+            S.pad1 = (full ? 1 : 0) | ((full && z0 == 1) ? 2 : 0);
+            S.pad2 = 0;
             segs.push_back(S);
         }
     }
@@ -507,7 +531,8 @@ void launch_coords32(Engine &e) {
     if (e.d_tab32) launch_phase32(e);
 }
 
-double rho_flops_per_pair(bool lq, bool ld);
+// FLOPs per (ion, k-vector) of the paired-nz formulation: 4 FMA with dipoles, 2 without
+static double rho32_flops_per_pair(bool ld) { return ld ? 8.0 : 4.0; }
 double ion_flops_per_pair(bool f, bool efg);
 void launch_rho_reduce32(Engine &e, const float2 *part, int nchunks, double2 *rho_raw);
 
@@ -527,7 +552,8 @@ void launch_rho32(Engine &e, const double *q, const double3 *mu, bool lq, bool l
     int chunk = ceil_div(std::max(cnt, 1), e.rho32_chunks);
     chunk = ceil_div(chunk, 4) * 4;
     dim3 grid(segblocks, e.rho32_chunks);
-    size_t smem = 2 * (sizeof(float2) * RHO32_TI * L.w + sizeof(float4) * RHO32_TI);
+    const int cw = L.w / 2 - (ZS / 2) * L.nzb_neg;
+    size_t smem = 2 * (sizeof(float4) * RHO32_TI * cw + sizeof(float4) * RHO32_TI);
     int ps = -1;
     e.prof_begin("k_rho", &ps);
     e.rho_chunks_used = e.rho32_chunks;
@@ -538,7 +564,7 @@ void launch_rho32(Engine &e, const double *q, const double3 *mu, bool lq, bool l
     else if (lq) rho32_launch<true, false>(e, grid, smem, cnt, idx, chunk, L, q, mu);
     else if (ld) rho32_launch<false, true>(e, grid, smem, cnt, idx, chunk, L, q, mu);
     else MDFF_CK(cudaMemsetAsync(e.d_rho_part32, 0, sizeof(float2) * (size_t)e.nk * e.rho32_chunks, e.stream));
-    e.prof_end("k_rho", ps, (lq || ld) ? rho_flops_per_pair(lq, ld) * (double)cnt * e.nk : 0.0);
+    e.prof_end("k_rho", ps, (lq || ld) ? rho32_flops_per_pair(ld) * (double)cnt * e.nk : 0.0);
 }
 
 template <int KZ, bool WF>
