@@ -23,10 +23,10 @@
 //             block's ion chunk, chunk partials summed in FP64 in a fixed order
 //             (k_rho_reduce32).
 // k_ion32   : per ion and k-slice the n-space sums of field (and force) terms.  Thread
-//             = ion; Ak rho(k) of the slice sits in shared memory as (rho_z, rho_-z)
-//             pairs; per row the phase base exp(2 pi i (nx tx + ny ty)) is reduced in
-//             FP64, E2[z] (z = 1..KZ) sits in registers, and the phases of +z and -z come
-//             from one product each (6 ops per pair of k).  Row sums FP32, rows FP64.
+//             = ion; per row the block stages the weights of Ak rho(+z) and Ak rho(-z)
+//             folded over the sign of nz, E2[z] (z = 1..KZ) sits in registers, the row
+//             sums cost 2 FMA per k-vector (3 with forces) and one product with the row
+//             phase exp(2 pi i (nx tx + ny ty)), reduced in FP64.  Row sums FP32, rows FP64.
 // Both passes take an optional ion index list (the polarisable ions of an induced-
 // dipole iteration, whose search directions vanish elsewhere).
 #include "engine.cuh"
@@ -254,47 +254,75 @@ struct Ion32Args {
     int ld;
 };
 
+// float4 entries per z pair of a staged row: the G and H weights, and K with forces
+__host__ __device__ constexpr int ion32_nv(bool wf) { return wf ? 6 : 4; }
+static int ion32_row_bytes(int KZ, bool wf) {
+    return (int)sizeof(float4) * (1 + (KZ / 2) * ion32_nv(wf)) + (int)sizeof(int2);
+}
+
+// With Y(k) = Ak rho(k) conj(exp(i k.r)), the field needs Im Y, the force Re Y, summed
+// over k with weights 1, nz (and nz^2).  In a row, exp(i k.r) = w E2[nz] with the row
+// phase w, and E2[-z] = conj E2[z] = (c, -d), so over the row
+//     sum Y = conj(w) G,  sum nz Y = conj(w) H,  sum nz^2 Y = conj(w) K,
+//     G = rho_0 + sum_z (a1 c + a2 d, a3 c + a4 d),   K = sum_z z^2 (same terms)
+//     H = sum_z z (-a4 c + a3 d, a2 c - a1 d)
+// with a1 = Re(rho_z + rho_-z), a2 = Im(rho_z - rho_-z), a3 = Im(rho_z + rho_-z),
+// a4 = Re(rho_-z - rho_z) of Ak rho.  The block stages a1..a4 (and their z, z^2
+// multiples) of its rows in shared memory as planar z pairs; per ion the sums cost
+// 2 FMA per k-vector (3 with forces), packed FP32x2 FMAs over the pairs.
 template <int KZ, bool WF>
 __global__ void __launch_bounds__(ION32_THREADS, ION32_MIN_BLOCKS) k_ion32(Ion32Args a) {
-    extern __shared__ float4 rk4[];          // [rows of the slice][KZ + 1]: (rho_z, rho_-z)
-    int2 *rnxy = (int2 *)(rk4 + a.rows_per_slice * (KZ + 1));   // (nx, ny) of the slice's rows
+    constexpr int NV = ion32_nv(WF), NP = KZ / 2, RS = 1 + NP * NV;
+    extern __shared__ float4 rk4[];          // [rows of the slice][RS]
+    int2 *rnxy = (int2 *)(rk4 + a.rows_per_slice * RS);   // (nx, ny) of the slice's rows
     int li = blockIdx.x * ION32_THREADS + threadIdx.x;
     int sl = blockIdx.y;
     int r0 = sl * a.rows_per_slice, r1 = min(a.nrow, r0 + a.rows_per_slice);
-    // Ak rho(k) of the slice's rows, padded to z = -KZ..KZ
     int nrs = r1 - r0;
     for (int e = threadIdx.x; e < nrs; e += ION32_THREADS) {
         KRow R = a.row[r0 + e];
         rnxy[e] = make_int2(R.nx, R.ny);
     }
-    // per row: entry 0 = (rho_0, 0); then for each z pair (2p+1, 2p+2) two planar
-    // entries, +z: (Re rho_z, Re rho_z', Im rho_z, Im rho_z') and the same for -z
-    for (int e = threadIdx.x; e < nrs * (KZ + 1); e += ION32_THREADS) {
-        int rr = e / (KZ + 1), zz = e - rr * (KZ + 1);
+    // per row: entry 0 = (rho_0, 0, 0); then per z pair (z, z') = (2p+1, 2p+2):
+    //   (a1, a1', a2, a2'), (a3, a3', a4, a4'), z (-a4, -a4', a3, a3'), z (a2, a2', -a1, -a1'),
+    //   [forces] z^2 (a1, a1', a2, a2'), z^2 (a3, a3', a4, a4')
+    for (int e = threadIdx.x; e < nrs * (NP + 1); e += ION32_THREADS) {
+        int rr = e / (NP + 1), pe = e - rr * (NP + 1);
         KRow R = a.row[r0 + rr];
         int zlo = R.z0, zhi = R.z0 + R.cnt - 1;
-        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (zz == 0) {
-            if (0 >= zlo && 0 <= zhi) {
-                double2 p = a.rho_s[R.koff - zlo];
-                v.x = (float)p.x;
-                v.y = (float)p.y;
-            }
-        } else {
-            int pr = (zz - 1) >> 1, sg = ((zz - 1) & 1) ? -1 : 1;
-            int za = sg * (2 * pr + 1), zb = sg * (2 * pr + 2);
-            if (za >= zlo && za <= zhi) {
-                double2 p = a.rho_s[R.koff + za - zlo];
-                v.x = (float)p.x;
-                v.z = (float)p.y;
-            }
-            if (zb >= zlo && zb <= zhi) {
-                double2 p = a.rho_s[R.koff + zb - zlo];
-                v.y = (float)p.x;
-                v.w = (float)p.y;
-            }
+        auto rho_at = [&](int z) {
+            if (z < zlo || z > zhi) return make_float2(0.f, 0.f);
+            double2 p = a.rho_s[R.koff + z - zlo];
+            return make_float2((float)p.x, (float)p.y);
+        };
+        float4 *o = rk4 + rr * RS;
+        if (pe == 0) {
+            float2 p = rho_at(0);
+            o[0] = make_float4(p.x, p.y, 0.f, 0.f);
+            continue;
         }
-        rk4[e] = v;
+        int pr = pe - 1;
+        float A1[2], A2[2], A3[2], A4[2], zz[2];
+#pragma unroll
+        for (int l = 0; l < 2; l++) {
+            int z = 2 * pr + 1 + l;
+            float2 rp = rho_at(z), rn = rho_at(-z);
+            A1[l] = rp.x + rn.x;
+            A2[l] = rp.y - rn.y;
+            A3[l] = rp.y + rn.y;
+            A4[l] = rn.x - rp.x;
+            zz[l] = (float)z;
+        }
+        float4 *q = o + 1 + NV * pr;
+        q[0] = make_float4(A1[0], A1[1], A2[0], A2[1]);
+        q[1] = make_float4(A3[0], A3[1], A4[0], A4[1]);
+        q[2] = make_float4(-zz[0] * A4[0], -zz[1] * A4[1], zz[0] * A3[0], zz[1] * A3[1]);
+        q[3] = make_float4(zz[0] * A2[0], zz[1] * A2[1], -zz[0] * A1[0], -zz[1] * A1[1]);
+        if (WF) {
+            float s0 = zz[0] * zz[0], s1 = zz[1] * zz[1];
+            q[4] = make_float4(s0 * A1[0], s1 * A1[1], s0 * A2[0], s1 * A2[1]);
+            q[5] = make_float4(s0 * A3[0], s1 * A3[1], s0 * A4[0], s1 * A4[1]);
+        }
     }
     bool act = li < a.cnt;
     int ion = act ? (a.idx ? a.idx[li] : li) : 0;
@@ -304,9 +332,9 @@ __global__ void __launch_bounds__(ION32_THREADS, ION32_MIN_BLOCKS) k_ion32(Ion32
     double ty = c.B[0][1] * ri.x + c.B[1][1] * ri.y + c.B[2][1] * ri.z;
     double tz = c.B[0][2] * ri.x + c.B[1][2] * ri.y + c.B[2][2] * ri.z;
     // E2[z], z = 1..KZ, as planar pairs over (2p+1, 2p+2)
-    float2 Ex[KZ / 2], Ey[KZ / 2];
+    float2 Ex[NP], Ey[NP];
 #pragma unroll
-    for (int pr = 0; pr < KZ / 2; pr++) {
+    for (int pr = 0; pr < NP; pr++) {
         float2 ea = cis2pi32((double)(2 * pr + 1) * tz), eb = cis2pi32((double)(2 * pr + 2) * tz);
         Ex[pr] = make_float2(ea.x, eb.x);
         Ey[pr] = make_float2(ea.y, eb.y);
@@ -324,48 +352,46 @@ __global__ void __launch_bounds__(ION32_THREADS, ION32_MIN_BLOCKS) k_ion32(Ion32
     for (int rr = 0; rr < nrs; rr++) {
         int2 R = rnxy[rr];
         float2 w = cis2pi32((double)R.x * tx + (double)R.y * ty);
-        const float4 *rho = rk4 + rr * (KZ + 1);
-        float4 r00 = rho[0];
-        // z = 0: phase w; z = 1..KZ in packed FP32x2 pairs (two z per lane pair)
-        const float2 wx = make_float2(w.x, w.x), wy = make_float2(w.y, w.y), nwx = make_float2(-w.x, -w.x);
-        float2 R1v = make_float2(r00.y * w.x - r00.x * w.y, 0.f), Rzv = make_float2(0.f, 0.f);
-        float2 Q0v = make_float2(0.f, 0.f), Q1v = Q0v, Q2v = Q0v;
-        if (WF) Q0v.x = r00.x * w.x + r00.y * w.y;
+        const float4 *Q = rk4 + rr * RS;
+        const float4 q0 = Q[0];
+        // two accumulators per component (the c and the d terms) for independent chains
+        const float2 zero = make_float2(0.f, 0.f);
+        float2 gx0 = zero, gx1 = zero, gy0 = zero, gy1 = zero, hx0 = zero, hx1 = zero, hy0 = zero, hy1 = zero;
+        float2 kx = zero, ky = zero;
 #pragma unroll
-        for (int pr = 0; pr < KZ / 2; pr++) {
-            const float4 A = rho[1 + 2 * pr], B = rho[2 + 2 * pr];
-            const float2 rpx = make_float2(A.x, A.y), rpy = make_float2(A.z, A.w);
-            const float2 rnx = make_float2(B.x, B.y), rny = make_float2(B.z, B.w);
+        for (int pr = 0; pr < NP; pr++) {
+            const float4 *q = Q + 1 + NV * pr;
+            const float4 g1 = q[0], g2 = q[1], h1 = q[2], h2 = q[3];
             const float2 ex = Ex[pr], ey = Ey[pr];
-            const float2 zq = make_float2((float)(2 * pr + 1), (float)(2 * pr + 2));
-            // w e = (p, s), w conj(e) = (p', s')
-            float2 u1 = __fmul2_rn(wy, ey), u2 = __fmul2_rn(wy, ex);
-            float2 p = __ffma2_rn(wx, ex, make_float2(-u1.x, -u1.y)), pp = __ffma2_rn(wx, ex, u1);
-            float2 sv = __ffma2_rn(wx, ey, u2), sp = __ffma2_rn(nwx, ey, u2);
-            // rho.y ph.x - rho.x ph.y (the sign convention of k_rec_ion) for +z and -z
-            float2 t1 = __fmul2_rn(rpx, sv), t2 = __fmul2_rn(rnx, sp);
-            float2 xp = __ffma2_rn(rpy, p, make_float2(-t1.x, -t1.y));
-            float2 xm = __ffma2_rn(rny, pp, make_float2(-t2.x, -t2.y));
-            R1v = __fadd2_rn(R1v, __fadd2_rn(xp, xm));
-            Rzv = __ffma2_rn(zq, __fadd2_rn(xp, make_float2(-xm.x, -xm.y)), Rzv);
+            gx0 = __ffma2_rn(make_float2(g1.x, g1.y), ex, gx0);
+            gx1 = __ffma2_rn(make_float2(g1.z, g1.w), ey, gx1);
+            gy0 = __ffma2_rn(make_float2(g2.x, g2.y), ex, gy0);
+            gy1 = __ffma2_rn(make_float2(g2.z, g2.w), ey, gy1);
+            hx0 = __ffma2_rn(make_float2(h1.x, h1.y), ex, hx0);
+            hx1 = __ffma2_rn(make_float2(h1.z, h1.w), ey, hx1);
+            hy0 = __ffma2_rn(make_float2(h2.x, h2.y), ex, hy0);
+            hy1 = __ffma2_rn(make_float2(h2.z, h2.w), ey, hy1);
             if (WF) {
-                float2 cp = __ffma2_rn(rpx, p, __fmul2_rn(rpy, sv)), cm = __ffma2_rn(rnx, pp, __fmul2_rn(rny, sp));
-                float2 cs = __fadd2_rn(cp, cm);
-                Q0v = __fadd2_rn(Q0v, cs);
-                Q1v = __ffma2_rn(zq, __fadd2_rn(cp, make_float2(-cm.x, -cm.y)), Q1v);
-                Q2v = __ffma2_rn(__fmul2_rn(zq, zq), cs, Q2v);
+                const float4 k1 = q[4], k2 = q[5];
+                kx = __ffma2_rn(make_float2(k1.z, k1.w), ey, __ffma2_rn(make_float2(k1.x, k1.y), ex, kx));
+                ky = __ffma2_rn(make_float2(k2.z, k2.w), ey, __ffma2_rn(make_float2(k2.x, k2.y), ex, ky));
             }
         }
-        float R1a = R1v.x, R1b = R1v.y, Rza = Rzv.x, Rzb = Rzv.y;
-        float Q0a = Q0v.x, Q0b = Q0v.y, Q1a = Q1v.x, Q1b = Q1v.y, Q2a = Q2v.x, Q2b = Q2v.y;
-    float R1 = R1a + R1b, Rz = Rza + Rzb;
-        float Q0 = Q0a + Q0b, Q1 = Q1a + Q1b, Q2 = Q2a + Q2b;
+        const float2 gx = __fadd2_rn(gx0, gx1), gy = __fadd2_rn(gy0, gy1);
+        const float2 hx = __fadd2_rn(hx0, hx1), hy = __fadd2_rn(hy0, hy1);
+        const float Gx = q0.x + (gx.x + gx.y), Gy = q0.y + (gy.x + gy.y);
+        const float Hx = hx.x + hx.y, Hy = hy.x + hy.y;
+        // Im conj(w) G and Im conj(w) H
+        const float R1 = w.x * Gy - w.y * Gx, Rz = w.x * Hy - w.y * Hx;
         double fx = (double)R.x, fy = (double)R.y;
         S0 += fx * (double)R1;
         S1 += fy * (double)R1;
         S2 += (double)Rz;
         if (WF) {
-            // sum_k (n.m) Re(conj(rho) ph) per component weight n: c0 = nx mx + ny my
+            const float Kx = kx.x + kx.y, Ky = ky.x + ky.y;
+            // Re conj(w) G, H, K: sum_k (n.m) Re(conj(rho) ph) per component weight n,
+            // c0 = nx mx + ny my
+            const float Q0 = w.x * Gx + w.y * Gy, Q1 = w.x * Hx + w.y * Hy, Q2 = w.x * Kx + w.y * Ky;
             double c0 = fx * mx + fy * my;
             double T1 = c0 * (double)Q0 + (double)mz * (double)Q1;
             double Tz = c0 * (double)Q1 + (double)mz * (double)Q2;
@@ -503,19 +529,19 @@ void setup_kspace32(Engine &e, const std::vector<KRow> &rows) {
     e.d_rho_part32 = dalloc<float2>((size_t)chunks * e.nk);
     // ion-pass slices are chosen per launch (ion32_slicing); room for the largest count
     e.nsm = nsm;
-    int maxrows = std::max(1, (48 * 1024) / ((kz_of(L.K2) + 1) * (int)sizeof(float4) + (int)sizeof(int2)));
+    int maxrows = std::max(1, (48 * 1024) / ion32_row_bytes(kz_of(L.K2), true));
     e.ion32_slices = std::max(std::min(32, e.nrow), ceil_div(e.nrow, maxrows));
     e.d_ion_part32 = dalloc<double>((size_t)e.ion32_slices * e.n * 6);
 }
 
 // k-row slices of one ion pass over `cnt` ions: about two full waves of resident blocks,
-// at most e.ion32_slices, each slice's Ak rho(k) within 48 KB of shared memory
-static void ion32_slicing(const Engine &e, int cnt, int &rows, int &slices) {
+// at most e.ion32_slices, each slice's staged rows within 48 KB of shared memory
+static void ion32_slicing(const Engine &e, int cnt, bool wf, int &rows, int &slices) {
     int KZ = kz_of(e.kmax[2]);
     int iblocks = ceil_div(std::max(cnt, 1), ION32_THREADS);
     int s = std::max(1, 2 * ION32_MIN_BLOCKS * e.nsm / iblocks);
     s = std::min(s, std::min(e.nrow, e.ion32_slices));
-    int maxrows = std::max(1, (48 * 1024) / ((KZ + 1) * (int)sizeof(float4) + (int)sizeof(int2)));
+    int maxrows = std::max(1, (48 * 1024) / ion32_row_bytes(KZ, wf));
     s = std::max(s, ceil_div(e.nrow, maxrows));
     rows = ceil_div(e.nrow, s);
     slices = ceil_div(e.nrow, rows);
@@ -582,7 +608,7 @@ static void ion32_dispatch(Engine &e, dim3 g, size_t smem, const Ion32Args &a, b
 void launch_ion32(Engine &e, const double *q, const double3 *mu, bool ld, const RecOut &o, const int *idx, int cnt) {
     bool wf = o.f != nullptr;
     int rows = 1, slices = 1;
-    ion32_slicing(e, cnt, rows, slices);
+    ion32_slicing(e, cnt, wf, rows, slices);
     Ion32Args a;
     a.cnt = cnt;
     a.nrow = e.nrow;
@@ -597,7 +623,7 @@ void launch_ion32(Engine &e, const double *q, const double3 *mu, bool ld, const 
     a.part = e.d_ion_part32;
     a.ld = ld;
     int KZ = kz_of(e.kmax[2]);
-    size_t smem = sizeof(float4) * rows * (KZ + 1) + sizeof(int2) * rows;
+    size_t smem = (size_t)ion32_row_bytes(KZ, wf) * rows;
     dim3 g(ceil_div(std::max(cnt, 1), ION32_THREADS), slices);
     int pi = -1;
     e.prof_begin("k_rec_ion", &pi);

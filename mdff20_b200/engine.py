@@ -173,10 +173,12 @@ _lib = None
 
 
 def load_library(path: str = LIB_PATH):
-    """Load libmdffgpu.so and declare every exported function.  Raises if it is missing."""
+    """Load libmdffgpu.so (or the build named by MDFFGPU_LIBRARY) and declare every
+    exported function.  Raises if it is missing."""
     global _lib
     if _lib is not None:
         return _lib
+    path = os.environ.get("MDFFGPU_LIBRARY", path)
     if not os.path.exists(path):
         raise FileNotFoundError(f"{path} is not built: run `make -C mdff20_b200` (or __graft_entry__.build())")
     L = C.CDLL(path)
