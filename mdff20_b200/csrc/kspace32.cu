@@ -26,7 +26,8 @@
 //             = ion; per row the block stages the weights of Ak rho(+z) and Ak rho(-z)
 //             folded over the sign of nz, E2[z] (z = 1..KZ) sits in registers, the row
 //             sums cost 2 FMA per k-vector (3 with forces) and one product with the row
-//             phase exp(2 pi i (nx tx + ny ty)), reduced in FP64.  Row sums FP32, rows FP64.
+//             phase exp(2 pi i (nx tx + ny ty)), from an FP64-reduced argument every
+//             ION32_RUN rows and by FP32 steps in ny between.  Row sums FP32, rows FP64.
 // Both passes take an optional ion index list (the polarisable ions of an induced-
 // dipole iteration, whose search directions vanish elsewhere).
 #include "engine.cuh"
@@ -41,6 +42,7 @@ constexpr int RHO32_TI = 32;        // ions per shared-memory tile (two tiles in
 constexpr int RHO32_MIN_BLOCKS = 5;
 constexpr int ION32_THREADS = 128;
 constexpr int ION32_MIN_BLOCKS = 5;
+constexpr int ION32_RUN = 4;        // rows per exact row phase in the ion pass
 
 __device__ __forceinline__ float2 cmul32(float2 a, float2 b) {
     return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -347,11 +349,24 @@ __global__ void __launch_bounds__(ION32_THREADS, ION32_MIN_BLOCKS) k_ion32(Ion32
         my = c.B[0][1] * m3.x + c.B[1][1] * m3.y + c.B[2][1] * m3.z;
         mz = (float)(c.B[0][2] * m3.x + c.B[1][2] * m3.y + c.B[2][2] * m3.z);
     }
+    // row phase: exact (FP64-reduced argument) at the start of a run of up to ION32_RUN
+    // rows (nx, ny), (nx, ny + 1), ..., the next ones times exp(2 pi i ty) in FP32
+    const float2 e1 = cis2pi32(ty);
+    float2 w = make_float2(1.f, 0.f);
+    int2 Rp = make_int2(0, 0);
+    int run = ION32_RUN;
     __syncthreads();
     double S0 = 0, S1 = 0, S2 = 0, P0 = 0, P1 = 0, P2 = 0;
     for (int rr = 0; rr < nrs; rr++) {
         int2 R = rnxy[rr];
-        float2 w = cis2pi32((double)R.x * tx + (double)R.y * ty);
+        if (run < ION32_RUN && R.x == Rp.x && R.y == Rp.y + 1) {
+            w = cmul32(w, e1);
+            run++;
+        } else {
+            w = cis2pi32((double)R.x * tx + (double)R.y * ty);
+            run = 1;
+        }
+        Rp = R;
         const float4 *Q = rk4 + rr * RS;
         const float4 q0 = Q[0];
         // two accumulators per component (the c and the d terms) for independent chains
