@@ -814,8 +814,11 @@ void Engine::pim_cg(bool fused) {
     if (fused) {
         MDFF_LAUNCH(*this, k_aspc_predict, nb, 256, 0, n, e, es, d_hist, d_mu_ind, cg_poly ? 1 : 0);
         MDFF_LAUNCH(*this, k_add3, nb, 256, 0, n, d_mu_static, d_mu_ind, d_mu_tot);
+        // the residual reads the field at the polarisable ions only
+        bool sub = use32 && rec32 && subset32 && npol > 0;
         if (use32 && real32)
-            launch_dir32(*this, d_q, d_mu_tot, p.alphaES, lqch != 0, true, ldmp != 0, false, true, d_tmp3, nullptr);
+            launch_dir32(*this, d_q, d_mu_tot, p.alphaES, lqch != 0, true, ldmp != 0, false, true, d_tmp3, nullptr,
+                         sub ? d_pidx : nullptr, npol);
         else
             launch_dir(*this, d_q, d_mu_tot, p.alphaES, lqch != 0, true, ldmp != 0, false, true, false, false,
                        d_tmp3, nullptr, nullptr);
@@ -825,6 +828,10 @@ void Engine::pim_cg(bool fused) {
         o.self2 = self2_of(p.alphaES);
         o.self_mu = d_mu_tot;
         o.rho_raw = d_rho_acc;
+        if (sub) {
+            o.out_idx = d_pidx;
+            o.out_cnt = npol;
+        }
         launch_rec(*this, d_q, d_mu_tot, lqch != 0, true, o);
         MDFF_LAUNCH(*this, k_cg_residual, nb, 256, 0, n, d_polar, d_invpol, d_muzero, d_ef_ind, d_mu_ind, d_cg_r);
     } else {

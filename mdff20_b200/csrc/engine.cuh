@@ -112,6 +112,8 @@ struct RecOut {
     bool energy = true;               // false: skip the energy/virial reduction (field-only passes)
     const int *idx = nullptr;         // mixed precision: only these ions (q, mu zero elsewhere;
     int cnt = -1;                     // outputs written at these ions only), cnt of them
+    const int *out_idx = nullptr;     // mixed precision: outputs at these ions only (the rho
+    int out_cnt = -1;                 // pass still sums over idx / all ions), out_cnt of them
 };
 void launch_rec(Engine &e, const double *q, const double3 *mu, bool lq, bool ld, const RecOut &o);
 // acc += (scal[num_slot] / scal[den_slot]) x over the k-vectors
@@ -122,11 +124,12 @@ void launch_reduce_slots(Engine &e, int first_slot, int nslots, int nparts);
 inline bool mixed_available() { return true; }
 // real32.cu: mixed-precision real space.  launch_pair_prep32 once per force evaluation
 // (in-cutoff list and dipole-field records); launch_dir32 as launch_dir (charges from
-// the fractional coordinates' w); launch_pol_field32: T mu at the polarisable ions from
-// the dipole-field records (zero at the others)
+// the fractional coordinates' w; a field-only pass may take an ion subset idx[cnt],
+// written there only); launch_pol_field32: T mu at the polarisable ions from the
+// dipole-field records (zero at the others)
 void launch_pair_prep32(Engine &e);
 void launch_dir32(Engine &e, const double *q, const double3 *mu, double alpha, bool lq, bool ld, bool damp,
-                  bool forces, bool ef, double3 *out_ef, double3 *out_f);
+                  bool forces, bool ef, double3 *out_ef, double3 *out_f, const int *idx = nullptr, int cnt = 0);
 void launch_pol_field32(Engine &e, const double3 *p, double3 *out_ef);
 // kspace32.cu: per force evaluation, the phase tables of the current positions
 void launch_coords32(Engine &e);

@@ -490,7 +490,8 @@ static void launch_rec32(Engine &e, const double *q, const double3 *mu, bool lq,
     }
     if (o.energy) e.reduce(S_REC_U, 7, nbr);
     if (!o.ef && !o.f) return;
-    launch_ion32(e, lq ? q : nullptr, mu, ld, o, o.idx, cnt);
+    if (o.out_idx) launch_ion32(e, lq ? q : nullptr, mu, ld, o, o.out_idx, o.out_cnt);
+    else launch_ion32(e, lq ? q : nullptr, mu, ld, o, o.idx, cnt);
 }
 
 void launch_rec(Engine &e, const double *q, const double3 *mu, bool lq, bool ld, const RecOut &o) {
@@ -499,7 +500,7 @@ void launch_rec(Engine &e, const double *q, const double3 *mu, bool lq, bool ld,
         launch_rec32(e, q, mu, lq, ld, o);
         return;
     }
-    if (o.idx) throw Error(MDFFGPU_ERR_STATE, "ion subsets are a mixed-precision k-space feature");
+    if (o.idx || o.out_idx) throw Error(MDFFGPU_ERR_STATE, "ion subsets are a mixed-precision k-space feature");
     int segblocks = ceil_div(e.nseg, RHO_THREADS);
     dim3 grid(segblocks, e.rho_chunks);
     int WT = (e.kmax[0] + 1) + (2 * e.kmax[1] + 1) + (2 * e.kmax[2] + 1);

@@ -164,6 +164,8 @@ __global__ void __launch_bounds__(PW32 * 32) k_pol_field32(int n, const int *__r
 
 struct Dir32bArgs {
     int n, nt, cap;
+    const int *idx;        // field only: these ions (cnt of them), all when null
+    int cnt;
     CellF3 c;
     const double4 *s;      // fractional coordinates, w = charge
     const float4 *qm;      // dipole, w = type
@@ -195,7 +197,9 @@ __global__ void __launch_bounds__(PW32 * 32) k_dir32b(Dir32bArgs a) {
         dt[e] = F;
     }
     __syncthreads();
-    int i = blockIdx.x * PW32 + (threadIdx.x >> 5);
+    int wi = blockIdx.x * PW32 + (threadIdx.x >> 5);
+    int i = wi;
+    if (a.idx) i = (wi < a.cnt) ? a.idx[wi] : a.n;
     int lane = threadIdx.x & 31;
     float acc[7] = {0, 0, 0, 0, 0, 0, 0};
     float fi[3] = {0, 0, 0}, ei[3] = {0, 0, 0};
@@ -410,17 +414,20 @@ static int uniform_tt_order(const Engine &e) {
 
 template <bool FORCES, bool EF>
 static void dir32_launch(Engine &e, const Dir32bArgs &a, int ktt) {
-    int nb = ceil_div(e.n, PW32);
+    int nb = ceil_div(a.idx ? a.cnt : e.n, PW32);
     if (ktt == 4) MDFF_LAUNCH(e, (k_dir32b<FORCES, EF, 4>), nb, PW32 * 32, 0, a);
     else MDFF_LAUNCH(e, (k_dir32b<FORCES, EF, 0>), nb, PW32 * 32, 0, a);
 }
 
 void launch_dir32(Engine &e, const double *q, const double3 *mu, double alpha, bool lq, bool ld, bool damp,
-                  bool forces, bool ef, double3 *out_ef, double3 *out_f) {
+                  bool forces, bool ef, double3 *out_ef, double3 *out_f, const int *idx, int cnt) {
+    if (idx && forces) throw Error(MDFFGPU_ERR_STATE, "ion subsets are for field-only passes");
     (void)q;   // charges travel in the w component of the fractional coordinates
     if (ld) MDFF_LAUNCH(e, k_pack_mu32, ceil_div(e.n, 256), 256, 0, e.n, mu, e.d_typ, e.d_qm32);
     Dir32bArgs a;
     a.n = e.n;
+    a.idx = idx;
+    a.cnt = idx ? cnt : e.n;
     a.nt = e.nt;
     a.cap = e.cap_co;
     a.c = cellf3(e.cell);
