@@ -693,6 +693,13 @@ void Engine::ensure_lists() {
 // ---------------------------------------------------------------- force evaluation
 void Engine::sr_forces(bool lj, double *u, double *pvir, double *tau) {
     launch_sr(*this, lj);
+    sr_finish(lj);
+    (void)u;
+    (void)pvir;
+    (void)tau;
+}
+
+void Engine::sr_finish(bool lj) {
     int slot = lj ? S_LJ_U : S_BH_U;
     reduce(slot, 7, ceil_div(n, 8));
     DevScalars *o = d_out;
@@ -700,9 +707,6 @@ void Engine::sr_forces(bool lj, double *u, double *pvir, double *tau) {
         MDFF_LAUNCH(*this, k_finalize_sr, 1, 1, 0, d_scal, slot, cell.inveOmegaPU, &o->u_lj, &o->pvir_lj, o->tau_lj);
     else
         MDFF_LAUNCH(*this, k_finalize_sr, 1, 1, 0, d_scal, slot, cell.inveOmegaPU, &o->u_bh, &o->pvir_bh, o->tau_bh);
-    (void)u;
-    (void)pvir;
-    (void)tau;
 }
 
 static double self2_of(double alpha) {

@@ -309,6 +309,7 @@ struct Engine {
     void ensure_lists();
     void engforce();
     void sr_forces(bool lj, double *u, double *pvir, double *tau);
+    void sr_finish(bool lj);   // reduce the short-range slot, u / virial / stress into d_out
     void multipole_es_dev(const double *d_qv, const double3 *d_muv, double alpha, int flags, double3 *d_ef_out,
                           double *d_efg_out, double3 *d_f_out);
     void field_of(const double *d_qv, const double3 *d_muv, bool lq, bool ld, bool damp, double3 *d_ef_out,

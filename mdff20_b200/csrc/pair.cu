@@ -4,35 +4,11 @@
 // combined with warp shuffles and written by lane 0 (no atomics); energies and
 // virials go to per-block partial sums reduced in a fixed order.
 #include "engine.cuh"
+#include "sr_pair.cuh"
 
 namespace mdffgpu {
 
 constexpr int PAIR_WARPS = 8;  // warps (= ions) per block
-
-struct TT {
-    double E[9];  // 1/k!, get_TT_damp src/tt_damp.c:34-40
-};
-
-__device__ __forceinline__ double powi(double x, int k) {
-    double r = 1.0;
-    while (k) {
-        if (k & 1) r *= x;
-        x *= x;
-        k >>= 1;
-    }
-    return r;
-}
-
-// TT_damping_functions, src/tt_damp.c:16-32
-__device__ __forceinline__ void tt_damp(const TT &tt, double b, double c, double r, int order, double &f,
-                                        double &fd) {
-    double br = b * r;
-    double ex = exp(-br) * c;
-    double ff = tt.E[order];
-    for (int k = order - 1; k > -1; k--) ff = ff * br + tt.E[k];
-    f = 1.0 - ff * ex;
-    fd = tt.E[order] * powi(br, order) * ex * b;
-}
 
 // block-level sum of NV per-warp values into part[(slot+v)*stride + blockIdx.x]
 template <int NV>
@@ -52,8 +28,9 @@ __device__ __forceinline__ void block_partials(const double (&v)[NV], double *pa
 // ---------------------------------------------------------------- short range
 // engforce_nmlj_pbc (src/nmlj.c:254-385) when LJ, engforce_bhmftd_pbc
 // (src/bhmftd.c:117-271) otherwise.  Adds forces into f; slot gets u (x2) and the
-// virial sum over the full list of (r_a f_b + r_b f_a).
-template <bool LJ>
+// virial sum over the full list of (r_a f_b + r_b f_a).  FAST (mixed precision,
+// Buckingham): bhm_pair_fast, the same function with fewer roundings and divisions.
+template <bool LJ, bool FAST = false>
 __global__ void __launch_bounds__(PAIR_WARPS * 32) k_sr(int n, Cell c, const double4 *__restrict__ s,
                                                         const int *__restrict__ typ, const PairSR *__restrict__ pr,
                                                         int nt, const int *__restrict__ nbl,
@@ -80,39 +57,9 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32) k_sr(int n, Cell c, const dou
             double r2 = norm2_exact(r);
             if (!(r2 < srcutsq)) continue;
             double u, w;
-            if (LJ) {
-                double sr2 = P.sigsq / r2;
-                double srp = P.ip >= 0 ? powi(sr2, P.ip) : pow(sr2, P.ptwo);
-                double srq = P.iq >= 0 ? powi(sr2, P.iq) : pow(sr2, P.qtwo);
-                u = (trunctype == 2) ? 0.0 : P.epsqp * (P.plj * srq - P.qlj * srp) - (trunctype == 1 ? P.uc : 0.0);
-                w = P.fc * (srq - srp) * sr2;
-            } else {
-                double ir2 = 1.0 / r2, d = sqrt(r2);
-                double erh = P.A * exp(-P.B * d);
-                double ir6 = ir2 * ir2 * ir2, ir8 = ir6 * ir2;
-                ir6 *= P.C;
-                ir8 *= P.D;
-                double f6 = 1.0, f8 = 1.0, fd6 = 0.0, fd8 = 0.0;
-                if (damped) {
-                    tt_damp(tt, P.BD, 1.0, d, 6, f6, fd6);
-                    tt_damp(tt, P.BD, 1.0, d, 8, f8, fd8);
-                }
-                double ir6d = ir6 * f6, ir8d = ir8 * f8;
-                double ir7 = 6.0 * ir6d / d, ir9 = 8.0 * ir8d / d;
-                u = erh - ir6d - ir8d;
-                w = (P.B * erh - ir7 - ir9 + ir6 * fd6 + ir8 * fd8) / d;
-            }
-            double gx = w * r.x, gy = w * r.y, gz = w * r.z;
-            fx += gx;
-            fy += gy;
-            fz += gz;
-            acc[0] += u;
-            acc[1] += r.x * gx + r.x * gx;
-            acc[2] += r.x * gy + r.y * gx;
-            acc[3] += r.x * gz + r.z * gx;
-            acc[4] += r.y * gy + r.y * gy;
-            acc[5] += r.y * gz + r.z * gy;
-            acc[6] += r.z * gz + r.z * gz;
+            if (FAST && !LJ) bhm_pair_fast(P, r2, damped, u, w);
+            else sr_pair<LJ>(P, r2, trunctype, damped, tt, u, w);
+            sr_accumulate(r, u, w, fx, fy, fz, acc);
         }
     }
     fx = warp_sum(fx);
@@ -132,14 +79,16 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32) k_sr(int n, Cell c, const dou
 }
 
 void launch_sr(Engine &e, bool lj) {
-    TT tt;
-    tt.E[0] = 1.0;
-    for (int k = 1; k < 9; k++) tt.E[k] = tt.E[k - 1] / (double)k;
+    TT tt = make_tt();
     int nb = ceil_div(e.n, PAIR_WARPS);
     if (lj)
         MDFF_LAUNCH(e, k_sr<true>, nb, PAIR_WARPS * 32, 0, e.n, e.cell, e.d_s, e.d_typ, e.d_pair, e.nt, e.d_nb,
                     e.d_nbn, e.cap_nb, e.srcutsq, e.p.trunctype, 0, tt, e.d_f, e.d_part, (int)S_LJ_U,
                     e.part_stride);
+    else if (e.use32)
+        MDFF_LAUNCH(e, (k_sr<false, true>), nb, PAIR_WARPS * 32, 0, e.n, e.cell, e.d_s, e.d_typ, e.d_pair, e.nt,
+                    e.d_nb, e.d_nbn, e.cap_nb, e.srcutsq, e.p.trunctype, e.p.lbhmftd, tt, e.d_f, e.d_part,
+                    (int)S_BH_U, e.part_stride);
     else
         MDFF_LAUNCH(e, k_sr<false>, nb, PAIR_WARPS * 32, 0, e.n, e.cell, e.d_s, e.d_typ, e.d_pair, e.nt, e.d_nb,
                     e.d_nbn, e.cap_nb, e.srcutsq, e.p.trunctype, e.p.lbhmftd, tt, e.d_f, e.d_part, (int)S_BH_U,

@@ -72,38 +72,55 @@ __global__ void k_pack_mu32(int n, const double3 *__restrict__ mu, const int *__
     out[i] = make_float4((float)m.x, (float)m.y, (float)m.z, (float)typ[i]);
 }
 
-// warp per ion: in-cutoff list nl (all ions) and dipole-field records (polarisable pairs)
-__global__ void __launch_bounds__(PW32 * 32) k_pair_prep32(int n, Cell c, const double4 *__restrict__ s,
-                                                           const int *__restrict__ col, const int *__restrict__ con,
-                                                           int cap, double lrcutsq, float alpha,
-                                                           const int *__restrict__ polar, int *__restrict__ nl,
-                                                           int *__restrict__ nln, int *__restrict__ pl,
-                                                           float4 *__restrict__ pu, int *__restrict__ pln) {
+struct Prep32Args {
+    int n;
+    Cell c;
+    const double4 *s;
+    const int *col, *con;    // Coulomb Verlet list
+    int cap;
+    double lrcutsq;
+    float alpha;
+    const int *polar;
+    int *nl, *nln, *pl, *pln;
+    float4 *pu;
+};
+
+// warp per ion: in-cutoff list nl (all ions) and dipole-field records (polarisable pairs).
+// The neighbour positions of the next chunk of 32 and the indices of the one after are
+// loaded while the current chunk is processed.
+__global__ void __launch_bounds__(PW32 * 32) k_pair_prep32(Prep32Args a) {
     int i = blockIdx.x * PW32 + (threadIdx.x >> 5);
     int lane = threadIdx.x & 31;
-    if (i >= n) return;
+    if (i >= a.n) return;
     const float rpi = 1.7724538509055160273f;
-    const float alpha2 = alpha * alpha, alpha3 = alpha2 * alpha;
-    double4 si = s[i];
-    bool pi = polar && polar[i];
-    int m = min(con[i], cap);
-    const int *L = col + (size_t)i * cap;
-    int *NL = nl + (size_t)i * cap;
-    int *PL = pl ? pl + (size_t)i * cap : nullptr;
-    float4 *PU = pu ? pu + (size_t)i * cap : nullptr;
+    const float alpha = a.alpha, alpha2 = alpha * alpha, alpha3 = alpha2 * alpha;
+    const Cell &c = a.c;
+    double4 si = a.s[i];
+    bool pi = a.polar && a.polar[i];
+    int m = min(a.con[i], a.cap);
+    const int *L = a.col + (size_t)i * a.cap;
+    int *NL = a.nl + (size_t)i * a.cap;
+    int *PL = a.pl ? a.pl + (size_t)i * a.cap : nullptr;
+    float4 *PU = a.pu ? a.pu + (size_t)i * a.cap : nullptr;
     int cnt = 0, pcnt = 0;
+    // software pipeline: positions one chunk ahead, indices two chunks ahead
+    int jc = lane < m ? L[lane] : 0;
+    int jn = lane + 32 < m ? L[lane + 32] : 0;
+    double4 sc = lane < m ? a.s[jc] : si;
     for (int k0 = 0; k0 < m; k0 += 32) {
         int k = k0 + lane;
+        int j = jc;
+        double4 sj = sc;
+        if (k + 32 < m) sc = a.s[jn];
+        jc = jn;
+        if (k + 64 < m) jn = L[k + 64];
         bool keep = false, kp = false;
-        int j = 0;
         float4 rec = make_float4(0.f, 0.f, 0.f, 0.f);
         if (k < m) {
-            j = L[k];
-            double4 sj = s[j];
             double3 r = pbc_frac(c, si.x - sj.x, si.y - sj.y, si.z - sj.z);
             double d2 = norm2_exact(r);
-            keep = !(d2 > lrcutsq);
-            if (keep && pi && polar[j]) {
+            keep = !(d2 > a.lrcutsq);
+            if (keep && pi && a.polar[j]) {
                 kp = true;
                 float3 rf = make_float3((float)r.x, (float)r.y, (float)r.z);
                 float fd2 = (float)d2;
@@ -116,13 +133,14 @@ __global__ void __launch_bounds__(PW32 * 32) k_pair_prep32(int n, Cell c, const 
                 rec = make_float4(g * rf.x, g * rf.y, g * rf.z, F1 * dm3);
             }
         }
+        const unsigned below = (1u << lane) - 1u;
         unsigned bk = __ballot_sync(0xffffffffu, keep);
-        if (keep) NL[cnt + __popc(bk & ((1u << lane) - 1u))] = j;
+        if (keep) NL[cnt + __popc(bk & below)] = j;
         cnt += __popc(bk);
         if (PL) {
             unsigned bp = __ballot_sync(0xffffffffu, kp);
             if (kp) {
-                int pos = pcnt + __popc(bp & ((1u << lane) - 1u));
+                int pos = pcnt + __popc(bp & below);
                 PL[pos] = j;
                 PU[pos] = rec;
             }
@@ -130,8 +148,8 @@ __global__ void __launch_bounds__(PW32 * 32) k_pair_prep32(int n, Cell c, const 
         }
     }
     if (lane == 0) {
-        nln[i] = cnt;
-        if (pln) pln[i] = pcnt;
+        a.nln[i] = cnt;
+        if (a.pln) a.pln[i] = pcnt;
     }
 }
 
@@ -386,10 +404,22 @@ void Engine::dfree32() {
 // per force evaluation, after the fractional coordinates e.d_s are current
 void launch_pair_prep32(Engine &e) {
     e.ensure_real32();
-    int nb = ceil_div(e.n, PW32);
-    MDFF_LAUNCH(e, k_pair_prep32, nb, PW32 * 32, 0, e.n, e.cell, e.d_s, e.d_co, e.d_con, e.cap_co, e.lrcutsq,
-                (float)e.p.alphaES, e.lpol ? e.d_polar : nullptr, e.d_nl32, e.d_nln32, e.d_pl32, e.d_pu32,
-                e.d_pln32);
+    Prep32Args a;
+    a.n = e.n;
+    a.c = e.cell;
+    a.s = e.d_s;
+    a.col = e.d_co;
+    a.con = e.d_con;
+    a.cap = e.cap_co;
+    a.lrcutsq = e.lrcutsq;
+    a.alpha = (float)e.p.alphaES;
+    a.polar = e.lpol ? e.d_polar : nullptr;
+    a.nl = e.d_nl32;
+    a.nln = e.d_nln32;
+    a.pl = e.d_pl32;
+    a.pln = e.d_pln32;
+    a.pu = e.d_pu32;
+    MDFF_LAUNCH(e, k_pair_prep32, ceil_div(e.n, PW32), PW32 * 32, 0, a);
 }
 
 void launch_pol_field32(Engine &e, const double3 *p, double3 *out_ef) {
