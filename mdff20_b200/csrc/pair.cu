@@ -31,7 +31,7 @@ __device__ __forceinline__ void block_partials(const double (&v)[NV], double *pa
 // virial sum over the full list of (r_a f_b + r_b f_a).  FAST (mixed precision,
 // Buckingham): bhm_pair_fast, the same function with fewer roundings and divisions.
 template <bool LJ, bool FAST = false>
-__global__ void __launch_bounds__(PAIR_WARPS * 32) k_sr(int n, Cell c, const double4 *__restrict__ s,
+__global__ void __launch_bounds__(PAIR_WARPS * 32, FAST ? 3 : 1) k_sr(int n, Cell c, const double4 *__restrict__ s,
                                                         const int *__restrict__ typ, const PairSR *__restrict__ pr,
                                                         int nt, const int *__restrict__ nbl,
                                                         const int *__restrict__ nbn, int cap, double srcutsq,
@@ -47,12 +47,21 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32) k_sr(int n, Cell c, const dou
         int m = nbn[i];
         if (m > cap) m = cap;
         const int *L = nbl + (size_t)i * cap;
+        // neighbour types and positions one round ahead, indices two rounds ahead
+        int jc = lane < m ? L[lane] : 0;
+        int jn = lane + 32 < m ? L[lane + 32] : 0;
+        int tc = lane < m ? typ[jc] : 0;
+        double4 sc = lane < m ? s[jc] : si;
         for (int k = lane; k < m; k += 32) {
-            int j = L[k];
-            int tj = typ[j];
+            int tj = tc;
+            double4 sj = sc;
+            if (k + 32 < m) {
+                tc = typ[jn];
+                sc = s[jn];
+            }
+            if (k + 64 < m) jn = L[k + 64];
             const PairSR &P = pr[ti * nt + tj];
             if (!LJ && P.A == 0.0) continue;
-            double4 sj = s[j];
             double3 r = pbc_frac(c, dsub(si.x, sj.x), dsub(si.y, sj.y), dsub(si.z, sj.z));
             double r2 = norm2_exact(r);
             if (!(r2 < srcutsq)) continue;

@@ -235,16 +235,27 @@ __global__ void __launch_bounds__(PW32 * 32) k_dir32b(Dir32bArgs a) {
         const DampF *Drow = dt + a.typ[i] * a.nt;
         int m = a.nln[i];
         const int *L = a.nl + (size_t)i * a.cap;
+        // neighbour positions and dipoles one round ahead, indices two rounds ahead
+        int jc = lane < m ? L[lane] : 0;
+        int jn = lane + 32 < m ? L[lane + 32] : 0;
+        double4 sc = lane < m ? a.s[jc] : si;
+        float4 qc = (a.ld && lane < m) ? a.qm[jc] : make_float4(0.f, 0.f, 0.f, 0.f);
         for (int k = lane; k < m; k += 32) {
-            int j = L[k];
-            double4 sj = a.s[j];
+            int j = jc;
+            double4 sj = sc;
+            float4 m4 = qc;
+            if (k + 32 < m) {
+                sc = a.s[jn];
+                if (a.ld) qc = a.qm[jn];
+            }
+            jc = jn;
+            if (k + 64 < m) jn = L[k + 64];
             float3 r = disp32(a.c, si, sj);
             float d2 = r.x * r.x + r.y * r.y + r.z * r.z;
             float qj = a.lq ? (float)sj.w : 0.f;
             float3 mj = make_float3(0.f, 0.f, 0.f);
             int tj = 0;
             if (a.ld) {
-                float4 m4 = a.qm[j];
                 mj = make_float3(m4.x, m4.y, m4.z);
                 tj = (int)m4.w;
             } else if (a.ldamp) {
