@@ -1,8 +1,8 @@
 """The tensor-core rho(k) pass (tcgen05 TF32 products of split operands, selected with
 MDFFGPU_KSPACE_TC=1) against the CUDA-core FP32 pass and the FP64 engine: forces of a full mixed-precision
 force evaluation (fused CG: every rho pass of the induced-dipole solve goes through it)
-for the N=24000 bench system and for a small system whose k box uses the narrowest MMA
-shape (N = 32)."""
+for the N=24000 bench system (kmax 14: 29 of the 32 MMA columns) and for a small system
+(kmax 5)."""
 import os
 
 import numpy as np
