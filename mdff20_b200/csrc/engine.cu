@@ -41,8 +41,10 @@ __global__ void k_cg_ap(int n, const int *polar, const double *invpol, const dou
                         double3 *ap, double *part, int stride, double *scal, unsigned *ticket);
 __global__ void k_cg_rz(int n, const int *polar, const double *pol, const double3 *r, double3 *z, double *part,
                         int stride, double *scal, unsigned *ticket);
-__global__ void k_cg_update(int n, double *scal, const double3 *p, const double3 *ap, double3 *x, double3 *r);
 __global__ void k_cg_dir(int n, const double *scal, const double3 *z, double3 *p);
+__global__ void k_cg_step(int n, int nk, const int *polar, const double *pol, double *scal, const double3 *p,
+                          const double3 *ap, double3 *x, double3 *r, double3 *z, const double2 *rho_p, double2 *acc,
+                          double *part, int stride, unsigned *ticket);
 __global__ void k_cg_check(cudaGraphConditionalHandle h, int first, const double *scal, DevScalars *out, int npol,
                            double tol, int maxit, unsigned *status);
 __global__ void k_upol_final(const double *scal, double coul, DevScalars *out);
@@ -854,10 +856,10 @@ void Engine::pim_cg(bool fused) {
         else field_of(d_qzero, d_cg_p, false, true, false, d_ef_ind, fused ? d_rho_it : nullptr);
         MDFF_LAUNCH(*this, k_cg_ap, nb, 256, 0, n, d_polar, d_invpol, d_cg_p, d_ef_ind, d_cg_ap, d_part, part_stride,
                     d_scal, d_ticket);
-        MDFF_LAUNCH(*this, k_cg_update, nb, 256, 0, n, d_scal, d_cg_p, d_cg_ap, d_mu_ind, d_cg_r);
-        if (fused) launch_rho_axpy(*this, S_RZOLD, S_PAP, d_rho_it, d_rho_acc);
-        MDFF_LAUNCH(*this, k_cg_rz, nb, 256, 0, n, d_polar, d_pol, d_cg_r, d_mu_save, d_part, part_stride, d_scal,
-                    d_ticket + 1);
+        // x, r update, rho(k) of the iterate, z = alpha r and the new r.z, r.r: one launch
+        MDFF_LAUNCH(*this, k_cg_step, nb + (fused ? ceil_div(nk, 256) : 0), 256, 0, n, nk, d_polar, d_pol, d_scal,
+                    d_cg_p, d_cg_ap, d_mu_ind, d_cg_r, d_mu_save, d_rho_it, fused ? d_rho_acc : nullptr, d_part,
+                    part_stride, d_ticket + 1);
     };
     if (capturing) {
         // graph: the loop is a while node whose condition the device test sets

@@ -116,8 +116,6 @@ struct RecOut {
     int out_cnt = -1;                 // pass still sums over idx / all ions), out_cnt of them
 };
 void launch_rec(Engine &e, const double *q, const double3 *mu, bool lq, bool ld, const RecOut &o);
-// acc += (scal[num_slot] / scal[den_slot]) x over the k-vectors
-void launch_rho_axpy(Engine &e, int num_slot, int den_slot, const double2 *x, double2 *acc);
 // integrate.cu
 void launch_reduce_slots(Engine &e, int first_slot, int nslots, int nparts);
 // true once the FP32 pair/k-space kernels exist in this build

@@ -368,6 +368,48 @@ __global__ void k_cg_update(int n, double *__restrict__ scal, const double3 *__r
     r[i] = make_double3(rr.x - a * q.x, rr.y - a * q.y, rr.z - a * q.z);
 }
 
+// One CG update in a single launch: x += a p, r -= a Ap (a = rz / pAp, rz kept as rz_old),
+// z = alpha r and the partial sums of r.z and r.r (as k_cg_update then k_cg_rz), and in
+// blocks past the ions (when acc is set) the rho(k) of the iterate, acc += a rho(p) (rho
+// is linear in the dipoles).  Those blocks add zero partials; the last block reduces the
+// slots as k_cg_rz does, so the scalars are the same bits.
+__global__ void k_cg_step(int n, int nk, const int *__restrict__ polar, const double *__restrict__ pol,
+                          double *scal, const double3 *__restrict__ p, const double3 *__restrict__ ap,
+                          double3 *__restrict__ x, double3 *__restrict__ r, double3 *__restrict__ z,
+                          const double2 *__restrict__ rho_p, double2 *__restrict__ acc, double *part, int stride,
+                          unsigned *ticket) {
+    const double rz = scal[S_RZ];
+    const double a = rz / scal[S_PAP];
+    const int nbi = (n + blockDim.x - 1) / blockDim.x;
+    double v[2] = {0.0, 0.0};
+    if ((int)blockIdx.x < nbi) {
+        int i = blockIdx.x * blockDim.x + threadIdx.x;
+        if (i == 0) scal[S_RZOLD] = rz;
+        if (i < n) {
+            double3 pp = p[i], q = ap[i], xx = x[i], rr = r[i];
+            x[i] = make_double3(xx.x + a * pp.x, xx.y + a * pp.y, xx.z + a * pp.z);
+            rr = make_double3(rr.x - a * q.x, rr.y - a * q.y, rr.z - a * q.z);
+            r[i] = rr;
+            if (polar[i]) {
+                double3 zz = pol_times(pol + (size_t)i * 9, rr);
+                z[i] = zz;
+                v[0] = rr.x * zz.x + rr.y * zz.y + rr.z * zz.z;
+                v[1] = rr.x * rr.x + rr.y * rr.y + rr.z * rr.z;
+            } else {
+                z[i] = make_double3(0, 0, 0);
+            }
+        }
+    } else {
+        int k = (blockIdx.x - nbi) * blockDim.x + threadIdx.x;
+        if (k < nk) {
+            double2 w = rho_p[k], s = acc[k];
+            acc[k] = make_double2(s.x + a * w.x, s.y + a * w.y);
+        }
+    }
+    block_sum_to_part<2>(v, part, S_RZ, stride);  // r.z, r.r
+    last_block_slots(part, stride, S_RZ, 2, scal, ticket);
+}
+
 // p = z + beta p, beta = rz_new / rz_old
 __global__ void k_cg_dir(int n, const double *__restrict__ scal, const double3 *__restrict__ z,
                          double3 *__restrict__ p) {

@@ -226,20 +226,6 @@ __global__ void __launch_bounds__(32) k_rho_from_acc(int nk, const double2 *__re
     rho_finish(k, nk, rho, Ak, kcoe, kv, rho_s, ppart, slot, stride);
 }
 
-// acc += (scal[num] / scal[den]) x: rho(k) of a CG iterate follows its update x += a p
-__global__ void k_rho_axpy(int nk, const double *__restrict__ scal, int num, int den, const double2 *__restrict__ x,
-                           double2 *__restrict__ acc) {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= nk) return;
-    double a = scal[num] / scal[den];
-    double2 v = x[k], s = acc[k];
-    acc[k] = make_double2(s.x + a * v.x, s.y + a * v.y);
-}
-
-void launch_rho_axpy(Engine &e, int num_slot, int den_slot, const double2 *x, double2 *acc) {
-    MDFF_LAUNCH(e, k_rho_axpy, ceil_div(e.nk, 256), 256, 0, e.nk, e.d_scal, num_slot, den_slot, x, acc);
-}
-
 // ---------------------------------------------------------------- pass 2: per ion
 struct IonArgs {
     int n, K0, K1, K2;
