@@ -95,6 +95,54 @@ __device__ __forceinline__ float warp_sumf(float v) {
     return v;
 }
 
+// block sums of NV per-thread values
+template <int NV>
+__device__ __forceinline__ void block_sum_to_part(double (&v)[NV], double *part, int slot, int stride) {
+    __shared__ double sh[32][NV];
+#pragma unroll
+    for (int k = 0; k < NV; k++) v[k] = warp_sum(v[k]);
+    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0)
+        for (int k = 0; k < NV; k++) sh[w][k] = v[k];
+    __syncthreads();
+    if (threadIdx.x < NV) {
+        double a = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); q++) a += sh[q][threadIdx.x];
+        part[(size_t)(slot + threadIdx.x) * stride + blockIdx.x] = a;
+    }
+}
+
+// The last block of a kernel to finish reduces the partials of slots first..first+nslots-1
+// exactly as k_reduce_slots does (same order), so the separate reduction launch is not
+// needed; ticket (zero between calls) counts the finished blocks.  The writers of the
+// partials fence their writes before arriving.
+__device__ __forceinline__ void last_block_slots(const double *part, int stride, int first, int nslots,
+                                                 double *scal, unsigned *ticket) {
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    __shared__ double sh[32];
+    for (int sl = first; sl < first + nslots; sl++) {
+        const volatile double *p = part + (size_t)sl * stride;
+        double a = 0.0;
+        for (int k = threadIdx.x; k < (int)gridDim.x; k += blockDim.x) a += p[k];
+        a = warp_sum(a);
+        if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = a;
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            double b = (threadIdx.x < (blockDim.x >> 5)) ? sh[threadIdx.x] : 0.0;
+            b = warp_sum(b);
+            if (threadIdx.x == 0) scal[sl] = b;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *ticket = 0u;
+}
+
 // Neumaier (compensated) summation for FP32 accumulations in the mixed path
 struct KahanF {
     float s, c;

@@ -741,7 +741,7 @@ void Engine::field_of(const double *d_qv, const double3 *d_muv, bool lq, bool ld
 
 // field of a CG search direction p, which vanishes off the polarisable ions: the
 // k-space passes run over those ions only and the field is written there only
-void Engine::field_pol(const double3 *d_p, double3 *d_out, double2 *rho_raw) {
+void Engine::field_pol(const double3 *d_p, double3 *d_out, double2 *rho_raw, bool cg_ap) {
     if (real32) launch_pol_field32(*this, d_p, d_tmp3);
     else launch_dir_field_cached(*this, d_p, d_tmp3);
     RecOut o;
@@ -753,6 +753,16 @@ void Engine::field_pol(const double3 *d_p, double3 *d_out, double2 *rho_raw) {
     o.idx = d_pidx;
     o.cnt = npol;
     o.energy = false;   // the matrix-vector product needs the field only
+    if (cg_ap) {
+        // the CG product (k_cg_ap) at the polarisable ions, in the same pass
+        o.cg.invpol = d_invpol;
+        o.cg.p = d_p;
+        o.cg.ap = d_cg_ap;
+        o.cg.part = d_part;
+        o.cg.stride = part_stride;
+        o.cg.scal = d_scal;
+        o.cg.ticket = d_ticket;
+    }
     launch_rec(*this, d_qzero, d_p, false, true, o);
 }
 
@@ -852,10 +862,13 @@ void Engine::pim_cg(bool fused) {
     int maxit = std::max(p.max_scf_pim_iter, 1);
     // one CG iteration up to the new residual norm (p <- z + beta p follows the test)
     auto iteration = [&]() {
-        if (fused && use32 && rec32 && subset32 && npol > 0) field_pol(d_cg_p, d_ef_ind, d_rho_it);   // T p
-        else field_of(d_qzero, d_cg_p, false, true, false, d_ef_ind, fused ? d_rho_it : nullptr);
-        MDFF_LAUNCH(*this, k_cg_ap, nb, 256, 0, n, d_polar, d_invpol, d_cg_p, d_ef_ind, d_cg_ap, d_part, part_stride,
-                    d_scal, d_ticket);
+        if (fused && use32 && rec32 && subset32 && npol > 0) {
+            field_pol(d_cg_p, d_ef_ind, d_rho_it, true);   // T p, Ap and p.Ap
+        } else {
+            field_of(d_qzero, d_cg_p, false, true, false, d_ef_ind, fused ? d_rho_it : nullptr);
+            MDFF_LAUNCH(*this, k_cg_ap, nb, 256, 0, n, d_polar, d_invpol, d_cg_p, d_ef_ind, d_cg_ap, d_part,
+                        part_stride, d_scal, d_ticket);
+        }
         // x, r update, rho(k) of the iterate, z = alpha r and the new r.z, r.r: one launch
         MDFF_LAUNCH(*this, k_cg_step, nb + (fused ? ceil_div(nk, 256) : 0), 256, 0, n, nk, d_polar, d_pol, d_scal,
                     d_cg_p, d_cg_ap, d_mu_ind, d_cg_r, d_mu_save, d_rho_it, fused ? d_rho_acc : nullptr, d_part,

@@ -96,6 +96,18 @@ void launch_dir(Engine &e, const double *q, const double3 *mu, double alpha, boo
 void launch_dir_prep(Engine &e, double alpha);
 void launch_dir_field_cached(Engine &e, const double3 *mu, double3 *out_ef);
 // kspace.cu
+// CG product formed where T p is formed (mixed-precision k-space combine, polarisable
+// ions): ap = invpol p - T p, block partials of p.ap into slot S_PAP of part, reduced
+// into scal by the kernel's last block
+struct CgAp {
+    const double *invpol = nullptr;
+    const double3 *p = nullptr;
+    double3 *ap = nullptr;            // null: not formed
+    double *part = nullptr;
+    int stride = 0;
+    double *scal = nullptr;
+    unsigned *ticket = nullptr;
+};
 struct RecOut {
     double3 *ef = nullptr;            // self2*mu + ef_dir + E_rec
     const double3 *ef_dir = nullptr;
@@ -114,6 +126,7 @@ struct RecOut {
     int cnt = -1;                     // outputs written at these ions only), cnt of them
     const int *out_idx = nullptr;     // mixed precision: outputs at these ions only (the rho
     int out_cnt = -1;                 // pass still sums over idx / all ions), out_cnt of them
+    CgAp cg;                          // mixed precision, field only: the CG product at the output ions
 };
 void launch_rec(Engine &e, const double *q, const double3 *mu, bool lq, bool ld, const RecOut &o);
 // integrate.cu
@@ -312,7 +325,7 @@ struct Engine {
                           double *d_efg_out, double3 *d_f_out);
     void field_of(const double *d_qv, const double3 *d_muv, bool lq, bool ld, bool damp, double3 *d_ef_out,
                   double2 *rho_raw = nullptr);
-    void field_pol(const double3 *d_p, double3 *d_out, double2 *rho_raw);
+    void field_pol(const double3 *d_p, double3 *d_out, double2 *rho_raw, bool cg_ap = false);
     void ensure_real32();
     void dfree32();
     void get_dipoles();

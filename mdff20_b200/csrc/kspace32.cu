@@ -442,51 +442,70 @@ struct Comb32Args {
     double3 *ef;
     const double3 *f_dir;
     double3 *f;
+    CgAp cg;
 };
 
 template <bool WF>
 __global__ void k_combine32(Comb32Args a) {
     int li = blockIdx.x * blockDim.x + threadIdx.x;
-    if (li >= a.cnt) return;
-    int i = a.idx ? a.idx[li] : li;
-    const int nv = WF ? 6 : 3;
-    double S[3] = {0, 0, 0}, P[3] = {0, 0, 0};
-    for (int s = 0; s < a.nslice; s++) {
-        const double *o = a.part + ((size_t)s * a.cnt + li) * nv;
-        for (int k = 0; k < 3; k++) S[k] += o[k];
-        if (WF)
-            for (int k = 0; k < 3; k++) P[k] += o[3 + k];
-    }
-    const Cell &c = a.c;
-    const double tpi = TPI_D;
-    double gS[3], gP[3];
-    for (int k = 0; k < 3; k++) {
-        gS[k] = tpi * (c.B[k][0] * S[0] + c.B[k][1] * S[1] + c.B[k][2] * S[2]);
-        gP[k] = tpi * tpi * (c.B[k][0] * P[0] + c.B[k][1] * P[1] + c.B[k][2] * P[2]);
-    }
-    if (a.ef) {
-        double3 mu = a.muself ? a.muself[i] : make_double3(0, 0, 0);
-        double3 b = make_double3(a.self2 * mu.x, a.self2 * mu.y, a.self2 * mu.z);
-        if (a.ef_dir) {
-            double3 d = a.ef_dir[i];
-            b.x += d.x;
-            b.y += d.y;
-            b.z += d.z;
+    double pap[1] = {0.0};
+    if (li < a.cnt) {
+        int i = a.idx ? a.idx[li] : li;
+        const int nv = WF ? 6 : 3;
+        double S[3] = {0, 0, 0}, P[3] = {0, 0, 0};
+        for (int s = 0; s < a.nslice; s++) {
+            const double *o = a.part + ((size_t)s * a.cnt + li) * nv;
+            for (int k = 0; k < 3; k++) S[k] += o[k];
+            if (WF)
+                for (int k = 0; k < 3; k++) P[k] += o[3 + k];
         }
-        a.ef[i] = make_double3(b.x + (-a.tfpiV * gS[0]), b.y + (-a.tfpiV * gS[1]), b.z + (-a.tfpiV * gS[2]));
-    }
-    if (WF && a.f) {
-        double qi = a.q ? a.q[i] : 0.0;
-        double3 fo = a.f[i];
-        if (a.f_dir) {
-            double3 d = a.f_dir[i];
-            fo.x += d.x * a.coul;
-            fo.y += d.y * a.coul;
-            fo.z += d.z * a.coul;
+        const Cell &c = a.c;
+        const double tpi = TPI_D;
+        double gS[3], gP[3];
+        for (int k = 0; k < 3; k++) {
+            gS[k] = tpi * (c.B[k][0] * S[0] + c.B[k][1] * S[1] + c.B[k][2] * S[2]);
+            gP[k] = tpi * tpi * (c.B[k][0] * P[0] + c.B[k][1] * P[1] + c.B[k][2] * P[2]);
         }
-        double fr[3];
-        for (int k = 0; k < 3; k++) fr[k] = a.tfpiV * (-qi * gS[k] + (a.ld ? gP[k] : 0.0));
-        a.f[i] = make_double3(fo.x + fr[0] * a.coul, fo.y + fr[1] * a.coul, fo.z + fr[2] * a.coul);
+        if (a.ef) {
+            double3 mu = a.muself ? a.muself[i] : make_double3(0, 0, 0);
+            double3 b = make_double3(a.self2 * mu.x, a.self2 * mu.y, a.self2 * mu.z);
+            if (a.ef_dir) {
+                double3 d = a.ef_dir[i];
+                b.x += d.x;
+                b.y += d.y;
+                b.z += d.z;
+            }
+            const double3 t =
+                make_double3(b.x + (-a.tfpiV * gS[0]), b.y + (-a.tfpiV * gS[1]), b.z + (-a.tfpiV * gS[2]));
+            a.ef[i] = t;
+            if (!WF && a.cg.ap) {
+                // k_cg_ap at a polarisable ion: ap = invpol p - T p, and p.ap
+                double3 m = a.cg.p[i];
+                const double *I = a.cg.invpol + (size_t)i * 9;
+                double3 ap = make_double3(I[0] * m.x + I[1] * m.y + I[2] * m.z - t.x,
+                                          I[3] * m.x + I[4] * m.y + I[5] * m.z - t.y,
+                                          I[6] * m.x + I[7] * m.y + I[8] * m.z - t.z);
+                a.cg.ap[i] = ap;
+                pap[0] = m.x * ap.x + m.y * ap.y + m.z * ap.z;
+            }
+        }
+        if (WF && a.f) {
+            double qi = a.q ? a.q[i] : 0.0;
+            double3 fo = a.f[i];
+            if (a.f_dir) {
+                double3 d = a.f_dir[i];
+                fo.x += d.x * a.coul;
+                fo.y += d.y * a.coul;
+                fo.z += d.z * a.coul;
+            }
+            double fr[3];
+            for (int k = 0; k < 3; k++) fr[k] = a.tfpiV * (-qi * gS[k] + (a.ld ? gP[k] : 0.0));
+            a.f[i] = make_double3(fo.x + fr[0] * a.coul, fo.y + fr[1] * a.coul, fo.z + fr[2] * a.coul);
+        }
+    }
+    if (!WF && a.cg.ap) {
+        block_sum_to_part<1>(pap, a.cg.part, S_PAP, a.cg.stride);
+        last_block_slots(a.cg.part, a.cg.stride, S_PAP, 1, a.cg.scal, a.cg.ticket);
     }
 }
 
@@ -663,6 +682,8 @@ void launch_ion32(Engine &e, const double *q, const double3 *mu, bool ld, const 
     b.ef = o.ef;
     b.f_dir = o.f_dir;
     b.f = o.f;
+    b.cg = o.cg;
+    if (b.cg.ap && (wf || !o.ef)) throw Error(MDFFGPU_ERR_STATE, "the CG product needs a field-only pass");
     int nb = ceil_div(std::max(cnt, 1), 256);
     if (wf) MDFF_LAUNCH(e, k_combine32<true>, nb, 256, 0, b);
     else MDFF_LAUNCH(e, k_combine32<false>, nb, 256, 0, b);
