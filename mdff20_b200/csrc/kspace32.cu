@@ -593,7 +593,8 @@ void launch_coords32(Engine &e) {
 
 // FLOPs per (ion, k-vector) of the paired-nz formulation: 4 FMA with dipoles, 2 without
 static double rho32_flops_per_pair(bool ld) { return ld ? 8.0 : 4.0; }
-double ion_flops_per_pair(bool f, bool efg);
+// FLOPs per (ion, k-vector) of the folded ion pass: 2 FMA for the field, 3 with forces
+static double ion32_flops_per_pair(bool f) { return f ? 6.0 : 4.0; }
 void launch_rho_reduce32(Engine &e, const float2 *part, int nchunks, double2 *rho_raw);
 
 template <bool LQ, bool LD>
@@ -665,7 +666,7 @@ void launch_ion32(Engine &e, const double *q, const double3 *mu, bool ld, const 
     else if (KZ == 14) ion32_dispatch<14>(e, g, smem, a, wf);
     else if (KZ == 16) ion32_dispatch<16>(e, g, smem, a, wf);
     else ion32_dispatch<32>(e, g, smem, a, wf);
-    e.prof_end("k_rec_ion", pi, ion_flops_per_pair(wf, false) * (double)cnt * e.nk);
+    e.prof_end("k_rec_ion", pi, ion32_flops_per_pair(wf) * (double)cnt * e.nk);
     Comb32Args b;
     b.cnt = cnt;
     b.nslice = slices;
