@@ -42,6 +42,7 @@ constexpr int RHO32_TI = 32;        // ions per shared-memory tile (two tiles in
 constexpr int RHO32_MIN_BLOCKS = 5;
 constexpr int ION32_THREADS = 128;
 constexpr int ION32_MIN_BLOCKS = 5;
+constexpr int ION32X2_MIN_BLOCKS = 4;   // field-only ion pass, two ions per thread
 constexpr int ION32_RUN = 4;        // rows per exact row phase in the ion pass
 
 __device__ __forceinline__ float2 cmul32(float2 a, float2 b) {
@@ -272,23 +273,18 @@ static int ion32_row_bytes(int KZ, bool wf) {
 // a4 = Re(rho_-z - rho_z) of Ak rho.  The block stages a1..a4 (and their z, z^2
 // multiples) of its rows in shared memory as planar z pairs; per ion the sums cost
 // 2 FMA per k-vector (3 with forces), packed FP32x2 FMAs over the pairs.
+// the slice's rows staged in shared memory: (nx, ny) of each row in rnxy, and per row
+// entry 0 = (rho_0, 0, 0), then per z pair (z, z') = (2p+1, 2p+2) the weights
+//   (a1, a1', a2, a2'), (a3, a3', a4, a4'), z (-a4, -a4', a3, a3'), z (a2, a2', -a1, -a1'),
+//   [forces] z^2 (a1, a1', a2, a2'), z^2 (a3, a3', a4, a4')
 template <int KZ, bool WF>
-__global__ void __launch_bounds__(ION32_THREADS, ION32_MIN_BLOCKS) k_ion32(Ion32Args a) {
+__device__ __forceinline__ void ion32_stage(const Ion32Args &a, float4 *rk4, int2 *rnxy, int r0, int nrs) {
     constexpr int NV = ion32_nv(WF), NP = KZ / 2, RS = 1 + NP * NV;
-    extern __shared__ float4 rk4[];          // [rows of the slice][RS]
-    int2 *rnxy = (int2 *)(rk4 + a.rows_per_slice * RS);   // (nx, ny) of the slice's rows
-    int li = blockIdx.x * ION32_THREADS + threadIdx.x;
-    int sl = blockIdx.y;
-    int r0 = sl * a.rows_per_slice, r1 = min(a.nrow, r0 + a.rows_per_slice);
-    int nrs = r1 - r0;
-    for (int e = threadIdx.x; e < nrs; e += ION32_THREADS) {
+    for (int e = threadIdx.x; e < nrs; e += (int)blockDim.x) {
         KRow R = a.row[r0 + e];
         rnxy[e] = make_int2(R.nx, R.ny);
     }
-    // per row: entry 0 = (rho_0, 0, 0); then per z pair (z, z') = (2p+1, 2p+2):
-    //   (a1, a1', a2, a2'), (a3, a3', a4, a4'), z (-a4, -a4', a3, a3'), z (a2, a2', -a1, -a1'),
-    //   [forces] z^2 (a1, a1', a2, a2'), z^2 (a3, a3', a4, a4')
-    for (int e = threadIdx.x; e < nrs * (NP + 1); e += ION32_THREADS) {
+    for (int e = threadIdx.x; e < nrs * (NP + 1); e += (int)blockDim.x) {
         int rr = e / (NP + 1), pe = e - rr * (NP + 1);
         KRow R = a.row[r0 + rr];
         int zlo = R.z0, zhi = R.z0 + R.cnt - 1;
@@ -326,6 +322,18 @@ __global__ void __launch_bounds__(ION32_THREADS, ION32_MIN_BLOCKS) k_ion32(Ion32
             q[5] = make_float4(s0 * A3[0], s1 * A3[1], s0 * A4[0], s1 * A4[1]);
         }
     }
+}
+
+template <int KZ, bool WF>
+__global__ void __launch_bounds__(ION32_THREADS, ION32_MIN_BLOCKS) k_ion32(Ion32Args a) {
+    constexpr int NV = ion32_nv(WF), NP = KZ / 2, RS = 1 + NP * NV;
+    extern __shared__ float4 rk4[];          // [rows of the slice][RS]
+    int2 *rnxy = (int2 *)(rk4 + a.rows_per_slice * RS);   // (nx, ny) of the slice's rows
+    int li = blockIdx.x * ION32_THREADS + threadIdx.x;
+    int sl = blockIdx.y;
+    int r0 = sl * a.rows_per_slice, r1 = min(a.nrow, r0 + a.rows_per_slice);
+    int nrs = r1 - r0;
+    ion32_stage<KZ, WF>(a, rk4, rnxy, r0, nrs);
     bool act = li < a.cnt;
     int ion = act ? (a.idx ? a.idx[li] : li) : 0;
     double4 ri = a.r[ion];
@@ -425,6 +433,90 @@ __global__ void __launch_bounds__(ION32_THREADS, ION32_MIN_BLOCKS) k_ion32(Ion32
         o[3] = P0;
         o[4] = P1;
         o[5] = P2;
+    }
+}
+
+// k_ion32 for a field-only pass with two ions per thread (ions li and li + ION32_THREADS
+// of a block of 2 ION32_THREADS): each staged weight loaded from shared memory feeds both
+// ions' packed FMAs, and the two ions' sums are independent chains.  Same arithmetic per
+// ion as k_ion32<KZ, false>.
+template <int KZ>
+__global__ void __launch_bounds__(ION32_THREADS, ION32X2_MIN_BLOCKS) k_ion32x2(Ion32Args a) {
+    constexpr int NV = ion32_nv(false), NP = KZ / 2, RS = 1 + NP * NV;
+    extern __shared__ float4 rk4[];          // [rows of the slice][RS]
+    int2 *rnxy = (int2 *)(rk4 + a.rows_per_slice * RS);
+    int sl = blockIdx.y;
+    int r0 = sl * a.rows_per_slice, r1 = min(a.nrow, r0 + a.rows_per_slice);
+    int nrs = r1 - r0;
+    ion32_stage<KZ, false>(a, rk4, rnxy, r0, nrs);
+    const Cell &c = a.c;
+    int li[2];
+    double tx[2], ty[2];
+    float2 Ex[2][NP], Ey[2][NP], e1[2], w[2];
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+        li[u] = blockIdx.x * (2 * ION32_THREADS) + u * ION32_THREADS + threadIdx.x;
+        int ion = li[u] < a.cnt ? (a.idx ? a.idx[li[u]] : li[u]) : 0;
+        double4 ri = a.r[ion];
+        tx[u] = c.B[0][0] * ri.x + c.B[1][0] * ri.y + c.B[2][0] * ri.z;
+        ty[u] = c.B[0][1] * ri.x + c.B[1][1] * ri.y + c.B[2][1] * ri.z;
+        double tz = c.B[0][2] * ri.x + c.B[1][2] * ri.y + c.B[2][2] * ri.z;
+#pragma unroll
+        for (int pr = 0; pr < NP; pr++) {
+            float2 ea = cis2pi32((double)(2 * pr + 1) * tz), eb = cis2pi32((double)(2 * pr + 2) * tz);
+            Ex[u][pr] = make_float2(ea.x, eb.x);
+            Ey[u][pr] = make_float2(ea.y, eb.y);
+        }
+        e1[u] = cis2pi32(ty[u]);
+        w[u] = make_float2(1.f, 0.f);
+    }
+    int2 Rp = make_int2(0, 0);
+    int run = ION32_RUN;
+    __syncthreads();
+    double S0[2] = {0, 0}, S1[2] = {0, 0}, S2[2] = {0, 0};
+    for (int rr = 0; rr < nrs; rr++) {
+        int2 R = rnxy[rr];
+        const bool step = run < ION32_RUN && R.x == Rp.x && R.y == Rp.y + 1;
+#pragma unroll
+        for (int u = 0; u < 2; u++) w[u] = step ? cmul32(w[u], e1[u]) : cis2pi32((double)R.x * tx[u] + (double)R.y * ty[u]);
+        run = step ? run + 1 : 1;
+        Rp = R;
+        const float4 *Q = rk4 + rr * RS;
+        const float4 q0 = Q[0];
+        const float2 zero = make_float2(0.f, 0.f);
+        float2 gx[2] = {zero, zero}, gy[2] = {zero, zero}, hx[2] = {zero, zero}, hy[2] = {zero, zero};
+#pragma unroll
+        for (int pr = 0; pr < NP; pr++) {
+            const float4 *q = Q + 1 + NV * pr;
+            const float4 g1 = q[0], g2 = q[1], h1 = q[2], h2 = q[3];
+#pragma unroll
+            for (int u = 0; u < 2; u++) {
+                const float2 ex = Ex[u][pr], ey = Ey[u][pr];
+                gx[u] = __ffma2_rn(make_float2(g1.z, g1.w), ey, __ffma2_rn(make_float2(g1.x, g1.y), ex, gx[u]));
+                gy[u] = __ffma2_rn(make_float2(g2.z, g2.w), ey, __ffma2_rn(make_float2(g2.x, g2.y), ex, gy[u]));
+                hx[u] = __ffma2_rn(make_float2(h1.z, h1.w), ey, __ffma2_rn(make_float2(h1.x, h1.y), ex, hx[u]));
+                hy[u] = __ffma2_rn(make_float2(h2.z, h2.w), ey, __ffma2_rn(make_float2(h2.x, h2.y), ex, hy[u]));
+            }
+        }
+        double fx = (double)R.x, fy = (double)R.y;
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const float Gx = q0.x + (gx[u].x + gx[u].y), Gy = q0.y + (gy[u].x + gy[u].y);
+            const float Hx = hx[u].x + hx[u].y, Hy = hy[u].x + hy[u].y;
+            // Im conj(w) G and Im conj(w) H
+            const float R1 = w[u].x * Gy - w[u].y * Gx, Rz = w[u].x * Hy - w[u].y * Hx;
+            S0[u] += fx * (double)R1;
+            S1[u] += fy * (double)R1;
+            S2[u] += (double)Rz;
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+        if (li[u] >= a.cnt) continue;
+        double *o = a.part + ((size_t)sl * a.cnt + li[u]) * 3;
+        o[0] = S0[u];
+        o[1] = S1[u];
+        o[2] = S2[u];
     }
 }
 
@@ -570,10 +662,15 @@ void setup_kspace32(Engine &e, const std::vector<KRow> &rows) {
 
 // k-row slices of one ion pass over `cnt` ions: about two full waves of resident blocks,
 // at most e.ion32_slices, each slice's staged rows within 48 KB of shared memory
+// two ions per thread: field-only passes with nz up to 16 (register budget)
+static bool ion32_x2(const Engine &e, bool wf) { return !wf && kz_of(e.kmax[2]) <= 16; }
+
 static void ion32_slicing(const Engine &e, int cnt, bool wf, int &rows, int &slices) {
     int KZ = kz_of(e.kmax[2]);
-    int iblocks = ceil_div(std::max(cnt, 1), ION32_THREADS);
-    int s = std::max(1, 2 * ION32_MIN_BLOCKS * e.nsm / iblocks);
+    // two ions per thread: the blocks fill the GPU once; one ion per thread: twice
+    const bool x2 = ion32_x2(e, wf);
+    int iblocks = ceil_div(std::max(cnt, 1), x2 ? 2 * ION32_THREADS : ION32_THREADS);
+    int s = std::max(1, (x2 ? ION32X2_MIN_BLOCKS : 2 * ION32_MIN_BLOCKS) * e.nsm / iblocks);
     s = std::min(s, std::min(e.nrow, e.ion32_slices));
     int maxrows = std::max(1, (48 * 1024) / ion32_row_bytes(KZ, wf));
     s = std::max(s, ceil_div(e.nrow, maxrows));
@@ -636,6 +733,7 @@ static void ion32_launch(Engine &e, dim3 g, size_t smem, const Ion32Args &a) {
 template <int KZ>
 static void ion32_dispatch(Engine &e, dim3 g, size_t smem, const Ion32Args &a, bool wf) {
     if (wf) ion32_launch<KZ, true>(e, g, smem, a);
+    else if (KZ <= 16) MDFF_LAUNCH(e, k_ion32x2<KZ <= 16 ? KZ : 16>, g, ION32_THREADS, smem, a);
     else ion32_launch<KZ, false>(e, g, smem, a);
 }
 
@@ -659,7 +757,7 @@ void launch_ion32(Engine &e, const double *q, const double3 *mu, bool ld, const 
     a.ld = ld;
     int KZ = kz_of(e.kmax[2]);
     size_t smem = (size_t)ion32_row_bytes(KZ, wf) * rows;
-    dim3 g(ceil_div(std::max(cnt, 1), ION32_THREADS), slices);
+    dim3 g(ceil_div(std::max(cnt, 1), ion32_x2(e, wf) ? 2 * ION32_THREADS : ION32_THREADS), slices);
     int pi = -1;
     e.prof_begin("k_rec_ion", &pi);
     if (KZ == 8) ion32_dispatch<8>(e, g, smem, a, wf);
