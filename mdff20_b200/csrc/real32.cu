@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(PW32 * 32) k_pair_prep32(Prep32Args a) {
     int i = blockIdx.x * PW32 + (threadIdx.x >> 5);
     int lane = threadIdx.x & 31;
     if (i >= a.n) return;
-    const float rpi = 1.7724538509055160273f;
+    const float irpi = 0.56418958354775628695f;   // 1 / sqrt(pi): a product, not a division
     const float alpha = a.alpha, alpha2 = alpha * alpha, alpha3 = alpha2 * alpha;
     const Cell &c = a.c;
     double4 si = a.s[i];
@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(PW32 * 32) k_pair_prep32(Prep32Args a) {
                 float3 rf = make_float3((float)r.x, (float)r.y, (float)r.z);
                 float fd2 = (float)d2;
                 float dm1 = rsqrtf(fd2), d = fd2 * dm1, dm2 = dm1 * dm1, dm3 = dm1 * dm2, dm5 = dm3 * dm2;
-                float expon = expf(-alpha2 * fd2) / rpi;
+                float expon = expf(-alpha2 * fd2) * irpi;
                 float F0 = erfcf(alpha * d);
                 float F1 = F0 + 2.f * alpha * d * expon;
                 float F2 = F1 + (4.f / 3.f) * alpha3 * fd2 * d * expon;
@@ -222,7 +222,7 @@ __global__ void __launch_bounds__(PW32 * 32) k_dir32b(Dir32bArgs a) {
     float acc[7] = {0, 0, 0, 0, 0, 0, 0};
     float fi[3] = {0, 0, 0}, ei[3] = {0, 0, 0};
     const float alpha = a.alpha, alpha2 = alpha * alpha, alpha3 = alpha2 * alpha;
-    const float rpi = 1.7724538509055160273f;
+    const float irpi = 0.56418958354775628695f;   // 1 / sqrt(pi): a product, not a division
     if (i < a.n) {
         double4 si = a.s[i];
         float qi = a.lq ? (float)si.w : 0.f;
@@ -264,7 +264,7 @@ __global__ void __launch_bounds__(PW32 * 32) k_dir32b(Dir32bArgs a) {
             bool dip_j = (mj.x != 0.f) || (mj.y != 0.f) || (mj.z != 0.f);
             float dm1 = rsqrtf(d2), d = d2 * dm1;
             float dm2 = dm1 * dm1, dm3 = dm1 * dm2, dm5 = dm3 * dm2;
-            float expon = expf(-alpha2 * d2) / rpi;
+            float expon = expf(-alpha2 * d2) * irpi;
             float F0 = erfcf(alpha * d);
             float F1 = F0 + 2.f * alpha * d * expon;
             float F2 = F1 + (4.f / 3.f) * alpha3 * d2 * d * expon;
@@ -279,8 +279,8 @@ __global__ void __launch_bounds__(PW32 * 32) k_dir32b(Dir32bArgs a) {
                     tt32<KTT>(D.b2, D.c2, d, D.k2, fd2, fdd2);
                     F1d1 = 1.f - fd1;
                     F1d2 = 1.f - fd2;
-                    F2d1 = F1d1 + (d / 3.f) * fdd1;
-                    F2d2 = F1d2 + (d / 3.f) * fdd2;
+                    F2d1 = F1d1 + (d * (1.f / 3.f)) * fdd1;
+                    F2d2 = F1d2 + (d * (1.f / 3.f)) * fdd2;
                 }
             }
             float F1_dm3 = F1 * dm3, F2_dm5 = 3.f * F2 * dm5;
