@@ -815,7 +815,8 @@ void Engine::pim_reference() {
 // preconditioned conjugate gradient on (alpha^-1 - T) mu = E_stat, polarisable ions;
 // initial guess extrapolated from the converged dipoles of the previous steps (the
 // polynomial through the last extrapolate_order + 1 of them: the CG needs no corrector,
-// so the more accurate predictor saves iterations; cg_poly false: ASPC coefficients); stops when the reference's residual measure
+// so the more accurate predictor saves iterations; cg_poly false: ASPC coefficients);
+// stops when the reference's residual measure
 // sqrt(sum (mu/alpha - E)^2 / npol) (src/pim.c:431-449) is below conv_tol_ind
 // fused: E_stat + T mu0 is one Ewald evaluation of (q, mu_static + mu0) (the residual
 // needs only their sum), and rho(k) of (q, mu_static + mu) follows the iterates

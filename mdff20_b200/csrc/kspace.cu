@@ -455,7 +455,8 @@ double ion_flops_per_pair(bool f, bool efg) { return 13.0 + (f ? 10.0 : 0.0) + (
 
 template <typename K>
 static void allow_smem(K kernel, size_t bytes) {
-    if (bytes > 48 * 1024) MDFF_CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    if (bytes > 48 * 1024)
+        MDFF_CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
 }
 
 // rho pass + reduction + ion pass.  `o` says where the per-ion results go:

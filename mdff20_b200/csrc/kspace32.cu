@@ -192,7 +192,8 @@ __global__ void __launch_bounds__(RHO32_THREADS, RHO32_MIN_BLOCKS)
                 float2 B1, B2 = make_float2(0.f, 0.f);
                 if (LD) {
                     float c0 = fnx * qm.y + fny * qm.z, c1 = qm.w;
-                    B1 = LQ ? make_float2(qm.x * b.x - c0 * b.y, qm.x * b.y + c0 * b.x) : make_float2(-c0 * b.y, c0 * b.x);
+                    B1 = LQ ? make_float2(qm.x * b.x - c0 * b.y, qm.x * b.y + c0 * b.x)
+                            : make_float2(-c0 * b.y, c0 * b.x);
                     B2 = make_float2(-c1 * b.y, c1 * b.x);
                 } else {
                     B1 = make_float2(qm.x * b.x, qm.x * b.y);
@@ -478,7 +479,8 @@ __global__ void __launch_bounds__(ION32_THREADS, ION32X2_MIN_BLOCKS) k_ion32x2(I
         int2 R = rnxy[rr];
         const bool step = run < ION32_RUN && R.x == Rp.x && R.y == Rp.y + 1;
 #pragma unroll
-        for (int u = 0; u < 2; u++) w[u] = step ? cmul32(w[u], e1[u]) : cis2pi32((double)R.x * tx[u] + (double)R.y * ty[u]);
+        for (int u = 0; u < 2; u++)
+            w[u] = step ? cmul32(w[u], e1[u]) : cis2pi32((double)R.x * tx[u] + (double)R.y * ty[u]);
         run = step ? run + 1 : 1;
         Rp = R;
         const float4 *Q = rk4 + rr * RS;

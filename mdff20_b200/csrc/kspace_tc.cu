@@ -45,7 +45,8 @@ constexpr int TC_SI = 16;          // ions per stage
 constexpr int TC_KS = 3 * TC_SI;   // K per stage: split terms (hh, hl, lh) x ions, term-major
 constexpr int TC_THREADS = 256;
 constexpr int TC_NSTG = 3;         // staged-row buffers: copies run TC_NSTG - 1 stages ahead
-constexpr int TC_IDX = 2048;       // ion indices of a chunk kept in shared memory (larger chunks read them from global memory)
+constexpr int TC_IDX = 2048;       // ion indices of a chunk kept in shared memory (larger
+                                   // chunks read them from global memory)
 constexpr int TC_ISSUER = 128;     // thread that issues the MMAs (warp 4: no B operand work)
 constexpr int TC_WIN = 12;         // stages per partial sum, at least (192 ions)
 constexpr uint32_t TC_A_LBO = (TC_M / 8) * 128;        // 2048: 16-byte K chunk stride of A
@@ -146,7 +147,7 @@ __global__ void k_qm_tc(int cnt, const int *__restrict__ idx, Cell c, const doub
 }
 
 struct RhoTcArgs {
-    int cnt, chunk, nstage_chunk, win, nwin, nrow, nk, K2;
+    int cnt, chunk, win, nwin, nrow, nk, K2;
     int tab_w;                 // float2 per table row
     int ha;                    // 16-byte units of E0 | E1 in a table row
     int skip;                  // 16-byte units of the nz <= 0 blocks (not staged)
@@ -440,7 +441,6 @@ bool launch_rho_tc(Engine &e, const double *q, const double3 *mu, bool lq, bool 
     a.win = std::min(stages, std::max(TC_WIN, ceil_div(stages, wmax)));
     a.nwin = ceil_div(stages, a.win);
     if (chunks * a.nwin > e.rho32_chunks) return false;
-    a.nstage_chunk = stages;
     size_t smem = rho_tc_smem(a.cw);
     MDFF_CK(cudaFuncSetAttribute(k_rho_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     MDFF_LAUNCH(e, k_rho_tc, dim3(mtiles, chunks), TC_THREADS, smem, a);

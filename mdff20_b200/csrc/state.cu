@@ -107,7 +107,8 @@ int Engine::load_state(const unsigned char *buf, size_t bytes) {
     if (bytes < sizeof(StateHeader)) throw Error(MDFFGPU_ERR_ARG, "state block too short");
     StateHeader h;
     memcpy(&h, buf, sizeof h);
-    if (memcmp(h.magic, MAGIC, 8) != 0 || h.version != VERSION) throw Error(MDFFGPU_ERR_ARG, "not an engine state block");
+    if (memcmp(h.magic, MAGIC, 8) != 0 || h.version != VERSION)
+        throw Error(MDFFGPU_ERR_ARG, "not an engine state block");
     if (bytes != state_bytes()) throw Error(MDFFGPU_ERR_ARG, "state block size does not match this system");
     const double *w = (const double *)(buf + sizeof h);
     if (h.nion != n || h.ntype != nt || h.egrator != p.egrator || h.nhc_n != p.nhc_n ||
