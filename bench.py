@@ -40,6 +40,9 @@ from typing import Optional
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+# the fit keeps one stream per configuration in flight: let them map onto more than the
+# default 8 hardware queues (read when the CUDA context is created)
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 METRIC = "MD ion-steps/s & batched fit-gradients/s: mixed vs FP64 GPU at ≤1e-5 force err"
 WORKLOAD = ("pim_silica_nvt_24000: 8000 Si + 16000 O, 2.20 g/cm^3, L=71.3 A, Buckingham rc 7 A, "
@@ -58,7 +61,13 @@ def parse():
     ap.add_argument("--fp64-steps", type=int, default=100, help="steps of the plain FP64 path timed beside")
     ap.add_argument("--force-check", type=int, default=1, help="mixed: force error against an FP64 evaluation")
     ap.add_argument("--e2e-steps", type=int, default=5)
-    ap.add_argument("--roof-kernel", default="k_rho")
+    ap.add_argument("--roof-kernel", default="k_rho,k_rec_ion",
+                    help="kernel families timed for the roofline (the one with the larger share is `roofline`)")
+    ap.add_argument("--drift-steps", type=int, default=1000,
+                    help="H_tot drift of mixed and FP64 runs over this many steps from the same start (0: skip)")
+    ap.add_argument("--named-configs", type=int, default=1, help="config 2 and config 3 lines (0: skip)")
+    ap.add_argument("--cpu-steps", type=int, default=20, help="reference CPU baseline: timed steps")
+    ap.add_argument("--cpu-warmup", type=int, default=5, help="reference CPU baseline: untimed steps before")
     ap.add_argument("--profile-steps", type=int, default=3)
     ap.add_argument("--fit-configs", type=int, default=512, help="batched fit configurations (0: skip)")
     ap.add_argument("--fit-evals", type=int, default=3)
@@ -119,27 +128,32 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------- cpu baseline
-def cpu_baseline(system, nsteps: int = 2) -> dict:
-    """The reference's own code on the host cores, `nsteps` MD steps after its t=0 forces."""
+def cpu_baseline(system, nsteps: int = 20, warm: int = 5) -> dict:
+    """The reference's own code on the host cores: after its t=0 forces, `warm` untimed
+    MD steps then `nsteps` timed ones (per-step wall clock inside the harness), step
+    indices from 6 on so that the ASPC order is the configured one from the start."""
     from oracle import ref
     threads = os.cpu_count() or 1
     if ref.available("tim"):
-        r = ref.run(system, "md", nsteps, 0, 6, variant="tim", threads=threads, timeout=1800)
-        wall = float(r["wall"][0])
+        r = ref.run(system, "md", warm + nsteps, 0, 6, variant="tim", threads=threads, timeout=3600)
+        wall = float(r["step_wall"][warm:warm + nsteps].sum())
         return {"value": system.nion * nsteps / wall, "unit": "ion-steps/s", "cores": threads,
                 "kind": "reference",
-                "sample": f"{nsteps} MD steps of the same 24000-ion system after its t=0 force evaluation, "
-                          f"mdff20 C code -O3 -Ofast -fopenmp, OMP_NUM_THREADS={threads}, {wall:.2f} s"}
+                "sample": f"{nsteps} MD steps after {warm} untimed ones of the same {system.nion}-ion system, "
+                          f"mdff20 C code -O3 -Ofast -fopenmp, OMP_NUM_THREADS={threads}, {wall:.2f} s timed"}
     from oracle.oracle import Oracle
     o = Oracle(system)
     o.gen_verletlist()
     o.engforce()
+    for s in range(6, 6 + warm):
+        o.md_step(s)
     t0 = time.perf_counter()
-    for s in range(1, nsteps + 1):
+    for s in range(6 + warm, 6 + warm + nsteps):
         o.md_step(s)
     wall = time.perf_counter() - t0
-    return {"value": system.nion * nsteps / wall, "unit": "ion-steps/s", "cores": 1, "kind": "port",
-            "sample": f"{nsteps} MD steps of the same system with the single-thread C restatement, {wall:.2f} s"}
+    return {"value": system.nion * nsteps / wall, "unit": "ion-steps/s", "cores": os.cpu_count() or 1,
+            "kind": "port",
+            "sample": f"{nsteps} MD steps after {warm} untimed ones with the C restatement (OpenMP), {wall:.2f} s"}
 
 
 # ---------------------------------------------------------------------------- arms
@@ -242,9 +256,10 @@ def run_fit(args, world, rank, dev, pg) -> Optional[dict]:
            "grad_max_rel_err_mixed_vs_fp64": float(np.max(np.abs(g32 - g64)) / np.max(np.abs(g64))),
            "loss_rel_err_mixed_vs_fp64": abs(res["mixed"]["loss"] - res["fp64"]["loss"]) / res["fp64"]["loss"],
            "params": list(fit.PARAM_NAMES), "host_threads": args.fit_threads, "setup_s": round(gen_s, 1),
-           "timing": "host clock around the synchronous batched C-ABI call (host parameters in, host loss and "
-                     "gradient out, target forces uploaded per call), device synchronised on both sides, "
-                     "max over ranks",
+           "timing": "host clock around the synchronous C-ABI evaluation (host parameters in, host loss and "
+                     "gradient out), device synchronised on both sides, max over ranks",
+           "path": "mdffgpu_fit_plan: each configuration's evaluation recorded once as a CUDA graph (device-side "
+                   "CG loops, theta in a shared device buffer), all configurations replayed concurrently",
            "data": "synthetic: seeded random silica configurations, targets = FP64 forces at +-5% parameters"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -259,10 +274,11 @@ def run_reference(args):
     from mdff20_b200 import synth
     if rank == 0:
         s = synth.config5()
-        nsteps = max(1, min(args.steps, 2))
-        cb = cpu_baseline(s, nsteps)
+        nsteps = max(1, min(args.steps, args.cpu_steps))
+        warm = max(0, min(args.warmup, args.cpu_warmup))
+        cb = cpu_baseline(s, nsteps, warm)
         line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "ion-steps/s",
-                "n_gpus": args.gpus, "steps": nsteps, "warmup": 0, "ms_per_step": 1000.0 * s.nion / cb["value"],
+                "n_gpus": args.gpus, "steps": nsteps, "warmup": warm, "ms_per_step": 1000.0 * s.nion / cb["value"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic: seeded beta-cristobalite silica, MB velocities",
                 "config": {"workload": WORKLOAD, "nion": s.nion, "parallelism": "host OpenMP"},
@@ -278,6 +294,169 @@ def run_reference(args):
     if pg is not None:
         pg.barrier()
         pg.destroy_process_group()
+
+
+def _events(n):
+    import torch
+    return [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
+
+
+def _max_over_ranks(x: float, dev: int, pg) -> float:
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], device=f"cuda:{dev}", dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def timed_md(eng, first: int, nsteps: int, flush, dev: int, pg):
+    """nsteps MD steps, each one call of the C ABI (a CUDA graph replay), bracketed by
+    CUDA events on the engine stream with the L2 flush written before each (untimed).
+    Returns (device ms summed over the steps, max over ranks; thermo records)."""
+    import numpy as np
+    import torch
+    st = torch.cuda.ExternalStream(eng.stream_handle(), device=dev)
+    evs = _events(nsteps)
+    th = []
+    if pg is not None:
+        pg.barrier()
+    torch.cuda.synchronize()
+    for k in range(nsteps):
+        with torch.cuda.stream(st):
+            flush.zero_()
+        evs[k][0].record(st)
+        th.append(eng.md_steps(first + k, 1)[0])
+        evs[k][1].record(st)
+    torch.cuda.synchronize()
+    if pg is not None:
+        pg.barrier()
+    ms = float(sum(a.elapsed_time(b) for a, b in evs))
+    return _max_over_ranks(ms, dev, pg), np.array(th)
+
+
+def profile_kernel(eng, name: str, first: int, nsteps: int, flush, stream):
+    """CUDA events around every launch of one kernel family over nsteps kernel-by-kernel
+    steps: (ms, launches, algorithmic flops)."""
+    import torch
+    eng.profile(name)
+    for k in range(nsteps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        eng.md_steps(first + k, 1)
+    torch.cuda.synchronize()
+    res = eng.profile_result()
+    eng.profile(None)
+    return res
+
+
+# algorithmic flops per (ion, k-vector) of each k-space family, counted from the kernels'
+# loop bodies (FMA = 2 flops), and the direct per-k evaluation they replace
+ROOF_NOTES = {
+    "k_rho": "flops counted on the paired-nz formulation: 8 per (ion, k) with dipoles, 4 without (a direct "
+             "evaluation of (q + i k.mu) exp(i k.r) per k costs about 14 plus a sincos)",
+    "k_rec_ion": "flops counted on the folded formulation: 8 per (ion, k) for the field, 12 with forces (a direct "
+                 "per-k evaluation costs about 20 plus a sincos)",
+}
+
+
+def md_drift(s, pos, dev: int, nsteps: int) -> dict:
+    """Conserved-quantity drift of the bench system over nsteps NHC steps from the same
+    start, mixed (fused CG, the bench's form) and FP64 (plain CG), each step a graph."""
+    import numpy as np
+
+    from mdff20_b200.engine import FP64, MIXED, PIM_CG, PIM_CG_FUSED, Engine
+    out = {"steps": nsteps}
+    for label, prec, solver in (("mixed", MIXED, PIM_CG_FUSED), ("fp64", FP64, PIM_CG)):
+        e = Engine(s, positions=pos, device=dev, precision=prec, pim_solver=solver)
+        e.gen_verletlist()
+        e.engforce()
+        th = e.md_steps(1, nsteps)
+        e.close()
+        h = th[:, 0] + th[:, 1] + th[:, 2] + th[:, 3] + th[:, 4] + th[:, 5]
+        t = np.arange(len(h), dtype=float)
+        slope = float(np.polyfit(t, h, 1)[0])
+        out[label] = {"ev_per_ion_per_step": (float(h[-1]) - float(h[0])) / (s.nion * (len(h) - 1)),
+                      "fit_slope_ev_per_ion_per_step": slope / s.nion,
+                      "h_rms_fluct_ev_per_ion": float(np.std(h - np.polyval(np.polyfit(t, h, 1), t))) / s.nion,
+                      "h_start_ev": float(h[0]), "h_end_ev": float(h[-1]),
+                      "scf_iter_mean": float(th[:, 10].mean()), "finite": bool(np.isfinite(th).all())}
+    out["ratio_mixed_over_fp64"] = (out["mixed"]["fit_slope_ev_per_ion_per_step"]
+                                    / out["fp64"]["fit_slope_ev_per_ion_per_step"])
+    return out
+
+
+def named_configs(dev: int, flush) -> dict:
+    """Throughput of the other named systems: config 2 (3000-ion rigid-ion silica, NHC
+    MD in FP64 and mixed) and config 3 (6000-ion polarisable silica single point, SCF to
+    1e-8 in FP64 and 1e-6 in mixed), device time with CUDA events."""
+    import numpy as np
+    import torch
+
+    from mdff20_b200 import synth
+    from mdff20_b200.cellmath import wrap_positions
+    from mdff20_b200.engine import FP64, MIXED, PIM_CG, PIM_CG_FUSED, Engine
+    out = {}
+    s2 = synth.config2()
+    p2 = wrap_positions(s2.cell, s2.pos)
+    c2 = {"workload": "config2: 1000 Si + 2000 O rigid ions, L=35.7 A, Buckingham rc 7 A, Ewald alpha 0.32 rc 10 A "
+                      "kmax 12, NHC 3000 K, dt 1 fs (random packing: a short window of steps)"}
+    forces = {}
+    for label, prec in (("fp64", FP64), ("mixed", MIXED)):
+        e = Engine(s2, positions=p2, device=dev, precision=prec)
+        e.gen_verletlist()
+        e.engforce()
+        forces[label] = e.forces()
+        e.md_steps(1, 3)
+        ms, th = timed_md(e, 4, 10, flush, dev, None)
+        e.close()
+        c2[label] = {"value": s2.nion * 10 / (ms / 1000.0), "unit": "ion-steps/s", "ms_per_step": ms / 10,
+                     "steps": 10}
+    c2["force_rms_rel_err_mixed_vs_fp64"] = _rms_rel(forces["mixed"], forces["fp64"])
+    c2["speedup_mixed_vs_fp64"] = c2["mixed"]["value"] / c2["fp64"]["value"]
+    out["config2"] = c2
+    s3 = synth.config3()
+    p3 = wrap_positions(s3.cell, s3.pos)
+    c3 = {"workload": "config3: 2000 Si + 4000 O polarisable, L=44.9 A, kmax 14, TT-damped, single point (energy, "
+                      "forces, stress, induced dipoles from zero), SCF 1e-8 (FP64) / 1e-6 (mixed)"}
+    res = {}
+    for label, prec, tol in (("fp64", FP64, 1e-8), ("mixed", MIXED, 1e-6)):
+        s3.conv_tol_ind = tol
+        e = Engine(s3, positions=p3, device=dev, precision=prec, pim_solver=PIM_CG_FUSED if prec else PIM_CG)
+        e.gen_verletlist()
+        zero = np.zeros((s3.nion, 6, 3))
+        st = torch.cuda.ExternalStream(e.stream_handle(), device=dev)
+        e.engforce()
+        reps = 5
+        evs = _events(reps)
+        for k in range(reps):
+            e.set_dipole_history(zero)
+            with torch.cuda.stream(st):
+                flush.zero_()
+            evs[k][0].record(st)
+            e.engforce()
+            evs[k][1].record(st)
+        torch.cuda.synchronize()
+        ms = float(sum(a.elapsed_time(b) for a, b in evs)) / reps
+        th = e.thermo()
+        res[label] = (e.forces(), e.dipole_history()[:, 0, :], th)
+        e.close()
+        c3[label] = {"ms_per_single_point": ms, "single_points_per_s": 1000.0 / ms,
+                     "ion_evals_per_s": s3.nion * 1000.0 / ms, "scf_iter": th["scf_iter"], "scf_tol": tol}
+    (f64, m64, t64), (f32, m32, t32) = res["fp64"], res["mixed"]
+    c3["errors_mixed_vs_fp64"] = {
+        "force_rms_rel": _rms_rel(f32, f64), "dipole_rms_rel": _rms_rel(m32, m64),
+        "u_coul_rel": abs(t32["u_coul"] - t64["u_coul"]) / abs(t64["u_coul"]),
+        "u_pol_rel": abs(t32["u_pol"] - t64["u_pol"]) / abs(t64["u_pol"]),
+        "tau_coul_rel": float(np.abs(t32["tau_coul"] - t64["tau_coul"]).max() / np.abs(t64["tau_coul"]).max())}
+    c3["speedup_mixed_vs_fp64"] = c3["fp64"]["ms_per_single_point"] / c3["mixed"]["ms_per_single_point"]
+    out["config3"] = c3
+    return out
+
+
+def _rms_rel(a, b) -> float:
+    import numpy as np
+    return float(np.sqrt(np.mean(np.sum((a - b) ** 2, 1))) / np.sqrt(np.mean(np.sum(b ** 2, 1))))
 
 
 def run_ours(args):
@@ -304,8 +483,7 @@ def run_ours(args):
         ref = Engine(s, positions=pos, device=dev, precision=FP64, pim_solver=solver)
         ref.gen_verletlist()
         ref.engforce()
-        f64, f32 = ref.forces(), eng.forces()
-        force_err = float(np.sqrt(np.mean(np.sum((f32 - f64) ** 2, 1))) / np.sqrt(np.mean(np.sum(f64 ** 2, 1))))
+        force_err = _rms_rel(eng.forces(), ref.forces())
         ref.close()
     istep = 1
     if args.warmup > 0:
@@ -316,85 +494,56 @@ def run_ours(args):
     peak = fma_peak_tflops(dev, prec)
 
     # ------------------------------------------------ device-resident timed region
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    thermo = []
     l0 = eng.launch_count()
-    if pg is not None:
-        pg.barrier()
-    torch.cuda.synchronize()
     clocks = ClockSampler(dev)
     clocks.start()
-    for k in range(args.steps):
-        with torch.cuda.stream(stream):
-            flush.zero_()
-        evs[k][0].record(stream)
-        thermo.append(eng.md_steps(istep, 1)[0])
-        evs[k][1].record(stream)
-        istep += 1
-    torch.cuda.synchronize()
-    if pg is not None:
-        pg.barrier()
+    total_ms, th = timed_md(eng, istep, args.steps, flush, dev, pg)
     clk = clocks.stop()
+    istep += args.steps
     launches = eng.launch_count() - l0
-    step_ms = [a.elapsed_time(b) for a, b in evs]
-    # the roofline kernel timed with CUDA events around each of its launches, over a few
-    # more steps issued kernel by kernel (events inside the step; L2 flushed before each)
-    eng.profile(args.roof_kernel)
-    for k in range(args.profile_steps):
-        with torch.cuda.stream(stream):
-            flush.zero_()
-        eng.md_steps(istep, 1)
-        istep += 1
-    torch.cuda.synchronize()
-    kms, kcount, kflops = eng.profile_result()
-    eng.profile(None)
-    total_ms = float(sum(step_ms))
-    if pg is not None:
-        t = torch.tensor([total_ms], device=f"cuda:{dev}", dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        total_ms = float(t.item())
-    th = np.array(thermo)
     value = world * s.nion * args.steps / (total_ms / 1000.0)
+    # the two k-space kernel families timed with CUDA events around each launch, over a few
+    # more steps issued kernel by kernel (events inside the step; L2 flushed before each)
+    roofs = []
+    for name in args.roof_kernel.split(","):
+        kms, kcount, kflops = profile_kernel(eng, name, istep, args.profile_steps, flush, stream)
+        istep += args.profile_steps
+        achieved = (kflops / (kms / 1000.0) / 1e12) if kms > 0 else None
+        roofs.append({"kernel": name, "bound": "fp64" if prec == FP64 else "fp32", "achieved": achieved,
+                      "peak": peak, "unit": "TFLOP/s", "frac": (achieved / peak) if achieved else None,
+                      "flops_note": ROOF_NOTES.get(name), "launches": kcount,
+                      "ms_per_launch": (kms / kcount) if kcount else None,
+                      "ms_per_step": kms / max(1, args.profile_steps),
+                      "share_of_step": (kms / max(1, args.profile_steps)) / (total_ms / args.steps)
+                      if world == 1 else None,
+                      "peak_source": "measured by mdffgpu_fma_peak (independent FMA chains) on this GPU"})
 
-    # ------------------------------------------------ the plain FP64 path (FP64, CG), same system
-    fp64_plain = None
-    if prec == MIXED and args.fp64_steps > 0:
-        e64 = Engine(s, positions=pos, device=dev, precision=FP64, pim_solver=PIM_CG)
+    # ------------------------------------------------ FP64 arms on the same system
+    def fp64_arm(solver64, label):
+        e64 = Engine(s, positions=pos, device=dev, precision=FP64, pim_solver=solver64)
         e64.gen_verletlist()
         e64.engforce()
         if args.warmup > 0:
             e64.md_steps(1, args.warmup)
-        st64 = torch.cuda.ExternalStream(e64.stream_handle(), device=dev)
-        ev64 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-                for _ in range(args.fp64_steps)]
-        th64 = []
-        if pg is not None:
-            pg.barrier()
-        torch.cuda.synchronize()
-        for k in range(args.fp64_steps):
-            with torch.cuda.stream(st64):
-                flush.zero_()
-            ev64[k][0].record(st64)
-            th64.append(e64.md_steps(1 + args.warmup + k, 1)[0])
-            ev64[k][1].record(st64)
-        torch.cuda.synchronize()
-        ms64 = float(sum(a.elapsed_time(b) for a, b in ev64))
-        if pg is not None:
-            t = torch.tensor([ms64], device=f"cuda:{dev}", dtype=torch.float64)
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            ms64 = float(t.item())
-        th64 = np.array(th64)
+        ms64, th64 = timed_md(e64, 1 + args.warmup, args.fp64_steps, flush, dev, pg)
         e64.close()
-        fp64_plain = {"value": world * s.nion * args.fp64_steps / (ms64 / 1000.0),
-                      "ms_per_step": ms64 / args.fp64_steps, "steps": args.fp64_steps, "precision": "fp64",
-                      "pim_solver": "cg", "graph": True, "h_tot_drift": h_drift(th64, s.nion)}
+        return {"value": world * s.nion * args.fp64_steps / (ms64 / 1000.0), "ms_per_step": ms64 / args.fp64_steps,
+                "steps": args.fp64_steps, "precision": "fp64", "pim_solver": label, "graph": True,
+                "scf_iter_mean": float(th64[:, 10].mean()), "h_tot_drift": h_drift(th64, s.nion)}
+
+    fp64_plain = fp64_fused = None
+    if prec == MIXED and args.fp64_steps > 0:
+        fp64_plain = fp64_arm(PIM_CG, "cg")
+        # the same algorithm as the mixed arm (fused CG, polarisable-ion subsets of the CG
+        # fields, polynomial predictor) in FP64: what precision alone buys
+        fp64_fused = fp64_arm(PIM_CG_FUSED, "fused")
 
     # ------------------------------------------------ end to end through the C ABI
     nE = max(1, args.e2e_steps)
     r, v, f = eng.state()
     r = np.ascontiguousarray(r)
     v = np.ascontiguousarray(v)
-    e_evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(nE)]
+    e_evs = _events(nE)
     if pg is not None:
         pg.barrier()
     torch.cuda.synchronize()
@@ -409,22 +558,22 @@ def run_ours(args):
         e_evs[k][1].record(stream)
         istep += 1
     torch.cuda.synchronize()
-    e2e_ms = float(sum(a.elapsed_time(b) for a, b in e_evs))
-    if pg is not None:
-        t = torch.tensor([e2e_ms], device=f"cuda:{dev}", dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = _max_over_ranks(float(sum(a.elapsed_time(b) for a, b in e_evs)), dev, pg)
     e2e_value = world * s.nion * nE / (e2e_ms / 1000.0)
     n = s.nion
     h2d = 2 * n * 3 * 8
     d2h = 3 * n * 3 * 8 + 12 * 8
+    eng.close()
 
+    line = None
     if rank == 0:
-        achieved = (kflops / (kms / 1000.0) / 1e12) if kms > 0 else None
-        traffic = None
+        traffic = {}
         tpath = os.path.join(ROOT, "profiles", "traffic.json")
         if os.path.exists(tpath):
-            traffic = json.load(open(tpath)).get(f"{args.roof_kernel}:{args.precision}")
+            traffic = json.load(open(tpath))
+        for r_ in roofs:
+            r_["traffic"] = traffic.get(f"{r_['kernel']}:{args.precision}")
+        dominant = max(roofs, key=lambda x: x["ms_per_step"]) if roofs else None
         line = {
             "metric": METRIC, "value": value, "unit": "ion-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -436,28 +585,29 @@ def run_ours(args):
                        "parallelism": f"replicas x{world}"},
             "e2e": {"value": e2e_value, "unit": "ion-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "steps": nE, "ms_per_step": e2e_ms / nE},
-            "roofline": {"kernel": args.roof_kernel, "bound": "fp64" if prec == FP64 else "fp32",
-                         "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                         "launches": kcount, "ms_per_launch": (kms / kcount) if kcount else None,
-                         "peak_source": "measured by mdffgpu_fma_peak (FMA chains) on this GPU",
-                         "share_of_step": ((kms / max(1, args.profile_steps)) / (total_ms / args.steps))
-                         if world == 1 else None},
+            "roofline": dict(dominant, dominant_of=[x["kernel"] for x in roofs]) if dominant else None,
+            "roofline_kernels": roofs,
             "clocks": clk,
             "gpu_launches": launches,
             "force_rms_rel_err_vs_fp64": force_err,
             "h_tot_drift": h_drift(th, n),
             "fp64_plain": fp64_plain,
+            "fp64_fused": fp64_fused,
+            "speedup_vs_fp64_plain": (value / fp64_plain["value"]) if fp64_plain else None,
+            "speedup_vs_fp64_fused": (value / fp64_fused["value"]) if fp64_fused else None,
             "scf_iter_mean": float(th[:, 10].mean()),
             "list_rebuilds": int(th[-1, 9] - th[0, 9]) + 1,
             "finite": bool(np.isfinite(th).all()),
         }
+        if world == 1 and args.drift_steps > 0:
+            line["h_tot_drift_long"] = md_drift(s, pos, dev, args.drift_steps)
+        if world == 1 and args.named_configs:
+            line["named_configs"] = named_configs(dev, flush)
         if world == 1 and not args.no_cpu_baseline:
             try:
-                line["cpu_baseline"] = cpu_baseline(s, 2)
+                line["cpu_baseline"] = cpu_baseline(s, args.cpu_steps, args.cpu_warmup)
             except Exception as exc:  # reported, not fatal
                 line["cpu_baseline"] = {"value": None, "error": str(exc)[:200]}
-    eng.close()
     fit_line = run_fit(args, world, rank, dev, pg) if args.fit_configs > 0 else None
     if rank == 0:
         if fit_line is not None:

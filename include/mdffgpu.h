@@ -3,9 +3,11 @@
  * The reference (mdff20, plain C) has no plugin interface: its "operator API" is a set
  * of void functions that read and write process globals.  Each entry point below
  * replaces one of them; the comment names the reference function (file:line inside
- * the mdff20 repository) and what the call takes instead of the globals.  Shims with
- * the reference's exact names, working on the reference's globals, are in
- * mdff20_b200/host/mdff_shim.c.
+ * the mdff20 repository) and what the call takes instead of the globals.  The shims
+ * with the reference's exact names and signatures, working on the reference's globals
+ * (engforce, prop_agate, check_verletlist, gen_pbc_verletlist, multipole_ES,
+ * get_dipoles), are mdff20_b200/host/mdff_shim.c; `make -C mdff20_b200 dropin` links
+ * them with the reference's own program.
  *
  * Conventions
  *  - every call returns an int status (MDFFGPU_OK = 0); the reference prints and calls
@@ -190,18 +192,18 @@ int mdffgpu_prop_agate(mdffgpu_ctx *ctx, int istep);
 int mdffgpu_md_steps(mdffgpu_ctx *ctx, int first, int nsteps, double *thermo);
 
 /* Neighbour-list build that allocates no memory.  No counterpart in the reference; it
- * is for callers that cannot allocate device memory (an application that owns all GPU
- * memory through its own pool and forbids allocations after start-up, or one that
- * records its MD step into a CUDA graph).  It runs the kernels of
+ * is for callers that cannot allocate device memory: an application that owns all GPU
+ * memory through its own pool and forbids allocations after start-up, or a host that
+ * runs the engine inside a fixed device-memory budget.  It runs the kernels of
  * mdffgpu_gen_verletlist without a context: d_pos is the caller's device array
  * [n][4] (x, y, z, unused; 32-byte aligned), cell the lattice rows [3][3] on the host,
  * cut_nb/cut_co the two list radii (rc + skin); the FULL lists go to the caller's
  * device buffers d_nb[n][cap_nb], d_nbn[n], d_co[n][cap_co], d_con[n] (each ion's
  * neighbours, both directions of every pair).  Scratch is a static device array of
  * about 5 MB, shared by every call on a device and holding the last call's data:
- * limits n <= 65536, at most 32768 cells, at most 4096 ions per cell (so n <= 4096 when
- * the cell is too small for a cell grid); larger inputs return MDFFGPU_ERR_ARG or
- * MDFFGPU_ERR_CELL.  Calls that overlap on the GPU (other streams, other threads) race
+ * limits n <= 65536 (more returns MDFFGPU_ERR_ARG), a cell grid of at most 32768 cells
+ * (a finer grid is coarsened to fit), at most 4096 ions per cell (so n <= 4096 when the
+ * cell is too small for a cell grid; more returns MDFFGPU_ERR_CELL).  Calls that overlap on the GPU (other streams, other threads) race
  * on that array.  The first call on a device looks up the array's device address (with
  * that device current); make that first call before any stream capture.  Runs on
  * `stream` (NULL: the default stream) and synchronises it; *status_out (may be NULL)
@@ -268,6 +270,26 @@ int mdffgpu_force_match(mdffgpu_ctx *ctx, int tSi, int tO, const double *fx_t, c
  * the configurations.  nthreads host threads drive the contexts' streams concurrently. */
 int mdffgpu_fit_batch(mdffgpu_ctx **ctx, int nconf, int tSi, int tO, const double *theta,
                       const double *const *targets, double scale, int nthreads, double *res);
+/* A fit plan: the batch above with each configuration's evaluation recorded once as a
+ * CUDA graph (no counterpart in the reference).  In the graph both conjugate-gradient
+ * solves (induced dipoles, adjoint) are device-controlled loops, theta is read from one
+ * device buffer the plan shares across its configurations, and the loss, gradient and
+ * status bits are assembled on the device, so an evaluation costs the host one copy of
+ * theta, one graph launch per configuration (on its context's stream, all in flight
+ * together) and one copy of the nconf results.  create: ctx[nconf] contexts on one
+ * device with a CG solver set, targets[c] the AoS target forces of context c (copied to
+ * the device once), scale as for mdffgpu_force_match.  eval: theta as above; res[0] =
+ * sum over configurations of sum_i |F_i - F_t,i|^2, res[1..10] = the summed gradient,
+ * summed in configuration order; the first eval (and the first after a context's
+ * precision or solver changed) records the graphs.  The contexts must not be used by
+ * other calls while an eval runs; after evals each context's tables hold the last
+ * theta.  mdffgpu_fit_plan_last_error: message of the last failed call. */
+typedef struct mdffgpu_fit_plan mdffgpu_fit_plan;
+int mdffgpu_fit_plan_create(mdffgpu_ctx **ctx, int nconf, int tSi, int tO, const double *const *targets,
+                            double scale, mdffgpu_fit_plan **out);
+int mdffgpu_fit_plan_eval(mdffgpu_fit_plan *plan, const double *theta, double *res);
+int mdffgpu_fit_plan_destroy(mdffgpu_fit_plan *plan);
+const char *mdffgpu_fit_plan_last_error(const mdffgpu_fit_plan *plan);
 
 #ifdef __cplusplus
 }

@@ -1,7 +1,9 @@
 // extern "C" entry points of libmdffgpu (declared in include/mdffgpu.h): argument
 // checks, host<->device transfer and conversion of engine exceptions to status codes.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
+#include <string>
 #include <thread>
 #include <vector>
 
@@ -41,6 +43,45 @@ void download(Engine &e, void *dst, const void *src, size_t bytes) {
     MDFF_CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, e.stream));
 }
 
+}  // namespace
+
+struct mdffgpu_fit_plan {
+    std::vector<mdffgpu_ctx *> ctx;
+    int tSi = 0, tO = 0, device = 0;
+    double scale = 0.0;
+    double *d_theta = nullptr;   // shared by every recorded evaluation
+    double *d_res = nullptr;     // [nconf][FIT_NRES]
+    double *h_theta = nullptr, *h_res = nullptr;   // pinned staging
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev_theta = nullptr;
+    std::vector<cudaEvent_t> ev_done;
+    std::string err;
+    ~mdffgpu_fit_plan() {
+        for (cudaEvent_t e : ev_done) cudaEventDestroy(e);
+        if (ev_theta) cudaEventDestroy(ev_theta);
+        if (stream) cudaStreamDestroy(stream);
+        cudaFree(d_theta);
+        cudaFree(d_res);
+        if (h_theta) cudaFreeHost(h_theta);
+        if (h_res) cudaFreeHost(h_res);
+    }
+};
+
+namespace {
+template <typename F>
+int plan_guarded(mdffgpu_fit_plan *plan, F &&f) {
+    if (!plan) return MDFFGPU_ERR_ARG;
+    try {
+        f(*plan);
+        return MDFFGPU_OK;
+    } catch (const Error &x) {
+        plan->err = x.what();
+        return x.code;
+    } catch (const std::exception &x) {
+        plan->err = x.what();
+        return MDFFGPU_ERR_CUDA;
+    }
+}
 }  // namespace
 
 extern "C" {
@@ -428,6 +469,100 @@ int mdffgpu_fit_batch(mdffgpu_ctx **ctx, int nconf, int tSi, int tO, const doubl
         for (int k = 0; k <= MDFFGPU_FIT_NPARAM; k++) res[k] += part[c][k];   // configuration order
     }
     return MDFFGPU_OK;
+}
+
+int mdffgpu_fit_plan_create(mdffgpu_ctx **ctx, int nconf, int tSi, int tO, const double *const *targets,
+                            double scale, mdffgpu_fit_plan **out) {
+    if (!ctx || nconf <= 0 || !targets || !out) return MDFFGPU_ERR_ARG;
+    *out = nullptr;
+    for (int c = 0; c < nconf; c++)
+        if (!ctx[c] || !ctx[c]->e || !targets[c] || ctx[c]->e->device != ctx[0]->e->device) return MDFFGPU_ERR_ARG;
+    mdffgpu_fit_plan *plan = new mdffgpu_fit_plan();
+    int rc = plan_guarded(plan, [&](mdffgpu_fit_plan &P) {
+        P.ctx.assign(ctx, ctx + nconf);
+        P.tSi = tSi;
+        P.tO = tO;
+        P.scale = scale;
+        P.device = ctx[0]->e->device;
+        MDFF_CK(cudaSetDevice(P.device));
+        MDFF_CK(cudaStreamCreateWithFlags(&P.stream, cudaStreamNonBlocking));
+        MDFF_CK(cudaEventCreateWithFlags(&P.ev_theta, cudaEventDisableTiming));
+        P.ev_done.assign(nconf, nullptr);
+        for (int c = 0; c < nconf; c++) MDFF_CK(cudaEventCreateWithFlags(&P.ev_done[c], cudaEventDisableTiming));
+        P.d_theta = mdffgpu::dalloc<double>(MDFFGPU_FIT_NPARAM);
+        P.d_res = mdffgpu::dalloc<double>((size_t)nconf * mdffgpu::FIT_NRES);
+        MDFF_CK(cudaMallocHost((void **)&P.h_theta, sizeof(double) * MDFFGPU_FIT_NPARAM));
+        MDFF_CK(cudaMallocHost((void **)&P.h_res, sizeof(double) * nconf * mdffgpu::FIT_NRES));
+        for (int c = 0; c < nconf; c++) {
+            Engine &e = *ctx[c]->e;
+            if (!e.d_ft) e.d_ft = mdffgpu::dalloc<double3>(e.n);
+            upload(e, e.d_ft, targets[c], sizeof(double3) * e.n);
+            MDFF_CK(cudaStreamSynchronize(e.stream));
+        }
+    });
+    if (rc != MDFFGPU_OK) {
+        delete plan;
+        return rc;
+    }
+    *out = plan;
+    return MDFFGPU_OK;
+}
+
+int mdffgpu_fit_plan_eval(mdffgpu_fit_plan *plan, const double *theta, double *res) {
+    if (!plan || !theta || !res) return MDFFGPU_ERR_ARG;
+    for (int k = 0; k < MDFFGPU_FIT_NPARAM; k++)
+        if (!std::isfinite(theta[k])) return MDFFGPU_ERR_ARG;
+    if (!(theta[7] > 0.0)) return MDFFGPU_ERR_ARG;   // the O polarisability is inverted
+    return plan_guarded(plan, [&](mdffgpu_fit_plan &P) {
+        const int nconf = (int)P.ctx.size(), NR = mdffgpu::FIT_NRES;
+        MDFF_CK(cudaSetDevice(P.device));
+        // record what is missing or stale before anything is in flight
+        for (int c = 0; c < nconf; c++) {
+            Engine &e = *P.ctx[c]->e;
+            if (!e.fit_exec || e.fit_graph_gen != e.gen) {
+                try {
+                    e.capture_fit(P.d_theta, P.tSi, P.tO, P.scale, P.d_res + (size_t)c * NR);
+                } catch (const Error &x) {
+                    throw Error(x.code, "configuration " + std::to_string(c) + ": " + x.what());
+                }
+            }
+        }
+        std::memcpy(P.h_theta, theta, sizeof(double) * MDFFGPU_FIT_NPARAM);
+        MDFF_CK(cudaMemcpyAsync(P.d_theta, P.h_theta, sizeof(double) * MDFFGPU_FIT_NPARAM, cudaMemcpyHostToDevice,
+                                P.stream));
+        MDFF_CK(cudaEventRecord(P.ev_theta, P.stream));
+        for (int c = 0; c < nconf; c++) {
+            Engine &e = *P.ctx[c]->e;
+            MDFF_CK(cudaStreamWaitEvent(e.stream, P.ev_theta, 0));
+            MDFF_CK(cudaGraphLaunch(e.fit_exec, e.stream));
+            MDFF_CK(cudaEventRecord(P.ev_done[c], e.stream));
+            MDFF_CK(cudaStreamWaitEvent(P.stream, P.ev_done[c], 0));
+        }
+        MDFF_CK(cudaMemcpyAsync(P.h_res, P.d_res, sizeof(double) * nconf * NR, cudaMemcpyDeviceToHost, P.stream));
+        MDFF_CK(cudaStreamSynchronize(P.stream));
+        for (int c = 0; c < nconf; c++) {
+            try {
+                mdffgpu::fit_status((unsigned)P.h_res[(size_t)c * NR + NR - 1]);
+            } catch (const Error &x) {
+                throw Error(x.code, "configuration " + std::to_string(c) + ": " + x.what());
+            }
+        }
+        for (int k = 0; k <= MDFFGPU_FIT_NPARAM; k++) res[k] = 0.0;
+        for (int c = 0; c < nconf; c++)   // configuration order
+            for (int k = 0; k <= MDFFGPU_FIT_NPARAM; k++) res[k] += P.h_res[(size_t)c * NR + k];
+        // the contexts' host copies of the parameters follow the device tables
+        for (int c = 0; c < nconf; c++) P.ctx[c]->e->fit_host_params(P.tSi, P.tO, theta);
+    });
+}
+
+int mdffgpu_fit_plan_destroy(mdffgpu_fit_plan *plan) {
+    if (!plan) return MDFFGPU_ERR_ARG;
+    delete plan;
+    return MDFFGPU_OK;
+}
+
+const char *mdffgpu_fit_plan_last_error(const mdffgpu_fit_plan *plan) {
+    return plan ? plan->err.c_str() : "null fit plan";
 }
 
 }  // extern "C"

@@ -5,6 +5,8 @@
 #include <cmath>
 #include <cstring>
 
+#include <functional>
+
 #include "engine.cuh"
 
 namespace mdffgpu {
@@ -208,7 +210,7 @@ Engine::~Engine() {
     dfree32();
     for (void *x : {(void *)d_fpart, (void *)d_fscal, (void *)d_w, (void *)d_lam, (void *)d_sv, (void *)d_fa,
                     (void *)d_fb, (void *)d_fc, (void *)d_qw, (void *)d_efg_rec, (void *)d_muw, (void *)d_rw,
-                    (void *)d_ft})
+                    (void *)d_ft, (void *)d_theta, (void *)d_fres})
         cudaFree(x);
     cudaFree(d_out);
     cudaFree(d_status);
@@ -216,6 +218,7 @@ Engine::~Engine() {
     if (h_out) cudaFreeHost(h_out);
     if (h_stage) cudaFreeHost(h_stage);
     if (step_exec) cudaGraphExecDestroy(step_exec);
+    if (fit_exec) cudaGraphExecDestroy(fit_exec);
     if (body_stream) cudaStreamDestroy(body_stream);
     if (stream) cudaStreamDestroy(stream);
 }
@@ -742,7 +745,7 @@ void Engine::field_of(const double *d_qv, const double3 *d_muv, bool lq, bool ld
 // field of a CG search direction p, which vanishes off the polarisable ions: the
 // k-space passes run over those ions only and the field is written there only
 void Engine::field_pol(const double3 *d_p, double3 *d_out, double2 *rho_raw, bool cg_ap) {
-    if (real32) launch_pol_field32(*this, d_p, d_tmp3);
+    if (use32 && real32) launch_pol_field32(*this, d_p, d_tmp3);
     else launch_dir_field_cached(*this, d_p, d_tmp3);
     RecOut o;
     o.ef = d_out;
@@ -812,6 +815,49 @@ void Engine::pim_reference() {
     MDFF_CK(cudaStreamSynchronize(stream));
 }
 
+// While recording: a device-controlled loop.  `first` issues the test that decides
+// whether the loop runs at all (it sets the condition through the handle), then the
+// while node is added and `body` (one iteration ending in the same test) is recorded
+// into its body graph on body_stream.  body_count receives the launches of one
+// iteration.
+void Engine::record_while(const std::function<void(cudaGraphConditionalHandle)> &first,
+                          const std::function<void(cudaGraphConditionalHandle)> &body) {
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t cgraph = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    cudaGraphConditionalHandle h;
+    MDFF_CK(cudaStreamGetCaptureInfo(stream, &cs, nullptr, &cgraph, nullptr, nullptr));
+    MDFF_CK(cudaGraphConditionalHandleCreate(&h, cgraph, 0, 0));
+    first(h);
+    MDFF_CK(cudaStreamGetCaptureInfo(stream, &cs, nullptr, &cgraph, &deps, &ndeps));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    MDFF_CK(cudaGraphAddNode(&node, cgraph, deps, ndeps, &cp));
+    cudaGraph_t bgraph = cp.conditional.phGraph_out[0];
+    MDFF_CK(cudaStreamUpdateCaptureDependencies(stream, &node, 1, cudaStreamSetCaptureDependencies));
+    cudaStream_t outer = stream;
+    stream = body_stream;
+    MDFF_CK(cudaStreamBeginCaptureToGraph(stream, bgraph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    try {
+        long long b0 = launches;
+        body(h);
+        body_count = launches - b0;
+    } catch (...) {
+        cudaGraph_t g2 = nullptr;
+        cudaStreamEndCapture(stream, &g2);
+        stream = outer;
+        throw;
+    }
+    cudaGraph_t g2 = nullptr;
+    MDFF_CK(cudaStreamEndCapture(stream, &g2));
+    stream = outer;
+}
+
 // preconditioned conjugate gradient on (alpha^-1 - T) mu = E_stat, polarisable ions;
 // initial guess extrapolated from the converged dipoles of the previous steps (the
 // polynomial through the last extrapolate_order + 1 of them: the CG needs no corrector,
@@ -831,8 +877,9 @@ void Engine::pim_cg(bool fused) {
     if (fused) {
         MDFF_LAUNCH(*this, k_aspc_predict, nb, 256, 0, n, e, es, d_hist, d_mu_ind, cg_poly ? 1 : 0);
         MDFF_LAUNCH(*this, k_add3, nb, 256, 0, n, d_mu_static, d_mu_ind, d_mu_tot);
-        // the residual reads the field at the polarisable ions only
-        bool sub = use32 && rec32 && subset32 && npol > 0;
+        // the residual reads the field at the polarisable ions only (FP64 real space
+        // evaluates every ion; the k-space ion pass and FP32 real space only those)
+        bool sub = subset32 && npol > 0;
         if (use32 && real32)
             launch_dir32(*this, d_q, d_mu_tot, p.alphaES, lqch != 0, true, ldmp != 0, false, true, d_tmp3, nullptr,
                          sub ? d_pidx : nullptr, npol);
@@ -863,8 +910,14 @@ void Engine::pim_cg(bool fused) {
     int maxit = std::max(p.max_scf_pim_iter, 1);
     // one CG iteration up to the new residual norm (p <- z + beta p follows the test)
     auto iteration = [&]() {
-        if (fused && use32 && rec32 && subset32 && npol > 0) {
-            field_pol(d_cg_p, d_ef_ind, d_rho_it, true);   // T p, Ap and p.Ap
+        if (fused && subset32 && npol > 0) {
+            // T p over the polarisable ions; Ap and p.Ap in the FP32 k-space combine, or
+            // by k_cg_ap after the FP64 one
+            bool ap_in_combine = use32 && rec32;
+            field_pol(d_cg_p, d_ef_ind, d_rho_it, ap_in_combine);
+            if (!ap_in_combine)
+                MDFF_LAUNCH(*this, k_cg_ap, nb, 256, 0, n, d_polar, d_invpol, d_cg_p, d_ef_ind, d_cg_ap, d_part,
+                            part_stride, d_scal, d_ticket);
         } else {
             field_of(d_qzero, d_cg_p, false, true, false, d_ef_ind, fused ? d_rho_it : nullptr);
             MDFF_LAUNCH(*this, k_cg_ap, nb, 256, 0, n, d_polar, d_invpol, d_cg_p, d_ef_ind, d_cg_ap, d_part,
@@ -877,42 +930,16 @@ void Engine::pim_cg(bool fused) {
     };
     if (capturing) {
         // graph: the loop is a while node whose condition the device test sets
-        cudaStreamCaptureStatus cs;
-        cudaGraph_t cgraph = nullptr;
-        const cudaGraphNode_t *deps = nullptr;
-        size_t ndeps = 0;
-        MDFF_CK(cudaStreamGetCaptureInfo(stream, &cs, nullptr, &cgraph, nullptr, nullptr));
-        MDFF_CK(cudaGraphConditionalHandleCreate(&cg_handle, cgraph, 0, 0));
-        MDFF_LAUNCH(*this, k_cg_check, 1, 32, 0, cg_handle, 1, d_scal, d_out, npol, p.conv_tol_ind, maxit, d_status);
-        MDFF_CK(cudaStreamGetCaptureInfo(stream, &cs, nullptr, &cgraph, &deps, &ndeps));
-        cudaGraphNodeParams cp = {};
-        cp.type = cudaGraphNodeTypeConditional;
-        cp.conditional.handle = cg_handle;
-        cp.conditional.type = cudaGraphCondTypeWhile;
-        cp.conditional.size = 1;
-        cudaGraphNode_t node;
-        MDFF_CK(cudaGraphAddNode(&node, cgraph, deps, ndeps, &cp));
-        cudaGraph_t body = cp.conditional.phGraph_out[0];
-        MDFF_CK(cudaStreamUpdateCaptureDependencies(stream, &node, 1, cudaStreamSetCaptureDependencies));
-        cudaStream_t outer = stream;
-        stream = body_stream;
-        MDFF_CK(cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-        try {
-            long long b0 = launches;
-            iteration();
-            MDFF_LAUNCH(*this, k_cg_check, 1, 32, 0, cg_handle, 0, d_scal, d_out, npol, p.conv_tol_ind, maxit,
-                        d_status);
-            MDFF_LAUNCH(*this, k_cg_dir, nb, 256, 0, n, d_scal, d_mu_save, d_cg_p);
-            body_count = launches - b0;
-        } catch (...) {
-            cudaGraph_t g2 = nullptr;
-            cudaStreamEndCapture(stream, &g2);
-            stream = outer;
-            throw;
-        }
-        cudaGraph_t g2 = nullptr;
-        MDFF_CK(cudaStreamEndCapture(stream, &g2));
-        stream = outer;
+        record_while(
+            [&](cudaGraphConditionalHandle h) {
+                MDFF_LAUNCH(*this, k_cg_check, 1, 32, 0, h, 1, d_scal, d_out, npol, p.conv_tol_ind, maxit, d_status);
+            },
+            [&](cudaGraphConditionalHandle h) {
+                iteration();
+                MDFF_LAUNCH(*this, k_cg_check, 1, 32, 0, h, 0, d_scal, d_out, npol, p.conv_tol_ind, maxit,
+                            d_status);
+                MDFF_LAUNCH(*this, k_cg_dir, nb, 256, 0, n, d_scal, d_mu_save, d_cg_p);
+            });
     } else {
         double rr = 0.0;
         MDFF_CK(cudaMemcpyAsync(&rr, d_scal + S_RR, sizeof(double), cudaMemcpyDeviceToHost, stream));
@@ -1272,6 +1299,9 @@ void Engine::drop_graph() {
     if (step_exec) cudaGraphExecDestroy(step_exec);
     step_exec = nullptr;
     graph_gen = -1;
+    if (fit_exec) cudaGraphExecDestroy(fit_exec);
+    fit_exec = nullptr;
+    fit_graph_gen = -1;
 }
 
 // record prop_agate + check_verletlist of one step (src/md.c:237-241) as a graph

@@ -1,6 +1,7 @@
 // mdffgpu engine: device state of one system and the launchers of its kernels.
 #pragma once
 
+#include <functional>
 #include <vector>
 
 #include "common.cuh"
@@ -129,6 +130,9 @@ struct RecOut {
     CgAp cg;                          // mixed precision, field only: the CG product at the output ions
 };
 void launch_rec(Engine &e, const double *q, const double3 *mu, bool lq, bool ld, const RecOut &o);
+// fit.cu: the status bits of a force-matching evaluation as an Error (none: returns)
+void fit_status(unsigned status);
+constexpr int FIT_NRES = 1 + MDFFGPU_FIT_NPARAM + 1;   // loss, gradient, status bits per evaluation
 // integrate.cu
 void launch_reduce_slots(Engine &e, int first_slot, int nslots, int nparts);
 // true once the FP32 pair/k-space kernels exist in this build
@@ -286,13 +290,19 @@ struct Engine {
     double3 *d_muw = nullptr;
     double2 *d_rw = nullptr;
     double3 *d_ft = nullptr;         // target forces
+    double *d_theta = nullptr;       // theta on the device (read by the result assembly)
+    double *d_fres = nullptr;        // [1 + NPARAM + 1]: the last evaluation's result and status
     int last_adj_iter = 0;
+    // one force-matching evaluation recorded as a CUDA graph (fit batches): both CG
+    // solves are while nodes, theta is read from a device buffer and the result is
+    // assembled on the device, so a replay needs no host round trip
+    cudaGraphExec_t fit_exec = nullptr;
+    long long fit_graph_gen = -1;
 
     // one MD step as a CUDA graph (md_steps): the induced-dipole CG loop is a while node
     // whose condition a device kernel sets, so a step needs no host round trip
     bool graph_on = true;
     bool capturing = false;                 // launches are being recorded
-    cudaGraphConditionalHandle cg_handle = 0;
     cudaStream_t body_stream = nullptr;     // records the CG loop body
     cudaGraphExec_t step_exec = nullptr;
     long long gen = 0, graph_gen = -1;      // gen: bumped when buffers or modes change
@@ -340,7 +350,14 @@ struct Engine {
     // force_match: res[0] = sum |F - F_t|^2, res[1..10] = dL/dtheta for
     // L = scale/2 sum |F - F_t|^2 (w = scale (F - F_t))
     void set_fit_params(int tSi, int tO, const double *theta);
+    void fit_host_params(int tSi, int tO, const double *theta);
     void force_match(const double3 *d_ft, double scale, double *res, int tSi, int tO);
+    // the pieces of force_match: buffers, the device-side parameter update from a device
+    // theta (recorded evaluations), the evaluation itself into d_res[0..NPARAM] (+ status)
+    void fit_alloc();
+    void fit_apply_theta(const double *d_th, int tSi, int tO);
+    void fit_issue(const double3 *d_ft, double scale, int tSi, int tO, const double *d_th, double *d_res);
+    void capture_fit(const double *d_th, int tSi, int tO, double scale, double *d_res);
     void solve_pim(const double3 *d_b, double3 *d_x, double rtol, int maxit);
     void fit_reduce(int first, int cnt, int nparts);
     void coul_forces(const double *d_qv, const double3 *d_muv, bool lq, bool ld, double3 *out);
@@ -350,6 +367,8 @@ struct Engine {
     int load_state(const unsigned char *buf, size_t bytes);
     bool graph_ok(int step) const;
     void capture_step(int step);
+    void record_while(const std::function<void(cudaGraphConditionalHandle)> &first,
+                      const std::function<void(cudaGraphConditionalHandle)> &body);
     void drop_graph();
     void sync_scalars();
     void check_status();

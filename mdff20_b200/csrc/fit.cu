@@ -36,8 +36,10 @@ enum FitSlot : int {
     F_LMU = 15,         // lambda . mu_ind on the polarisable ions
     F_SS = 16, F_RR = 17,   // s.s, r.r (adjoint CG)
     F_RZ = 18, F_PAP = 19, F_RZOLD = 20,
+    F_ADJ_RR0 = 21, F_ADJ_IT = 22,   // adjoint CG: initial r.r and iteration count (recorded loop)
     NFSLOT = 24
 };
+constexpr int NRES = FIT_NRES;
 
 __global__ void k_reduce_slots(const double *part, int stride, int first, int nparts, double *scal);
 // preconditioned CG kernels of integrate.cu
@@ -349,33 +351,100 @@ __global__ void __launch_bounds__(FIT_WARPS * 32) k_bhm_sens(int n, Cell c, cons
 }
 
 // ------------------------------------------------------------------ engine side
-__global__ void k_set_charges(int n, const int *__restrict__ typ, double qSi, int tSi, int tO, double *__restrict__ q,
-                              double4 *__restrict__ r) {
+// the device half of set_fit_params from a device theta (recorded evaluations): the
+// Born-Mayer-Huggins entries of (Si, O), (O, Si), (O, O) and the damping b, c of every
+// damped direction (one thread per type pair) ...
+__global__ void k_fit_tables(const double *__restrict__ th, int tSi, int tO, int nt, PairSR *__restrict__ pair,
+                             PairDamp *__restrict__ damp) {
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= nt * nt) return;
+    int x = e / nt, y = e - x * nt;
+    PairSR &P = pair[e];
+    if ((x == tSi && y == tO) || (x == tO && y == tSi)) {
+        P.A = th[0];
+        P.B = th[1];
+        P.C = th[2];
+    } else if (x == tO && y == tO) {
+        P.A = th[3];
+        P.B = th[4];
+        P.C = th[5];
+    }
+    PairDamp &D = damp[e];
+    if (D.pad & 1) {
+        D.b1 = th[8];
+        D.c1 = th[9];
+    }
+    if (D.pad & 2) {
+        D.b2 = th[8];
+        D.c2 = th[9];
+    }
+}
+
+// ... and the charges (q_Si = theta_6, q_O = -theta_6 / 2) and O polarisabilities
+__global__ void k_fit_ions(int n, const int *__restrict__ typ, const double *__restrict__ th, int tSi, int tO,
+                           double *__restrict__ q, double4 *__restrict__ r, double *__restrict__ pol,
+                           double *__restrict__ invpol) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int t = typ[i];
     double v = q[i];
-    if (t == tSi) v = qSi;
-    else if (t == tO) v = -0.5 * qSi;
+    if (t == tSi) v = th[6];
+    else if (t == tO) v = -0.5 * th[6];
     q[i] = v;
     double4 x = r[i];
     x.w = v;
     r[i] = x;
-}
-
-__global__ void k_set_pol(int n, const int *__restrict__ typ, int tO, double alpha, double *__restrict__ pol,
-                          double *__restrict__ invpol) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n || typ[i] != tO) return;
-    for (int k = 0; k < 9; k++) {
-        pol[(size_t)i * 9 + k] = (k % 4 == 0) ? alpha : 0.0;
-        invpol[(size_t)i * 9 + k] = (k % 4 == 0) ? 1.0 / alpha : 0.0;
+    if (t == tO) {
+        double alpha = th[7];
+        for (int k = 0; k < 9; k++) {
+            pol[(size_t)i * 9 + k] = (k % 4 == 0) ? alpha : 0.0;
+            invpol[(size_t)i * 9 + k] = (k % 4 == 0) ? 1.0 / alpha : 0.0;
+        }
     }
 }
 
-void Engine::set_fit_params(int tSi, int tO, const double *th) {
+// loss and gradient from the reduced slots (see the file comment for the q_Si, alpha_O,
+// b and c terms); res[NRES - 1] = the context's status bits
+__global__ void k_fm_result(const double *__restrict__ sc, const double *__restrict__ th, double coul,
+                            const unsigned *__restrict__ status, double *__restrict__ res) {
+    if (threadIdx.x || blockIdx.x) return;
+    res[0] = sc[F_LOSS];
+    for (int k = 0; k < 6; k++) res[1 + k] = sc[F_BHM + k];
+    double wqq = sc[F_WFQ0], wqm = sc[F_WFALL] - sc[F_WFQ0] - sc[F_WF0M];
+    res[7] = (2.0 * wqq + wqm + sc[F_LESTAT]) / th[6];
+    res[8] = sc[F_LMU] / (th[7] * th[7]);
+    res[9] = coul * sc[F_DAMP + 0] + sc[F_DAMP + 2];
+    res[10] = coul * sc[F_DAMP + 1] + sc[F_DAMP + 3];
+    res[NRES - 1] = (double)*status;
+}
+
+// the adjoint CG's loop test (recorded loop): continue while |r|^2 > rtol^2 |r0|^2 and
+// the iteration limit is not reached; the limit or a non-finite residual sets a status bit
+__global__ void k_adj_check(cudaGraphConditionalHandle h, int first, const double *__restrict__ scal,
+                            double *__restrict__ fscal, double rtol2, int maxit, unsigned *status) {
+    if (threadIdx.x || blockIdx.x) return;
+    double rr = scal[S_RR];
+    if (first) {
+        fscal[F_ADJ_RR0] = rr;
+        fscal[F_ADJ_IT] = 0.0;
+    } else {
+        fscal[F_ADJ_IT] += 1.0;
+    }
+    int it = (int)fscal[F_ADJ_IT];
+    unsigned go = 0;
+    if (!isfinite(rr)) atomicOr(status, (unsigned)ST_NONFINITE);
+    else if (rr > rtol2 * fscal[F_ADJ_RR0] && rr > 0.0) {
+        if (it < maxit) go = 1;
+        else atomicOr(status, (unsigned)ST_SCF);
+    }
+    cudaGraphSetConditional(h, go);
+}
+
+// theta into the host copies of the parameters (p, the pair and damping tables, the
+// charges); set_fit_params then copies them to the device
+void Engine::fit_host_params(int tSi, int tO, const double *th) {
     if (tSi < 0 || tO < 0 || tSi >= nt || tO >= nt || tSi == tO) throw Error(MDFFGPU_ERR_ARG, "bad fit types");
-    if (th[7] <= 0.0) throw Error(MDFFGPU_ERR_ARG, "polarisability must be positive");
+    if (!(th[7] > 0.0)) throw Error(MDFFGPU_ERR_ARG, "polarisability must be positive");
     // Born-Mayer-Huggins tables (symmetric)
     for (int pair = 0; pair < 2; pair++) {
         int a = pair == 0 ? tSi : tO, b = tO;
@@ -390,19 +459,15 @@ void Engine::set_fit_params(int tSi, int tO, const double *th) {
             P.C = th[3 * pair + 2];
         }
     }
-    MDFF_CK(cudaMemcpyAsync(d_pair, h_pair.data(), sizeof(PairSR) * nt * nt, cudaMemcpyHostToDevice, stream));
     // charges: q_Si = theta, q_O = -theta / 2
     p.qit[tSi] = th[6];
     p.qit[tO] = -0.5 * th[6];
     for (int i = 0; i < n; i++)
         if (h_typ[i] == tSi) h_q[i] = th[6];
         else if (h_typ[i] == tO) h_q[i] = -0.5 * th[6];
-    int nb = ceil_div(n, 256);
-    MDFF_LAUNCH(*this, k_set_charges, nb, 256, 0, n, d_typ, th[6], tSi, tO, d_q, d_r);
     // isotropic O polarisability
     for (int a = 0; a < 3; a++)
         for (int b = 0; b < 3; b++) p.polit[tO][a][b] = (a == b) ? th[7] : 0.0;
-    MDFF_LAUNCH(*this, k_set_pol, nb, 256, 0, n, d_typ, tO, th[7], d_pol, d_invpol);
     // Tang-Toennies b and c of every damped direction
     for (int t = 0; t < nt; t++)
         for (int i = 0; i < nt; i++)
@@ -423,12 +488,24 @@ void Engine::set_fit_params(int tSi, int tO, const double *th) {
                 D.c2 = th[9];
             }
         }
-    MDFF_CK(cudaMemcpyAsync(d_damp, h_damp.data(), sizeof(PairDamp) * nt * nt, cudaMemcpyHostToDevice, stream));
+}
+
+void Engine::set_fit_params(int tSi, int tO, const double *th) {
+    fit_host_params(tSi, tO, th);
+    fit_alloc();
+    MDFF_CK(cudaMemcpyAsync(d_theta, th, sizeof(double) * MDFFGPU_FIT_NPARAM, cudaMemcpyHostToDevice, stream));
+    fit_apply_theta(d_theta, tSi, tO);
     MDFF_CK(cudaStreamSynchronize(stream));
     gen++;
 }
 
-// CG on A x = b over the polarisable ions, x0 = 0, until |r| <= rtol |b|
+void Engine::fit_apply_theta(const double *d_th, int tSi, int tO) {
+    MDFF_LAUNCH(*this, k_fit_tables, 1, 256, 0, d_th, tSi, tO, nt, d_pair, d_damp);
+    MDFF_LAUNCH(*this, k_fit_ions, ceil_div(n, 256), 256, 0, n, d_typ, d_th, tSi, tO, d_q, d_r, d_pol, d_invpol);
+}
+
+// CG on A x = b over the polarisable ions, x0 = 0, until |r| <= rtol |b|; while
+// recording, the loop is a device-controlled while node (k_adj_check)
 void Engine::solve_pim(const double3 *d_b, double3 *d_x, double rtol, int maxit) {
     int nb = ceil_div(n, 256);
     MDFF_CK(cudaMemsetAsync(d_x, 0, sizeof(double3) * n, stream));
@@ -436,18 +513,37 @@ void Engine::solve_pim(const double3 *d_b, double3 *d_x, double rtol, int maxit)
     MDFF_LAUNCH(*this, k_cg_rz, nb, 256, 0, n, d_polar, d_pol, d_cg_r, d_mu_save, d_part, part_stride, d_scal,
                 d_ticket + 1);
     MDFF_CK(cudaMemcpyAsync(d_cg_p, d_mu_save, sizeof(double3) * n, cudaMemcpyDeviceToDevice, stream));
+    // A p: the search direction vanishes off the polarisable ions, so the field passes
+    // run over those ions only
+    auto iteration = [&]() {
+        if (subset32 && npol > 0) field_pol(d_cg_p, d_ef_ind, nullptr, false);
+        else field_of(d_qzero, d_cg_p, false, true, false, d_ef_ind);
+        MDFF_LAUNCH(*this, k_cg_ap, nb, 256, 0, n, d_polar, d_invpol, d_cg_p, d_ef_ind, d_cg_ap, d_part, part_stride,
+                    d_scal, d_ticket);
+        MDFF_LAUNCH(*this, k_cg_update, nb, 256, 0, n, d_scal, d_cg_p, d_cg_ap, d_x, d_cg_r);
+        MDFF_LAUNCH(*this, k_cg_rz, nb, 256, 0, n, d_polar, d_pol, d_cg_r, d_mu_save, d_part, part_stride, d_scal,
+                    d_ticket + 1);
+    };
+    if (capturing) {
+        double rtol2 = rtol * rtol;
+        record_while(
+            [&](cudaGraphConditionalHandle h) {
+                MDFF_LAUNCH(*this, k_adj_check, 1, 32, 0, h, 1, d_scal, d_fscal, rtol2, maxit, d_status);
+            },
+            [&](cudaGraphConditionalHandle h) {
+                iteration();
+                MDFF_LAUNCH(*this, k_adj_check, 1, 32, 0, h, 0, d_scal, d_fscal, rtol2, maxit, d_status);
+                MDFF_LAUNCH(*this, k_cg_dir, nb, 256, 0, n, d_scal, d_mu_save, d_cg_p);
+            });
+        return;
+    }
     double rr0 = 0.0, rr = 0.0;
     MDFF_CK(cudaMemcpyAsync(&rr0, d_scal + S_RR, sizeof(double), cudaMemcpyDeviceToHost, stream));
     MDFF_CK(cudaStreamSynchronize(stream));
     rr = rr0;
     int it = 0;
     while (rr > rtol * rtol * rr0 && rr > 0.0 && it < maxit) {
-        field_of(d_qzero, d_cg_p, false, true, false, d_ef_ind);
-        MDFF_LAUNCH(*this, k_cg_ap, nb, 256, 0, n, d_polar, d_invpol, d_cg_p, d_ef_ind, d_cg_ap, d_part, part_stride,
-                    d_scal, d_ticket);
-        MDFF_LAUNCH(*this, k_cg_update, nb, 256, 0, n, d_scal, d_cg_p, d_cg_ap, d_x, d_cg_r);
-        MDFF_LAUNCH(*this, k_cg_rz, nb, 256, 0, n, d_polar, d_pol, d_cg_r, d_mu_save, d_part, part_stride, d_scal,
-                    d_ticket + 1);
+        iteration();
         MDFF_CK(cudaMemcpyAsync(&rr, d_scal + S_RR, sizeof(double), cudaMemcpyDeviceToHost, stream));
         MDFF_CK(cudaStreamSynchronize(stream));
         if (!std::isfinite(rr)) throw Error(MDFFGPU_ERR_NONFINITE, "adjoint CG diverged");
@@ -473,24 +569,40 @@ void Engine::coul_forces(const double *d_qv, const double3 *d_muv, bool lq, bool
     launch_rec(*this, d_qv, d_muv, lq, ld, o);
 }
 
-void Engine::force_match(const double3 *d_ft, double scale, double *h_res, int tSi, int tO) {
+// the status bits of an evaluation as the C ABI's error codes
+void fit_status(unsigned st) {
+    if (st & ST_CELL_OVERFLOW) throw Error(MDFFGPU_ERR_LIST_OVERFLOW, "a cell holds more ions than its capacity");
+    if (st & ST_NONFINITE) throw Error(MDFFGPU_ERR_NONFINITE, "non-finite forces or CG residual");
+    if (st & ST_TC_TIMEOUT) throw Error(MDFFGPU_ERR_TIMEOUT, "tensor-core k-space pass timed out waiting on its MMAs");
+    if (st & ST_SCF) throw Error(MDFFGPU_ERR_SCF, "induced-dipole or adjoint CG did not converge");
+}
+
+void Engine::fit_alloc() {
+    if (d_fpart) return;
+    d_fpart = dalloc<double>((size_t)NFSLOT * part_stride);
+    d_fscal = dalloc<double>(NFSLOT);
+    d_w = dalloc<double3>(n);
+    d_lam = dalloc<double3>(n);
+    d_sv = dalloc<double3>(n);
+    d_fa = dalloc<double3>(n);
+    d_fb = dalloc<double3>(n);
+    d_fc = dalloc<double3>(n);
+    d_qw = dalloc<double>(n);
+    d_muw = dalloc<double3>(n);
+    d_efg_rec = dalloc<double>((size_t)n * 9);
+    d_rw = dalloc<double2>((size_t)4 * nk);
+    d_theta = dalloc<double>(MDFFGPU_FIT_NPARAM);
+    d_fres = dalloc<double>(NRES);
+}
+
+// one evaluation on the stream: forces at the converged dipoles, the adjoint solve and
+// the parameter sensitivities; d_res[0..NPARAM] = (sum |F - F_t|^2, dL/dtheta) with the
+// q_Si and alpha_O terms taken at d_th[6], d_th[7]; d_res[NPARAM + 1] = status bits
+void Engine::fit_issue(const double3 *d_ft, double scale, int tSi, int tO, const double *d_th, double *d_res) {
     if (!p.lcoulombic || !lpol) throw Error(MDFFGPU_ERR_STATE, "force matching needs the polarisable Coulomb model");
     if (pim_solver != MDFFGPU_PIM_CG && pim_solver != MDFFGPU_PIM_CG_FUSED)
         throw Error(MDFFGPU_ERR_STATE, "force matching needs a CG induced-dipole solver");
-    if (!d_fpart) {
-        d_fpart = dalloc<double>((size_t)NFSLOT * part_stride);
-        d_fscal = dalloc<double>(NFSLOT);
-        d_w = dalloc<double3>(n);
-        d_lam = dalloc<double3>(n);
-        d_sv = dalloc<double3>(n);
-        d_fa = dalloc<double3>(n);
-        d_fb = dalloc<double3>(n);
-        d_fc = dalloc<double3>(n);
-        d_qw = dalloc<double>(n);
-        d_muw = dalloc<double3>(n);
-        d_efg_rec = dalloc<double>((size_t)n * 9);
-        d_rw = dalloc<double2>((size_t)4 * nk);
-    }
+    fit_alloc();
     const double *q = d_q;
     int nb = ceil_div(n, 256), nbw = ceil_div(n, FIT_WARPS);
     MDFF_CK(cudaMemsetAsync(d_fpart, 0, sizeof(double) * NFSLOT * part_stride, stream));
@@ -526,8 +638,12 @@ void Engine::force_match(const double3 *d_ft, double scale, double *h_res, int t
     // s: real space
     MDFF_LAUNCH(*this, k_adj_dir, nbw, FIT_WARPS * 32, 0, a);
     // s: k space, drho_w from three rho passes of (q w_a, mu w_a)
-    bool saved32 = use32;
-    use32 = false;   // the adjoint runs in FP64
+    struct PrecisionScope {   // the adjoint runs in FP64; the context's precision comes back
+        bool &flag;
+        bool saved;
+        ~PrecisionScope() { flag = saved; }
+    } fp64_scope{use32, use32};
+    use32 = false;
     for (int comp = 0; comp < 3; comp++) {
         MDFF_LAUNCH(*this, k_scale_by_w, nb, 256, 0, n, comp, q, d_mu_tot, d_w, d_qw, d_muw);
         RecOut o;
@@ -575,18 +691,60 @@ void Engine::force_match(const double3 *d_ft, double scale, double *h_res, int t
     MDFF_LAUNCH(*this, k_dot3, nb, 256, 0, n, d_lam, d_fb, d_polar, d_fpart, (int)F_LESTAT, part_stride);
     MDFF_LAUNCH(*this, k_dot3, nb, 256, 0, n, d_lam, d_mu_ind, d_polar, d_fpart, (int)F_LMU, part_stride);
     fit_reduce(F_WFALL, 5, nb);
-    use32 = saved32;
-    double sc[NFSLOT];
-    MDFF_CK(cudaMemcpyAsync(sc, d_fscal, sizeof(double) * NFSLOT, cudaMemcpyDeviceToHost, stream));
+    MDFF_LAUNCH(*this, k_fm_result, 1, 32, 0, d_fscal, d_th, coul_unit, d_status, d_res);
+}
+
+void Engine::force_match(const double3 *d_ft, double scale, double *h_res, int tSi, int tO) {
+    fit_alloc();
+    // theta of the current parameters (set_fit_params keeps the device copy current;
+    // here the q_Si and alpha_O the result assembly divides by)
+    double th[MDFFGPU_FIT_NPARAM] = {p.Abhmftd[tSi][tO], p.Bbhmftd[tSi][tO], p.Cbhmftd[tSi][tO],
+                                     p.Abhmftd[tO][tO],  p.Bbhmftd[tO][tO],  p.Cbhmftd[tO][tO],
+                                     p.qit[tSi],         p.polit[tO][0][0],  0.0, 0.0};
+    MDFF_CK(cudaMemcpyAsync(d_theta, th, sizeof(double) * 8, cudaMemcpyHostToDevice, stream));
+    MDFF_CK(cudaMemsetAsync(d_status, 0, sizeof(unsigned), stream));
+    fit_issue(d_ft, scale, tSi, tO, d_theta, d_fres);
+    double res[NRES];
+    MDFF_CK(cudaMemcpyAsync(res, d_fres, sizeof(double) * NRES, cudaMemcpyDeviceToHost, stream));
     MDFF_CK(cudaStreamSynchronize(stream));
-    double qSi = p.qit[tSi], alO = p.polit[tO][0][0];
-    h_res[0] = sc[F_LOSS];
-    for (int k = 0; k < 6; k++) h_res[1 + k] = sc[F_BHM + k];
-    double wqq = sc[F_WFQ0], wqm = sc[F_WFALL] - sc[F_WFQ0] - sc[F_WF0M];
-    h_res[7] = (2.0 * wqq + wqm + sc[F_LESTAT]) / qSi;
-    h_res[8] = sc[F_LMU] / (alO * alO);
-    h_res[9] = coul_unit * sc[F_DAMP + 0] + sc[F_DAMP + 2];
-    h_res[10] = coul_unit * sc[F_DAMP + 1] + sc[F_DAMP + 3];
+    fit_status((unsigned)res[NRES - 1]);
+    for (int k = 0; k <= MDFFGPU_FIT_NPARAM; k++) h_res[k] = res[k];
+}
+
+// record one evaluation (theta from d_th, result into d_res) as a CUDA graph: the
+// parameter update, forces with the induced-dipole CG, adjoint CG and sensitivities
+void Engine::capture_fit(const double *d_th, int tSi, int tO, double scale, double *d_res) {
+    if (fit_exec) cudaGraphExecDestroy(fit_exec);
+    fit_exec = nullptr;
+    if (p.lverletL && !list_ready) gen_verletlist();
+    fit_alloc();
+    if (use32 && real32 && p.lcoulombic) ensure_real32();   // no allocation while recording
+    MDFF_CK(cudaStreamSynchronize(stream));
+    long long l0 = launches;
+    MDFF_CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    capturing = true;
+    cudaGraph_t graph = nullptr;
+    try {
+        MDFF_CK(cudaMemsetAsync(d_status, 0, sizeof(unsigned), stream));
+        fit_apply_theta(d_th, tSi, tO);
+        fit_issue(d_ft, scale, tSi, tO, d_th, d_res);
+    } catch (...) {
+        capturing = false;
+        cudaStreamEndCapture(stream, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        launches = l0;
+        throw;
+    }
+    capturing = false;
+    MDFF_CK(cudaStreamEndCapture(stream, &graph));
+    cudaError_t err = cudaGraphInstantiate(&fit_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (err != cudaSuccess) {
+        fit_exec = nullptr;
+        MDFF_CK(err);
+    }
+    launches = l0;
+    fit_graph_gen = gen;
 }
 
 }  // namespace mdffgpu

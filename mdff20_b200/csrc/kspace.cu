@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(RHO_THREADS, RHO_MIN_BLOCKS) k_rho(int n, int 
                                                     const double4 *__restrict__ r, const double *__restrict__ q,
                                                     const double3 *__restrict__ mu, int nseg,
                                                     const KSeg *__restrict__ seg, double2 *__restrict__ part,
-                                                    int nk) {
+                                                    int nk, const int *__restrict__ idx) {
     extern __shared__ double2 sm[];
     const int W0 = K0 + 1, W1 = 2 * K1 + 1, W2 = 2 * K2 + 1, WT = W0 + W1 + W2;
     double2 *E = sm;                                   // [RHO_TI][WT]
@@ -72,7 +72,7 @@ __global__ void __launch_bounds__(RHO_THREADS, RHO_MIN_BLOCKS) k_rho(int n, int 
         if (threadIdx.x < 3 * RHO_TI) {
             int slot = threadIdx.x % RHO_TI, dim = threadIdx.x / RHO_TI;
             if (slot < nt) {
-                int ia = t0 + slot;
+                int ia = idx ? idx[t0 + slot] : t0 + slot;   // ion subset: q, mu vanish elsewhere
                 double4 ri = r[ia];
                 double3 t = phase_coord(c, ri.x, ri.y, ri.z);
                 double td = dim == 0 ? t.x : (dim == 1 ? t.y : t.z);
@@ -228,7 +228,8 @@ __global__ void __launch_bounds__(32) k_rho_from_acc(int nk, const double2 *__re
 
 // ---------------------------------------------------------------- pass 2: per ion
 struct IonArgs {
-    int n, K0, K1, K2;
+    int n, K0, K1, K2;      // n: ions in the pass (idx[n] when idx is set)
+    const int *idx;         // output ions (null: 0..n-1); partials are indexed by position in idx
     Cell c;
     const double4 *r;
     const double *q;
@@ -255,9 +256,10 @@ struct IonArgs {
 template <bool WF, bool WEFG>
 __global__ void __launch_bounds__(ION_THREADS) k_rec_ion(IonArgs a) {
     extern __shared__ double2 rk[];
-    int i = blockIdx.x * ION_THREADS + threadIdx.x;
+    int ii = blockIdx.x * ION_THREADS + threadIdx.x;
     int tl = blockIdx.y;
-    bool act = i < a.n;
+    bool act = ii < a.n;
+    int i = act ? (a.idx ? a.idx[ii] : ii) : 0;
     int r0 = a.tile_row[tl], r1 = a.tile_row[tl + 1];
     int k0 = a.tile_k[tl], k1 = a.tile_k[tl + 1];
     for (int k = k0 + threadIdx.x; k < k1; k += ION_THREADS) rk[k - k0] = a.rho_s[k];
@@ -360,7 +362,7 @@ __global__ void __launch_bounds__(ION_THREADS) k_rec_ion(IonArgs a) {
         }
     }
     if (!act) return;
-    double *o = a.part + ((size_t)tl * a.n + i) * ION_NV;
+    double *o = a.part + ((size_t)tl * a.n + ii) * ION_NV;
     o[0] = S0;
     o[1] = S1;
     o[2] = S2;
@@ -376,11 +378,12 @@ __global__ void __launch_bounds__(ION_THREADS) k_rec_ion(IonArgs a) {
 // sum the slices of each ion (fixed order) and write field, force and EFG
 template <bool WF, bool WEFG>
 __global__ void k_rec_combine(IonArgs a) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.n) return;
+    int ii = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ii >= a.n) return;
+    int i = a.idx ? a.idx[ii] : ii;
     double S0 = 0, S1 = 0, S2 = 0, P0 = 0, P1 = 0, P2 = 0, H[6] = {0, 0, 0, 0, 0, 0};
     for (int tl = 0; tl < a.ntile; tl++) {
-        const double *o = a.part + ((size_t)tl * a.n + i) * ION_NV;
+        const double *o = a.part + ((size_t)tl * a.n + ii) * ION_NV;
         S0 += o[0];
         S1 += o[1];
         S2 += o[2];
@@ -487,7 +490,13 @@ void launch_rec(Engine &e, const double *q, const double3 *mu, bool lq, bool ld,
         launch_rec32(e, q, mu, lq, ld, o);
         return;
     }
-    if (o.idx || o.out_idx) throw Error(MDFFGPU_ERR_STATE, "ion subsets are a mixed-precision k-space feature");
+    // ion subsets: the rho pass sums over o.idx (all ions when null; q and mu vanish
+    // elsewhere), the ion pass writes at o.out_idx, else at o.idx, else at every ion
+    const int *rho_idx = o.idx;
+    int rho_n = o.idx ? o.cnt : e.n;
+    const int *out_idx = o.out_idx ? o.out_idx : o.idx;
+    int out_n = o.out_idx ? o.out_cnt : (o.idx ? o.cnt : e.n);
+    int chunk = std::max(1, ceil_div(rho_n, e.rho_chunks));   // the same chunk count, shorter chunks
     int segblocks = ceil_div(e.nseg, RHO_THREADS);
     dim3 grid(segblocks, e.rho_chunks);
     int WT = (e.kmax[0] + 1) + (2 * e.kmax[1] + 1) + (2 * e.kmax[2] + 1);
@@ -503,28 +512,29 @@ void launch_rec(Engine &e, const double *q, const double3 *mu, bool lq, bool ld,
     if (o.rho_acc) {
     } else if (lq && ld) {
         allow_smem(k_rho<true, true>, smem);
-        MDFF_LAUNCH(e, (k_rho<true, true>), grid, RHO_THREADS, smem, e.n, e.rho_chunk, e.cell, e.kmax[0], e.kmax[1],
-                    e.kmax[2], e.d_r, q, mu, e.nseg, e.d_seg, e.d_rho_part, e.nk);
+        MDFF_LAUNCH(e, (k_rho<true, true>), grid, RHO_THREADS, smem, rho_n, chunk, e.cell, e.kmax[0], e.kmax[1],
+                    e.kmax[2], e.d_r, q, mu, e.nseg, e.d_seg, e.d_rho_part, e.nk, rho_idx);
     } else if (lq) {
         allow_smem(k_rho<true, false>, smem);
-        MDFF_LAUNCH(e, (k_rho<true, false>), grid, RHO_THREADS, smem, e.n, e.rho_chunk, e.cell, e.kmax[0],
-                    e.kmax[1], e.kmax[2], e.d_r, q, mu, e.nseg, e.d_seg, e.d_rho_part, e.nk);
+        MDFF_LAUNCH(e, (k_rho<true, false>), grid, RHO_THREADS, smem, rho_n, chunk, e.cell, e.kmax[0],
+                    e.kmax[1], e.kmax[2], e.d_r, q, mu, e.nseg, e.d_seg, e.d_rho_part, e.nk, rho_idx);
     } else if (ld) {
         allow_smem(k_rho<false, true>, smem);
-        MDFF_LAUNCH(e, (k_rho<false, true>), grid, RHO_THREADS, smem, e.n, e.rho_chunk, e.cell, e.kmax[0],
-                    e.kmax[1], e.kmax[2], e.d_r, q, mu, e.nseg, e.d_seg, e.d_rho_part, e.nk);
+        MDFF_LAUNCH(e, (k_rho<false, true>), grid, RHO_THREADS, smem, rho_n, chunk, e.cell, e.kmax[0],
+                    e.kmax[1], e.kmax[2], e.d_r, q, mu, e.nseg, e.d_seg, e.d_rho_part, e.nk, rho_idx);
     } else {
         MDFF_CK(cudaMemsetAsync(e.d_rho_part, 0, sizeof(double2) * (size_t)e.nk * e.rho_chunks, e.stream));
     }
     if (!o.rho_acc) {
-        e.prof_end("k_rho", ps, (lq || ld) ? rho_flops_per_pair(lq, ld) * (double)e.n * e.nk : 0.0);
+        e.prof_end("k_rho", ps, (lq || ld) ? rho_flops_per_pair(lq, ld) * (double)rho_n * e.nk : 0.0);
         MDFF_LAUNCH(e, k_rho_reduce<double2>, nbr, 256, 0, e.nk, e.rho_chunks, e.d_rho_part, e.d_Ak, e.d_kcoe, e.d_kvec,
                     e.d_rho, o.rho_raw, e.d_part, (int)S_REC_U, e.part_stride);
         e.reduce(S_REC_U, 7, nbr);
     }
 
     IonArgs a;
-    a.n = e.n;
+    a.n = out_n;
+    a.idx = out_idx;
     a.K0 = e.kmax[0];
     a.K1 = e.kmax[1];
     a.K2 = e.kmax[2];
@@ -555,8 +565,8 @@ void launch_rec(Engine &e, const double *q, const double3 *mu, bool lq, bool ld,
     a.efg_dir = o.efg_dir;
     if (!a.want_ef && !a.want_f && !a.want_efg) return;
     size_t smem2 = sizeof(double2) * e.tile_kmax;
-    dim3 g2(ceil_div(e.n, ION_THREADS), e.ntile);
-    int nb = ceil_div(e.n, 256);
+    dim3 g2(ceil_div(out_n, ION_THREADS), e.ntile);
+    int nb = ceil_div(out_n, 256);
     int pi = -1;
     e.prof_begin("k_rec_ion", &pi);
     if (a.want_efg)
@@ -565,7 +575,7 @@ void launch_rec(Engine &e, const double *q, const double3 *mu, bool lq, bool ld,
         MDFF_LAUNCH(e, (k_rec_ion<true, false>), g2, ION_THREADS, smem2, a);
     else
         MDFF_LAUNCH(e, (k_rec_ion<false, false>), g2, ION_THREADS, smem2, a);
-    e.prof_end("k_rec_ion", pi, ion_flops_per_pair(a.want_f || a.want_efg, a.want_efg) * (double)e.n * e.nk);
+    e.prof_end("k_rec_ion", pi, ion_flops_per_pair(a.want_f || a.want_efg, a.want_efg) * (double)out_n * e.nk);
     if (a.want_efg)
         MDFF_LAUNCH(e, (k_rec_combine<true, true>), nb, 256, 0, a);
     else if (a.want_f)

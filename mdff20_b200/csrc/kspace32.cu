@@ -25,7 +25,7 @@
 // k_ion32   : per ion and k-slice the n-space sums of field (and force) terms.  Thread
 //             = ion; per row the block stages the weights of Ak rho(+z) and Ak rho(-z)
 //             folded over the sign of nz, E2[z] (z = 1..KZ) sits in registers, the row
-//             sums cost 2 FMA per k-vector (3 with forces) and one product with the row
+//             sums cost 4 FMA per k-vector (6 with forces) and one product with the row
 //             phase exp(2 pi i (nx tx + ny ty)), from an FP64-reduced argument every
 //             ION32_RUN rows and by FP32 steps in ny between.  Row sums FP32, rows FP64.
 // Both passes take an optional ion index list (the polarisable ions of an induced-
@@ -273,7 +273,8 @@ static int ion32_row_bytes(int KZ, bool wf) {
 // with a1 = Re(rho_z + rho_-z), a2 = Im(rho_z - rho_-z), a3 = Im(rho_z + rho_-z),
 // a4 = Re(rho_-z - rho_z) of Ak rho.  The block stages a1..a4 (and their z, z^2
 // multiples) of its rows in shared memory as planar z pairs; per ion the sums cost
-// 2 FMA per k-vector (3 with forces), packed FP32x2 FMAs over the pairs.
+// 4 FMA per k-vector (6 with forces: G, H and K are complex, each |z| serves +z and -z),
+// packed FP32x2 FMAs over the pairs.
 // the slice's rows staged in shared memory: (nx, ny) of each row in rnxy, and per row
 // entry 0 = (rho_0, 0, 0), then per z pair (z, z') = (2p+1, 2p+2) the weights
 //   (a1, a1', a2, a2'), (a3, a3', a4, a4'), z (-a4, -a4', a3, a3'), z (a2, a2', -a1, -a1'),
@@ -692,8 +693,11 @@ void launch_coords32(Engine &e) {
 
 // FLOPs per (ion, k-vector) of the paired-nz formulation: 4 FMA with dipoles, 2 without
 static double rho32_flops_per_pair(bool ld) { return ld ? 8.0 : 4.0; }
-// FLOPs per (ion, k-vector) of the folded ion pass: 2 FMA for the field, 3 with forces
-static double ion32_flops_per_pair(bool f) { return f ? 6.0 : 4.0; }
+// FLOPs per (ion, k-vector) of the folded ion pass, counted from the loop body: per z
+// pair (z, z') a thread issues 8 packed FFMA2 for G and H (16 FMA) per ion, covering the
+// four k-vectors +-z, +-z' of the row: 4 FMA = 8 flops per (ion, k) for the field; the
+// force pass adds the two K sums (4 FFMA2 more): 6 FMA = 12 flops
+static double ion32_flops_per_pair(bool f) { return f ? 12.0 : 8.0; }
 void launch_rho_reduce32(Engine &e, const float2 *part, int nchunks, double2 *rho_raw);
 
 template <bool LQ, bool LD>

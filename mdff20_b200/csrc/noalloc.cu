@@ -5,8 +5,9 @@
 // lists.  It runs the same kernels as mdffgpu_gen_verletlist (lists.cu).
 //
 // For callers that cannot allocate device memory: an application that owns all GPU
-// memory through its own pool and forbids allocations once it has started, or one that
-// records its whole MD step into a CUDA graph and needs the list rebuilt inside it.
+// memory through its own pool and forbids allocations once it has started (so a
+// cudaMalloc from a library would either fail or break its accounting), or a host that
+// runs the engine inside a fixed device-memory budget set at start-up.
 #include <mutex>
 
 #include "engine.cuh"
@@ -109,15 +110,22 @@ extern "C" int mdffgpu_build_lists_noalloc(const double *d_pos, int n, const dou
     for (int i = 0; i < 3; i++)
         for (int j = 0; j < 3; j++)
             if (i != j && c.A[i][j] != 0.0) c.ortho = 0;
-    // cell grid as Engine::setup_cells
+    // cell grid as Engine::setup_cells, then coarsened to the scratch's cell limit: the
+    // largest dimension loses one cell at a time, so every cell stays at least one list
+    // radius wide and the pair sets are those of the finer grid (32768 = 32^3, so no
+    // dimension drops below 3)
     double cut = cut_nb > cut_co ? cut_nb : cut_co;
     int nc[3];
     for (int d = 0; d < 3; d++) {
         int k = (int)std::floor(c.w[d] / cut);
         nc[d] = (k >= 3 && c.ortho) ? (k < 64 ? k : 64) : 1;
     }
+    while ((long long)nc[0] * nc[1] * nc[2] > NA_MAX_CELLS) {
+        int d = (nc[1] > nc[0]) ? 1 : 0;
+        if (nc[2] > nc[d]) d = 2;
+        nc[d]--;
+    }
     int ncell = nc[0] * nc[1] * nc[2];
-    if (ncell > NA_MAX_CELLS) return MDFFGPU_ERR_ARG;
     if (ncell == 1 && n > NA_CELL_CAP) return MDFFGPU_ERR_CELL;   // one cell must hold every ion
     NaPtrs P;
     int rc = na_pointers(&P);

@@ -77,8 +77,16 @@ void Engine::save_state(unsigned char *buf) {
     size_t n3 = 3 * (size_t)n;
     std::vector<double> packed(2 * n3);
     int nb = ceil_div(n, 256);
-    double *d_tmp = nullptr;
-    MDFF_CK(cudaMallocAsync((void **)&d_tmp, sizeof(double) * 2 * n3, stream));
+    // stream-ordered scratch, returned to the pool on every exit (errors throw)
+    struct AsyncScratch {
+        double *p;
+        cudaStream_t s;
+        ~AsyncScratch() {
+            if (p) cudaFreeAsync(p, s);
+        }
+    } scratch{nullptr, stream};
+    MDFF_CK(cudaMallocAsync((void **)&scratch.p, sizeof(double) * 2 * n3, stream));
+    double *d_tmp = scratch.p;
     MDFF_LAUNCH(*this, k_pack3, nb, 256, 0, n, d_r, d_tmp);
     MDFF_LAUNCH(*this, k_pack3, nb, 256, 0, n, d_svl, d_tmp + n3);
     MDFF_CK(cudaMemcpyAsync(packed.data(), d_tmp, sizeof(double) * 2 * n3, cudaMemcpyDeviceToHost, stream));
@@ -120,8 +128,16 @@ int Engine::load_state(const unsigned char *buf, size_t bytes) {
     const double *r = w, *v = r + n3, *f = v + n3, *rs = f + n3, *svl = rs + n3, *mu = svl + n3, *hist = mu + n3,
                  *nhc = hist + 18 * (size_t)n;
     int nb = ceil_div(n, 256);
-    double *d_tmp = nullptr;
-    MDFF_CK(cudaMallocAsync((void **)&d_tmp, sizeof(double) * 2 * n3, stream));
+    // stream-ordered scratch, returned to the pool on every exit (errors throw)
+    struct AsyncScratch {
+        double *p;
+        cudaStream_t s;
+        ~AsyncScratch() {
+            if (p) cudaFreeAsync(p, s);
+        }
+    } scratch{nullptr, stream};
+    MDFF_CK(cudaMallocAsync((void **)&scratch.p, sizeof(double) * 2 * n3, stream));
+    double *d_tmp = scratch.p;
     MDFF_CK(cudaMemcpyAsync(d_tmp, r, sizeof(double) * n3, cudaMemcpyHostToDevice, stream));
     MDFF_CK(cudaMemcpyAsync(d_tmp + n3, svl, sizeof(double) * n3, cudaMemcpyHostToDevice, stream));
     MDFF_LAUNCH(*this, k_unpack4, nb, 256, 0, n, d_tmp, d_q, d_r);
@@ -158,6 +174,7 @@ int Engine::load_state(const unsigned char *buf, size_t bytes) {
         if (!list_ready) throw Error(MDFFGPU_ERR_LIST_OVERFLOW, "neighbour list capacity could not be grown");
         launch_kardir(*this, d_r, d_s);   // as a finished step leaves it
     }
+    scratch.p = nullptr;
     MDFF_CK(cudaFreeAsync(d_tmp, stream));
     int nbuilds = h.nbuilds;
     MDFF_CK(cudaMemcpyAsync(&d_out->nbuilds, &nbuilds, sizeof(int), cudaMemcpyHostToDevice, stream));

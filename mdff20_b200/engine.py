@@ -163,6 +163,7 @@ EXPORTS = (
     "mdffgpu_get_dipoles", "mdffgpu_prop_agate", "mdffgpu_md_steps", "mdffgpu_launch_count",
     "mdffgpu_stream", "mdffgpu_fma_peak", "mdffgpu_profile", "mdffgpu_profile_result",
     "mdffgpu_build_lists_noalloc", "mdffgpu_fit_set_params", "mdffgpu_force_match", "mdffgpu_fit_batch",
+    "mdffgpu_fit_plan_create", "mdffgpu_fit_plan_eval", "mdffgpu_fit_plan_destroy", "mdffgpu_fit_plan_last_error",
     "mdffgpu_state_size", "mdffgpu_save_state", "mdffgpu_load_state",
     "mdffgpu_rdf_create", "mdffgpu_rdf_destroy", "mdffgpu_rdf_last_error", "mdffgpu_rdf_reset", "mdffgpu_rdf_add",
     "mdffgpu_rdf_add_ctx", "mdffgpu_rdf_counts",
@@ -220,6 +221,9 @@ def load_library(path: str = LIB_PATH):
         "mdffgpu_fit_set_params": [vp, I, I, dp],
         "mdffgpu_force_match": [vp, I, I, dp, dp, dp, D, dp],
         "mdffgpu_fit_batch": [vpp, I, I, I, dp, C.POINTER(dp), D, I, dp],
+        "mdffgpu_fit_plan_create": [vpp, I, I, I, C.POINTER(dp), D, vpp],
+        "mdffgpu_fit_plan_eval": [vp, dp, dp],
+        "mdffgpu_fit_plan_destroy": [vp],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -241,6 +245,8 @@ def load_library(path: str = LIB_PATH):
     L.mdffgpu_build_lists_noalloc.restype = C.c_int
     L.mdffgpu_rdf_last_error.argtypes = [vp]
     L.mdffgpu_rdf_last_error.restype = C.c_char_p
+    L.mdffgpu_fit_plan_last_error.argtypes = [vp]
+    L.mdffgpu_fit_plan_last_error.restype = C.c_char_p
     _lib = L
     return L
 
@@ -460,3 +466,44 @@ class Engine:
         res = np.zeros(1 + FIT_NPARAM)
         self._check(self.L.mdffgpu_force_match(self.h, tSi, tO, _dp(fx), _dp(fy), _dp(fz), scale, _dp(res)))
         return float(res[0]), res[1:].copy()
+
+
+class FitPlan:
+    """mdffgpu_fit_plan: force matching over a set of contexts with each configuration's
+    evaluation recorded once as a CUDA graph (device-side CG loops, theta in one device
+    buffer), replayed per evaluation."""
+
+    def __init__(self, engines, tSi: int, tO: int, targets, scale: float):
+        self.L = load_library()
+        n = len(engines)
+        self._engines = list(engines)   # the contexts must outlive the plan
+        self._ctx = (C.c_void_p * n)(*[e.h.value for e in engines])
+        self._tgt_arrays = [np.ascontiguousarray(np.asarray(t, float).reshape(-1, 3)) for t in targets]
+        tg = (C.POINTER(C.c_double) * n)(*[t.ctypes.data_as(C.POINTER(C.c_double)) for t in self._tgt_arrays])
+        h = C.c_void_p()
+        rc = self.L.mdffgpu_fit_plan_create(self._ctx, n, tSi, tO, tg, scale, C.byref(h))
+        if rc != 0:
+            raise MdffgpuError(rc, "mdffgpu_fit_plan_create failed")
+        self.h = h
+
+    def eval(self, theta):
+        """(sum of |F - F_t|^2 over every configuration, the summed gradient)."""
+        th = np.ascontiguousarray(np.asarray(theta, float))
+        assert th.shape == (FIT_NPARAM,)
+        res = np.zeros(1 + FIT_NPARAM)
+        rc = self.L.mdffgpu_fit_plan_eval(self.h, _dp(th), _dp(res))
+        if rc != 0:
+            msg = self.L.mdffgpu_fit_plan_last_error(self.h)
+            raise MdffgpuError(rc, msg.decode() if msg else "mdffgpu_fit_plan_eval failed")
+        return float(res[0]), res[1:].copy()
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.mdffgpu_fit_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

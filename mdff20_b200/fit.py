@@ -120,6 +120,26 @@ def ewald_tune(L: float, n: int, eps: float = 1e-6, rc_max: float = 10.0, skin: 
     return best
 
 
+def ewald_converged(L: float, rc: float, eps: float = 1e-12) -> EwaldChoice:
+    """Ewald parameters at the real-space cutoff rc whose truncation errors are below eps
+    (default 1e-12): the converged sum a tuned choice at the same rc is measured against.
+    (The cutoff itself is kept: the reference applies the Tang-Toennies damping
+    correction -(1 - f_k(b r)) T to the pairs inside it only, src/ewald.c:536-539 and
+    :567-600, so with damping the sum depends on rc whatever alpha and kmax.)"""
+    alpha = _erfc_root(eps) / rc
+    kmax = max(1, math.ceil(alpha * L * math.sqrt(-math.log(eps)) / math.pi))
+    return EwaldChoice(alpha=float(alpha), rc=float(rc), kmax=int(kmax), cost=float("nan"))
+
+
+def with_ewald(s: System, ch: EwaldChoice) -> System:
+    """A copy of `s` with the Ewald splitting, real-space cutoff and kmax of `ch`."""
+    s2 = copy.deepcopy(s)
+    s2.alphaES = ch.alpha
+    s2.cutlongrange = ch.rc
+    s2.kES = (ch.kmax, ch.kmax, ch.kmax)
+    return s2
+
+
 # ---------------------------------------------------------------------------- config 4
 def config4_sizes(nconf: int = 512, seed: int = 4) -> List[int]:
     rng = np.random.Generator(np.random.PCG64(seed))
@@ -190,12 +210,18 @@ def allreduce_loss_grad(loss: float, grad, group=None):
 
 # ---------------------------------------------------------------------------- batch
 class ForceMatchBatch:
-    """Engines for a list of configurations; loss and adjoint gradient at theta."""
+    """Engines for a list of configurations; loss and adjoint gradient at theta.
+
+    recorded (default): every configuration's evaluation is recorded once as a CUDA graph
+    (mdffgpu_fit_plan) and replayed per evaluation, all configurations in flight at once;
+    otherwise mdffgpu_fit_batch drives the contexts from `threads` host threads."""
 
     def __init__(self, systems: Sequence[System], targets: Optional[Sequence[np.ndarray]], device: int = -1,
-                 precision: int = 0, threads: int = 8, ntot: Optional[int] = None):
+                 precision: int = 0, threads: int = 8, ntot: Optional[int] = None, recorded: bool = True):
         """ntot: ions of the whole fit when these systems are one shard of it (the loss is
         normalised by 3 ntot), default the ions of these systems."""
+        self.recorded = recorded
+        self._plan = None
         from .engine import PIM_CG, Engine, load_library
         from .cellmath import wrap_positions
         self.L = load_library()
@@ -222,6 +248,12 @@ class ForceMatchBatch:
     def loss_grad(self, theta) -> tuple:
         """(L, dL/dtheta) of L = sum |F - F_t|^2 / (3 N_total)."""
         th = np.ascontiguousarray(np.asarray(theta, float))
+        if self.recorded:
+            if self._plan is None:
+                from .engine import FitPlan
+                self._plan = FitPlan(self.engines, SI_TYPE, O_TYPE, self.targets, self.scale)
+            sq, grad = self._plan.eval(th)
+            return 0.5 * self.scale * sq, grad
         res = np.zeros(1 + NPARAM)
         rc = self.L.mdffgpu_fit_batch(self._ctx, len(self.engines), SI_TYPE, O_TYPE,
                                       th.ctypes.data_as(C.POINTER(C.c_double)), self._tgt, self.scale,
@@ -232,6 +264,9 @@ class ForceMatchBatch:
         return 0.5 * self.scale * res[0], res[1:].copy()
 
     def set_targets(self, targets: Sequence[np.ndarray]):
+        if getattr(self, "_plan", None) is not None:   # the plan holds the old targets on the device
+            self._plan.close()
+            self._plan = None
         self.targets = [np.ascontiguousarray(np.asarray(t, float).reshape(-1, 3)) for t in targets]
         n = len(self.engines)
         self._tgt = (C.POINTER(C.c_double) * n)(*[t.ctypes.data_as(C.POINTER(C.c_double))
@@ -246,6 +281,9 @@ class ForceMatchBatch:
         return out
 
     def close(self):
+        if self._plan is not None:
+            self._plan.close()
+            self._plan = None
         for e in self.engines:
             e.close()
         self.engines = []

@@ -5,7 +5,8 @@
  * only once, at set-up, to invert per-ion polarisability tensors (src/config.c:171).
  * Gauss-Jordan elimination with partial pivoting: for a diagonal input every inverse
  * entry is exactly 1.0/a_ii, as LAPACK's triangular inverse gives.
- * Test infrastructure only (part of the compiled-reference checker). */
+ * Linked into the drop-in build of the reference program (Makefile target dropin) and
+ * into the compiled-reference checker. */
 #include <math.h>
 #include <stdio.h>
 

@@ -1192,8 +1192,9 @@ static void rec_thermo(const orc_ctx *c, double *t) {
     t[8] = c->th.pvir_coul; t[9] = (double)c->nbuilds; t[10] = (double)c->th.scf_iter; t[11] = c->th.scf_rmsd;
 }
 
-/* the run_md loop (src/md.c:196-247): forces at t=0, then nsteps steps */
-int orc_md(orc_ctx *c, int nsteps, double *thermo) {
+/* the run_md loop (src/md.c:196-247): forces at t=0, then nsteps steps with step indices
+ * first, first+1, ... (the index drives the ASPC order, src/pim.c:321-333) */
+int orc_md_from(orc_ctx *c, int first, int nsteps, double *thermo) {
     if (c->p.lverletL && !c->list_ok) {
         int rc = orc_gen_verletlist(c);
         if (rc) return rc;
@@ -1204,12 +1205,14 @@ int orc_md(orc_ctx *c, int nsteps, double *thermo) {
     if (rc) return rc;
     if (thermo) rec_thermo(c, thermo);
     for (int s = 1; s <= nsteps; s++) {
-        rc = orc_md_step(c, s);
+        rc = orc_md_step(c, first + s - 1);
         if (rc) return rc;
         if (thermo) rec_thermo(c, thermo + 12 * s);
     }
     return 0;
 }
+
+int orc_md(orc_ctx *c, int nsteps, double *thermo) { return orc_md_from(c, 1, nsteps, thermo); }
 
 /* ------------------------------------------------------------------ g(r) */
 /* get_gr, src/radial_distribution.c:180-230, for one configuration: every ordered pair

@@ -108,6 +108,8 @@ int orc_md_step(orc_ctx *c, int istep);
 /* nsteps steps; thermo (nsteps+1, 12) records like the harness: e_kin u_lj u_bhmftd
  * u_coul u_pol e_nvt pvir_lj pvir_bhmftd pvir_coul nlist_builds scf_iter scf_rmsd */
 int orc_md(orc_ctx *c, int nsteps, double *thermo);
+/* the same with step indices first .. first+nsteps-1 (the index sets the ASPC order) */
+int orc_md_from(orc_ctx *c, int first, int nsteps, double *thermo);
 
 /* get_gr (src/radial_distribution.c:180-230) of one configuration: pos (N,3) Cartesian,
  * cell9 the rows of A, typ per ion; adds ordered-pair counts to hist[nbins][nt][nt]. */

@@ -158,7 +158,7 @@ def lib():
         for name, args in [("orc_gen_verletlist", [vp]), ("orc_check_verletlist", [vp]),
                            ("orc_get_verletlist", [vp, I, ip, ip, I]), ("orc_engforce", [vp]),
                            ("orc_multipole_es", [vp, dp, dp, I, D, dp, dp, dp, dp, dp, dp]),
-                           ("orc_md_step", [vp, I]), ("orc_md", [vp, I, dp]), ("orc_nion", [vp]),
+                           ("orc_md_step", [vp, I]), ("orc_md", [vp, I, dp]), ("orc_md_from", [vp, I, I, dp]), ("orc_nion", [vp]),
                            ("orc_nk", [vp])]:
             getattr(L, name).argtypes = args
             getattr(L, name).restype = C.c_int
@@ -296,9 +296,10 @@ class Oracle:
         return dict(u=u[0], pvir=pv[0], tau=tau.reshape(3, 3), ef=ef, efg=efg.reshape(self.n, 3, 3), f=f)
 
     # ---------------------------------------------------------------- md
-    def md(self, nsteps: int):
+    def md(self, nsteps: int, first: int = 1):
+        """Forces at t = 0, then nsteps steps with step indices first, first + 1, ..."""
         th = np.zeros((nsteps + 1, 12))
-        rc = self.L.orc_md(self.h, nsteps, _dp(th))
+        rc = self.L.orc_md_from(self.h, first, nsteps, _dp(th))
         if rc:
             raise RuntimeError(f"orc_md failed {rc}")
         return th

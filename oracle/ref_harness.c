@@ -274,17 +274,22 @@ int main(int argc, char *argv[]) {
     } while (0)
         REC_THERMO(0);
         if (every > 0) REC_FRAME();
+        double *step_wall = calloc((size_t)nsteps + 1, sizeof(double));
         double t0 = omp_get_wtime();
         /* the MD loop body of src/md.c:229-247 without its output */
         for (istep = first; istep < npas + 1; istep++) {
+            double ts = omp_get_wtime();
             prop_agate(istep);
             if (lverletL) check_verletlist();
             if ((rescale_allowed) && (istep < nequil) && (istep % nequilT == 0)) rescale_velocities(1);
+            step_wall[istep - first] = omp_get_wtime() - ts;
             REC_THERMO(istep - first + 1);
             if (every > 0 && istep % every == 0) REC_FRAME();
         }
         double t1 = omp_get_wtime();
         put_s("wall", t1 - t0);
+        put_d("step_wall", step_wall, nsteps);
+        free(step_wall);
         put_d("thermo", th, 12LL * nrec);
         if (every > 0) put_d("traj", traj, 9LL * nion * iframe);
         put_xyz("r", rx, ry, rz);

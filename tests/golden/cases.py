@@ -85,6 +85,11 @@ def silica96_ko():
 
 CASES["silica96_ko"] = silica96_ko
 
+# ASPC order 4 (the config-5 bench setting) over NHC steps started at step index 6, past the
+# reference's first-steps order switch (src/pim.c:321-333)
+ASPC4_FIRST, ASPC4_STEPS = 6, 10
+CASES["crist192_pim_nhc_aspc4"] = lambda: crist192(True, integrator="nvt-nhcn", temp=2500.0, extrapolate_order=4)
+
 
 # ---------------------------------------------------------------- C host (mdff20gpu.x)
 def _with(s, **kw):

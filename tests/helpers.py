@@ -18,3 +18,17 @@ def rel_err(a, b) -> float:
     b = np.asarray(b, float)
     scale = max(float(np.abs(b).max()), 1e-300)
     return float(np.abs(a - b).max()) / scale
+
+
+def rms_rel(a, b) -> float:
+    """RMS over rows of |a_i - b_i| divided by the RMS of |b_i| (the force-error measure)."""
+    a = np.asarray(a, float).reshape(-1, 3)
+    b = np.asarray(b, float).reshape(-1, 3)
+    return float(np.sqrt(np.mean(np.sum((a - b) ** 2, axis=1))) / np.sqrt(np.mean(np.sum(b ** 2, axis=1))))
+
+
+def tensor_rel(a, b) -> float:
+    """max |a_kl - b_kl| / max |b_kl| over a 3x3 stress tensor."""
+    a = np.asarray(a, float).ravel()
+    b = np.asarray(b, float).ravel()
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))

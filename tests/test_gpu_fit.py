@@ -96,3 +96,45 @@ def test_mixed_precision_gradient_close_to_fp64():
     assert np.max(np.abs(g32 - g64)) < 1e-4 * np.max(np.abs(g64))
     ref.close()
     mix.close()
+
+
+@pytest.mark.parametrize("precision", [0, MIXED])
+def test_recorded_plan_matches_host_driven_batch(precision):
+    """mdffgpu_fit_plan (each configuration's evaluation recorded once as a CUDA graph,
+    theta from a device buffer, both CG loops device-controlled) against the host-driven
+    batch, over several theta values replayed through the same graphs."""
+    systems = fit.config4(sizes=[96, 288, 192, 384], conv_tol=1e-9)
+    th0 = fit.theta_of(systems[0])
+    targets = fit.target_forces(systems, fit.perturbed_theta(th0, seed=7))
+    rec = fit.ForceMatchBatch(systems, targets, precision=precision)
+    host = fit.ForceMatchBatch(systems, targets, precision=precision, threads=4, recorded=False)
+    rng = np.random.default_rng(3)
+    for k in range(3):
+        th = th0 * (1.0 + 0.02 * rng.standard_normal(fit.NPARAM)) if k else th0
+        l1, g1 = rec.loss_grad(th)
+        l2, g2 = host.loss_grad(th)
+        assert abs(l1 - l2) <= 1e-9 * l2, (k, l1, l2)
+        assert np.max(np.abs(g1 - g2)) <= 1e-8 * np.max(np.abs(g2)), (k, g1, g2)
+    # after the replays a context holds the last theta on the device and in its host
+    # copies: a single evaluation without setting theta agrees with the host-driven one
+    a = rec.engines[1].force_match(fit.SI_TYPE, fit.O_TYPE, targets[1], rec.scale)
+    b = host.engines[1].force_match(fit.SI_TYPE, fit.O_TYPE, targets[1], host.scale)
+    assert abs(a[0] - b[0]) <= 1e-9 * b[0]
+    assert np.max(np.abs(a[1] - b[1])) <= 1e-8 * np.max(np.abs(b[1]))
+    rec.close()
+    host.close()
+
+
+def test_recorded_plan_reports_nonconvergence():
+    """An iteration cap the induced-dipole CG cannot meet comes back as ERR_SCF from a
+    replayed evaluation, with the configuration named."""
+    from mdff20_b200.engine import MdffgpuError
+    systems = fit.config4(sizes=[96, 192], conv_tol=1e-10)
+    systems[1].max_scf_pim_iter = 1
+    th0 = fit.theta_of(systems[0])
+    targets = fit.target_forces(fit.config4(sizes=[96, 192]), fit.perturbed_theta(th0))
+    b = fit.ForceMatchBatch(systems, targets)
+    with pytest.raises(MdffgpuError) as ex:
+        b.loss_grad(th0)
+    assert ex.value.code == 4 and "configuration 1" in str(ex.value)
+    b.close()

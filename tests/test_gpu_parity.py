@@ -12,7 +12,7 @@ from mdff20_b200 import synth
 from mdff20_b200.engine import PIM_CG, PIM_CG_FUSED, Engine, MdffgpuError
 from oracle.oracle import Oracle, wrapped_positions
 from tests.golden import cases
-from tests.helpers import load_golden, rel_err
+from tests.helpers import load_golden, rel_err, rms_rel, tensor_rel
 
 pytestmark = pytest.mark.gpu
 
@@ -296,13 +296,15 @@ def test_list_capacity_grows():
 
 
 # ---------------------------------------------------------------------------- mixed precision
-def _rms_rel(a, b):
-    return float(np.sqrt(np.mean(np.sum((a - b) ** 2, axis=1))) / np.sqrt(np.mean(np.sum(b ** 2, axis=1))))
+# Mixed FP32/FP64 bars (relative): forces and induced dipoles 1e-5 RMS over ions, energies
+# and virials 1e-5, stress tensors 1e-5 of their largest component.
+_rms_rel = rms_rel
 
 
-@pytest.mark.parametrize("name", ["silica450_pim", "silica96_rigid"])
-def test_mixed_precision_force_error_small(name):
-    """Mixed FP32/FP64 forces within 1e-5 relative RMS of the reference's FP64 forces."""
+@pytest.mark.parametrize("name", ["silica450_pim", "silica96_rigid", "silica96_pim"])
+def test_mixed_precision_errors_small(name):
+    """Mixed FP32/FP64 forces, induced dipoles, energies and stress against the
+    reference's FP64 results."""
     from mdff20_b200.engine import MIXED
     e, g, s = _engine_for(name, precision=MIXED)
     e.gen_verletlist()
@@ -311,6 +313,13 @@ def test_mixed_precision_force_error_small(name):
     assert _rms_rel(e.forces(), fr) < 1e-5
     th = e.thermo()
     assert abs(th["u_coul"] - float(g["u_coul"][0])) < 1e-6 * abs(float(g["u_coul"][0]))
+    for k in ("u_bhmftd", "u_pol", "pvir_coul", "pvir_bhmftd"):
+        ref = float(g[k][0])
+        assert abs(th[k] - ref) <= 1e-5 * max(abs(ref), 1e-12), k
+    for k in ("tau_coul", "tau_bhmftd"):
+        assert tensor_rel(th[k], g[k]) < 1e-5, k
+    if "mu_ind" in g:
+        assert _rms_rel(e.dipole_history()[:, 0, :], g["mu_ind"].reshape(-1, 3)) < 1e-5
 
 
 def test_mixed_precision_force_error_full_size():
@@ -330,7 +339,11 @@ def test_mixed_precision_force_error_full_size():
     a, b = mix.thermo(), ref.thermo()
     # energies: same 1e-5 relative bar as the forces (u_pol carries the SCF
     # convergence tolerance on top of the FP32 field error)
-    for k in ("u_coul", "u_pol", "u_bhmftd"):
+    for k in ("u_coul", "u_pol", "u_bhmftd", "pvir_coul", "pvir_bhmftd"):
         assert abs(a[k] - b[k]) < 1e-5 * max(1.0, abs(b[k])), k
+    for k in ("tau_coul", "tau_bhmftd"):
+        assert tensor_rel(a[k], b[k]) < 1e-5, k
+    mu_err = _rms_rel(mix.dipole_history()[:, 0, :], ref.dipole_history()[:, 0, :])
+    assert mu_err < 1e-5, mu_err
     th = mix.md_steps(1, 3)
     assert np.isfinite(th).all()

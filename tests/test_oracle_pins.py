@@ -15,7 +15,9 @@ from oracle import ref
 from oracle.oracle import Oracle
 from tests.golden import cases
 
-REFERENCE_SRC = os.environ.get("MDFF20_REFERENCE", "/root/reference")
+# the reference checkout: $MDFF20_REFERENCE, else a sibling directory of this repository
+REFERENCE_SRC = os.environ.get("MDFF20_REFERENCE", os.path.join(os.path.dirname(os.path.dirname(
+    os.path.dirname(os.path.abspath(__file__)))), "reference"))
 
 
 def _oracle_for(name, wrap_from_golden=True):
@@ -84,6 +86,22 @@ def test_md_vs_reference(name, nsteps):
     assert th[-1, 9] == ref_th[-1, 9]  # same number of list rebuilds
     pos, vel, f = o.state()
     assert rel_err(vel, g["md_v"].reshape(-1, 3)) < 1e-7
+
+
+def test_md_aspc_order4_vs_reference():
+    """ASPC order 4 (the config-5 setting): NHC steps from step index 6, where the
+    predictor runs at the full order from the first step."""
+    o, g, s = _oracle_for("crist192_pim_nhc_aspc4")
+    th = o.md(cases.ASPC4_STEPS, first=cases.ASPC4_FIRST)
+    ref_th = g["md_thermo"].reshape(-1, 12)
+    for col in (0, 1, 2, 3, 4, 5):
+        scale = max(1.0, float(np.abs(ref_th[:, col]).max()))
+        assert np.abs(th[:, col] - ref_th[:, col]).max() < 1e-9 * scale, col
+    pos, vel, f = o.state()
+    assert rel_err(vel, g["md_v"].reshape(-1, 3)) < 1e-9
+    assert rel_err(f, g["md_f"].reshape(-1, 3)) < 1e-9
+    xi, vxi = o.nhc()
+    assert np.allclose(xi, g["xi"], rtol=1e-8, atol=1e-14)
 
 
 @pytest.mark.skipif(not ref.available("fix"), reason="compiled reference not built (make -C oracle ref)")
