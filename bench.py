@@ -201,7 +201,8 @@ def fit_cpu_baseline(sizes, sample: int = 4) -> dict:
         for k in range(2 * fit.NPARAM + 1):
             th = th0.copy()
             if k:
-                th[(k - 1) // 2] *= 1.0 + (1e-5 if k % 2 else -1e-5)
+                p = (k - 1) // 2
+                th[p] += fit.fd_step(th0, p) * (1.0 if k % 2 else -1.0)
             ref.run(fit.with_theta(s, th), "engforce", variant="tim", threads=threads, timeout=600)
     wall = time.perf_counter() - t0
     return {"value": len(idx) / wall, "unit": "config-gradients/s", "cores": threads, "kind": "reference",

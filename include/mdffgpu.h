@@ -256,12 +256,15 @@ int mdffgpu_fma_peak(int device, int precision, double *tflops);
  * vector of the polarisable silica model, types tSi and tO of the context:
  *   theta = { A, B, C (Si-O), A, B, C (O-O), q_Si (q_O = -q_Si/2), alpha_O (isotropic,
  *             A^3), b, c (Tang-Toennies damping of every declared charge-dipole
- *             damping) }
- * mdffgpu_fit_set_params writes theta into the context's tables.  mdffgpu_force_match
- * evaluates the forces F at the converged induced dipoles (a CG solver must be set),
- * res[0] = sum_i |F_i - F_t,i|^2 and res[1..10] = dL/dtheta of L = scale/2 res[0],
- * from one adjoint induced-dipole solve (FP64 adjoint arithmetic). */
-#define MDFFGPU_FIT_NPARAM 10
+ *             damping), D (Si-O), D (O-O) (the C8 dispersion, -D/r^8) }
+ * of the Born-Mayer-Huggins form without dispersion damping (lbhmft,
+ * src/bhmftd.c:177-199 with f6 = f8 = 1: the damping BD of the lbhmftd variant is not a
+ * parameter of this model).  mdffgpu_fit_set_params writes theta into the context's
+ * tables.  mdffgpu_force_match evaluates the forces F at the converged induced dipoles
+ * (a CG solver must be set), res[0] = sum_i |F_i - F_t,i|^2 and
+ * res[1..MDFFGPU_FIT_NPARAM] = dL/dtheta of L = scale/2 res[0], from one adjoint
+ * induced-dipole solve (FP64 adjoint arithmetic). */
+#define MDFFGPU_FIT_NPARAM 12
 int mdffgpu_fit_set_params(mdffgpu_ctx *ctx, int tSi, int tO, const double *theta);
 int mdffgpu_force_match(mdffgpu_ctx *ctx, int tSi, int tO, const double *fx_t, const double *fy_t,
                         const double *fz_t, double scale, double *res);
@@ -279,7 +282,8 @@ int mdffgpu_fit_batch(mdffgpu_ctx **ctx, int nconf, int tSi, int tO, const doubl
  * together) and one copy of the nconf results.  create: ctx[nconf] contexts on one
  * device with a CG solver set, targets[c] the AoS target forces of context c (copied to
  * the device once), scale as for mdffgpu_force_match.  eval: theta as above; res[0] =
- * sum over configurations of sum_i |F_i - F_t,i|^2, res[1..10] = the summed gradient,
+ * sum over configurations of sum_i |F_i - F_t,i|^2, res[1..MDFFGPU_FIT_NPARAM] = the
+ * summed gradient,
  * summed in configuration order; the first eval (and the first after a context's
  * precision or solver changed) records the graphs.  The contexts must not be used by
  * other calls while an eval runs; after evals each context's tables hold the last

@@ -156,6 +156,19 @@ struct KahanF {
     __device__ __forceinline__ double value() const { return (double)s + (double)c; }
 };
 
+// complex product in FP32
+__device__ __forceinline__ float2 cmul32(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// exp(2 pi i x) for an FP64 argument: exact reduction to [-1/2, 1/2], FP32 sincospi
+__device__ __forceinline__ float2 cis2pi32(double x) {
+    x -= rint(x);
+    float sn, cs;
+    sincospif((float)(2.0 * x), &sn, &cs);
+    return make_float2(cs, sn);
+}
+
 inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
 
 }  // namespace mdffgpu

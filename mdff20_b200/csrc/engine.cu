@@ -205,6 +205,9 @@ Engine::~Engine() {
     cudaFree(d_ion_part32);
     cudaFree(d_pidx);
     cudaFree(d_qm_tc);
+    cudaFree(d_ion_order);
+    cudaFree(d_ion_atab);
+    cudaFree(d_ion_wtab);
     cudaFree(d_ion_part);
     cudaFree(d_coef);
     dfree32();
@@ -330,6 +333,13 @@ void Engine::setup_types() {
     for (int i = 0; i < n; i++)
         if (polar[i]) pidx.push_back(i);
     npol = (int)pidx.size();
+    {   // all ions, polarisable ones first (the tensor-core ion pass's positions)
+        std::vector<int> order(pidx);
+        for (int i = 0; i < n; i++)
+            if (!polar[i]) order.push_back(i);
+        d_ion_order = dalloc<int>(n);
+        MDFF_CK(cudaMemcpy(d_ion_order, order.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    }
     if (npol) {
         d_pidx = dalloc<int>(npol);
         MDFF_CK(cudaMemcpy(d_pidx, pidx.data(), sizeof(int) * npol, cudaMemcpyHostToDevice));

@@ -152,6 +152,14 @@ void launch_coords32(Engine &e);
 void setup_kspace32(Engine &e, const std::vector<KRow> &rows);
 void launch_phase32(Engine &e);
 void launch_rho32(Engine &e, const double *q, const double3 *mu, bool lq, bool ld, const int *idx, int cnt);
+void launch_combine32(Engine &e, const double *q, const double3 *mu, bool ld, const RecOut &o, const int *idx,
+                      int cnt, int slices, bool wf);
+// kspace_ion_tc.cu: the ion pass on the tensor cores (false: not applicable, nothing
+// launched); launch_ion_tc_table writes its per-ion operand of the current positions
+bool launch_ion_tc(Engine &e, const double *q, const double3 *mu, bool ld, const RecOut &o, const int *idx,
+                   int cnt);
+void launch_ion_tc_table(Engine &e);
+void setup_ion_tc(Engine &e);
 // kspace_tc.cu: the same rho chunk partials from tcgen05 TF32 MMAs (false: k box out of range)
 bool launch_rho_tc(Engine &e, const double *q, const double3 *mu, bool lq, bool ld, const int *idx, int cnt,
                    int tab_w, int z_off, int nzb_neg, int *chunks_used);
@@ -245,6 +253,11 @@ struct Engine {
     int rho32_chunks = 0;
     int rho_chunks_used = 0;                            // chunk partials the last rho pass wrote
     bool rho_tc = false;                                // rho pass on the tensor cores (kspace_tc.cu)
+    // ion pass on the tensor cores (kspace_ion_tc.cu): positions in the order polarisable
+    // ions first, the per-ion operand tiles of the current positions, per-pass weights
+    bool ion_tc = false;
+    int *d_ion_order = nullptr;
+    float4 *d_ion_atab = nullptr, *d_ion_wtab = nullptr;
     // CG initial guess: polynomial extrapolation through the last extrapolate_order + 1
     // converged dipoles (false: the reference's ASPC coefficients)
     bool cg_poly = true;

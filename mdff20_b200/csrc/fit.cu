@@ -29,15 +29,13 @@ constexpr int FIT_WARPS = 8;
 // partial-sum slots of the fit (e.d_fpart / e.d_fscal)
 enum FitSlot : int {
     F_LOSS = 0,
-    F_BHM = 1,          // 6: A B C (Si-O), A B C (O-O)
-    F_DAMP = 7,         // 4: w.dF/db, w.dF/dc, lambda.dE/db, lambda.dE/dc
-    F_WFALL = 11, F_WFQ0 = 12, F_WF0M = 13,   // w.F_coul(q,mu), w.F_coul(q,0), w.F_coul(0,mu)
-    F_LESTAT = 14,      // lambda . E(q, 0)
-    F_LMU = 15,         // lambda . mu_ind on the polarisable ions
-    F_SS = 16, F_RR = 17,   // s.s, r.r (adjoint CG)
-    F_RZ = 18, F_PAP = 19, F_RZOLD = 20,
-    F_ADJ_RR0 = 21, F_ADJ_IT = 22,   // adjoint CG: initial r.r and iteration count (recorded loop)
-    NFSLOT = 24
+    F_BHM = 1,          // 8: A B C (Si-O), A B C (O-O), D (Si-O), D (O-O)
+    F_DAMP = 9,         // 4: w.dF/db, w.dF/dc, lambda.dE/db, lambda.dE/dc
+    F_WFALL = 13, F_WFQ0 = 14, F_WF0M = 15,   // w.F_coul(q,mu), w.F_coul(q,0), w.F_coul(0,mu)
+    F_LESTAT = 16,      // lambda . E(q, 0)
+    F_LMU = 17,         // lambda . mu_ind on the polarisable ions
+    F_ADJ_RR0 = 18, F_ADJ_IT = 19,   // adjoint CG: initial r.r and iteration count (recorded loop)
+    NFSLOT = 20
 };
 constexpr int NRES = FIT_NRES;
 
@@ -317,7 +315,7 @@ __global__ void __launch_bounds__(FIT_WARPS * 32) k_bhm_sens(int n, Cell c, cons
                                                              double *part, int stride) {
     int i = blockIdx.x * FIT_WARPS + (threadIdx.x >> 5);
     int lane = threadIdx.x & 31;
-    double acc[6] = {0, 0, 0, 0, 0, 0};
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // A B C (Si-O), A B C (O-O), D (Si-O), D (O-O)
     if (i < n) {
         double4 si = s[i];
         double3 wi = w[i];
@@ -345,9 +343,10 @@ __global__ void __launch_bounds__(FIT_WARPS * 32) k_bhm_sens(int n, Cell c, cons
             acc[slot + 0] += h * P.B * ex;
             acc[slot + 1] += h * P.A * ex * (1.0 - P.B * d);
             acc[slot + 2] += h * (-6.0 / (d8 / d));   // d/dC of -6 C / d^7 (h holds the 1/d)
+            acc[6 + slot / 3] += h * (-8.0 / (d8 * d));   // d/dD of -8 D / d^9
         }
     }
-    fit_block_sum<6>(acc, part, F_BHM, stride);
+    fit_block_sum<8>(acc, part, F_BHM, stride);
 }
 
 // ------------------------------------------------------------------ engine side
@@ -364,10 +363,12 @@ __global__ void k_fit_tables(const double *__restrict__ th, int tSi, int tO, int
         P.A = th[0];
         P.B = th[1];
         P.C = th[2];
+        P.D = th[10];
     } else if (x == tO && y == tO) {
         P.A = th[3];
         P.B = th[4];
         P.C = th[5];
+        P.D = th[11];
     }
     PairDamp &D = damp[e];
     if (D.pad & 1) {
@@ -415,6 +416,8 @@ __global__ void k_fm_result(const double *__restrict__ sc, const double *__restr
     res[8] = sc[F_LMU] / (th[7] * th[7]);
     res[9] = coul * sc[F_DAMP + 0] + sc[F_DAMP + 2];
     res[10] = coul * sc[F_DAMP + 1] + sc[F_DAMP + 3];
+    res[11] = sc[F_BHM + 6];
+    res[12] = sc[F_BHM + 7];
     res[NRES - 1] = (double)*status;
 }
 
@@ -453,10 +456,12 @@ void Engine::fit_host_params(int tSi, int tO, const double *th) {
             p.Abhmftd[x][y] = th[3 * pair + 0];
             p.Bbhmftd[x][y] = th[3 * pair + 1];
             p.Cbhmftd[x][y] = th[3 * pair + 2];
+            p.Dbhmftd[x][y] = th[10 + pair];
             PairSR &P = h_pair[(size_t)x * nt + y];
             P.A = th[3 * pair + 0];
             P.B = th[3 * pair + 1];
             P.C = th[3 * pair + 2];
+            P.D = th[10 + pair];
         }
     }
     // charges: q_Si = theta, q_O = -theta / 2
@@ -678,7 +683,7 @@ void Engine::fit_issue(const double3 *d_ft, double scale, int tSi, int tO, const
     // parameter sensitivities
     MDFF_LAUNCH(*this, k_bhm_sens, nbw, FIT_WARPS * 32, 0, n, cell, d_s, d_typ, d_pair, nt, d_nb, d_nbn, cap_nb,
                 srcutsq, tSi, tO, d_w, d_fpart, part_stride);
-    fit_reduce(F_BHM, 6, nbw);
+    fit_reduce(F_BHM, 8, nbw);
     MDFF_LAUNCH(*this, k_damp_sens, nbw, FIT_WARPS * 32, 0, a);
     fit_reduce(F_DAMP, 4, nbw);
     coul_forces(q, d_mu_tot, true, true, d_fa);      // F(q, mu)
@@ -700,7 +705,8 @@ void Engine::force_match(const double3 *d_ft, double scale, double *h_res, int t
     // here the q_Si and alpha_O the result assembly divides by)
     double th[MDFFGPU_FIT_NPARAM] = {p.Abhmftd[tSi][tO], p.Bbhmftd[tSi][tO], p.Cbhmftd[tSi][tO],
                                      p.Abhmftd[tO][tO],  p.Bbhmftd[tO][tO],  p.Cbhmftd[tO][tO],
-                                     p.qit[tSi],         p.polit[tO][0][0],  0.0, 0.0};
+                                     p.qit[tSi],         p.polit[tO][0][0],  0.0, 0.0,
+                                     p.Dbhmftd[tSi][tO], p.Dbhmftd[tO][tO]};
     MDFF_CK(cudaMemcpyAsync(d_theta, th, sizeof(double) * 8, cudaMemcpyHostToDevice, stream));
     MDFF_CK(cudaMemsetAsync(d_status, 0, sizeof(unsigned), stream));
     fit_issue(d_ft, scale, tSi, tO, d_theta, d_fres);

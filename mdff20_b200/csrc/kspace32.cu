@@ -45,10 +45,6 @@ constexpr int ION32_MIN_BLOCKS = 5;
 constexpr int ION32X2_MIN_BLOCKS = 4;   // field-only ion pass, two ions per thread
 constexpr int ION32_RUN = 4;        // rows per exact row phase in the ion pass
 
-__device__ __forceinline__ float2 cmul32(float2 a, float2 b) {
-    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-
 // asynchronous global -> shared copy of 16 bytes (both addresses 16-byte aligned)
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
     unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -58,14 +54,6 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
-
-// exp(2 pi i x) for an FP64 argument: exact reduction to [-1/2, 1/2], FP32 sincospi
-__device__ __forceinline__ float2 cis2pi32(double x) {
-    x -= rint(x);
-    float sn, cs;
-    sincospif((float)(2.0 * x), &sn, &cs);
-    return make_float2(cs, sn);
 }
 
 // ---------------------------------------------------------------- phase tables
@@ -661,6 +649,7 @@ void setup_kspace32(Engine &e, const std::vector<KRow> &rows) {
     int maxrows = std::max(1, (48 * 1024) / ion32_row_bytes(kz_of(L.K2), true));
     e.ion32_slices = std::max(std::min(32, e.nrow), ceil_div(e.nrow, maxrows));
     e.d_ion_part32 = dalloc<double>((size_t)e.ion32_slices * e.n * 6);
+    setup_ion_tc(e);
 }
 
 // k-row slices of one ion pass over `cnt` ions: about two full waves of resident blocks,
@@ -689,6 +678,7 @@ void launch_phase32(Engine &e) {
 
 void launch_coords32(Engine &e) {
     if (e.d_tab32) launch_phase32(e);
+    if (e.ion_tc) launch_ion_tc_table(e);
 }
 
 // FLOPs per (ion, k-vector) of the paired-nz formulation: 4 FMA with dipoles, 2 without
@@ -746,6 +736,7 @@ static void ion32_dispatch(Engine &e, dim3 g, size_t smem, const Ion32Args &a, b
 // field (and force) terms of Ak rho(k) (e.d_rho) at `cnt` ions, then slice sums + self/direct terms
 void launch_ion32(Engine &e, const double *q, const double3 *mu, bool ld, const RecOut &o, const int *idx, int cnt) {
     bool wf = o.f != nullptr;
+    if (e.ion_tc && launch_ion_tc(e, q, mu, ld, o, idx, cnt)) return;   // tensor-core pass
     int rows = 1, slices = 1;
     ion32_slicing(e, cnt, wf, rows, slices);
     Ion32Args a;
@@ -771,6 +762,13 @@ void launch_ion32(Engine &e, const double *q, const double3 *mu, bool ld, const 
     else if (KZ == 16) ion32_dispatch<16>(e, g, smem, a, wf);
     else ion32_dispatch<32>(e, g, smem, a, wf);
     e.prof_end("k_rec_ion", pi, ion32_flops_per_pair(wf) * (double)cnt * e.nk);
+    launch_combine32(e, q, mu, ld, o, idx, cnt, slices, wf);
+}
+
+// the slice partials of an ion pass (e.d_ion_part32, [slice][cnt][3 or 6]) summed per ion
+// and turned into field / force / self terms at ion idx[li] (li when idx is null)
+void launch_combine32(Engine &e, const double *q, const double3 *mu, bool ld, const RecOut &o, const int *idx,
+                      int cnt, int slices, bool wf) {
     Comb32Args b;
     b.cnt = cnt;
     b.nslice = slices;

@@ -1,0 +1,452 @@
+// The ion pass of the mixed-precision reciprocal sum on the 5th-generation tensor cores
+// (tcgen05, sm_100a): the field (and force) k-sums of kspace32.cu's k_ion32 as a TF32
+// matrix product with FP32 accumulation in tensor memory.
+//
+// Per row (nx, ny) of the k-set the ion pass needs, for every ion, the complex z-sums
+//     G = rho_0 + sum_z (a1 c_z + a2 d_z) + i (a3 c_z + a4 d_z)
+//     H = sum_z z (-a4 c_z + a3 d_z) + i z (a2 c_z - a1 d_z)
+//     K = sum_z z^2 (a1 c_z + a2 d_z) + i z^2 (a3 c_z + a4 d_z)        (forces only)
+// with E2[z] = (c_z, d_z) = exp(2 pi i z t_z) of the ion and a1..a4 the weights of
+// Ak rho(+z) and Ak rho(-z) folded over the sign of nz (kspace32.cu).  Their real and
+// imaginary parts are one real product
+//     D[ion][(row, comp)] = sum_k V[ion][k] W[(row, comp)][k],
+//     V = (c_1..c_K2, d_1..d_K2, 1, 0 ...)   (32 values per ion, fixed while the
+//                                             positions are: one table per force evaluation)
+//     W = the matching weights of Gx, Gy, Hx, Hy (Kx, Ky)   (per pass, from Ak rho)
+// Every value x is split as x = h + l, both TF32, and the product taken as
+// V_h W_h + V_h W_l + V_l W_h (K = 96), the dropped l l term 2^-22 of it.
+//
+// CTA = 128 ions (one tensor-memory lane each) and a slice of rows; 6 warps.  Warp 4
+// copies the ions' operand tile once and the weight chunks of IT_RPC rows into two
+// shared-memory buffers (bulk copies completing on mbarriers), warp 5 issues the 12 MMAs
+// (M = 128, N = IT_RPC x components, K = 8) of each chunk into one of two accumulators
+// in tensor memory and commits them, warps 0-3 read an accumulator back (tcgen05.ld)
+// while the next chunk's MMAs run and finish the rows exactly as the CUDA-core pass:
+// the row phase w (an FP64-reduced argument every IT_RUN rows, FP32 steps in ny between),
+// Im conj(w) G and Im conj(w) H (and the Re parts with the ion's dipole for forces), FP64
+// sums over the rows.  The slice sums go to the same partial buffer as k_ion32's, summed
+// per ion by k_combine32.
+//
+// Every mbarrier wait is bounded: on expiry the kernel sets ST_TC_TIMEOUT, stops issuing,
+// waits (bounded) for the copies and MMAs it has in flight, frees its tensor memory and
+// returns; the host turns the flag into MDFFGPU_ERR_TIMEOUT.
+#include <mutex>
+
+#include "engine.cuh"
+#include "tc_common.cuh"
+
+namespace mdffgpu {
+
+constexpr int IT_M = 128;          // ions per tile: MMA M, one tensor-memory lane each
+constexpr int IT_KV = 32;          // operand values per ion: c_1..c_K2, d_1..d_K2, 1, zeros
+constexpr int IT_K = 3 * IT_KV;    // K of one chunk's product: (h, h, l) x (h, l, h)
+constexpr int IT_RPC = 32;         // k-rows per weight chunk
+constexpr int IT_THREADS = 192;    // warps 0-3 rows (lane = ion), 4 copies, 5 MMAs
+constexpr int IT_RUN = 4;          // rows per exact row phase, as in the CUDA-core pass
+constexpr int IT_MAXK2 = (IT_KV - 1) / 2;            // nz up to 15
+constexpr uint32_t IT_A_LBO = (IT_M / 8) * 128;      // 16-byte K chunk stride of the ion tile
+constexpr uint32_t IT_A_BYTES = (IT_K / 4) * IT_A_LBO;   // 48 KB
+constexpr uint32_t IT_COPY = 16384;                  // bytes per bulk copy
+
+template <int NC>
+struct ItShape {
+    static constexpr int N = IT_RPC * NC;                        // MMA N: (row, component)
+    static constexpr uint32_t LBO = (N / 8) * 128;
+    static constexpr uint32_t BYTES = (IT_K / 4) * LBO;          // one weight chunk
+    static constexpr uint32_t TMEM_COLS = (2 * N <= 256) ? 256u : 512u;   // two accumulators
+    static constexpr size_t SMEM = IT_A_BYTES + 2 * (size_t)BYTES;
+};
+
+// ---------------------------------------------------------------- operands
+// per position j (ion order[j]): V of E2[z] = exp(2 pi i z t_z) from FP64-reduced
+// arguments, split into TF32 h + l, stored as the K-major no-swizzle operand tile of its
+// 128 positions with K = (h | h | l)
+__global__ void k_ion_tc_table(int n, int K2, Cell c, const double4 *__restrict__ r, const int *__restrict__ order,
+                               float4 *__restrict__ atab) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    double4 ri = r[order[j]];
+    double tz = c.B[0][2] * ri.x + c.B[1][2] * ri.y + c.B[2][2] * ri.z;
+    float h[IT_KV], l[IT_KV];
+#pragma unroll
+    for (int k = 0; k < IT_KV; k++) {
+        float v = 0.f;
+        if (k < 2 * K2) {
+            int z = k < K2 ? k + 1 : k - K2 + 1;
+            float2 e = cis2pi32((double)z * tz);
+            v = k < K2 ? e.x : e.y;
+        } else if (k == 2 * K2) {
+            v = 1.f;
+        }
+        split2(v, h[k], l[k]);
+    }
+    unsigned char *T = (unsigned char *)atab + (size_t)(j / IT_M) * IT_A_BYTES;
+    const int x = j % IT_M;
+#pragma unroll
+    for (int kg = 0; kg < IT_K / 4; kg++) {
+        const int t = kg / (IT_KV / 4), v0 = (kg % (IT_KV / 4)) * 4;
+        const float *s = t == 2 ? l : h;
+        *(float4 *)(T + kmaj(x, 4 * kg, IT_A_LBO)) = make_float4(s[v0], s[v0 + 1], s[v0 + 2], s[v0 + 3]);
+    }
+}
+
+// per pass: the weights of every (row, component) from Ak rho(k), as K-major chunks of
+// IT_RPC rows with K = (h | l | h); rows past nrow are zero.  Components: Gx, Gy, Hx,
+// Hy (and Kx, Ky): the coefficients of c_z, of d_z and of the constant 1 in the sums above
+template <int NC>
+__global__ void k_ion_tc_weights(int nrow, int nchunk, int K2, const KRow *__restrict__ row,
+                                 const double2 *__restrict__ rho, float4 *__restrict__ wtab) {
+    using S = ItShape<NC>;
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= nchunk * S::N) return;
+    const int ch = g / S::N, nn = g - ch * S::N;
+    const int rloc = nn / NC, comp = nn - rloc * NC, rr = ch * IT_RPC + rloc;
+    KRow R;
+    R.nx = R.ny = R.z0 = R.cnt = R.koff = 0;
+    const bool ok = rr < nrow;
+    if (ok) R = row[rr];
+    const int zlo = R.z0, zhi = R.z0 + R.cnt - 1;
+    auto rho_at = [&](int z) {
+        if (!ok || z < zlo || z > zhi) return make_double2(0.0, 0.0);
+        return rho[R.koff + z - zlo];
+    };
+    float h[IT_KV], l[IT_KV];
+#pragma unroll
+    for (int k = 0; k < IT_KV; k++) {
+        double v = 0.0;
+        if (k < 2 * K2) {
+            const bool cpart = k < K2;
+            const int z = cpart ? k + 1 : k - K2 + 1;
+            const double2 rp = rho_at(z), rn = rho_at(-z);
+            const double a1 = rp.x + rn.x, a2 = rp.y - rn.y, a3 = rp.y + rn.y, a4 = rn.x - rp.x;
+            const double fz = (double)z;
+            switch (comp) {
+            case 0: v = cpart ? a1 : a2; break;
+            case 1: v = cpart ? a3 : a4; break;
+            case 2: v = cpart ? -fz * a4 : fz * a3; break;
+            case 3: v = cpart ? fz * a2 : -fz * a1; break;
+            case 4: v = fz * fz * (cpart ? a1 : a2); break;
+            default: v = fz * fz * (cpart ? a3 : a4); break;
+            }
+        } else if (k == 2 * K2 && comp < 2) {
+            const double2 r0 = rho_at(0);
+            v = comp == 0 ? r0.x : r0.y;
+        }
+        split2((float)v, h[k], l[k]);
+    }
+    unsigned char *T = (unsigned char *)wtab + (size_t)ch * S::BYTES;
+#pragma unroll
+    for (int kg = 0; kg < IT_K / 4; kg++) {
+        const int t = kg / (IT_KV / 4), v0 = (kg % (IT_KV / 4)) * 4;
+        const float *s = t == 1 ? l : h;
+        *(float4 *)(T + kmaj(nn, 4 * kg, S::LBO)) = make_float4(s[v0], s[v0 + 1], s[v0 + 2], s[v0 + 3]);
+    }
+}
+
+// ---------------------------------------------------------------- the pass
+struct IonTcArgs {
+    int cnt;                 // positions 0..cnt-1 of order
+    int nrow, rows_per_slice;   // rows_per_slice: a multiple of IT_RPC
+    int ld;
+    const int *order;
+    Cell c;
+    const double4 *r;
+    const double3 *mu;
+    const KRow *row;
+    const float4 *atab, *wtab;
+    double *part;            // [slice][cnt][3 or 6], as k_ion32
+    unsigned *status;
+};
+
+template <int NC>
+__global__ void __launch_bounds__(IT_THREADS, 1) k_ion_tc(IonTcArgs a) {
+    using S = ItShape<NC>;
+    constexpr bool WF = NC == 6;
+    extern __shared__ __align__(1024) unsigned char sm[];
+    unsigned char *sA = sm;                                   // the ion tile
+    unsigned char *sB = sm + IT_A_BYTES;                      // [2] weight chunks
+    int2 *rnxy = (int2 *)(sB + 2 * S::BYTES);                 // (nx, ny) of the slice's rows
+    uint64_t *bar = (uint64_t *)(rnxy + a.rows_per_slice);
+    // bar: 0 tile landed, 1-2 chunk landed, 3-4 chunk consumed, 5-6 accumulator ready,
+    // 7-8 accumulator read
+    volatile int *abort_flag = (volatile int *)(bar + 9);
+    uint32_t *tmem_slot = (uint32_t *)(bar + 10);
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int sl = blockIdx.y;
+    const int r0 = sl * a.rows_per_slice, nrs = max(0, min(a.nrow, r0 + a.rows_per_slice) - r0);
+    const int nch = (nrs + IT_RPC - 1) / IT_RPC, ch0 = r0 / IT_RPC;
+
+    for (int e = tid; e < nrs; e += IT_THREADS) {
+        KRow R = a.row[r0 + e];
+        rnxy[e] = make_int2(R.nx, R.ny);
+    }
+    if (tid == 0) {
+        mbar_init(smem_u32(&bar[0]), 1);
+        for (int b = 0; b < 2; b++) {
+            mbar_init(smem_u32(&bar[1 + b]), 1);
+            mbar_init(smem_u32(&bar[3 + b]), 1);
+            mbar_init(smem_u32(&bar[5 + b]), 1);
+            mbar_init(smem_u32(&bar[7 + b]), 4);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        *abort_flag = 0;
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(S::TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    auto fail = [&]() {
+        if (!*abort_flag) atomicOr(a.status, (unsigned)ST_TC_TIMEOUT);
+        *abort_flag = 1;
+    };
+
+    if (warp == 4) {
+        // ------------------------------------------------ copies
+        if (lane == 0) {
+            const uint32_t ba = smem_u32(&bar[0]);
+            mbar_expect_tx(ba, IT_A_BYTES);
+            const unsigned char *gA = (const unsigned char *)a.atab + (size_t)blockIdx.x * IT_A_BYTES;
+            for (uint32_t o = 0; o < IT_A_BYTES; o += IT_COPY) bulk_g2s(smem_u32(sA) + o, gA + o, IT_COPY, ba);
+            int issued = 0;
+            for (int c = 0; c < nch && !*abort_flag; c++) {
+                const int b = c & 1;
+                if (c >= 2 && !mbar_wait(smem_u32(&bar[3 + b]), ((c >> 1) - 1) & 1)) {
+                    fail();
+                    break;
+                }
+                const uint32_t bf = smem_u32(&bar[1 + b]);
+                mbar_expect_tx(bf, S::BYTES);
+                const unsigned char *gB = (const unsigned char *)a.wtab + (size_t)(ch0 + c) * S::BYTES;
+                for (uint32_t o = 0; o < S::BYTES; o += IT_COPY) {
+                    const uint32_t sz = S::BYTES - o < IT_COPY ? S::BYTES - o : IT_COPY;
+                    bulk_g2s(smem_u32(sB + b * S::BYTES) + o, gB + o, sz, bf);
+                }
+                issued = c + 1;
+            }
+            // nothing may land after the CTA is gone: wait (bounded) for what is in flight
+            mbar_wait(ba, 0);
+            for (int c = max(0, issued - 2); c < issued; c++) mbar_wait(smem_u32(&bar[1 + (c & 1)]), (c >> 1) & 1);
+        }
+    } else if (warp == 5) {
+        // ------------------------------------------------ MMAs
+        if (lane == 0) {
+            const uint32_t idesc = idesc_tf32(IT_M, S::N);
+            int last = -1;
+            if (!mbar_wait(smem_u32(&bar[0]), 0)) fail();
+            for (int c = 0; c < nch && !*abort_flag; c++) {
+                const int b = c & 1;
+                if (!mbar_wait(smem_u32(&bar[1 + b]), (c >> 1) & 1)) {
+                    fail();
+                    break;
+                }
+                if (c >= 2 && !mbar_wait(smem_u32(&bar[7 + b]), ((c >> 1) - 1) & 1)) {
+                    fail();
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t ab = smem_u32(sA), bb = smem_u32(sB + b * S::BYTES);
+                const uint32_t d = tmem + (uint32_t)(b * S::N);
+#pragma unroll
+                for (int q = 0; q < IT_K / 8; q++) {
+                    const uint64_t da = smem_desc(ab + 2 * q * IT_A_LBO, IT_A_LBO, 128);
+                    const uint64_t db = smem_desc(bb + 2 * q * S::LBO, S::LBO, 128);
+                    mma_tf32(d, da, db, idesc, q > 0 ? 1u : 0u);
+                }
+                mma_commit(smem_u32(&bar[3 + b]));   // the weight buffer is free again
+                mma_commit(smem_u32(&bar[5 + b]));   // the accumulator is ready
+                last = c;
+            }
+            // every MMA issued must finish before the tensor memory is freed
+            if (last >= 0) mbar_wait(smem_u32(&bar[5 + (last & 1)]), (last >> 1) & 1);
+        }
+    } else {
+        // ------------------------------------------------ rows (lane = ion of the tile)
+        const int pos = blockIdx.x * IT_M + tid;
+        const bool act = pos < a.cnt;
+        const int ion = act ? a.order[pos] : 0;
+        const Cell &c = a.c;
+        double tx = 0.0, ty = 0.0, mx = 0.0, my = 0.0;
+        float mz = 0.f;
+        if (act) {
+            const double4 ri = a.r[ion];
+            tx = c.B[0][0] * ri.x + c.B[1][0] * ri.y + c.B[2][0] * ri.z;
+            ty = c.B[0][1] * ri.x + c.B[1][1] * ri.y + c.B[2][1] * ri.z;
+            if (WF && a.ld) {
+                const double3 m3 = a.mu[ion];
+                mx = c.B[0][0] * m3.x + c.B[1][0] * m3.y + c.B[2][0] * m3.z;
+                my = c.B[0][1] * m3.x + c.B[1][1] * m3.y + c.B[2][1] * m3.z;
+                mz = (float)(c.B[0][2] * m3.x + c.B[1][2] * m3.y + c.B[2][2] * m3.z);
+            }
+        }
+        const float2 e1 = cis2pi32(ty);
+        float2 w = make_float2(1.f, 0.f);
+        int2 Rp = make_int2(0, 0);
+        int run = IT_RUN;
+        double S0 = 0, S1 = 0, S2 = 0, P0 = 0, P1 = 0, P2 = 0;
+        const uint32_t lanebase = tmem + ((uint32_t)(warp * 32) << 16);
+        bool ok = true;
+        for (int ch = 0; ch < nch; ch++) {
+            const int b = ch & 1;
+            int got = 1;
+            if (lane == 0) got = (!*abort_flag && mbar_wait(smem_u32(&bar[5 + b]), (ch >> 1) & 1)) ? 1 : 0;
+            got = __shfl_sync(0xffffffffu, got, 0);
+            if (!got) {
+                if (lane == 0) fail();
+                ok = false;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll 1
+            for (int j0 = 0; j0 < IT_RPC; j0 += 8) {
+                float v[8 * NC];
+#pragma unroll
+                for (int q = 0; q < NC; q++) tmem_ld8(lanebase + (uint32_t)(b * S::N + j0 * NC + 8 * q), v + 8 * q);
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    const int rr = ch * IT_RPC + j0 + j;
+                    if (rr >= nrs) break;
+                    const int2 R = rnxy[rr];
+                    if (run < IT_RUN && R.x == Rp.x && R.y == Rp.y + 1) {
+                        w = cmul32(w, e1);
+                        run++;
+                    } else {
+                        w = cis2pi32((double)R.x * tx + (double)R.y * ty);
+                        run = 1;
+                    }
+                    Rp = R;
+                    const float *g = v + j * NC;
+                    const float Gx = g[0], Gy = g[1], Hx = g[2], Hy = g[3];
+                    // Im conj(w) G and Im conj(w) H
+                    const float R1 = w.x * Gy - w.y * Gx, Rz = w.x * Hy - w.y * Hx;
+                    const double fx = (double)R.x, fy = (double)R.y;
+                    S0 += fx * (double)R1;
+                    S1 += fy * (double)R1;
+                    S2 += (double)Rz;
+                    if (WF) {
+                        const float Kx = g[4], Ky = g[5];
+                        // Re conj(w) G, H, K with the ion's dipole, c0 = nx mx + ny my
+                        const float Q0 = w.x * Gx + w.y * Gy, Q1 = w.x * Hx + w.y * Hy, Q2 = w.x * Kx + w.y * Ky;
+                        const double c0 = fx * mx + fy * my;
+                        const double T1 = c0 * (double)Q0 + (double)mz * (double)Q1;
+                        const double Tz = c0 * (double)Q1 + (double)mz * (double)Q2;
+                        P0 += fx * T1;
+                        P1 += fy * T1;
+                        P2 += Tz;
+                    }
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&bar[7 + b]));
+        }
+        if (ok && act) {
+            const int nv = WF ? 6 : 3;
+            double *o = a.part + ((size_t)sl * a.cnt + pos) * nv;
+            o[0] = S0;
+            o[1] = S1;
+            o[2] = S2;
+            if (WF) {
+                o[3] = P0;
+                o[4] = P1;
+                o[5] = P2;
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(S::TMEM_COLS) : "memory");
+    }
+}
+
+// ---------------------------------------------------------------- host side
+static int ion_tc_tiles(int n) { return ceil_div(n, IT_M); }
+
+// buffers of the pass (at set-up: nothing may be allocated while steps are recorded)
+void setup_ion_tc(Engine &e) {
+    if (e.d_ion_atab || e.kmax[2] > IT_MAXK2) return;
+    e.d_ion_atab = dalloc<float4>((size_t)ion_tc_tiles(e.n) * (IT_A_BYTES / 16));
+    e.d_ion_wtab = dalloc<float4>((size_t)ceil_div(e.nrow, IT_RPC) * (ItShape<6>::BYTES / 16));
+}
+
+void launch_ion_tc_table(Engine &e) {
+    if (!e.d_ion_atab) return;
+    MDFF_LAUNCH(e, k_ion_tc_table, ceil_div(e.n, 128), 128, 0, e.n, e.kmax[2], e.cell, e.d_r, e.d_ion_order,
+                e.d_ion_atab);
+}
+
+// slices of the rows over the CTAs (one per SM): the fewest waves of (tiles x slices),
+// counting a fixed set-up per CTA against the chunks it runs
+static int ion_tc_slices(const Engine &e, int tiles, int nchunk, bool wf) {
+    const double setup = 3.0, per_chunk = wf ? 1.4 : 1.0;   // relative costs
+    int best = 1;
+    double best_t = 1e300;
+    for (int s = 1; s <= std::min(std::min(8, nchunk), e.ion32_slices); s++) {
+        int waves = ceil_div((long long)tiles * s, e.nsm);
+        double t = waves * (setup + per_chunk * ceil_div(nchunk, s));
+        if (t < best_t - 1e-9) {
+            best_t = t;
+            best = s;
+        }
+    }
+    return best;
+}
+
+template <int NC>
+static void ion_tc_run(Engine &e, const IonTcArgs &a, int tiles, int slices, int nchunk) {
+    using S = ItShape<NC>;
+    MDFF_LAUNCH(e, k_ion_tc_weights<NC>, ceil_div(nchunk * S::N, 128), 128, 0, e.nrow, nchunk, e.kmax[2], e.d_row,
+                e.d_rho, e.d_ion_wtab);
+    size_t smem = S::SMEM + sizeof(int2) * a.rows_per_slice + 16 * sizeof(uint64_t);
+    // the largest request once per process (the attribute call is not recorded in graphs)
+    static std::once_flag once;
+    std::call_once(once, [] {
+        MDFF_CK(cudaFuncSetAttribute(k_ion_tc<NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    });
+    MDFF_LAUNCH(e, k_ion_tc<NC>, dim3(tiles, slices), IT_THREADS, smem, a);
+}
+
+bool launch_ion_tc(Engine &e, const double *q, const double3 *mu, bool ld, const RecOut &o, const int *idx,
+                   int cnt) {
+    if (!e.d_ion_atab || cnt <= 0) return false;
+    // positions 0..cnt-1 of the order: every ion, or the polarisable ones
+    if (!(idx == nullptr && cnt == e.n) && !(idx == e.d_pidx && cnt == e.npol)) return false;
+    const bool wf = o.f != nullptr;
+    const int nchunk = ceil_div(e.nrow, IT_RPC), tiles = ion_tc_tiles(cnt);
+    int slices = ion_tc_slices(e, tiles, nchunk, wf);
+    IonTcArgs a;
+    a.cnt = cnt;
+    a.nrow = e.nrow;
+    a.rows_per_slice = ceil_div(nchunk, slices) * IT_RPC;
+    slices = ceil_div(e.nrow, a.rows_per_slice);
+    a.ld = ld;
+    a.order = e.d_ion_order;
+    a.c = e.cell;
+    a.r = e.d_r;
+    a.mu = mu;
+    a.row = e.d_row;
+    a.atab = e.d_ion_atab;
+    a.wtab = e.d_ion_wtab;
+    a.part = e.d_ion_part32;
+    a.status = e.d_status;
+    int pi = -1;
+    e.prof_begin("k_rec_ion", &pi);
+    if (wf) ion_tc_run<6>(e, a, tiles, slices, nchunk);
+    else ion_tc_run<4>(e, a, tiles, slices, nchunk);
+    // the same algorithmic count as the CUDA-core pass (8 / 12 flops per ion and k)
+    e.prof_end("k_rec_ion", pi, (wf ? 12.0 : 8.0) * (double)cnt * e.nk);
+    launch_combine32(e, q, mu, ld, o, idx ? idx : e.d_ion_order, cnt, slices, wf);
+    return true;
+}
+
+}  // namespace mdffgpu

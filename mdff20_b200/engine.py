@@ -168,7 +168,7 @@ EXPORTS = (
     "mdffgpu_rdf_create", "mdffgpu_rdf_destroy", "mdffgpu_rdf_last_error", "mdffgpu_rdf_reset", "mdffgpu_rdf_add",
     "mdffgpu_rdf_add_ctx", "mdffgpu_rdf_counts",
 )
-FIT_NPARAM = 10
+FIT_NPARAM = 12
 
 _lib = None
 

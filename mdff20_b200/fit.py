@@ -4,7 +4,8 @@ The workload of the fit tools of the reference (bin/ drives the mdff20 executabl
 perturbed inputs and compares forces): many independent configurations, one force-
 matching loss and its gradient with respect to the force-field parameters
 
-    theta = (A, B, C of Si-O, A, B, C of O-O, q_Si (q_O = -q_Si/2), alpha_O, b, c)
+    theta = (A, B, C of Si-O, A, B, C of O-O, q_Si (q_O = -q_Si/2), alpha_O, b, c,
+             D of Si-O, D of O-O)
 
 with L(theta) = sum_c sum_i |F_i(theta) - F_i^target|^2 / (3 N_total).  The forces come
 from the CUDA engine at the converged induced dipoles; the gradient from one adjoint
@@ -30,7 +31,7 @@ import numpy as np
 from . import synth
 from .system import System
 
-PARAM_NAMES = ("A_SiO", "B_SiO", "C_SiO", "A_OO", "B_OO", "C_OO", "q_Si", "alpha_O", "b", "c")
+PARAM_NAMES = ("A_SiO", "B_SiO", "C_SiO", "A_OO", "B_OO", "C_OO", "q_Si", "alpha_O", "b", "c", "D_SiO", "D_OO")
 NPARAM = len(PARAM_NAMES)
 O_TYPE, SI_TYPE = synth.O, synth.SI
 NUMBER_DENSITY = 0.066151   # silica ions per A^3 at 2.2 g/cm^3
@@ -45,7 +46,8 @@ def theta_of(s: System) -> np.ndarray:
     c = damp[0][4] if damp else 0.0
     return np.array([s.Abhmftd[si, o], s.Bbhmftd[si, o], s.Cbhmftd[si, o],
                      s.Abhmftd[o, o], s.Bbhmftd[o, o], s.Cbhmftd[o, o],
-                     s.qit[si], s.polit[o][0, 0], b, c], float)
+                     s.qit[si], s.polit[o][0, 0], b, c,
+                     s.Dbhmftd[si, o], s.Dbhmftd[o, o]], float)
 
 
 def with_theta(s: System, theta) -> System:
@@ -56,6 +58,9 @@ def with_theta(s: System, theta) -> System:
     for arr, k in ((s2.Abhmftd, 0), (s2.Bbhmftd, 1), (s2.Cbhmftd, 2)):
         arr[si, o] = arr[o, si] = t[k]
         arr[o, o] = t[3 + k]
+    s2.Dbhmftd = np.array(s2.Dbhmftd, float)
+    s2.Dbhmftd[si, o] = s2.Dbhmftd[o, si] = t[10]
+    s2.Dbhmftd[o, o] = t[11]
     s2.qit = list(s2.qit)
     s2.qit[si] = t[6]
     s2.qit[o] = -0.5 * t[6]
@@ -63,6 +68,14 @@ def with_theta(s: System, theta) -> System:
     s2.polit[o] = np.eye(3) * t[7]
     s2.poldamp = [(d[0], d[1], d[2], t[8], t[9], d[5]) for d in s2.poldamp]
     return s2
+
+
+def fd_step(theta, k: int, rel: float = 1e-5) -> float:
+    """Central-difference step of parameter k: rel |theta_k|, or for a parameter at zero
+    (the C8 dispersion D of the Buckingham configurations) rel times a typical magnitude
+    (D ~ 1e3 eV A^8)."""
+    t = abs(float(theta[k]))
+    return rel * (t if t > 0.0 else 1e3)
 
 
 def perturbed_theta(theta0, seed: int = 5, frac: float = 0.05) -> np.ndarray:

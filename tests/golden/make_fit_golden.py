@@ -6,7 +6,8 @@ gradient from the compiled reference.
 One seeded 96-ion configuration of the batched fit (mdff20_b200.fit.config4 with the SCF
 converged to 1e-11): the reference's forces at the perturbed parameters are the
 targets, L(theta) = sum |F(theta) - F_t|^2 / (3 N) from the reference's forces, and the
-gradient is the central finite difference of that L (relative steps 1e-5), every force
+gradient is the central finite difference of that L (relative steps 1e-5; for the C8
+dispersion D, which is zero in this model, fit.fd_step's absolute step), every force
 an output of the reference mdff20 C code (OMP_NUM_THREADS=1).
 """
 from __future__ import annotations
@@ -44,7 +45,7 @@ def main():
     l0, r0 = loss(th0)
     grad = np.zeros(fit.NPARAM)
     for k in range(fit.NPARAM):
-        h = STEP * abs(th0[k])
+        h = fit.fd_step(th0, k, STEP)
         tp = th0.copy()
         tp[k] += h
         tm = th0.copy()
