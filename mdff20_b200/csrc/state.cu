@@ -90,6 +90,7 @@ void Engine::save_state(unsigned char *buf) {
     MDFF_LAUNCH(*this, k_pack3, nb, 256, 0, n, d_r, d_tmp);
     MDFF_LAUNCH(*this, k_pack3, nb, 256, 0, n, d_svl, d_tmp + n3);
     MDFF_CK(cudaMemcpyAsync(packed.data(), d_tmp, sizeof(double) * 2 * n3, cudaMemcpyDeviceToHost, stream));
+    scratch.p = nullptr;
     MDFF_CK(cudaFreeAsync(d_tmp, stream));
     std::vector<double> v(n3), f(n3), rs(n3), mu(n3), hist(18 * (size_t)n), nhc(32);
     MDFF_CK(cudaMemcpyAsync(v.data(), d_v, sizeof(double) * n3, cudaMemcpyDeviceToHost, stream));

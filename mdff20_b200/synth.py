@@ -235,10 +235,11 @@ def config3() -> System:
     return s
 
 
-def config5(structure: str = "cristobalite") -> System:
+def config5(structure: str = "cristobalite", cells: int = 10) -> System:
     """N = 24000 polarisable silica, NHC (chain 3) at 2500 K, 1 Å skin, SCF to 1e-6 with
     ASPC order 4.  MD starts from a 10^3 beta-cristobalite supercell at 2.20 g/cm^3
     (L = 71.3 Å) with 0.05 Å seeded displacements: a random packing of these ions falls
-    into the Buckingham short-range divergence within tens of steps."""
-    return silica(8000, seed=6, polarizable=True, kmax=14, temp=2500.0, npas=10000,
+    into the Buckingham short-range divergence within tens of steps.  `cells` < 10: the
+    same model on a cells^3 supercell (24 cells^3 ions), the small case of profiles."""
+    return silica(8 * cells ** 3, seed=6, polarizable=True, kmax=14, temp=2500.0, npas=10000,
                   conv_tol=1e-6, extrapolate_order=4, dmin=PIM_DMIN, structure=structure)

@@ -13,7 +13,9 @@ Tolerances, stated per quantity (relative measures of tests/helpers.py):
 |-------------------------------|--------------|--------------|----------|--------------|
 | FP64, same Jacobi iterations  | 1e-10 max    | 1e-10 max    | 1e-10    | 1e-10 tensor |
 | FP64 CG (stops elsewhere
-  inside the 1e-8 SCF tolerance) | 1e-8 max     | 1e-7 max     | 1e-9     | 1e-8 tensor  |
+  inside the 1e-8 SCF tolerance) | 1e-8 max     | 1e-7 max     | 1e-9 (u_pol,
+                                                                 first order in
+                                                                 the dipoles: 1e-7) | 1e-8 tensor  |
 | mixed, CG to 1e-6 (config 3's
   mixed tolerance)               | 1e-5 RMS     | 1e-5 RMS     | 1e-5     | 1e-5 tensor  |
 """
@@ -98,7 +100,7 @@ def test_config3_fp64_cg(solver):
     assert err["f_max"] < 1e-8, err
     assert err["mu_max"] < 1e-7, err
     for k in ENERGIES + VIRIALS:
-        assert err[k] < 1e-9, (k, err)
+        assert err[k] < (1e-7 if k == "u_pol" else 1e-9), (k, err)
     for k in STRESS:
         assert err[k] < 1e-8, (k, err)
 

