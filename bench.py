@@ -232,16 +232,21 @@ def run_fit(args, world, rank, dev, pg) -> Optional[dict]:
     tht = fit.perturbed_theta(th0)
     b = fit.ForceMatchBatch(systems, None, device=dev, precision=FP64, threads=args.fit_threads, ntot=sum(sizes))
     b.set_targets(b.forces(tht))   # FP64 forces at the perturbed parameters
+    # a fit moves theta every evaluation: a seeded sequence of distinct parameter vectors
+    # (1% Gaussian steps), so no evaluation starts from dipoles converged at its own theta
+    rng = np.random.default_rng(17)
+    # (both precisions run the same sequence, so their last results compare)
+    seq = [th0 * (1.0 + 0.01 * rng.standard_normal(len(th0))) for _ in range(args.fit_evals + 1)]
     res = {}
     for label, prec in (("fp64", FP64), ("mixed", MIXED)):
         b.set_precision(prec)
-        b.loss_grad(th0)                       # warm-up (first CG solves, allocations)
+        b.loss_grad(seq[0])                    # warm-up (recording, first CG solves)
         if pg is not None:
             pg.barrier()
         torch.cuda.synchronize()
         t = time.perf_counter()
-        for _ in range(args.fit_evals):
-            loss, grad = b.loss_grad(th0)      # synchronous: every configuration's stream done
+        for k in range(args.fit_evals):
+            loss, grad = b.loss_grad(seq[1 + k])   # synchronous: every configuration's stream done
             if pg is not None:
                 loss, grad = fit.allreduce_loss_grad(loss, grad)
         torch.cuda.synchronize()
@@ -261,7 +266,8 @@ def run_fit(args, world, rank, dev, pg) -> Optional[dict]:
            "loss_rel_err_mixed_vs_fp64": abs(res["mixed"]["loss"] - res["fp64"]["loss"]) / res["fp64"]["loss"],
            "params": list(fit.PARAM_NAMES), "host_threads": args.fit_threads, "setup_s": round(gen_s, 1),
            "timing": "host clock around the synchronous C-ABI evaluation (host parameters in, host loss and "
-                     "gradient out), device synchronised on both sides, max over ranks",
+                     "gradient out), device synchronised on both sides, max over ranks; each evaluation at a new "
+                     "theta (seeded 1% steps)",
            "path": "mdffgpu_fit_plan: each configuration's evaluation recorded once as a CUDA graph (device-side "
                    "CG loops, theta in a shared device buffer), all configurations replayed concurrently",
            "data": "synthetic: seeded random silica configurations, targets = FP64 forces at +-5% parameters"}

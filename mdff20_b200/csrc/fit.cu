@@ -670,15 +670,19 @@ void Engine::fit_issue(const double3 *d_ft, double scale, int tSi, int tO, const
         launch_rec(*this, q, d_mu_tot, true, true, o);
     }
     MDFF_LAUNCH(*this, k_adj_rhs, nb, 256, 0, n, d_polar, coul_unit, d_sv, d_fa, d_efg_rec, d_w, d_sv);
-    // adjoint solve A lambda = s (cached dipole-field factors valid for these positions)
+    // adjoint solve A lambda = s in the context's precision: FP64 (cached dipole-field
+    // factors of these positions) to a 1e-11 relative residual, or mixed (the FP32
+    // dipole-field records and phase tables of the force evaluation above) to 1e-6
     {
         struct CoefScope {
             bool &flag;
             ~CoefScope() { flag = false; }
         } scope{coef_ready};
-        launch_dir_prep(*this, p.alphaES);
+        use32 = fp64_scope.saved;
+        if (!(use32 && real32)) launch_dir_prep(*this, p.alphaES);
         coef_ready = true;
-        solve_pim(d_sv, d_lam, 1e-11, 500);
+        solve_pim(d_sv, d_lam, use32 ? 1e-6 : 1e-11, 500);
+        use32 = false;
     }
     // parameter sensitivities
     MDFF_LAUNCH(*this, k_bhm_sens, nbw, FIT_WARPS * 32, 0, n, cell, d_s, d_typ, d_pair, nt, d_nb, d_nbn, cap_nb,

@@ -16,16 +16,18 @@
 // Every value x is split as x = h + l, both TF32, and the product taken as
 // V_h W_h + V_h W_l + V_l W_h (K = 96), the dropped l l term 2^-22 of it.
 //
-// CTA = 128 ions (one tensor-memory lane each) and a slice of rows; 6 warps.  Warp 4
+// CTA = 128 ions (one tensor-memory lane each) and a slice of rows; 10 warps.  Warp 8
 // copies the ions' operand tile once and the weight chunks of IT_RPC rows into two
-// shared-memory buffers (bulk copies completing on mbarriers), warp 5 issues the 12 MMAs
+// shared-memory buffers (bulk copies completing on mbarriers), warp 9 issues the 12 MMAs
 // (M = 128, N = IT_RPC x components, K = 8) of each chunk into one of two accumulators
-// in tensor memory and commits them, warps 0-3 read an accumulator back (tcgen05.ld)
-// while the next chunk's MMAs run and finish the rows exactly as the CUDA-core pass:
-// the row phase w (an FP64-reduced argument every IT_RUN rows, FP32 steps in ny between),
-// Im conj(w) G and Im conj(w) H (and the Re parts with the ion's dipole for forces), FP64
-// sums over the rows.  The slice sums go to the same partial buffer as k_ion32's, summed
-// per ion by k_combine32.
+// in tensor memory and commits them, warps 0-7 read an accumulator back (tcgen05.ld;
+// warp w takes the lanes of quarter w % 4 and half w / 4 of the chunk's rows) while the
+// next chunk's MMAs run, and finish the rows as the CUDA-core pass does: the row phase w
+// (an FP64-reduced argument every IT_RUN rows, FP32 steps in ny between), Im conj(w) G and
+// Im conj(w) H (and the Re parts with the ion's dipole for forces), FP32 sums over a
+// warp's rows of a chunk, FP64 across chunks.  Each (slice, half) goes to the partial
+// buffer of k_ion32 as a slice of its own, summed per ion by k_combine32.  The field pass
+// (96 KB of shared memory) runs two CTAs per SM, 16 row warps per SM.
 //
 // Every mbarrier wait is bounded: on expiry the kernel sets ST_TC_TIMEOUT, stops issuing,
 // waits (bounded) for the copies and MMAs it has in flight, frees its tensor memory and
@@ -40,8 +42,10 @@ namespace mdffgpu {
 constexpr int IT_M = 128;          // ions per tile: MMA M, one tensor-memory lane each
 constexpr int IT_KV = 32;          // operand values per ion: c_1..c_K2, d_1..d_K2, 1, zeros
 constexpr int IT_K = 3 * IT_KV;    // K of one chunk's product: (h, h, l) x (h, l, h)
-constexpr int IT_RPC = 32;         // k-rows per weight chunk
-constexpr int IT_THREADS = 192;    // warps 0-3 rows (lane = ion), 4 copies, 5 MMAs
+constexpr int IT_RPC = 16;         // k-rows per weight chunk
+constexpr int IT_EPI = 8;          // row warps: lane quarter w % 4, half w / 4 of a chunk's rows
+constexpr int IT_HALF = IT_RPC / 2;
+constexpr int IT_THREADS = 32 * (IT_EPI + 2);   // + one copy warp, one MMA warp
 constexpr int IT_RUN = 4;          // rows per exact row phase, as in the CUDA-core pass
 constexpr int IT_MAXK2 = (IT_KV - 1) / 2;            // nz up to 15
 constexpr uint32_t IT_A_LBO = (IT_M / 8) * 128;      // 16-byte K chunk stride of the ion tile
@@ -53,8 +57,9 @@ struct ItShape {
     static constexpr int N = IT_RPC * NC;                        // MMA N: (row, component)
     static constexpr uint32_t LBO = (N / 8) * 128;
     static constexpr uint32_t BYTES = (IT_K / 4) * LBO;          // one weight chunk
-    static constexpr uint32_t TMEM_COLS = (2 * N <= 256) ? 256u : 512u;   // two accumulators
+    static constexpr uint32_t TMEM_COLS = (2 * N <= 128) ? 128u : ((2 * N <= 256) ? 256u : 512u);   // two accumulators
     static constexpr size_t SMEM = IT_A_BYTES + 2 * (size_t)BYTES;
+    static constexpr int MINB = SMEM <= 100 * 1024 ? 2 : 1;      // resident CTAs per SM
 };
 
 // ---------------------------------------------------------------- operands
@@ -92,14 +97,17 @@ __global__ void k_ion_tc_table(int n, int K2, Cell c, const double4 *__restrict_
 
 // per pass: the weights of every (row, component) from Ak rho(k), as K-major chunks of
 // IT_RPC rows with K = (h | l | h); rows past nrow are zero.  Components: Gx, Gy, Hx,
-// Hy (and Kx, Ky): the coefficients of c_z, of d_z and of the constant 1 in the sums above
+// Hy (and Kx, Ky): the coefficients of c_z, of d_z and of the constant 1 in the sums above.
+// One thread per (chunk, row-component, group of 4 of the 32 values).
 template <int NC>
 __global__ void k_ion_tc_weights(int nrow, int nchunk, int K2, const KRow *__restrict__ row,
                                  const double2 *__restrict__ rho, float4 *__restrict__ wtab) {
     using S = ItShape<NC>;
+    constexpr int G = IT_KV / 4;
     int g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= nchunk * S::N) return;
-    const int ch = g / S::N, nn = g - ch * S::N;
+    if (g >= nchunk * S::N * G) return;
+    const int grp = g % G, t = g / G;
+    const int ch = t / S::N, nn = t - ch * S::N;
     const int rloc = nn / NC, comp = nn - rloc * NC, rr = ch * IT_RPC + rloc;
     KRow R;
     R.nx = R.ny = R.z0 = R.cnt = R.koff = 0;
@@ -110,9 +118,10 @@ __global__ void k_ion_tc_weights(int nrow, int nchunk, int K2, const KRow *__res
         if (!ok || z < zlo || z > zhi) return make_double2(0.0, 0.0);
         return rho[R.koff + z - zlo];
     };
-    float h[IT_KV], l[IT_KV];
+    float h[4], l[4];
 #pragma unroll
-    for (int k = 0; k < IT_KV; k++) {
+    for (int u = 0; u < 4; u++) {
+        const int k = grp * 4 + u;
         double v = 0.0;
         if (k < 2 * K2) {
             const bool cpart = k < K2;
@@ -132,15 +141,13 @@ __global__ void k_ion_tc_weights(int nrow, int nchunk, int K2, const KRow *__res
             const double2 r0 = rho_at(0);
             v = comp == 0 ? r0.x : r0.y;
         }
-        split2((float)v, h[k], l[k]);
+        split2((float)v, h[u], l[u]);
     }
     unsigned char *T = (unsigned char *)wtab + (size_t)ch * S::BYTES;
-#pragma unroll
-    for (int kg = 0; kg < IT_K / 4; kg++) {
-        const int t = kg / (IT_KV / 4), v0 = (kg % (IT_KV / 4)) * 4;
-        const float *s = t == 1 ? l : h;
-        *(float4 *)(T + kmaj(nn, 4 * kg, S::LBO)) = make_float4(s[v0], s[v0 + 1], s[v0 + 2], s[v0 + 3]);
-    }
+    const float4 hv = make_float4(h[0], h[1], h[2], h[3]), lv = make_float4(l[0], l[1], l[2], l[3]);
+    *(float4 *)(T + kmaj(nn, grp * 4, S::LBO)) = hv;
+    *(float4 *)(T + kmaj(nn, IT_KV + grp * 4, S::LBO)) = lv;
+    *(float4 *)(T + kmaj(nn, 2 * IT_KV + grp * 4, S::LBO)) = hv;
 }
 
 // ---------------------------------------------------------------- the pass
@@ -159,7 +166,7 @@ struct IonTcArgs {
 };
 
 template <int NC>
-__global__ void __launch_bounds__(IT_THREADS, 1) k_ion_tc(IonTcArgs a) {
+__global__ void __launch_bounds__(IT_THREADS, ItShape<NC>::MINB) k_ion_tc(IonTcArgs a) {
     using S = ItShape<NC>;
     constexpr bool WF = NC == 6;
     extern __shared__ __align__(1024) unsigned char sm[];
@@ -168,7 +175,7 @@ __global__ void __launch_bounds__(IT_THREADS, 1) k_ion_tc(IonTcArgs a) {
     int2 *rnxy = (int2 *)(sB + 2 * S::BYTES);                 // (nx, ny) of the slice's rows
     uint64_t *bar = (uint64_t *)(rnxy + a.rows_per_slice);
     // bar: 0 tile landed, 1-2 chunk landed, 3-4 chunk consumed, 5-6 accumulator ready,
-    // 7-8 accumulator read
+    // 7-8 accumulator read (one arrival per row warp)
     volatile int *abort_flag = (volatile int *)(bar + 9);
     uint32_t *tmem_slot = (uint32_t *)(bar + 10);
 
@@ -187,7 +194,7 @@ __global__ void __launch_bounds__(IT_THREADS, 1) k_ion_tc(IonTcArgs a) {
             mbar_init(smem_u32(&bar[1 + b]), 1);
             mbar_init(smem_u32(&bar[3 + b]), 1);
             mbar_init(smem_u32(&bar[5 + b]), 1);
-            mbar_init(smem_u32(&bar[7 + b]), 4);
+            mbar_init(smem_u32(&bar[7 + b]), IT_EPI);
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         *abort_flag = 0;
@@ -208,7 +215,7 @@ __global__ void __launch_bounds__(IT_THREADS, 1) k_ion_tc(IonTcArgs a) {
         *abort_flag = 1;
     };
 
-    if (warp == 4) {
+    if (warp == IT_EPI) {
         // ------------------------------------------------ copies
         if (lane == 0) {
             const uint32_t ba = smem_u32(&bar[0]);
@@ -235,7 +242,7 @@ __global__ void __launch_bounds__(IT_THREADS, 1) k_ion_tc(IonTcArgs a) {
             mbar_wait(ba, 0);
             for (int c = max(0, issued - 2); c < issued; c++) mbar_wait(smem_u32(&bar[1 + (c & 1)]), (c >> 1) & 1);
         }
-    } else if (warp == 5) {
+    } else if (warp == IT_EPI + 1) {
         // ------------------------------------------------ MMAs
         if (lane == 0) {
             const uint32_t idesc = idesc_tf32(IT_M, S::N);
@@ -269,20 +276,21 @@ __global__ void __launch_bounds__(IT_THREADS, 1) k_ion_tc(IonTcArgs a) {
         }
     } else {
         // ------------------------------------------------ rows (lane = ion of the tile)
-        const int pos = blockIdx.x * IT_M + tid;
+        const int qd = warp & 3, hsel = warp >> 2;
+        const int pos = blockIdx.x * IT_M + qd * 32 + lane;
         const bool act = pos < a.cnt;
         const int ion = act ? a.order[pos] : 0;
         const Cell &c = a.c;
-        double tx = 0.0, ty = 0.0, mx = 0.0, my = 0.0;
-        float mz = 0.f;
+        double tx = 0.0, ty = 0.0;
+        float mx = 0.f, my = 0.f, mz = 0.f;
         if (act) {
             const double4 ri = a.r[ion];
             tx = c.B[0][0] * ri.x + c.B[1][0] * ri.y + c.B[2][0] * ri.z;
             ty = c.B[0][1] * ri.x + c.B[1][1] * ri.y + c.B[2][1] * ri.z;
             if (WF && a.ld) {
                 const double3 m3 = a.mu[ion];
-                mx = c.B[0][0] * m3.x + c.B[1][0] * m3.y + c.B[2][0] * m3.z;
-                my = c.B[0][1] * m3.x + c.B[1][1] * m3.y + c.B[2][1] * m3.z;
+                mx = (float)(c.B[0][0] * m3.x + c.B[1][0] * m3.y + c.B[2][0] * m3.z);
+                my = (float)(c.B[0][1] * m3.x + c.B[1][1] * m3.y + c.B[2][1] * m3.z);
                 mz = (float)(c.B[0][2] * m3.x + c.B[1][2] * m3.y + c.B[2][2] * m3.z);
             }
         }
@@ -291,7 +299,7 @@ __global__ void __launch_bounds__(IT_THREADS, 1) k_ion_tc(IonTcArgs a) {
         int2 Rp = make_int2(0, 0);
         int run = IT_RUN;
         double S0 = 0, S1 = 0, S2 = 0, P0 = 0, P1 = 0, P2 = 0;
-        const uint32_t lanebase = tmem + ((uint32_t)(warp * 32) << 16);
+        const uint32_t lanebase = tmem + ((uint32_t)(qd * 32) << 16);
         bool ok = true;
         for (int ch = 0; ch < nch; ch++) {
             const int b = ch & 1;
@@ -304,53 +312,59 @@ __global__ void __launch_bounds__(IT_THREADS, 1) k_ion_tc(IonTcArgs a) {
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-#pragma unroll 1
-            for (int j0 = 0; j0 < IT_RPC; j0 += 8) {
-                float v[8 * NC];
+            float v[IT_HALF * NC];
 #pragma unroll
-                for (int q = 0; q < NC; q++) tmem_ld8(lanebase + (uint32_t)(b * S::N + j0 * NC + 8 * q), v + 8 * q);
-                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-                for (int j = 0; j < 8; j++) {
-                    const int rr = ch * IT_RPC + j0 + j;
-                    if (rr >= nrs) break;
-                    const int2 R = rnxy[rr];
-                    if (run < IT_RUN && R.x == Rp.x && R.y == Rp.y + 1) {
-                        w = cmul32(w, e1);
-                        run++;
-                    } else {
-                        w = cis2pi32((double)R.x * tx + (double)R.y * ty);
-                        run = 1;
-                    }
-                    Rp = R;
-                    const float *g = v + j * NC;
-                    const float Gx = g[0], Gy = g[1], Hx = g[2], Hy = g[3];
-                    // Im conj(w) G and Im conj(w) H
-                    const float R1 = w.x * Gy - w.y * Gx, Rz = w.x * Hy - w.y * Hx;
-                    const double fx = (double)R.x, fy = (double)R.y;
-                    S0 += fx * (double)R1;
-                    S1 += fy * (double)R1;
-                    S2 += (double)Rz;
-                    if (WF) {
-                        const float Kx = g[4], Ky = g[5];
-                        // Re conj(w) G, H, K with the ion's dipole, c0 = nx mx + ny my
-                        const float Q0 = w.x * Gx + w.y * Gy, Q1 = w.x * Hx + w.y * Hy, Q2 = w.x * Kx + w.y * Ky;
-                        const double c0 = fx * mx + fy * my;
-                        const double T1 = c0 * (double)Q0 + (double)mz * (double)Q1;
-                        const double Tz = c0 * (double)Q1 + (double)mz * (double)Q2;
-                        P0 += fx * T1;
-                        P1 += fy * T1;
-                        P2 += Tz;
-                    }
-                }
-            }
+            for (int q = 0; q < NC; q++)
+                tmem_ld8(lanebase + (uint32_t)(b * S::N + hsel * IT_HALF * NC + 8 * q), v + 8 * q);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncwarp();
-            if (lane == 0) mbar_arrive(smem_u32(&bar[7 + b]));
+            if (lane == 0) mbar_arrive(smem_u32(&bar[7 + b]));   // the accumulator is in registers
+            float s0 = 0.f, s1 = 0.f, s2 = 0.f, p0 = 0.f, p1 = 0.f, p2 = 0.f;
+#pragma unroll
+            for (int j = 0; j < IT_HALF; j++) {
+                const int rr = ch * IT_RPC + hsel * IT_HALF + j;
+                if (rr >= nrs) break;
+                const int2 R = rnxy[rr];
+                if (run < IT_RUN && R.x == Rp.x && R.y == Rp.y + 1) {
+                    w = cmul32(w, e1);
+                    run++;
+                } else {
+                    w = cis2pi32((double)R.x * tx + (double)R.y * ty);
+                    run = 1;
+                }
+                Rp = R;
+                const float *g = v + j * NC;
+                const float Gx = g[0], Gy = g[1], Hx = g[2], Hy = g[3];
+                // Im conj(w) G and Im conj(w) H
+                const float R1 = w.x * Gy - w.y * Gx, Rz = w.x * Hy - w.y * Hx;
+                const float fx = (float)R.x, fy = (float)R.y;
+                s0 = fmaf(fx, R1, s0);
+                s1 = fmaf(fy, R1, s1);
+                s2 += Rz;
+                if (WF) {
+                    const float Kx = g[4], Ky = g[5];
+                    // Re conj(w) G, H, K with the ion's dipole, c0 = nx mx + ny my
+                    const float Q0 = w.x * Gx + w.y * Gy, Q1 = w.x * Hx + w.y * Hy, Q2 = w.x * Kx + w.y * Ky;
+                    const float c0 = fx * mx + fy * my;
+                    const float T1 = c0 * Q0 + mz * Q1, Tz = c0 * Q1 + mz * Q2;
+                    p0 = fmaf(fx, T1, p0);
+                    p1 = fmaf(fy, T1, p1);
+                    p2 += Tz;
+                }
+            }
+            S0 += (double)s0;
+            S1 += (double)s1;
+            S2 += (double)s2;
+            if (WF) {
+                P0 += (double)p0;
+                P1 += (double)p1;
+                P2 += (double)p2;
+            }
         }
         if (ok && act) {
             const int nv = WF ? 6 : 3;
-            double *o = a.part + ((size_t)sl * a.cnt + pos) * nv;
+            double *o = a.part + ((size_t)(2 * sl + hsel) * a.cnt + pos) * nv;
             o[0] = S0;
             o[1] = S1;
             o[2] = S2;
@@ -385,14 +399,15 @@ void launch_ion_tc_table(Engine &e) {
                 e.d_ion_atab);
 }
 
-// slices of the rows over the CTAs (one per SM): the fewest waves of (tiles x slices),
-// counting a fixed set-up per CTA against the chunks it runs
-static int ion_tc_slices(const Engine &e, int tiles, int nchunk, bool wf) {
-    const double setup = 3.0, per_chunk = wf ? 1.4 : 1.0;   // relative costs
+// slices of the rows over the CTAs (MINB resident per SM): the fewest waves of
+// (tiles x slices), counting a fixed set-up per CTA against the chunks it runs; each slice
+// writes two partial slices (the halves of its rows), within the partial buffer
+static int ion_tc_slices(const Engine &e, int tiles, int nchunk, bool wf, int minb) {
+    const double setup = 3.0, per_chunk = wf ? 0.7 : 0.5;   // relative costs
     int best = 1;
     double best_t = 1e300;
-    for (int s = 1; s <= std::min(std::min(8, nchunk), e.ion32_slices); s++) {
-        int waves = ceil_div((long long)tiles * s, e.nsm);
+    for (int s = 1; s <= std::min(std::min(8, nchunk), e.ion32_slices / 2); s++) {
+        int waves = ceil_div((long long)tiles * s, (long long)e.nsm * minb);
         double t = waves * (setup + per_chunk * ceil_div(nchunk, s));
         if (t < best_t - 1e-9) {
             best_t = t;
@@ -405,8 +420,8 @@ static int ion_tc_slices(const Engine &e, int tiles, int nchunk, bool wf) {
 template <int NC>
 static void ion_tc_run(Engine &e, const IonTcArgs &a, int tiles, int slices, int nchunk) {
     using S = ItShape<NC>;
-    MDFF_LAUNCH(e, k_ion_tc_weights<NC>, ceil_div(nchunk * S::N, 128), 128, 0, e.nrow, nchunk, e.kmax[2], e.d_row,
-                e.d_rho, e.d_ion_wtab);
+    MDFF_LAUNCH(e, k_ion_tc_weights<NC>, ceil_div(nchunk * S::N * (IT_KV / 4), 128), 128, 0, e.nrow, nchunk,
+                e.kmax[2], e.d_row, e.d_rho, e.d_ion_wtab);
     size_t smem = S::SMEM + sizeof(int2) * a.rows_per_slice + 16 * sizeof(uint64_t);
     // the largest request once per process (the attribute call is not recorded in graphs)
     static std::once_flag once;
@@ -418,12 +433,12 @@ static void ion_tc_run(Engine &e, const IonTcArgs &a, int tiles, int slices, int
 
 bool launch_ion_tc(Engine &e, const double *q, const double3 *mu, bool ld, const RecOut &o, const int *idx,
                    int cnt) {
-    if (!e.d_ion_atab || cnt <= 0) return false;
+    if (!e.d_ion_atab || cnt <= 0 || e.ion32_slices < 2) return false;
     // positions 0..cnt-1 of the order: every ion, or the polarisable ones
     if (!(idx == nullptr && cnt == e.n) && !(idx == e.d_pidx && cnt == e.npol)) return false;
     const bool wf = o.f != nullptr;
     const int nchunk = ceil_div(e.nrow, IT_RPC), tiles = ion_tc_tiles(cnt);
-    int slices = ion_tc_slices(e, tiles, nchunk, wf);
+    int slices = ion_tc_slices(e, tiles, nchunk, wf, wf ? ItShape<6>::MINB : ItShape<4>::MINB);
     IonTcArgs a;
     a.cnt = cnt;
     a.nrow = e.nrow;
@@ -445,7 +460,7 @@ bool launch_ion_tc(Engine &e, const double *q, const double3 *mu, bool ld, const
     else ion_tc_run<4>(e, a, tiles, slices, nchunk);
     // the same algorithmic count as the CUDA-core pass (8 / 12 flops per ion and k)
     e.prof_end("k_rec_ion", pi, (wf ? 12.0 : 8.0) * (double)cnt * e.nk);
-    launch_combine32(e, q, mu, ld, o, idx ? idx : e.d_ion_order, cnt, slices, wf);
+    launch_combine32(e, q, mu, ld, o, idx ? idx : e.d_ion_order, cnt, 2 * slices, wf);
     return true;
 }
 

@@ -62,12 +62,13 @@ def test_tensor_core_ion_pass_matches(which):
     for k in ("u_coul", "u_pol", "pvir_coul"):
         assert abs(ttc[k] - t64[k]) < 1e-5 * max(1.0, abs(t64[k])), k
     if which != "silica96_rigid":
-        # induced dipoles: both solvers stop at the SCF tolerance; the bench system's
-        # dipoles are small, so the bar is absolute: RMS |d mu| within 5 x tol x alpha_O
-        # (alpha_O = 1 A^3) over the polarisable ions, which come first
+        # induced dipoles over the polarisable ions (they come first): the solvers stop at
+        # the SCF tolerance and the FP32 fields carry ~1e-6 of the dipoles, so RMS |d mu|
+        # within 5 x tol x alpha_O (alpha_O = 1 A^3) + 1e-5 RMS |mu|
         pol = s.nionit[0]
         dmu = mtc[:pol] - m64[:pol]
-        assert float(np.sqrt(np.mean(np.sum(dmu ** 2, 1)))) < 5.0 * s.conv_tol_ind
+        rms = lambda x: float(np.sqrt(np.mean(np.sum(x ** 2, 1))))
+        assert rms(dmu) < 5.0 * s.conv_tol_ind + 1e-5 * rms(m64[:pol]), (rms(dmu), rms(m64[:pol]))
 
 
 def test_tensor_core_ion_pass_md_steps():
