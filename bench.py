@@ -66,6 +66,8 @@ def parse():
     ap.add_argument("--drift-steps", type=int, default=1000,
                     help="H_tot drift of mixed and FP64 runs over this many steps from the same start (0: skip)")
     ap.add_argument("--named-configs", type=int, default=1, help="config 2 and config 3 lines (0: skip)")
+    ap.add_argument("--tune", type=int, default=1,
+                    help="mixed: pick the k-space launch shapes on this system first (mdffgpu_tune_launch)")
     ap.add_argument("--cpu-steps", type=int, default=20, help="reference CPU baseline: timed steps")
     ap.add_argument("--cpu-warmup", type=int, default=5, help="reference CPU baseline: untimed steps before")
     ap.add_argument("--profile-steps", type=int, default=3)
@@ -504,6 +506,9 @@ def run_ours(args):
         ref.engforce()
         force_err = _rms_rel(eng.forces(), ref.forces())
         ref.close()
+    tuning = None
+    if prec == MIXED and args.tune and s.polit is not None:
+        tuning = eng.tune_launch(10)                  # untimed: launch shapes for this system
     istep = 1
     if args.warmup > 0:
         eng.md_steps(istep, args.warmup)
@@ -610,6 +615,7 @@ def run_ours(args):
             "roofline_kernels": roofs,
             "clocks": clk,
             "gpu_launches": launches,
+            "launch_tuning": tuning,
             "force_rms_rel_err_vs_fp64": force_err,
             "h_tot_drift": h_drift(th, n),
             "fp64_plain": fp64_plain,

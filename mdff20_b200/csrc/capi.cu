@@ -140,6 +140,10 @@ int mdffgpu_set_precision(mdffgpu_ctx *ctx, int precision) {
     });
 }
 
+int mdffgpu_tune_launch(mdffgpu_ctx *ctx, int reps, int *choice, double *ms) {
+    return guarded(ctx, [&](Engine &e) { e.tune_launch(reps, choice, ms); });
+}
+
 int mdffgpu_set_pim_solver(mdffgpu_ctx *ctx, int solver) {
     return guarded(ctx, [&](Engine &e) {
         if (solver != MDFFGPU_PIM_REFERENCE && solver != MDFFGPU_PIM_CG && solver != MDFFGPU_PIM_CG_FUSED)

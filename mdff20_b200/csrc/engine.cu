@@ -779,6 +779,78 @@ void Engine::field_pol(const double3 *d_p, double3 *d_out, double2 *rho_raw, boo
     launch_rec(*this, d_qzero, d_p, false, true, o);
 }
 
+// Launch shapes of the mixed k space timed on this system.  The pass timed is the CG
+// field pass (the field of the current induced dipoles at the polarisable ions: rho pass
+// over them, its reduction, ion pass, combine), run about three times per MD step; the
+// candidates are {CUDA-core, tensor-core ion pass} x {0.5, 1, 2 x the default rho-pass ion
+// chunks} x {tensor-core row slices: the cost model's, 1..4}; each is timed over `reps`
+// passes with CUDA events after two untimed ones, and the fastest is kept.  A force
+// evaluation runs first (phase tables, dipole-field records and dipoles of the current
+// positions); the state of the system is not changed.
+void Engine::tune_launch(int reps, int *choice, double *ms) {
+    if (!(use32 && real32 && rec32 && p.lcoulombic && lpol && npol > 0))
+        throw Error(MDFFGPU_ERR_STATE, "launch tuning applies to the mixed-precision polarisable k space");
+    reps = std::max(reps, 1);
+    engforce();
+    struct Cand {
+        int tc, chunks, slices;
+    };
+    std::vector<int> chunk_set;
+    for (int c : {std::max(1, rho32_chunks / 2), rho32_chunks, std::min(rho32_chunks_max, 2 * rho32_chunks)})
+        if (std::find(chunk_set.begin(), chunk_set.end(), c) == chunk_set.end()) chunk_set.push_back(c);
+    std::vector<Cand> cands;
+    for (int tc = 0; tc < (d_ion_atab ? 2 : 1); tc++)
+        for (int c : chunk_set) {
+            if (!tc) {
+                cands.push_back({0, c, 0});
+                continue;
+            }
+            for (int sl = 0; sl <= 4; sl++) cands.push_back({1, c, sl});
+        }
+    cudaEvent_t t0, t1;
+    MDFF_CK(cudaEventCreate(&t0));
+    MDFF_CK(cudaEventCreate(&t1));
+    struct EvScope {
+        cudaEvent_t a, b;
+        ~EvScope() {
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+        }
+    } evs{t0, t1};
+    Cand best{ion_tc ? 1 : 0, rho32_chunks, ion_tc_slices_set};
+    double best_ms = 1e300;
+    for (const Cand &c : cands) {
+        ion_tc = c.tc != 0;
+        rho32_chunks = c.chunks;
+        ion_tc_slices_set = c.slices;
+        if (ion_tc) launch_ion_tc_table(*this);
+        for (int w = 0; w < 2; w++) field_pol(d_mu_ind, d_ef_ind, nullptr, false);
+        MDFF_CK(cudaEventRecord(t0, stream));
+        for (int r = 0; r < reps; r++) field_pol(d_mu_ind, d_ef_ind, nullptr, false);
+        MDFF_CK(cudaEventRecord(t1, stream));
+        MDFF_CK(cudaEventSynchronize(t1));
+        float el = 0.f;
+        MDFF_CK(cudaEventElapsedTime(&el, t0, t1));
+        double t = el / reps;
+        if (t < best_ms) {
+            best_ms = t;
+            best = c;
+        }
+    }
+    ion_tc = best.tc != 0;
+    rho32_chunks = best.chunks;
+    ion_tc_slices_set = best.slices;
+    if (ion_tc) launch_ion_tc_table(*this);
+    MDFF_CK(cudaStreamSynchronize(stream));
+    gen++;   // recorded steps use the chosen shapes from now on
+    if (choice) {
+        choice[0] = best.tc;
+        choice[1] = best.chunks;
+        choice[2] = best.slices;
+    }
+    if (ms) *ms = best_ms;
+}
+
 // momentpolaSCF (src/pim.c:177-306) with extrapolate_dipole_aspc (src/pim.c:314-424)
 void Engine::pim_reference() {
     int nb = ceil_div(n, 256);

@@ -250,7 +250,8 @@ struct Engine {
     KSeg *d_seg32 = nullptr;                            // rho segments: (row, block of |nz|), both signs
     int nseg32 = 0, tab_w = 0;
     float2 *d_tab32 = nullptr;                          // phase table rows [n][tab_w]
-    int rho32_chunks = 0;
+    int rho32_chunks = 0, rho32_chunks_max = 0;         // chunks of the rho pass; room for the most
+    int ion_tc_slices_set = 0;                          // tensor-core ion pass slices (0: cost model)
     int rho_chunks_used = 0;                            // chunk partials the last rho pass wrote
     bool rho_tc = false;                                // rho pass on the tensor cores (kspace_tc.cu)
     // ion pass on the tensor cores (kspace_ion_tc.cu): positions in the order polarisable
@@ -380,6 +381,9 @@ struct Engine {
     int load_state(const unsigned char *buf, size_t bytes);
     bool graph_ok(int step) const;
     void capture_step(int step);
+    // launch shapes of the mixed k space timed on this system (the field pass of the CG):
+    // choice = {tensor-core ion pass, rho chunks, ion-pass slices}, ms = its time
+    void tune_launch(int reps, int *choice, double *ms);
     void record_while(const std::function<void(cudaGraphConditionalHandle)> &first,
                       const std::function<void(cudaGraphConditionalHandle)> &body);
     void drop_graph();

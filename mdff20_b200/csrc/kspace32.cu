@@ -643,7 +643,9 @@ void setup_kspace32(Engine &e, const std::vector<KRow> &rows) {
     int chunks = std::max(1, RHO32_MIN_BLOCKS * nsm / segblocks);
     chunks = std::min(chunks, std::max(1, ceil_div(e.n, RHO32_TI)));
     e.rho32_chunks = chunks;
-    e.d_rho_part32 = dalloc<float2>((size_t)chunks * e.nk);
+    // room for twice the chunks: the launch tuner tries 0.5x, 1x and 2x
+    e.rho32_chunks_max = std::max(chunks, std::min(2 * chunks, std::max(1, ceil_div(e.n, RHO32_TI))));
+    e.d_rho_part32 = dalloc<float2>((size_t)e.rho32_chunks_max * e.nk);
     // ion-pass slices are chosen per launch (ion32_slicing); room for the largest count
     e.nsm = nsm;
     int maxrows = std::max(1, (48 * 1024) / ion32_row_bytes(kz_of(L.K2), true));

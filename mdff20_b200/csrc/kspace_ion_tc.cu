@@ -438,7 +438,8 @@ bool launch_ion_tc(Engine &e, const double *q, const double3 *mu, bool ld, const
     if (!(idx == nullptr && cnt == e.n) && !(idx == e.d_pidx && cnt == e.npol)) return false;
     const bool wf = o.f != nullptr;
     const int nchunk = ceil_div(e.nrow, IT_RPC), tiles = ion_tc_tiles(cnt);
-    int slices = ion_tc_slices(e, tiles, nchunk, wf, wf ? ItShape<6>::MINB : ItShape<4>::MINB);
+    int slices = e.ion_tc_slices_set > 0 ? std::min(std::min(e.ion_tc_slices_set, nchunk), e.ion32_slices / 2)
+                                         : ion_tc_slices(e, tiles, nchunk, wf, wf ? ItShape<6>::MINB : ItShape<4>::MINB);
     IonTcArgs a;
     a.cnt = cnt;
     a.nrow = e.nrow;

@@ -362,10 +362,10 @@ bool launch_rho_tc(Engine &e, const double *q, const double3 *mu, bool lq, bool 
     a.chunk = ceil_div(ceil_div(cnt, chunks), TC_SI) * TC_SI;
     chunks = ceil_div(cnt, a.chunk);
     int stages = a.chunk / TC_SI;
-    int wmax = std::max(1, e.rho32_chunks / chunks);
+    int wmax = std::max(1, e.rho32_chunks_max / chunks);
     a.win = std::min(stages, std::max(TC_WIN, ceil_div(stages, wmax)));
     a.nwin = ceil_div(stages, a.win);
-    if (chunks * a.nwin > e.rho32_chunks) return false;
+    if (chunks * a.nwin > e.rho32_chunks_max) return false;
     size_t smem = rho_tc_smem(a.cw);
     MDFF_CK(cudaFuncSetAttribute(k_rho_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     MDFF_LAUNCH(e, k_rho_tc, dim3(mtiles, chunks), TC_THREADS, smem, a);

@@ -155,7 +155,7 @@ def params_from_system(s: System) -> Params:
 
 EXPORTS = (
     "mdffgpu_create", "mdffgpu_destroy", "mdffgpu_last_error", "mdffgpu_set_precision",
-    "mdffgpu_set_pim_solver", "mdffgpu_set_graph", "mdffgpu_set_positions", "mdffgpu_set_velocities",
+    "mdffgpu_set_pim_solver", "mdffgpu_tune_launch", "mdffgpu_set_graph", "mdffgpu_set_positions", "mdffgpu_set_velocities",
     "mdffgpu_get_state",
     "mdffgpu_set_dipole_history", "mdffgpu_get_dipole_history", "mdffgpu_set_nhc", "mdffgpu_get_nhc",
     "mdffgpu_get_thermo", "mdffgpu_gen_verletlist", "mdffgpu_check_verletlist", "mdffgpu_get_verletlist",
@@ -191,6 +191,7 @@ def load_library(path: str = LIB_PATH):
         "mdffgpu_set_precision": [vp, I],
         "mdffgpu_set_pim_solver": [vp, I],
         "mdffgpu_set_graph": [vp, I],
+        "mdffgpu_tune_launch": [vp, I, ip, dp],
         "mdffgpu_set_positions": [vp, dp, dp, dp],
         "mdffgpu_set_velocities": [vp, dp, dp, dp],
         "mdffgpu_get_state": [vp, dp, dp, dp, dp, dp, dp, dp, dp, dp],
@@ -298,6 +299,15 @@ class Engine:
         self.h = h
         self._check(self.L.mdffgpu_set_precision(self.h, precision))
         self._check(self.L.mdffgpu_set_pim_solver(self.h, pim_solver))
+
+    def tune_launch(self, reps: int = 10) -> dict:
+        """Time the mixed k-space launch shapes on this system and keep the fastest
+        (mdffgpu_tune_launch)."""
+        ch = np.zeros(3, np.int32)
+        ms = C.c_double(0.0)
+        self._check(self.L.mdffgpu_tune_launch(self.h, reps, _ip(ch), C.byref(ms)))
+        return {"tensor_core_ion_pass": bool(ch[0]), "rho_chunks": int(ch[1]), "ion_tc_slices": int(ch[2]),
+                "field_pass_ms": ms.value}
 
     def set_graph(self, on: bool):
         """Replay MD steps as CUDA graphs (default on); off issues every kernel."""

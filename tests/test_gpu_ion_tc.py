@@ -93,3 +93,24 @@ def test_tensor_core_ion_pass_md_steps():
         scale = max(1.0, float(np.abs(tb[:, col]).max()))
         assert np.abs(ta[:, col] - tb[:, col]).max() < 1e-5 * scale, col
     assert rms_rel(fa, fb) < 1e-5
+
+
+def test_launch_tuner_keeps_results():
+    """mdffgpu_tune_launch times the k-space launch shapes on the system and keeps the
+    fastest; the forces afterwards are the mixed path's within its bar, whichever shape
+    won, and the system's state is unchanged."""
+    s = cases.silica450(True)
+    pos = wrapped_positions(s)
+    f64, _, _ = _forces(s, pos, False, pim_solver=PIM_CG)
+    e = Engine(s, positions=pos, pim_solver=PIM_CG_FUSED, precision=MIXED)
+    e.gen_verletlist()
+    e.engforce()
+    r0 = e.state()[0].copy()
+    t = e.tune_launch(3)
+    assert t["field_pass_ms"] > 0.0 and t["rho_chunks"] >= 1
+    assert np.array_equal(e.state()[0], r0)
+    e.engforce()
+    assert rms_rel(e.forces(), f64) < 1e-5
+    th = e.md_steps(1, 6)
+    assert np.isfinite(th).all()
+    e.close()
