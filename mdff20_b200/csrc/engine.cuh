@@ -256,7 +256,7 @@ struct Engine {
     bool rho_tc = false;                                // rho pass on the tensor cores (kspace_tc.cu)
     // ion pass on the tensor cores (kspace_ion_tc.cu): positions in the order polarisable
     // ions first, the per-ion operand tiles of the current positions, per-pass weights
-    bool ion_tc = false;
+    bool ion_tc = true;
     int *d_ion_order = nullptr;
     float4 *d_ion_atab = nullptr, *d_ion_wtab = nullptr;
     // CG initial guess: polynomial extrapolation through the last extrapolate_order + 1
