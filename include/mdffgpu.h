@@ -111,11 +111,13 @@ int mdffgpu_set_pim_solver(mdffgpu_ctx *ctx, int solver);
 /* No reference counterpart: the launch-shape half of the autotuner (the Ewald alpha and
  * kmax half is mdff20_b200/fit.py's ewald_tune).  For a mixed-precision context with
  * polarisable ions, times the CG field pass of the current system over candidate launch
- * shapes of the k space -- CUDA-core or tensor-core ion pass, 0.5x / 1x / 2x the default
- * rho-pass ion chunks, the tensor-core pass's row slices -- `reps` passes each, and keeps
- * the fastest for this context.  choice (may be NULL) receives {tensor-core ion pass 0/1,
- * rho chunks, row slices (0: cost model)}, ms (may be NULL) the chosen pass's time.  Runs
- * one force evaluation first; the system's state is not changed. */
+ * shapes of the k space -- CUDA-core rho pass at 0.5x / 1x / 2x the default ion chunks or
+ * tensor-core rho pass, CUDA-core or tensor-core ion pass at 0 (cost model) to 4 row
+ * slices -- `reps` passes each, and keeps the fastest for this context.  choice (may be
+ * NULL, else 4 ints) receives {tensor-core ion pass 0/1, CUDA-core rho chunks (0 with the
+ * tensor-core rho pass), ion-pass row slices, tensor-core rho pass 0/1}, ms (may be NULL)
+ * the chosen pass's time.  Runs one force evaluation first; the system's state is not
+ * changed. */
 int mdffgpu_tune_launch(mdffgpu_ctx *ctx, int reps, int *choice, double *ms);
 /* No reference counterpart.  on != 0 (the default): mdffgpu_md_steps replays each MD
  * step as one CUDA graph (the CG loop a device-controlled while node) whenever the step

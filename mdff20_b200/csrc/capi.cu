@@ -133,8 +133,8 @@ int mdffgpu_set_precision(mdffgpu_ctx *ctx, int precision) {
             e.rec32 = strstr(v, "rec") != nullptr;
         }
         if (const char *v = getenv("MDFFGPU_PIM_SUBSET")) e.subset32 = atoi(v) != 0;
-        e.rho_tc = false;   // MDFFGPU_KSPACE_TC=1: the rho pass on the tensor cores (kspace_tc.cu)
-        if (const char *v = getenv("MDFFGPU_KSPACE_TC")) e.rho_tc = atoi(v) != 0;
+        e.rho_tc = true;    // the rho pass on the tensor cores (kspace_tc.cu); MDFFGPU_RHO_TC=0: CUDA cores
+        if (const char *v = getenv("MDFFGPU_RHO_TC")) e.rho_tc = atoi(v) != 0;
         e.ion_tc = true;    // the ion pass on the tensor cores (kspace_ion_tc.cu); MDFFGPU_ION_TC=0: CUDA cores
         if (const char *v = getenv("MDFFGPU_ION_TC")) e.ion_tc = atoi(v) != 0;
     });

@@ -65,7 +65,7 @@ struct NhcArgs {
     int nn, yo, mults;
     double dt, temp, L, w[7];
 };
-__global__ void k_nhc_chain(NhcArgs a, double *nhc, const double *scal, DevScalars *out);
+void launch_nhc_chain(Engine &e, const NhcArgs &a, double *nhc, const double *scal, DevScalars *out);
 __global__ void k_nhc_energy(int nn, double L, double temp, const double *nhc, const double *scal,
                              DevScalars *out);
 __global__ void k_set_ekin(const double *scal, DevScalars *out);
@@ -205,6 +205,8 @@ Engine::~Engine() {
     cudaFree(d_ion_part32);
     cudaFree(d_pidx);
     cudaFree(d_qm_tc);
+    cudaFree(d_rho_btab);
+    cudaFree(d_rho_etab);
     cudaFree(d_ion_order);
     cudaFree(d_ion_atab);
     cudaFree(d_ion_wtab);
@@ -793,20 +795,19 @@ void Engine::tune_launch(int reps, int *choice, double *ms) {
     reps = std::max(reps, 1);
     engforce();
     struct Cand {
-        int tc, chunks, slices;
+        int tc, chunks, slices, rtc;
     };
     std::vector<int> chunk_set;
     for (int c : {std::max(1, rho32_chunks / 2), rho32_chunks, std::min(rho32_chunks_max, 2 * rho32_chunks)})
         if (std::find(chunk_set.begin(), chunk_set.end(), c) == chunk_set.end()) chunk_set.push_back(c);
+    // rho pass: the CUDA-core pass at each chunk count, or the tensor-core pass (its own
+    // chunks); ion pass: the CUDA-core pass, or the tensor-core pass at 0 (cost model) to 4
+    // row slices
     std::vector<Cand> cands;
-    for (int tc = 0; tc < (d_ion_atab ? 2 : 1); tc++)
-        for (int c : chunk_set) {
-            if (!tc) {
-                cands.push_back({0, c, 0});
-                continue;
-            }
-            for (int sl = 0; sl <= 4; sl++) cands.push_back({1, c, sl});
-        }
+    for (int rtc = 0; rtc < (d_rho_btab ? 2 : 1); rtc++)
+        for (int c : (rtc ? std::vector<int>{rho32_chunks} : chunk_set))
+            for (int tc = 0; tc < (d_ion_atab ? 2 : 1); tc++)
+                for (int sl = 0; sl <= (tc ? 4 : 0); sl++) cands.push_back({tc, c, sl, rtc});
     cudaEvent_t t0, t1;
     MDFF_CK(cudaEventCreate(&t0));
     MDFF_CK(cudaEventCreate(&t1));
@@ -817,13 +818,18 @@ void Engine::tune_launch(int reps, int *choice, double *ms) {
             cudaEventDestroy(b);
         }
     } evs{t0, t1};
-    Cand best{ion_tc ? 1 : 0, rho32_chunks, ion_tc_slices_set};
+    Cand best{ion_tc ? 1 : 0, rho32_chunks, ion_tc_slices_set, rho_tc ? 1 : 0};
     double best_ms = 1e300;
-    for (const Cand &c : cands) {
+    auto apply = [&](const Cand &c) {
         ion_tc = c.tc != 0;
         rho32_chunks = c.chunks;
         ion_tc_slices_set = c.slices;
+        rho_tc = c.rtc != 0;
         if (ion_tc) launch_ion_tc_table(*this);
+        if (rho_tc) launch_rho_tc_tables(*this);
+    };
+    for (const Cand &c : cands) {
+        apply(c);
         for (int w = 0; w < 2; w++) field_pol(d_mu_ind, d_ef_ind, nullptr, false);
         MDFF_CK(cudaEventRecord(t0, stream));
         for (int r = 0; r < reps; r++) field_pol(d_mu_ind, d_ef_ind, nullptr, false);
@@ -837,16 +843,14 @@ void Engine::tune_launch(int reps, int *choice, double *ms) {
             best = c;
         }
     }
-    ion_tc = best.tc != 0;
-    rho32_chunks = best.chunks;
-    ion_tc_slices_set = best.slices;
-    if (ion_tc) launch_ion_tc_table(*this);
+    apply(best);
     MDFF_CK(cudaStreamSynchronize(stream));
     gen++;   // recorded steps use the chosen shapes from now on
     if (choice) {
         choice[0] = best.tc;
-        choice[1] = best.chunks;
+        choice[1] = best.rtc ? 0 : best.chunks;
         choice[2] = best.slices;
+        choice[3] = best.rtc;
     }
     if (ms) *ms = best_ms;
 }
@@ -1342,13 +1346,13 @@ void Engine::prop_agate(int step) {
         if (a.nn < 2 || a.nn > 16) throw Error(MDFFGPU_ERR_ARG, "nhc_n must be in 2..16");
         MDFF_LAUNCH(*this, k_scale_kin, nb, 256, 0, n, d_out, 0, d_mass, d_v, d_part, part_stride);
         reduce(S_KIN, 1, nb);
-        MDFF_LAUNCH(*this, k_nhc_chain, 1, 1, 0, a, d_nhc, d_scal, d_out);
+        launch_nhc_chain(*this, a, d_nhc, d_scal, d_out);
         MDFF_LAUNCH(*this, k_scale_kin, nb, 256, 0, n, d_out, 1, d_mass, d_v, d_part, part_stride);
         MDFF_LAUNCH(*this, k_pv1, nb, 256, 0, n, dt, dt * 0.5, d_invmass, d_r, d_v, d_f);
         engforce();
         MDFF_LAUNCH(*this, k_pv2, nb, 256, 0, n, dt * 0.5, d_invmass, d_mass, d_v, d_f, d_part, part_stride);
         reduce(S_KIN, 1, nb);
-        MDFF_LAUNCH(*this, k_nhc_chain, 1, 1, 0, a, d_nhc, d_scal, d_out);
+        launch_nhc_chain(*this, a, d_nhc, d_scal, d_out);
         MDFF_LAUNCH(*this, k_scale_kin, nb, 256, 0, n, d_out, 1, d_mass, d_v, d_part, part_stride);
         reduce(S_KIN, 1, nb);
         MDFF_LAUNCH(*this, k_nhc_energy, 1, 1, 0, a.nn, a.L, temp, d_nhc, d_scal, d_out);

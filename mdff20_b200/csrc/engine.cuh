@@ -160,9 +160,13 @@ bool launch_ion_tc(Engine &e, const double *q, const double3 *mu, bool ld, const
                    int cnt);
 void launch_ion_tc_table(Engine &e);
 void setup_ion_tc(Engine &e);
-// kspace_tc.cu: the same rho chunk partials from tcgen05 TF32 MMAs (false: k box out of range)
+// kspace_tc.cu: the same rho chunk partials from tcgen05 TF32 MMAs (false: not applicable,
+// nothing launched); launch_rho_tc_tables lays out its per-stage inputs of the current
+// positions (after the phase table)
 bool launch_rho_tc(Engine &e, const double *q, const double3 *mu, bool lq, bool ld, const int *idx, int cnt,
-                   int tab_w, int z_off, int nzb_neg, int *chunks_used);
+                   int z_off, int *chunks_used);
+void launch_rho_tc_tables(Engine &e);
+void setup_rho_tc(Engine &e, int lz);
 void launch_ion32(Engine &e, const double *q, const double3 *mu, bool ld, const RecOut &o, const int *idx, int cnt);
 
 // ---------------------------------------------------------------- engine state
@@ -253,7 +257,11 @@ struct Engine {
     int rho32_chunks = 0, rho32_chunks_max = 0;         // chunks of the rho pass; room for the most
     int ion_tc_slices_set = 0;                          // tensor-core ion pass slices (0: cost model)
     int rho_chunks_used = 0;                            // chunk partials the last rho pass wrote
-    bool rho_tc = false;                                // rho pass on the tensor cores (kspace_tc.cu)
+    // rho pass on the tensor cores (kspace_tc.cu): per-stage E operand tiles and E0 | E1
+    // rows of the current positions, the chunk count (0: two CTAs per SM)
+    bool rho_tc = true;
+    float4 *d_rho_btab = nullptr, *d_rho_etab = nullptr;
+    int rho_tc_lz = 0, rho_tc_chunks_set = 0;
     // ion pass on the tensor cores (kspace_ion_tc.cu): positions in the order polarisable
     // ions first, the per-ion operand tiles of the current positions, per-pass weights
     bool ion_tc = true;

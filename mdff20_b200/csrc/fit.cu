@@ -566,7 +566,13 @@ void Engine::fit_reduce(int first, int cnt, int nparts) {
 // Coulomb forces (electrostatic part only, energy units) of (q, mu) into out
 void Engine::coul_forces(const double *d_qv, const double3 *d_muv, bool lq, bool ld, double3 *out) {
     MDFF_CK(cudaMemsetAsync(out, 0, sizeof(double3) * n, stream));
-    launch_dir(*this, d_qv, d_muv, p.alphaES, lq, ld, ldmp != 0, true, false, false, false, nullptr, nullptr, d_tmp3);
+    // mixed: the FP32 real-space pass reads the context's charges from the packed
+    // fractional coordinates, so d_qv may only be the charges themselves or absent (lq)
+    if (use32 && real32)
+        launch_dir32(*this, d_qv, d_muv, p.alphaES, lq, ld, ldmp != 0, true, false, nullptr, d_tmp3);
+    else
+        launch_dir(*this, d_qv, d_muv, p.alphaES, lq, ld, ldmp != 0, true, false, false, false, nullptr, nullptr,
+                   d_tmp3);
     RecOut o;
     o.f = out;
     o.f_dir = d_tmp3;
@@ -642,13 +648,9 @@ void Engine::fit_issue(const double3 *d_ft, double scale, int tSi, int tO, const
     a.stride = part_stride;
     // s: real space
     MDFF_LAUNCH(*this, k_adj_dir, nbw, FIT_WARPS * 32, 0, a);
-    // s: k space, drho_w from three rho passes of (q w_a, mu w_a)
-    struct PrecisionScope {   // the adjoint runs in FP64; the context's precision comes back
-        bool &flag;
-        bool saved;
-        ~PrecisionScope() { flag = saved; }
-    } fp64_scope{use32, use32};
-    use32 = false;
+    // s: k space, drho_w from three rho passes of (q w_a, mu w_a).  These passes, the
+    // adjoint solve and the Coulomb force evaluations below run in the context's precision;
+    // the EFG pass runs in FP64 (launch_rec routes EFG requests to the FP64 kernels)
     for (int comp = 0; comp < 3; comp++) {
         MDFF_LAUNCH(*this, k_scale_by_w, nb, 256, 0, n, comp, q, d_mu_tot, d_w, d_qw, d_muw);
         RecOut o;
@@ -670,19 +672,17 @@ void Engine::fit_issue(const double3 *d_ft, double scale, int tSi, int tO, const
         launch_rec(*this, q, d_mu_tot, true, true, o);
     }
     MDFF_LAUNCH(*this, k_adj_rhs, nb, 256, 0, n, d_polar, coul_unit, d_sv, d_fa, d_efg_rec, d_w, d_sv);
-    // adjoint solve A lambda = s in the context's precision: FP64 (cached dipole-field
-    // factors of these positions) to a 1e-11 relative residual, or mixed (the FP32
-    // dipole-field records and phase tables of the force evaluation above) to 1e-6
+    // adjoint solve A lambda = s: FP64 (cached dipole-field factors of these positions) to
+    // a 1e-11 relative residual, or mixed (the FP32 dipole-field records and phase tables
+    // of the force evaluation above) to 1e-6
     {
         struct CoefScope {
             bool &flag;
             ~CoefScope() { flag = false; }
         } scope{coef_ready};
-        use32 = fp64_scope.saved;
         if (!(use32 && real32)) launch_dir_prep(*this, p.alphaES);
         coef_ready = true;
         solve_pim(d_sv, d_lam, use32 ? 1e-6 : 1e-11, 500);
-        use32 = false;
     }
     // parameter sensitivities
     MDFF_LAUNCH(*this, k_bhm_sens, nbw, FIT_WARPS * 32, 0, n, cell, d_s, d_typ, d_pair, nt, d_nb, d_nbn, cap_nb,

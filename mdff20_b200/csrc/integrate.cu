@@ -511,36 +511,52 @@ __global__ void k_lf(int n, double dtsq, double idt, const double *__restrict__ 
 
 // chain_nhcn (src/integration.c:189-294) on one thread: thermostat variables in
 // d_nhc (xi[16], vxi[16]); kin from the S_KIN slot (sum m v^2); writes s.  The
-// second sweep stops at nhc_n-2 as in the reference (src/integration.c:269).
+// second sweep stops at nhc_n-2 as in the reference (src/integration.c:269).  NN > 0:
+// the chain length known at compile time, the chain held in registers (the loops
+// unrolled); NN = 0: any length up to 16, the chain in local memory.  Either way the
+// variables are read once and written once, and the arithmetic is the same.
 struct NhcArgs {
     int nn, yo, mults;
     double dt, temp, L, w[7];
 };
+template <int NN>
 __global__ void k_nhc_chain(NhcArgs a, double *__restrict__ nhc, const double *__restrict__ scal, DevScalars *out) {
     if (threadIdx.x || blockIdx.x) return;
-    double *xi = nhc, *vxi = nhc + 16, *Q = nhc + 32;
-    double kin = 0.5 * scal[S_KIN];
-    double G[16];
-    for (int k = 0; k < 16; k++) G[k] = 0.0;
-    double dty[7];
-    for (int k = 0; k < 7; k++) dty[k] = a.w[k] * a.dt / ((double)a.mults);
+    constexpr int M = NN > 0 ? NN : 16;
+    const int nn = NN > 0 ? NN : a.nn;
+    double xi[M], vxi[M], Q[M], G[M];
+#pragma unroll
+    for (int i = 0; i < M; i++) {
+        const bool on = i < nn;
+        xi[i] = on ? nhc[i] : 0.0;
+        vxi[i] = on ? nhc[16 + i] : 0.0;
+        Q[i] = on ? nhc[32 + i] : 1.0;
+        G[i] = 0.0;
+    }
+    const double kin = 0.5 * scal[S_KIN];
     double s = 1.0;
-    int nn = a.nn;
     G[0] = 2.0 * kin - a.L * a.temp;
     for (int k = 0; k < a.mults; k++) {
         for (int j = 0; j < a.yo && j < 7; j++) {
-            double dts = dty[j], dts2 = dts * 0.5, dts4 = dts2 * 0.5, dts8 = dts4 * 0.5;
+            const double dts = a.w[j] * a.dt / ((double)a.mults);
+            const double dts2 = dts * 0.5, dts4 = dts2 * 0.5, dts8 = dts4 * 0.5;
             G[nn - 1] = (vxi[nn - 2] * vxi[nn - 2] / Q[nn - 2] - a.temp);
             vxi[nn - 1] += G[nn - 1] * dts4;
-            for (int inh = nn - 2; inh > -1; inh--) {
+#pragma unroll
+            for (int inh = M - 2; inh > -1; inh--) {
+                if (inh > nn - 2) continue;
                 vxi[inh] *= exp(-vxi[inh + 1] * dts8 / Q[inh + 1]);
                 vxi[inh] += G[inh] * dts4;
                 vxi[inh] *= exp(-vxi[inh + 1] * dts8 / Q[inh + 1]);
             }
             s *= exp(-vxi[0] * dts2 / Q[0]);
-            for (int i = 0; i < nn; i++) xi[i] += vxi[i] * dts2 / Q[i];
+#pragma unroll
+            for (int i = 0; i < M; i++)
+                if (i < nn) xi[i] += vxi[i] * dts2 / Q[i];
             G[0] = 2.0 * kin * s * s - a.L * a.temp;
-            for (int inh = 0; inh < nn - 2; inh++) {
+#pragma unroll
+            for (int inh = 0; inh < M - 2; inh++) {
+                if (inh >= nn - 2) break;
                 vxi[inh] *= exp(-vxi[inh + 1] * dts8 / Q[inh + 1]);
                 vxi[inh] += G[inh] * dts4;
                 vxi[inh] *= exp(-vxi[inh + 1] * dts8 / Q[inh + 1]);
@@ -549,7 +565,23 @@ __global__ void k_nhc_chain(NhcArgs a, double *__restrict__ nhc, const double *_
             vxi[nn - 1] += G[nn - 1] * dts4;
         }
     }
+#pragma unroll
+    for (int i = 0; i < M; i++)
+        if (i < nn) {
+            nhc[i] = xi[i];
+            nhc[16 + i] = vxi[i];
+        }
     out->nhc_s = s;
+}
+
+void launch_nhc_chain(Engine &e, const NhcArgs &a, double *nhc, const double *scal, DevScalars *out) {
+    switch (a.nn) {
+    case 2: MDFF_LAUNCH(e, k_nhc_chain<2>, 1, 1, 0, a, nhc, scal, out); break;
+    case 3: MDFF_LAUNCH(e, k_nhc_chain<3>, 1, 1, 0, a, nhc, scal, out); break;
+    case 4: MDFF_LAUNCH(e, k_nhc_chain<4>, 1, 1, 0, a, nhc, scal, out); break;
+    case 5: MDFF_LAUNCH(e, k_nhc_chain<5>, 1, 1, 0, a, nhc, scal, out); break;
+    default: MDFF_LAUNCH(e, k_nhc_chain<0>, 1, 1, 0, a, nhc, scal, out); break;
+    }
 }
 
 // e_kin and the NHC conserved-quantity term e_nvt (src/integration.c:156-176)

@@ -652,6 +652,7 @@ void setup_kspace32(Engine &e, const std::vector<KRow> &rows) {
     e.ion32_slices = std::max(std::min(32, e.nrow), ceil_div(e.nrow, maxrows));
     e.d_ion_part32 = dalloc<double>((size_t)e.ion32_slices * e.n * 6);
     setup_ion_tc(e);
+    setup_rho_tc(e, L.z);
 }
 
 // k-row slices of one ion pass over `cnt` ions: about two full waves of resident blocks,
@@ -681,6 +682,7 @@ void launch_phase32(Engine &e) {
 void launch_coords32(Engine &e) {
     if (e.d_tab32) launch_phase32(e);
     if (e.ion_tc) launch_ion_tc_table(e);
+    if (e.rho_tc && e.d_tab32) launch_rho_tc_tables(e);
 }
 
 // FLOPs per (ion, k-vector) of the paired-nz formulation: 4 FMA with dipoles, 2 without
@@ -714,7 +716,7 @@ void launch_rho32(Engine &e, const double *q, const double3 *mu, bool lq, bool l
     e.prof_begin("k_rho", &ps);
     e.rho_chunks_used = e.rho32_chunks;
     int used = 0;
-    if ((lq || ld) && e.rho_tc && launch_rho_tc(e, q, mu, lq, ld, idx, cnt, L.w, L.z, L.nzb_neg, &used)) {
+    if ((lq || ld) && e.rho_tc && launch_rho_tc(e, q, mu, lq, ld, idx, cnt, L.z, &used)) {
         e.rho_chunks_used = used;
     } else if (lq && ld) rho32_launch<true, true>(e, grid, smem, cnt, idx, chunk, L, q, mu);
     else if (lq) rho32_launch<true, false>(e, grid, smem, cnt, idx, chunk, L, q, mu);

@@ -1,5 +1,6 @@
-// rho(k) on the 5th-generation tensor cores (tcgen05, sm_100a): the mixed-precision
-// structure-factor pass as a TF32 matrix product with FP32 accumulation in tensor memory.
+// The rho pass of the mixed-precision reciprocal sum on the 5th-generation tensor cores
+// (tcgen05, sm_100a): kspace32.cu's k_rho32 as a TF32 matrix product with FP32
+// accumulation in tensor memory.
 //
 // With e^{ik.r_i} = E0_i[nx] E1_i[ny] E2_i[nz] and E2_i[-z] = conj E2_i[z] = (c, -d), the
 // summand of k = (nx, ny, nz) is (B1 + nz B2) E2[nz] with, per row (nx, ny) and ion,
@@ -7,65 +8,136 @@
 // (m = 2 pi B mu), and the eight sums over ions of B1x c, B1y d, B1x d, B1y c and the same
 // with B2 give rho(+z) and rho(-z) (kspace32.cu).  So the pass is one real product
 //     C[(coef, row)][col] = sum_i A[(coef, row)][i] E[col][i],
-// A = (B1x, B1y, B2x, B2y) of each row and ion (M = 4 x 32 rows per CTA), E = (1, c_1..c_K2,
-// d_1..d_K2) of each ion (N = 32, the 1 for nz = 0): only A depends on the row, one
-// complex product per (row, ion) to form it.  Every value x is split as x = h + l, both
-// TF32 (round to nearest), and the product taken as hh + hl + lh (the dropped ll is 2^-22
-// of it): K = 3 per ion.
+// A = (B1x, B1y, B2x, B2y) of each row and ion (M = 4 coefficients x 32 rows per MMA),
+// E = (1, c_1..c_K2, d_1..d_K2, 0 ...) of each ion (N = 32; the 1 gives nz = 0).  Only A
+// depends on the row: one complex product per (row, ion) forms it, the MMA does the nz
+// sums.  Every value x is split as x = h + l, both TF32, and the product taken as
+// A_h E_h + A_h E_l + A_l E_h (the dropped l l term is 2^-22 of it): three MMAs per
+// K step, the A_h tile read by two of them, so a producer stores each value twice
+// (h and l), not three times.
 //
-// CTA = 32 k-rows and a chunk of ions, 8 warps.  Per stage of 16 ions the phase-table
-// rows are staged in shared memory (asynchronous copies, three stages ahead), all warps
-// write the split operands into one of two K-major no-swizzle buffers, one thread issues
-// the six tcgen05.mma (M=128, N=32, K=8) and commits them to the buffer's mbarrier, and
-// the next stage is written while they run.  Every window of stages (about 200 ions) the
-// accumulator is read back (tcgen05.ld), combined into rho(+z), rho(-z) and written as one
-// FP32 chunk partial per k; partials are summed in FP64 in a fixed order (k_rho_reduce),
-// as for the CUDA-core pass.
+// CTA = 64 k-rows (two M = 128 MMA tiles sharing every staged ion) and a chunk of ions
+// in stages of 16, 14 warps:
+//   warp 8      bulk-copies each stage's inputs -- the ions' E0 | E1 phase rows, their
+//               (q, 2 pi B mu) and the E operand tile, all three laid out per stage once
+//               per force evaluation (k_rho_tc_tables) or per pass (k_qm_tc) -- into one
+//               of four input slots, completing on mbarriers;
+//   warps 0-7   form A (warp w: tile w % 2, ions 4 (w / 2) .. + 3 of the stage, lane =
+//               row), split it and store it K-major into one of two A buffers;
+//   warp 9      issues the 12 MMAs (M = 128, N = 32, K = 8) of a stage -- the A_h E_h
+//               products into the current window's accumulator of each tile, the small
+//               A_h E_l and A_l E_h products into one accumulator per tile for the whole
+//               chunk -- and commits them to the buffers' barriers;
+//   warps 10-13 read each finished window (RT_WIN stages, 32 ions) back (tcgen05.ld;
+//               warp w takes lane quarter w % 4) while the next window accumulates, add
+//               it to FP32 running sums kept in tensor memory, and at the end add the
+//               small-product sums, combine into rho(+z), rho(-z) and write the chunk
+//               partial.
+// The chunk partials are summed in FP64 in a fixed order (k_rho_reduce32), as the
+// CUDA-core pass's are.  The tensor cores' FP32 accumulation is not round-to-nearest: each
+// MMA into an accumulator costs up to an ulp of it, toward zero, which shrinks |rho| and
+// so the energy.  So the large products take 4 MMA steps per window before a
+// round-to-nearest FP32 add, and the small ones (2^-11 of the sum) accumulate apart.
 //
-// Selected with MDFFGPU_KSPACE_TC=1; the CUDA-core pass (kspace32.cu) is the default.
-// Measured on the bench system (24000 ions, 12194 k, B200): forces within 3.4e-6 of FP64
-// (CUDA-core pass 2.6e-6) and 2.8 instead of 2.9 CG iterations per step, but 114 us per
-// dipole pass against 71 us: each 16-ion stage costs two CTA-wide barriers and a short
-// dependent chain (staged loads, complex product, split, store) with four warps per
-// scheduler, so the tensor pipe idles most of the time.
-//
-// Every wait on an mbarrier is bounded: on expiry the kernel sets ST_TC_TIMEOUT in the
-// status word, waits (bounded) for its MMAs once more, frees its tensor memory and
+// Every mbarrier wait is bounded: on expiry the kernel sets ST_TC_TIMEOUT, stops issuing,
+// waits (bounded) for the copies and MMAs it has in flight, frees its tensor memory and
 // returns; the host turns the flag into MDFFGPU_ERR_TIMEOUT.
-#include <cstdint>
+#include <mutex>
 
 #include "engine.cuh"
 #include "tc_common.cuh"
 
 namespace mdffgpu {
 
-constexpr int TC_M = 128;          // MMA M: 4 coefficients x 32 k-rows, m = coef * 32 + row
-constexpr int TC_ROWS = 32;
-constexpr int TC_N = 32;           // MMA N: nz = 0, c_1..c_K2, d_1..d_K2, zero padding
-constexpr int TC_SI = 16;          // ions per stage
-constexpr int TC_KS = 3 * TC_SI;   // K per stage: split terms (hh, hl, lh) x ions, term-major
-constexpr int TC_THREADS = 256;
-constexpr int TC_NSTG = 3;         // staged-row buffers: copies run TC_NSTG - 1 stages ahead
-constexpr int TC_IDX = 2048;       // ion indices of a chunk kept in shared memory (larger
-                                   // chunks read them from global memory)
-constexpr int TC_ISSUER = 128;     // thread that issues the MMAs (warp 4: no B operand work)
-constexpr int TC_WIN = 12;         // stages per partial sum, at least (192 ions)
-constexpr uint32_t TC_A_LBO = (TC_M / 8) * 128;        // 2048: 16-byte K chunk stride of A
-constexpr uint32_t TC_B_LBO = (TC_N / 8) * 128;        // 512
-constexpr uint32_t TC_A_BYTES = (TC_KS / 4) * TC_A_LBO;
-constexpr uint32_t TC_OP_BYTES = TC_A_BYTES + (TC_KS / 4) * TC_B_LBO;
-constexpr int TC_XS = TC_N + 1;    // padded row of the read-back accumulator
+constexpr int RT_MT = 2;                        // MMA tiles (32 k-rows each) per CTA
+constexpr int RT_ROWS = 32 * RT_MT;
+constexpr int RT_M = 128;                       // MMA M: m = coefficient * 32 + row
+constexpr int RT_N = 32;                        // MMA N: 1, c_1..c_K2, d_1..d_K2, zeros
+constexpr int RT_SI = 16;                       // ions per stage
+constexpr int RT_NIN = 4;                       // input slots: copies run up to 3 stages ahead
+constexpr int RT_PROD = 8;                      // producer warps
+constexpr int RT_COPY = RT_PROD;                // copy warp
+constexpr int RT_MMA = RT_PROD + 1;             // MMA warp
+constexpr int RT_EPI0 = RT_PROD + 2;            // first of the 4 read-back warps
+constexpr int RT_THREADS = 32 * (RT_PROD + 6);
+constexpr int RT_WIN = 2;                       // stages per accumulation window (32 ions)
+constexpr int RT_MAXK2 = (RT_N - 1) / 2;        // nz up to 15
+constexpr uint32_t RT_A_LBO = (RT_M / 8) * 128;                    // 2048
+constexpr uint32_t RT_A_TILE = (2 * RT_SI / 4) * RT_A_LBO;         // K = (h | l) x 16 ions: 16 KB
+constexpr uint32_t RT_A_BYTES = RT_MT * RT_A_TILE;                 // 32 KB per buffer
+constexpr uint32_t RT_B_LBO = (RT_N / 8) * 128;                    // 512
+constexpr uint32_t RT_B_TERM = (RT_SI / 4) * RT_B_LBO;             // 2 KB
+constexpr uint32_t RT_B_BYTES = 2 * RT_B_TERM;                     // (h | l): 4 KB per stage
+constexpr uint32_t RT_Q_BYTES = RT_SI * 16;
+constexpr int RT_XS = RT_N + 1;                                    // padded read-back row
+// tensor memory: two windows x RT_MT accumulators of the large products, RT_MT
+// accumulators of the small ones, RT_MT running sums
+constexpr uint32_t RT_SMALL_COL = 2 * RT_MT * RT_N;
+constexpr uint32_t RT_RUN_COL = RT_SMALL_COL + RT_MT * RT_N;
+constexpr uint32_t RT_TMEM_COLS = 256;
+static_assert(RT_RUN_COL + RT_MT * RT_N <= RT_TMEM_COLS, "tensor memory columns");
+static_assert(RT_MT * RT_M * RT_XS * 4 <= 2 * RT_A_BYTES, "read-back buffer within the A buffers");
 
-__device__ __forceinline__ void cp_async16_tc(void *smem, const void *gmem) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
+// shared memory of the pass: [2][A] [NIN][B] [NIN][E rows] [NIN][qm] barriers flags
+struct RtSmem {
+    uint32_t b, e, q, bar, total;
+};
+__host__ __device__ inline RtSmem rt_smem(int lz) {
+    RtSmem s;
+    s.b = 2 * RT_A_BYTES;
+    s.e = s.b + RT_NIN * RT_B_BYTES;
+    s.q = s.e + RT_NIN * (uint32_t)(RT_SI * lz * 8);
+    s.bar = s.q + RT_NIN * RT_Q_BYTES;
+    s.total = s.bar + 16 * 8 + 16;   // 16 barriers, the abort flag and the tensor-memory address
+    return s;
 }
 
-// (q, 2 pi (B mu)) per listed ion, as the CUDA-core pass forms it
-__global__ void k_qm_tc(int cnt, const int *__restrict__ idx, Cell c, const double *__restrict__ q,
+// ---------------------------------------------------------------- per-stage tables
+// Once per force evaluation, for position p of order (stage p / RT_SI, slot p % RT_SI):
+// the E0 | E1 prefix of the ion's phase-table row (lz float2, the values k_rho32 reads)
+// into etab, and the E operand (1, c_z, d_z of E2[z] = exp(2 pi i z t_z), the values of
+// the phase table's z blocks) split into TF32 h + l, K-major, into btab.  Positions past n
+// are zero.  One thread per (position, 16-byte unit of the E0 | E1 prefix or column).
+__global__ void k_rho_tc_tables(int n, int npad, int lz, int tab_w, int K2, Cell c, const double4 *__restrict__ r,
+                                const int *__restrict__ order, const float4 *__restrict__ tab,
+                                float4 *__restrict__ etab, float *__restrict__ btab) {
+    const int hl = lz / 2;   // 16-byte units of a prefix
+    const int per = hl + RT_N;
+    long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= (long long)npad * per) return;
+    const int p = (int)(g / per), u = (int)(g - (long long)p * per);
+    const int ion = p < n ? order[p] : -1;
+    if (u < hl) {
+        etab[(size_t)p * hl + u] = ion >= 0 ? tab[(size_t)ion * (tab_w / 2) + u] : make_float4(0.f, 0.f, 0.f, 0.f);
+        return;
+    }
+    const int col = u - hl;
+    float v = 0.f;
+    if (ion >= 0) {
+        if (col == 0) {
+            v = 1.f;
+        } else if (col <= 2 * K2) {
+            const int z = col <= K2 ? col : col - K2;
+            const double4 ri = r[ion];
+            const double tz = c.B[0][2] * ri.x + c.B[1][2] * ri.y + c.B[2][2] * ri.z;
+            const float2 e = cis2pi32((double)z * tz);
+            v = col <= K2 ? e.x : e.y;
+        }
+    }
+    float h, l;
+    split2(v, h, l);
+    unsigned char *T = (unsigned char *)btab + (size_t)(p / RT_SI) * RT_B_BYTES;
+    const int j = p % RT_SI;
+    *(float *)(T + kmaj(col, j, RT_B_LBO)) = h;
+    *(float *)(T + RT_B_TERM + kmaj(col, j, RT_B_LBO)) = l;
+}
+
+// per pass: (q, 2 pi (B mu)) of positions 0..cnt-1 of order, as k_rho32 forms them
+__global__ void k_qm_tc(int cnt, const int *__restrict__ order, Cell c, const double *__restrict__ q,
                         const double3 *__restrict__ mu, int lq, int ld, float4 *__restrict__ out) {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= cnt) return;
-    int ion = idx ? idx[t] : t;
+    int ion = order[t];
     const double tpi = TPI_D;
     float4 v = make_float4(lq ? (float)q[ion] : 0.f, 0.f, 0.f, 0.f);
     if (ld) {
@@ -77,50 +149,94 @@ __global__ void k_qm_tc(int cnt, const int *__restrict__ idx, Cell c, const doub
     out[t] = v;
 }
 
+// ---------------------------------------------------------------- the pass
 struct RhoTcArgs {
-    int cnt, chunk, win, nwin, nrow, nk, K2;
-    int tab_w;                 // float2 per table row
-    int ha;                    // 16-byte units of E0 | E1 in a table row
-    int skip;                  // 16-byte units of the nz <= 0 blocks (not staged)
-    int cw;                    // staged 16-byte units per ion: E0 | E1 | nz > 0 blocks
-    int e1, K1;                // float2 offset of E1[-K1]
-    const int *idx;
-    const float2 *tab;
-    const float4 *qm;          // per listed ion: (q, 2 pi B0.mu, 2 pi B1.mu, 2 pi B2.mu)
+    int cnt, chunk, nrow, nk, K2, K1, e1, lz;
+    const float4 *etab;      // [stage][RT_SI][lz / 2]
+    const float4 *btab;      // [stage][RT_B_BYTES / 16]
+    const float4 *qm;        // [position]
     const KRow *row;
-    float2 *part;              // [partial][nk]
+    float2 *part;            // [chunk][nk]
     unsigned *status;
 };
 
-__global__ void __launch_bounds__(TC_THREADS, 2) k_rho_tc(RhoTcArgs a) {
+__device__ __forceinline__ void tmem_st8(uint32_t addr, const float *v) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(addr),
+                 "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+                 "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
+                 "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7]))
+                 : "memory");
+}
+
+// the 12 MMAs of a stage (tiles 0 and 1, K chunks 0 and 1 of 8 ions): large products
+// A_h E_h into h0 / h1 (accumulating when acc_h), small products A_h E_l, A_l E_h into
+// s0 / s1 (accumulating when acc_s); a: descriptors of the A buffer (tile-major: A_h and
+// A_l of tile 0, then tile 1), e: of the E tile
+__device__ __forceinline__ void mma_stage(uint32_t h0, uint32_t h1, uint32_t s0, uint32_t s1, uint64_t a, uint64_t e,
+                                          uint32_t idesc, uint32_t acc_h, uint32_t acc_s) {
+    // descriptor start addresses are in 16-byte units (shared-memory offsets stay far below
+    // the field's 2^18 bytes, so the additions do not carry out of it)
+    constexpr uint64_t LO = (RT_SI / 4) * RT_A_LBO / 16, Q1 = 2 * RT_A_LBO / 16, T1 = RT_A_TILE / 16;
+    constexpr uint64_t EL = RT_B_TERM / 16, EQ1 = 2 * RT_B_LBO / 16;
+    asm volatile(
+        "{\n\t.reg .pred ph, ps, pt;\n\t"
+        "setp.ne.b32 ph, %17, 0;\n\t"
+        "setp.ne.b32 ps, %18, 0;\n\t"
+        "setp.ne.b32 pt, %16, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %4, %12, %16, ph;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %6, %14, %16, pt;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%2], %4, %13, %16, ps;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%2], %5, %12, %16, pt;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%2], %6, %15, %16, pt;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%2], %7, %14, %16, pt;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%1], %8, %12, %16, ph;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%1], %10, %14, %16, pt;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%3], %8, %13, %16, ps;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%3], %9, %12, %16, pt;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%3], %10, %15, %16, pt;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%3], %11, %14, %16, pt;\n\t}"
+        :
+        : "r"(h0), "r"(h1), "r"(s0), "r"(s1), "l"(a), "l"(a + LO), "l"(a + Q1), "l"(a + LO + Q1), "l"(a + T1),
+          "l"(a + T1 + LO), "l"(a + T1 + Q1), "l"(a + T1 + LO + Q1), "l"(e), "l"(e + EL), "l"(e + EQ1),
+          "l"(e + EL + EQ1), "r"(idesc), "r"(acc_h), "r"(acc_s));
+}
+
+__global__ void __launch_bounds__(RT_THREADS, 2) k_rho_tc(RhoTcArgs a) {
     extern __shared__ __align__(1024) unsigned char sm[];
-    const int cw = a.cw;
-    unsigned char *op = sm;                                              // [2][TC_OP_BYTES]
-    float4 *stg = (float4 *)(sm + 2 * TC_OP_BYTES);                      // [TC_NSTG][TC_SI][cw]
-    float4 *stq = stg + TC_NSTG * TC_SI * cw;                            // [TC_NSTG][TC_SI]
-    float *X = (float *)(stq + TC_NSTG * TC_SI);                         // [TC_M][TC_XS]
-    int *sidx = (int *)(X + TC_M * TC_XS);                               // [TC_IDX]
-    uint64_t *mbar = (uint64_t *)(sidx + TC_IDX);                        // [2]
-    int *abort_flag = (int *)(mbar + 2);
-    uint32_t *tmem_slot = (uint32_t *)(abort_flag + 1);
+    const RtSmem L = rt_smem(a.lz);
+    const uint32_t ebytes = (uint32_t)(RT_SI * a.lz * 8);
+    unsigned char *sA = sm, *sB = sm + L.b, *sE = sm + L.e, *sQ = sm + L.q;
+    uint64_t *bar = (uint64_t *)(sm + L.bar);
+    // bar: 0-3 inputs landed, 4-7 inputs consumed (8 producer warps + the MMAs), 8-9 A
+    // written (8 producer warps), 10-11 A consumed (MMAs), 12-13 window accumulated,
+    // 14-15 window read back (4 warps)
+    constexpr int IN_FULL = 0, IN_EMPTY = 4, A_FULL = 8, A_EMPTY = 10, ACC_FULL = 12, ACC_EMPTY = 14;
+    volatile int *abort_flag = (volatile int *)(bar + 16);
+    uint32_t *tmem_slot = (uint32_t *)(bar + 16) + 1;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int row0 = blockIdx.x * TC_ROWS;
+    const int row0 = blockIdx.x * RT_ROWS;
     const int a0 = blockIdx.y * a.chunk, a1 = min(a.cnt, a0 + a.chunk);
-    const int nstage = a1 > a0 ? (a1 - a0 + TC_SI - 1) / TC_SI : 0;
+    const int nst = a1 > a0 ? (a1 - a0 + RT_SI - 1) / RT_SI : 0;
+    const int nwin = (nst + RT_WIN - 1) / RT_WIN;
 
-    const bool lidx = a.idx && a1 - a0 <= TC_IDX;   // chunk's ion list in shared memory
-    if (lidx)
-        for (int t = tid; t < a1 - a0; t += TC_THREADS) sidx[t] = __ldg(a.idx + a0 + t);
     if (tid == 0) {
-        for (int b = 0; b < 2; b++)
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[b])) : "memory");
+        for (int i = 0; i < RT_NIN; i++) {
+            mbar_init(smem_u32(&bar[IN_FULL + i]), 1);
+            mbar_init(smem_u32(&bar[IN_EMPTY + i]), RT_PROD + 1);
+        }
+        for (int b = 0; b < 2; b++) {
+            mbar_init(smem_u32(&bar[A_FULL + b]), RT_PROD);
+            mbar_init(smem_u32(&bar[A_EMPTY + b]), 1);
+            mbar_init(smem_u32(&bar[ACC_FULL + b]), 1);
+            mbar_init(smem_u32(&bar[ACC_EMPTY + b]), 4);
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         *abort_flag = 0;
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(32)
+                     "r"(RT_TMEM_COLS)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -129,156 +245,178 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_rho_tc(RhoTcArgs a) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
 
-    // operand roles: A unit (row r, coefficient pair cp, ion quad jq), B unit (column n, quad)
-    const int r = tid & 31, jq = (tid >> 5) & 3, cp = tid >> 7;
-    const bool rok = row0 + r < a.nrow;
-    KRow R;
-    R.nx = R.ny = R.z0 = R.cnt = R.koff = 0;
-    if (rok) R = a.row[row0 + r];
-    const float fnx = (float)R.nx, fny = (float)R.ny;
-    const int o0 = R.nx, o1 = a.e1 + a.K1 + R.ny;
-    const int mx = 2 * cp * 32 + r, my = mx + 32;
-    const int n = tid & 31;   // B column (threads < 128)
-    int zsrc = 0;   // B column n: float offset in a staged row (x, y: Re E2[z], Re E2[z+1]; z, w: Im)
-    if (n >= 1 && n <= 2 * a.K2) {
-        int z = n <= a.K2 ? n : n - a.K2;
-        zsrc = 4 * (a.ha + 9 * ((z - 1) / 16) + ((z - 1) % 16) / 2) + ((z - 1) & 1) + (n <= a.K2 ? 0 : 2);
-    }
-
-    // staged rows of stage s into stage buffer s % TC_NSTG (16-byte asynchronous copies,
-    // warp w copies rows w, w + 8); one commit group per stage, empty past the last
-    auto issue = [&](int s) {
-        if (s < nstage) {
-            const int t0 = a0 + s * TC_SI, nt = min(TC_SI, a1 - t0);
-            float4 *dst = stg + (s % TC_NSTG) * TC_SI * cw;
-            for (int j = warp; j < nt; j += TC_THREADS / 32) {
-                int ion = lidx ? sidx[t0 - a0 + j] : (a.idx ? __ldg(a.idx + t0 + j) : t0 + j);
-                const float4 *src = (const float4 *)(a.tab + (size_t)ion * a.tab_w);
-                for (int u = lane; u < cw; u += 32) cp_async16_tc(dst + j * cw + u, src + (u < a.ha ? u : u + a.skip));
-            }
-            if (tid < nt) cp_async16_tc(stq + (s % TC_NSTG) * TC_SI + tid, a.qm + t0 + tid);
-        }
-        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    auto fail = [&]() {
+        if (!*abort_flag) atomicOr(a.status, (unsigned)ST_TC_TIMEOUT);
+        *abort_flag = 1;
+    };
+    // a bounded wait that gives up at once when another warp has already given up
+    auto wait = [&](int i, int parity) -> bool {
+        const uint32_t ba = smem_u32(&bar[i]);
+        if (mbar_test(ba, (uint32_t)parity)) return true;
+        if (*abort_flag) return false;
+        if (mbar_wait(ba, (uint32_t)parity)) return true;
+        fail();
+        return false;
     };
 
-    const uint32_t idesc = idesc_tf32(TC_M, TC_N);
-    int done_win = 0, last = -1;
-    for (int s = 0; s < TC_NSTG - 1; s++) issue(s);
-    for (int s = 0; s < nstage; s++) {
-        const int buf = s & 1;
-        asm volatile("cp.async.wait_group %0;\n" ::"n"(TC_NSTG - 2) : "memory");   // stage s has landed
-        if (tid == TC_ISSUER && s >= 2 && !mbar_wait(smem_u32(&mbar[buf]), ((s - 2) >> 1) & 1)) *abort_flag = 1;
-        __syncthreads();
-        if (*abort_flag) break;
-        issue(s + TC_NSTG - 1);   // into the buffer that stage s - 1 read
-        const int t0 = a0 + s * TC_SI;
-        const float4 *cur = stg + (s % TC_NSTG) * TC_SI * cw;
-        const float4 *cq = stq + (s % TC_NSTG) * TC_SI;
-        unsigned char *A = op + buf * TC_OP_BYTES, *B = A + TC_A_BYTES;
-        {
-            // A: coefficients of 4 ions for one row and one coefficient pair
-            float xv[4], yv[4];
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                const int jj = jq * 4 + j;
-                xv[j] = yv[j] = 0.f;
-                if (rok && t0 + jj < a1) {
-                    const float2 *Rw = (const float2 *)(cur + jj * cw);
-                    const float2 e0 = Rw[o0], e1 = Rw[o1];
-                    const float bx = e0.x * e1.x - e0.y * e1.y, by = e0.x * e1.y + e0.y * e1.x;
-                    const float4 qm = cq[jj];
-                    if (cp == 0) {
-                        const float c0 = fnx * qm.y + fny * qm.z;
-                        xv[j] = qm.x * bx - c0 * by;
-                        yv[j] = qm.x * by + c0 * bx;
-                    } else {
-                        xv[j] = -qm.w * by;
-                        yv[j] = qm.w * bx;
-                    }
-                }
+    if (warp == RT_COPY) {
+        // ------------------------------------------------ copies (lane 0)
+        if (lane == 0) {
+            int issued = 0;
+            for (int s = 0; s < nst; s++) {
+                const int slot = s % RT_NIN, u = s / RT_NIN;
+                if (u > 0 && !wait(IN_EMPTY + slot, (u - 1) & 1)) break;
+                if (*abort_flag) break;
+                const int st = (a0 + s * RT_SI) / RT_SI;
+                const uint32_t bf = smem_u32(&bar[IN_FULL + slot]);
+                mbar_expect_tx(bf, ebytes + RT_Q_BYTES + RT_B_BYTES);
+                bulk_g2s(smem_u32(sE + slot * ebytes), a.etab + (size_t)st * (ebytes / 16), ebytes, bf);
+                bulk_g2s(smem_u32(sQ + slot * RT_Q_BYTES), a.qm + (size_t)st * RT_SI, RT_Q_BYTES, bf);
+                bulk_g2s(smem_u32(sB + slot * RT_B_BYTES), a.btab + (size_t)st * (RT_B_BYTES / 16), RT_B_BYTES, bf);
+                issued = s + 1;
             }
-            float xh[4], xl[4], yh[4], yl[4];
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                split2(xv[j], xh[j], xl[j]);
-                split2(yv[j], yh[j], yl[j]);
-            }
-#pragma unroll
-            for (int t = 0; t < 3; t++) {   // A terms h h l
-                const int k = t * TC_SI + jq * 4;
-                const float *x = t == 2 ? xl : xh, *y = t == 2 ? yl : yh;
-                *(float4 *)(A + kmaj(mx, k, TC_A_LBO)) = make_float4(x[0], x[1], x[2], x[3]);
-                *(float4 *)(A + kmaj(my, k, TC_A_LBO)) = make_float4(y[0], y[1], y[2], y[3]);
-            }
+            // nothing may land after the CTA is gone: wait (bounded) for what is in flight
+            for (int s = max(0, issued - RT_NIN); s < issued; s++)
+                mbar_wait(smem_u32(&bar[IN_FULL + s % RT_NIN]), (s / RT_NIN) & 1);
         }
-        if (tid < 128) {
-            // B: column n of 4 ions
-            float v[4];
+    } else if (warp == RT_MMA) {
+        // ------------------------------------------------ MMAs (lane 0)
+        if (lane == 0) {
+            const uint32_t idesc = idesc_tf32(RT_M, RT_N);
+            // descriptors of A buffer 0 and input slot 0; the others differ only in the start address
+            const uint64_t dA = smem_desc(smem_u32(sA), RT_A_LBO, 128), dB = smem_desc(smem_u32(sB), RT_B_LBO, 128);
+            int last = -1;
+            for (int s = 0; s < nst; s++) {
+                const int b = s & 1, slot = s % RT_NIN, w = s / RT_WIN, sw = s % RT_WIN;
+                if (sw == 0 && w >= 2 && !wait(ACC_EMPTY + (w & 1), ((w >> 1) - 1) & 1)) break;
+                if (!wait(A_FULL + b, (s >> 1) & 1) || !wait(IN_FULL + slot, (s / RT_NIN) & 1)) break;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t hb = tmem + (uint32_t)((w & 1) * RT_MT * RT_N);
+                mma_stage(hb, hb + RT_N, tmem + RT_SMALL_COL, tmem + RT_SMALL_COL + RT_N,
+                          dA + (uint64_t)(b * (RT_A_BYTES / 16)), dB + (uint64_t)(slot * (RT_B_BYTES / 16)), idesc,
+                          sw != 0 ? 1u : 0u, s != 0 ? 1u : 0u);
+                mma_commit(smem_u32(&bar[A_EMPTY + b]));        // the A buffer is free again
+                mma_commit(smem_u32(&bar[IN_EMPTY + slot]));    // so is the E tile (with 8 arrivals)
+                if (sw == RT_WIN - 1 || s == nst - 1) mma_commit(smem_u32(&bar[ACC_FULL + (w & 1)]));
+                last = s;
+            }
+            // every MMA issued must finish before the tensor memory is freed
+            if (last >= 0) mbar_wait(smem_u32(&bar[A_EMPTY + (last & 1)]), (last >> 1) & 1);
+        }
+    } else if (warp < RT_PROD) {
+        // ------------------------------------------------ A operand (lane = row)
+        const int mt = warp % RT_MT, g = warp / RT_MT;
+        const int rr = row0 + mt * 32 + lane;
+        const bool rok = rr < a.nrow;
+        KRow R;
+        R.nx = R.ny = R.z0 = R.cnt = R.koff = 0;
+        if (rok) R = a.row[rr];
+        const float fnx = (float)R.nx, fny = (float)R.ny;
+        const int o0 = R.nx, o1 = a.e1 + a.K1 + R.ny;
+        for (int s = 0; s < nst; s++) {
+            const int b = s & 1, slot = s % RT_NIN;
+            if (!__all_sync(0xffffffffu, wait(IN_FULL + slot, (s / RT_NIN) & 1))) break;
+            const int t0 = a0 + s * RT_SI;
+            const float2 *E = (const float2 *)(sE + slot * ebytes);
+            const float4 *Q = (const float4 *)(sQ + slot * RT_Q_BYTES);
+            float h[4][4], l[4][4];   // [coefficient][ion]
 #pragma unroll
             for (int j = 0; j < 4; j++) {
-                const int jj = jq * 4 + j;
-                v[j] = 0.f;
-                if (t0 + jj < a1) {
-                    if (n == 0) {
-                        v[j] = 1.f;
-                    } else if (n <= 2 * a.K2) {
-                        v[j] = ((const float *)(cur + jj * cw))[zsrc];
-                    }
-                }
+                const int jj = g * 4 + j;
+                const bool on = rok && t0 + jj < a1;
+                const float2 e0 = E[jj * a.lz + o0], e1 = E[jj * a.lz + o1];
+                const float4 qm = Q[jj];
+                const float bx = e0.x * e1.x - e0.y * e1.y, by = e0.x * e1.y + e0.y * e1.x;
+                const float c0 = fnx * qm.y + fny * qm.z;
+                const float v0 = qm.x * bx - c0 * by, v1 = qm.x * by + c0 * bx;
+                const float v2 = -qm.w * by, v3 = qm.w * bx;
+                split2(on ? v0 : 0.f, h[0][j], l[0][j]);
+                split2(on ? v1 : 0.f, h[1][j], l[1][j]);
+                split2(on ? v2 : 0.f, h[2][j], l[2][j]);
+                split2(on ? v3 : 0.f, h[3][j], l[3][j]);
             }
-            float h[4], l[4];
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&bar[IN_EMPTY + slot]));   // E rows and qm read
+            // the A buffer of stage s - 2 must have been consumed by its MMAs (the values
+            // above are formed while those run)
+            if (!__all_sync(0xffffffffu, s < 2 || wait(A_EMPTY + b, ((s >> 1) - 1) & 1))) break;
+            unsigned char *A = sA + b * RT_A_BYTES + mt * RT_A_TILE;
 #pragma unroll
-            for (int j = 0; j < 4; j++) split2(v[j], h[j], l[j]);
-#pragma unroll
-            for (int t = 0; t < 3; t++) {   // B terms h l h
-                const int k = t * TC_SI + jq * 4;
-                const float *w = t == 1 ? l : h;
-                *(float4 *)(B + kmaj(n, k, TC_B_LBO)) = make_float4(w[0], w[1], w[2], w[3]);
+            for (int c = 0; c < 4; c++) {
+                *(float4 *)(A + kmaj(c * 32 + lane, g * 4, RT_A_LBO)) = make_float4(h[c][0], h[c][1], h[c][2], h[c][3]);
+                *(float4 *)(A + kmaj(c * 32 + lane, RT_SI + g * 4, RT_A_LBO)) =
+                    make_float4(l[c][0], l[c][1], l[c][2], l[c][3]);
             }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&bar[A_FULL + b]));
         }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        const bool first = s % a.win == 0, end = s % a.win == a.win - 1 || s == nstage - 1;
-        if (tid == TC_ISSUER) {
+    } else {
+        // ------------------------------------------------ read-back (warps 10-13)
+        const int qd = warp & 3;
+        const uint32_t lanebase = tmem + ((uint32_t)(qd * 32) << 16);
+        for (int w = 0; w < nwin; w++) {
+            const int b = w & 1;
+            if (!__all_sync(0xffffffffu, wait(ACC_FULL + b, (w >> 1) & 1))) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t ab = smem_u32(A), bb = smem_u32(B);
 #pragma unroll
-            for (int q = 0; q < TC_KS / 8; q++) {
-                uint64_t da = smem_desc(ab + 2 * q * TC_A_LBO, TC_A_LBO, 128);
-                uint64_t db = smem_desc(bb + 2 * q * TC_B_LBO, TC_B_LBO, 128);
-                mma_tf32(tmem, da, db, idesc, (first && q == 0) ? 0u : 1u);
+            for (int mt = 0; mt < RT_MT; mt++) {
+#pragma unroll
+                for (int c8 = 0; c8 < RT_N / 8; c8++) {
+                    float v[8], s[8];
+                    tmem_ld8(lanebase + (uint32_t)((b * RT_MT + mt) * RT_N + 8 * c8), v);
+                    const uint32_t ra = lanebase + RT_RUN_COL + (uint32_t)(mt * RT_N + 8 * c8);
+                    if (w > 0) tmem_ld8(ra, s);
+                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                    for (int k = 0; k < 8; k++) s[k] = w > 0 ? s[k] + v[k] : v[k];
+                    tmem_st8(ra, s);
+                }
             }
-            mma_commit(smem_u32(&mbar[buf]));
+            asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&bar[ACC_EMPTY + b]));   // the window's columns are read
         }
-        last = s;
-        if (!end) continue;
-        // ------------------------------------------------ window end: read back, combine
-        if (tid == TC_ISSUER && !mbar_wait(smem_u32(&mbar[buf]), (s >> 1) & 1)) *abort_flag = 1;
-        __syncthreads();
-        if (*abort_flag) break;
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        {
-            const int qd = warp & 3, ch = warp >> 2;
-            float v[16];
-            const uint32_t base = tmem + ((uint32_t)(qd * 32) << 16) + (uint32_t)(ch * 16);
-            tmem_ld8(base, v);
-            tmem_ld8(base + 8, v + 8);
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            float *xr = X + (qd * 32 + lane) * TC_XS + ch * 16;
+        // every window read (or the pass abandoned): the A buffers are free for the sums
+        asm volatile("bar.sync 1, 128;" ::: "memory");
+        const bool done = !*abort_flag;
+        float *X = (float *)sA;   // [RT_MT][RT_M][RT_XS]
+        if (done) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
-            for (int c = 0; c < 16; c++) xr[c] = v[c];
+            for (int mt = 0; mt < RT_MT; mt++) {
+                float *xr = X + ((size_t)mt * RT_M + qd * 32 + lane) * RT_XS;
+#pragma unroll
+                for (int c8 = 0; c8 < RT_N / 8; c8++) {
+                    float s[8], v[8];
+                    if (nwin > 0) {
+                        tmem_ld8(lanebase + RT_RUN_COL + (uint32_t)(mt * RT_N + 8 * c8), s);
+                        tmem_ld8(lanebase + RT_SMALL_COL + (uint32_t)(mt * RT_N + 8 * c8), v);
+                        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                        for (int k = 0; k < 8; k++) s[k] += v[k];
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < 8; k++) s[k] = 0.f;
+                    }
+#pragma unroll
+                    for (int k = 0; k < 8; k++) xr[8 * c8 + k] = s[k];
+                }
+            }
         }
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads();
-        {
-            float2 *P0 = a.part + ((size_t)blockIdx.y * a.nwin + done_win) * a.nk;
-            // item it: row it & 31 (= r, TC_THREADS being a multiple of 32), nz = it >> 5
-            for (int it = tid; it < TC_ROWS * (a.K2 + 1) && rok; it += TC_THREADS) {
-                const int rr = r, z = it >> 5;
+        asm volatile("bar.sync 1, 128;" ::: "memory");
+        if (done) {
+            // item it: row it % RT_ROWS of the CTA, nz = it / RT_ROWS
+            const int et = tid - 32 * RT_EPI0;
+            for (int it = et; it < RT_ROWS * (a.K2 + 1); it += 128) {
+                const int rl = it % RT_ROWS, z = it / RT_ROWS;
+                if (row0 + rl >= a.nrow) continue;
+                const KRow R = a.row[row0 + rl];
                 const bool full = R.z0 <= 0;
-                float2 *P = P0 + (R.koff - R.z0);
-                const float *x0 = X + rr * TC_XS, *x1 = X + (32 + rr) * TC_XS;
-                const float *x2 = X + (64 + rr) * TC_XS, *x3 = X + (96 + rr) * TC_XS;
+                float2 *P = a.part + (size_t)blockIdx.y * a.nk + (R.koff - R.z0);
+                const float *xb = X + ((size_t)(rl / 32) * RT_M + rl % 32) * RT_XS;
+                const float *x0 = xb, *x1 = xb + 32 * RT_XS, *x2 = xb + 64 * RT_XS, *x3 = xb + 96 * RT_XS;
                 if (z == 0) {
                     if (full) P[0] = make_float2(x0[0], x1[0]);
                     continue;
@@ -291,85 +429,77 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_rho_tc(RhoTcArgs a) {
                 if (full) P[-z] = make_float2(sa + sb - fz * (ta + tb), sd - sc + fz * (tc - td));
             }
         }
-        done_win++;
     }
-    const bool aborted = *abort_flag != 0;
-    if (!aborted) {
-        // windows of this chunk without ions: zero partials
-        for (; done_win < a.nwin; done_win++) {
-            float2 *P0 = a.part + ((size_t)blockIdx.y * a.nwin + done_win) * a.nk;
-            for (int it = tid; it < TC_ROWS * (a.K2 + 1) && rok; it += TC_THREADS) {
-                const int z = it >> 5;
-                const bool full = R.z0 <= 0;
-                float2 *P = P0 + (R.koff - R.z0);
-                if (z == 0) {
-                    if (full) P[0] = make_float2(0.f, 0.f);
-                    continue;
-                }
-                P[z] = make_float2(0.f, 0.f);
-                if (full) P[-z] = make_float2(0.f, 0.f);
-            }
-        }
-    } else {
-        if (tid == TC_ISSUER) {
-            atomicOr(a.status, (unsigned)ST_TC_TIMEOUT);
-            // the last committed stage covers every MMA issued before it
-            if (last >= 0) mbar_wait(smem_u32(&mbar[last & 1]), (last >> 1) & 1);
-        }
-    }
-    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(32) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(RT_TMEM_COLS) : "memory");
     }
 }
 
-static size_t rho_tc_smem(int cw) {
-    return 2 * (size_t)TC_OP_BYTES + sizeof(float4) * (TC_NSTG * TC_SI * (size_t)cw + TC_NSTG * TC_SI) +
-           sizeof(float) * TC_M * TC_XS + sizeof(int) * TC_IDX + 2 * sizeof(uint64_t) + 16;
+// ---------------------------------------------------------------- host side
+static int rt_npad(const Engine &e) { return ceil_div(e.n, RT_SI) * RT_SI; }
+
+// buffers of the pass (at set-up: nothing may be allocated while steps are recorded);
+// lz: float2 entries of a phase-table row's E0 | E1 prefix (even)
+void setup_rho_tc(Engine &e, int lz) {
+    if (e.d_rho_btab || e.kmax[2] > RT_MAXK2 || rt_smem(lz).total > 227 * 1024) return;
+    const int npad = rt_npad(e);
+    e.rho_tc_lz = lz;
+    e.d_rho_btab = dalloc<float4>((size_t)(npad / RT_SI) * (RT_B_BYTES / 16));
+    e.d_rho_etab = dalloc<float4>((size_t)npad * (lz / 2));
+    e.d_qm_tc = dalloc<float4>(npad);
 }
 
-// rho(k) partials of `cnt` ions (idx: subset) into e.d_rho_part32 on the tensor cores;
-// returns false (nothing launched) when the k box is outside the kernel's range.
+void launch_rho_tc_tables(Engine &e) {
+    if (!e.d_rho_btab) return;
+    const int npad = rt_npad(e), lz = e.rho_tc_lz;
+    const long long tot = (long long)npad * (lz / 2 + RT_N);
+    MDFF_LAUNCH(e, k_rho_tc_tables, (unsigned)((tot + 255) / 256), 256, 0, e.n, npad, lz, e.tab_w, e.kmax[2], e.cell,
+                e.d_r, e.d_ion_order, (const float4 *)e.d_tab32, e.d_rho_etab, (float *)e.d_rho_btab);
+}
+
+// ions per chunk of a pass over `cnt` ions: a whole number of stages; by default two
+// resident CTAs per SM over the row tiles; never more chunks than the partial buffer holds
+static int rho_tc_chunk(const Engine &e, int cnt) {
+    const int tiles = ceil_div(e.nrow, RT_ROWS), stages = ceil_div(std::max(cnt, 1), RT_SI);
+    int c = e.rho_tc_chunks_set > 0 ? e.rho_tc_chunks_set : std::max(1, 2 * e.nsm / tiles);
+    c = std::max(1, std::min(c, std::min(stages, e.rho32_chunks_max)));
+    return ceil_div(stages, c) * RT_SI;
+}
+
+// rho(k) partials of positions 0..cnt-1 of the order (every ion, or the polarisable
+// ones) into e.d_rho_part32; false (nothing launched) for any other ion subset
 bool launch_rho_tc(Engine &e, const double *q, const double3 *mu, bool lq, bool ld, const int *idx, int cnt,
-                   int tab_w, int z_off, int nzb_neg, int *chunks_used) {
-    int K2 = e.kmax[2];
-    if (2 * K2 + 1 > TC_N || cnt <= 0) return false;
-    if (!e.d_qm_tc) e.d_qm_tc = dalloc<float4>(e.n);
-    MDFF_LAUNCH(e, k_qm_tc, ceil_div(cnt, 256), 256, 0, cnt, idx, e.cell, q, mu, lq ? 1 : 0, ld ? 1 : 0, e.d_qm_tc);
+                   int z_off, int *chunks_used) {
+    if (!e.d_rho_btab || cnt <= 0 || z_off != e.rho_tc_lz) return false;
+    if (!(idx == nullptr && cnt == e.n) && !(idx == e.d_pidx && cnt == e.npol)) return false;
+    MDFF_LAUNCH(e, k_qm_tc, ceil_div(cnt, 256), 256, 0, cnt, e.d_ion_order, e.cell, q, mu, lq ? 1 : 0, ld ? 1 : 0,
+                e.d_qm_tc);
     RhoTcArgs a;
     a.cnt = cnt;
+    a.chunk = rho_tc_chunk(e, cnt);
+    const int chunks = ceil_div(cnt, a.chunk);
     a.nrow = e.nrow;
     a.nk = e.nk;
-    a.K2 = K2;
-    a.tab_w = tab_w;
-    a.ha = z_off / 2;
-    a.skip = 9 * nzb_neg;
-    a.cw = tab_w / 2 - a.skip;
-    a.e1 = e.kmax[0] + 1;
+    a.K2 = e.kmax[2];
     a.K1 = e.kmax[1];
-    a.idx = idx;
-    a.tab = e.d_tab32;
+    a.e1 = e.kmax[0] + 1;
+    a.lz = e.rho_tc_lz;
+    a.etab = e.d_rho_etab;
+    a.btab = e.d_rho_btab;
     a.qm = e.d_qm_tc;
     a.row = e.d_row;
     a.part = e.d_rho_part32;
     a.status = e.d_status;
-    // two CTAs per SM; chunk partials (ion chunks x windows) within the partial buffer
-    int mtiles = ceil_div(e.nrow, TC_ROWS);
-    int chunks = std::max(1, std::min(2 * e.nsm / mtiles, ceil_div(cnt, TC_SI)));
-    a.chunk = ceil_div(ceil_div(cnt, chunks), TC_SI) * TC_SI;
-    chunks = ceil_div(cnt, a.chunk);
-    int stages = a.chunk / TC_SI;
-    int wmax = std::max(1, e.rho32_chunks_max / chunks);
-    a.win = std::min(stages, std::max(TC_WIN, ceil_div(stages, wmax)));
-    a.nwin = ceil_div(stages, a.win);
-    if (chunks * a.nwin > e.rho32_chunks_max) return false;
-    size_t smem = rho_tc_smem(a.cw);
-    MDFF_CK(cudaFuncSetAttribute(k_rho_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    MDFF_LAUNCH(e, k_rho_tc, dim3(mtiles, chunks), TC_THREADS, smem, a);
-    *chunks_used = chunks * a.nwin;
+    // the largest request once per process (the attribute call is not recorded in graphs)
+    static std::once_flag once;
+    std::call_once(once, [] {
+        MDFF_CK(cudaFuncSetAttribute(k_rho_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    });
+    MDFF_LAUNCH(e, k_rho_tc, dim3(ceil_div(e.nrow, RT_ROWS), chunks), RT_THREADS, rt_smem(a.lz).total, a);
+    *chunks_used = chunks;
     return true;
 }
 

@@ -33,8 +33,23 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
     return ok != 0;
 }
 
+// non-blocking test of the phase
+__device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
 // polls until the phase completes or TC_WAIT_CYCLES SM clock cycles (about a second) pass
+// (a phase already complete returns after one test, without reading the clock)
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    if (mbar_test(bar, parity)) return true;
     const long long t0 = clock64();
     while (!mbar_try(bar, parity))
         if (clock64() - t0 > TC_WAIT_CYCLES) return false;

@@ -303,11 +303,11 @@ class Engine:
     def tune_launch(self, reps: int = 10) -> dict:
         """Time the mixed k-space launch shapes on this system and keep the fastest
         (mdffgpu_tune_launch)."""
-        ch = np.zeros(3, np.int32)
+        ch = np.zeros(4, np.int32)
         ms = C.c_double(0.0)
         self._check(self.L.mdffgpu_tune_launch(self.h, reps, _ip(ch), C.byref(ms)))
-        return {"tensor_core_ion_pass": bool(ch[0]), "rho_chunks": int(ch[1]), "ion_tc_slices": int(ch[2]),
-                "field_pass_ms": ms.value}
+        return {"tensor_core_rho_pass": bool(ch[3]), "tensor_core_ion_pass": bool(ch[0]), "rho_chunks": int(ch[1]),
+                "ion_tc_slices": int(ch[2]), "field_pass_ms": ms.value}
 
     def set_graph(self, on: bool):
         """Replay MD steps as CUDA graphs (default on); off issues every kernel."""
