@@ -17,9 +17,9 @@ set of 512 configurations (427k ions); metric config-gradients/s.
 
 ours      : state resident on the GPU; each timed step is bracketed by CUDA events on
             the engine stream, with a 256 MB L2 flush between steps (not timed).
-            `e2e` repeats the measurement through the C ABI with host buffers:
-            positions and velocities uploaded, one step, positions, velocities and
-            forces downloaded, every step.
+            `e2e` repeats the measurement through the C ABI with page-locked host
+            arrays in the reference's per-component layout: positions and velocities
+            uploaded, one step, positions, velocities and forces downloaded, every step.
 reference : the reference's own CPU code (oracle/_ref, -O3 -Ofast -fopenmp) on all host
             cores, on a bounded sample of steps of the same system.
 N > 1 GPUs: one process per GPU (torchrun).  MD: an independent replica per rank (the
@@ -388,13 +388,19 @@ def md_drift(s, pos, dev: int, nsteps: int) -> dict:
         h = th[:, 0] + th[:, 1] + th[:, 2] + th[:, 3] + th[:, 4] + th[:, 5]
         t = np.arange(len(h), dtype=float)
         slope = float(np.polyfit(t, h, 1)[0])
+        fluct = float(np.std(h - np.polyval(np.polyfit(t, h, 1), t))) / s.nion
         out[label] = {"ev_per_ion_per_step": (float(h[-1]) - float(h[0])) / (s.nion * (len(h) - 1)),
                       "fit_slope_ev_per_ion_per_step": slope / s.nion,
-                      "h_rms_fluct_ev_per_ion": float(np.std(h - np.polyval(np.polyfit(t, h, 1), t))) / s.nion,
+                      # the slope a residual of this size gives when it is correlated over
+                      # the whole window, sqrt(12) sigma / T: the scale below which fitted
+                      # slopes of two decorrelated trajectories cannot be told apart
+                      "fit_slope_noise_ev_per_ion_per_step": float(np.sqrt(12.0)) * fluct / len(h),
+                      "h_rms_fluct_ev_per_ion": fluct,
                       "h_start_ev": float(h[0]), "h_end_ev": float(h[-1]),
                       "scf_iter_mean": float(th[:, 10].mean()), "finite": bool(np.isfinite(th).all())}
-    out["ratio_mixed_over_fp64"] = (out["mixed"]["fit_slope_ev_per_ion_per_step"]
-                                    / out["fp64"]["fit_slope_ev_per_ion_per_step"])
+    # end-to-end drift ratio (a ratio of fitted slopes divides by a slope near zero once
+    # the two trajectories have decorrelated)
+    out["ratio_mixed_over_fp64"] = out["mixed"]["ev_per_ion_per_step"] / out["fp64"]["ev_per_ion_per_step"]
     return out
 
 
@@ -563,10 +569,11 @@ def run_ours(args):
         fp64_fused = fp64_arm(PIM_CG_FUSED, "fused")
 
     # ------------------------------------------------ end to end through the C ABI
+    # page-locked host arrays in the reference's per-component layout (rx[], ry[], ...):
+    # positions and velocities in, positions, velocities and forces out, every step
     nE = max(1, args.e2e_steps)
-    r, v, f = eng.state()
-    r = np.ascontiguousarray(r)
-    v = np.ascontiguousarray(v)
+    host = [torch.empty(s.nion, dtype=torch.float64).pin_memory().numpy() for _ in range(9)]
+    eng.state_soa(*host)
     e_evs = _events(nE)
     if pg is not None:
         pg.barrier()
@@ -575,10 +582,10 @@ def run_ours(args):
         with torch.cuda.stream(stream):
             flush.zero_()
         e_evs[k][0].record(stream)
-        eng.set_positions(r)
-        eng.set_velocities(v)
+        eng.set_positions_soa(*host[0:3])
+        eng.set_velocities_soa(*host[3:6])
         eng.md_steps(istep, 1)
-        r, v, f = eng.state()
+        eng.state_soa(*host)
         e_evs[k][1].record(stream)
         istep += 1
     torch.cuda.synchronize()

@@ -45,6 +45,10 @@ void download(Engine &e, void *dst, const void *src, size_t bytes) {
 
 }  // namespace
 
+// ions from which the mixed k space runs on the tensor cores by default (the batched fit's
+// configurations of 96 to 1536 ions evaluate faster on the CUDA-core passes)
+constexpr int TC_MIN_IONS = 4096;
+
 struct mdffgpu_fit_plan {
     std::vector<mdffgpu_ctx *> ctx;
     int tSi = 0, tO = 0, device = 0;
@@ -127,15 +131,18 @@ int mdffgpu_set_precision(mdffgpu_ctx *ctx, int precision) {
         e.precision = precision;
         e.use32 = (precision == MDFFGPU_MIXED);
         e.gen++;
-        e.real32 = e.rec32 = e.subset32 = true;
+        e.real32 = e.rec32 = e.subset32 = e.sr32 = true;
         if (const char *v = getenv("MDFFGPU_MIXED_PARTS")) {
             e.real32 = strstr(v, "real") != nullptr;
             e.rec32 = strstr(v, "rec") != nullptr;
+            e.sr32 = strstr(v, "sr") != nullptr;
         }
         if (const char *v = getenv("MDFFGPU_PIM_SUBSET")) e.subset32 = atoi(v) != 0;
-        e.rho_tc = true;    // the rho pass on the tensor cores (kspace_tc.cu); MDFFGPU_RHO_TC=0: CUDA cores
+        // the rho and ion passes on the tensor cores (kspace_tc.cu, kspace_ion_tc.cu) from
+        // TC_MIN_IONS ions on; below, where a pass is a few microseconds, the CUDA-core passes
+        // (fewer kernels per pass).  MDFFGPU_RHO_TC / MDFFGPU_ION_TC = 0 / 1 override.
+        e.rho_tc = e.ion_tc = e.n >= TC_MIN_IONS;
         if (const char *v = getenv("MDFFGPU_RHO_TC")) e.rho_tc = atoi(v) != 0;
-        e.ion_tc = true;    // the ion pass on the tensor cores (kspace_ion_tc.cu); MDFFGPU_ION_TC=0: CUDA cores
         if (const char *v = getenv("MDFFGPU_ION_TC")) e.ion_tc = atoi(v) != 0;
     });
 }

@@ -150,7 +150,7 @@ Engine::Engine(const mdffgpu_params &prm, int dev) : p(prm) {
     d_out = dalloc<DevScalars>(1);
     d_nhc = dalloc<double>(48);
     MDFF_CK(cudaMallocHost((void **)&h_out, sizeof(DevScalars)));
-    MDFF_CK(cudaMallocHost((void **)&h_stage, sizeof(double) * 10 * (size_t)n));
+    d_soa = dalloc<double>(9 * (size_t)n);
     memset(h_out, 0, sizeof(DevScalars));
     if (p.lcoulombic) setup_kspace();
     int nkb = nk > 0 ? ceil_div(nk, RHOR_K) : 1;
@@ -221,7 +221,7 @@ Engine::~Engine() {
     cudaFree(d_status);
     cudaFree(d_ticket);
     if (h_out) cudaFreeHost(h_out);
-    if (h_stage) cudaFreeHost(h_stage);
+    cudaFree(d_soa);
     if (step_exec) cudaGraphExecDestroy(step_exec);
     if (fit_exec) cudaGraphExecDestroy(fit_exec);
     if (body_stream) cudaStreamDestroy(body_stream);
@@ -599,42 +599,57 @@ void Engine::alloc_lists(int cnb, int cco) {
 }
 
 // ---------------------------------------------------------------- state
-// host<->device transfers go through one pinned staging block h_stage (10 doubles/ion)
+// host<->device transfers of the reference's per-component arrays (rx[], ry[], ... ):
+// one copy per array into (or out of) the device block d_soa, packed into (unpacked from)
+// the engine's double4 / double3 arrays by a kernel.  From page-locked host arrays the
+// copies are direct DMA; each call returns once its copies are done.
+__global__ void k_pack_r(int n, const double *__restrict__ soa, const double *__restrict__ q, double4 *__restrict__ r) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) r[i] = make_double4(soa[i], soa[n + i], soa[2 * (size_t)n + i], q[i]);
+}
+__global__ void k_pack_v(int n, const double *__restrict__ soa, double3 *__restrict__ v) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = make_double3(soa[3 * (size_t)n + i], soa[4 * (size_t)n + i], soa[5 * (size_t)n + i]);
+}
+__global__ void k_unpack_state(int n, const double4 *__restrict__ r, const double3 *__restrict__ v,
+                               const double3 *__restrict__ f, double *__restrict__ soa) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double4 a = r[i];
+    const double3 b = v[i], c = f[i];
+    const double x[9] = {a.x, a.y, a.z, b.x, b.y, b.z, c.x, c.y, c.z};
+#pragma unroll
+    for (int k = 0; k < 9; k++) soa[(size_t)k * n + i] = x[k];
+}
+
 void Engine::set_positions(const double *rx, const double *ry, const double *rz) {
-    double4 *r4 = (double4 *)h_stage;
-    for (int i = 0; i < n; i++) r4[i] = make_double4(rx[i], ry[i], rz[i], h_q[i]);
-    MDFF_CK(cudaMemcpyAsync(d_r, r4, sizeof(double4) * n, cudaMemcpyHostToDevice, stream));
+    const double *src[3] = {rx, ry, rz};
+    for (int k = 0; k < 3; k++)
+        MDFF_CK(cudaMemcpyAsync(d_soa + (size_t)k * n, src[k], sizeof(double) * n, cudaMemcpyHostToDevice, stream));
+    MDFF_LAUNCH(*this, k_pack_r, ceil_div(n, 256), 256, 0, n, d_soa, d_q, d_r);
     MDFF_CK(cudaStreamSynchronize(stream));
     if (!p.lverletL) list_ready = false;
 }
 
 void Engine::set_velocities(const double *vx, const double *vy, const double *vz) {
-    double3 *v = (double3 *)(h_stage + 4 * (size_t)n);
-    for (int i = 0; i < n; i++) v[i] = make_double3(vx ? vx[i] : 0.0, vy ? vy[i] : 0.0, vz ? vz[i] : 0.0);
-    MDFF_CK(cudaMemcpyAsync(d_v, v, sizeof(double3) * n, cudaMemcpyHostToDevice, stream));
+    const double *src[3] = {vx, vy, vz};
+    for (int k = 0; k < 3; k++) {
+        double *dst = d_soa + (size_t)(3 + k) * n;
+        if (src[k]) MDFF_CK(cudaMemcpyAsync(dst, src[k], sizeof(double) * n, cudaMemcpyHostToDevice, stream));
+        else MDFF_CK(cudaMemsetAsync(dst, 0, sizeof(double) * n, stream));
+    }
+    MDFF_LAUNCH(*this, k_pack_v, ceil_div(n, 256), 256, 0, n, d_soa, d_v);
     MDFF_CK(cudaStreamSynchronize(stream));
 }
 
 void Engine::get_state(double *rx, double *ry, double *rz, double *vx, double *vy, double *vz, double *fx,
                        double *fy, double *fz) {
-    double4 *r = (double4 *)h_stage;
-    double3 *v = (double3 *)(h_stage + 4 * (size_t)n);
-    double3 *f = (double3 *)(h_stage + 7 * (size_t)n);
-    if (rx || ry || rz) MDFF_CK(cudaMemcpyAsync(r, d_r, sizeof(double4) * n, cudaMemcpyDeviceToHost, stream));
-    if (vx || vy || vz) MDFF_CK(cudaMemcpyAsync(v, d_v, sizeof(double3) * n, cudaMemcpyDeviceToHost, stream));
-    if (fx || fy || fz) MDFF_CK(cudaMemcpyAsync(f, d_f, sizeof(double3) * n, cudaMemcpyDeviceToHost, stream));
+    MDFF_LAUNCH(*this, k_unpack_state, ceil_div(n, 256), 256, 0, n, d_r, d_v, d_f, d_soa);
+    double *dst[9] = {rx, ry, rz, vx, vy, vz, fx, fy, fz};
+    for (int k = 0; k < 9; k++)
+        if (dst[k])
+            MDFF_CK(cudaMemcpyAsync(dst[k], d_soa + (size_t)k * n, sizeof(double) * n, cudaMemcpyDeviceToHost, stream));
     MDFF_CK(cudaStreamSynchronize(stream));
-    for (int i = 0; i < n; i++) {
-        if (rx) rx[i] = r[i].x;
-        if (ry) ry[i] = r[i].y;
-        if (rz) rz[i] = r[i].z;
-        if (vx) vx[i] = v[i].x;
-        if (vy) vy[i] = v[i].y;
-        if (vz) vz[i] = v[i].z;
-        if (fx) fx[i] = f[i].x;
-        if (fy) fy[i] = f[i].y;
-        if (fz) fz[i] = f[i].z;
-    }
 }
 
 void Engine::sync_scalars() {

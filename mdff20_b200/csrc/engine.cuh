@@ -192,7 +192,7 @@ struct Engine {
     // ---- host copies of per-ion constants
     std::vector<int> h_typ;
     std::vector<double> h_q;
-    double *h_stage = nullptr;   // pinned staging for state transfers, 10 doubles per ion
+    double *d_soa = nullptr;     // per-component state arrays of host transfers, 9 doubles per ion
     // ---- device per-ion arrays
     double4 *d_r = nullptr;      // Cartesian x y z, w = charge
     double4 *d_s = nullptr;      // fractional (kardir) x y z, w = charge
@@ -221,9 +221,10 @@ struct Engine {
     int *d_nb = nullptr, *d_nbn = nullptr, *d_co = nullptr, *d_con = nullptr;
     double2 *d_coef = nullptr;   // [n][cap_co] cached dipole-field pair factors
     bool use32 = false;          // mixed precision: FP32 Ewald kernels
-    // parts of the mixed path (all on by default; MDFFGPU_MIXED_PARTS=real|rec keeps
-    // only that part in FP32, MDFFGPU_PIM_SUBSET=0 runs the CG field over all ions)
-    bool real32 = true, rec32 = true, subset32 = true;
+    // parts of the mixed path (all on by default; MDFFGPU_MIXED_PARTS=real|rec|sr keeps
+    // only the named parts in FP32 -- real-space Ewald, k space, short-range pairs --,
+    // MDFFGPU_PIM_SUBSET=0 runs the CG field over all ions)
+    bool real32 = true, rec32 = true, subset32 = true, sr32 = true;
     // mixed-precision real space (real32.cu), sized like the Coulomb list
     int *d_nl32 = nullptr, *d_nln32 = nullptr;   // in-cutoff neighbours [n][cap32]
     int *d_pl32 = nullptr, *d_pln32 = nullptr;   // polarisable neighbours of polarisable ions

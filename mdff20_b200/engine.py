@@ -270,6 +270,12 @@ def _ip(a):
     return a.ctypes.data_as(C.POINTER(C.c_int)) if a is not None else None
 
 
+def _soa_arg(x, n):
+    if not (isinstance(x, np.ndarray) and x.dtype == np.float64 and x.flags.c_contiguous and x.size == n):
+        raise ValueError("per-component arrays must be contiguous float64 of length n")
+    return x
+
+
 def _soa(x):
     x = np.ascontiguousarray(x, float)
     return (np.ascontiguousarray(x[:, 0]), np.ascontiguousarray(x[:, 1]), np.ascontiguousarray(x[:, 2]))
@@ -342,6 +348,20 @@ class Engine:
         a = [np.zeros(self.n) for _ in range(9)]
         self._check(self.L.mdffgpu_get_state(self.h, *[_dp(x) for x in a]))
         return np.stack(a[0:3], 1), np.stack(a[3:6], 1), np.stack(a[6:9], 1)
+
+    # the reference's per-component arrays as they are (contiguous float64 of length n,
+    # e.g. page-locked buffers): no conversion on the Python side
+    def set_positions_soa(self, rx, ry, rz):
+        self._check(self.L.mdffgpu_set_positions(self.h, *[_dp(_soa_arg(x, self.n)) for x in (rx, ry, rz)]))
+
+    def set_velocities_soa(self, vx, vy, vz):
+        self._check(self.L.mdffgpu_set_velocities(self.h, *[_dp(_soa_arg(x, self.n)) for x in (vx, vy, vz)]))
+
+    def state_soa(self, *out):
+        """Positions, velocities and forces into nine given arrays (rx .. fz)."""
+        if len(out) != 9:
+            raise ValueError("state_soa takes nine arrays")
+        self._check(self.L.mdffgpu_get_state(self.h, *[_dp(_soa_arg(x, self.n)) for x in out]))
 
     def forces(self):
         return self.state()[2]
