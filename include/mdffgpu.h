@@ -125,7 +125,10 @@ int mdffgpu_tune_launch(mdffgpu_ctx *ctx, int reps, int *choice, double *ms);
  * value); 0: every step is issued kernel by kernel.  Results are the same either way. */
 int mdffgpu_set_graph(mdffgpu_ctx *ctx, int on);
 
-/* State transfer (the reference's rx..fz globals, src/config.h:38-40). */
+/* State transfer (the reference's rx..fz globals, src/config.h:38-40).  One copy per
+ * array, packed / unpacked on the device; each call returns when its copies are done.
+ * Page-locked arrays (cudaHostAlloc) are copied by DMA directly, others through the
+ * driver's staging. */
 int mdffgpu_set_positions(mdffgpu_ctx *ctx, const double *rx, const double *ry, const double *rz);
 int mdffgpu_set_velocities(mdffgpu_ctx *ctx, const double *vx, const double *vy, const double *vz);
 int mdffgpu_get_state(mdffgpu_ctx *ctx, double *rx, double *ry, double *rz, double *vx, double *vy,

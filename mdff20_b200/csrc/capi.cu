@@ -131,11 +131,10 @@ int mdffgpu_set_precision(mdffgpu_ctx *ctx, int precision) {
         e.precision = precision;
         e.use32 = (precision == MDFFGPU_MIXED);
         e.gen++;
-        e.real32 = e.rec32 = e.subset32 = e.sr32 = true;
+        e.real32 = e.rec32 = e.subset32 = true;
         if (const char *v = getenv("MDFFGPU_MIXED_PARTS")) {
             e.real32 = strstr(v, "real") != nullptr;
             e.rec32 = strstr(v, "rec") != nullptr;
-            e.sr32 = strstr(v, "sr") != nullptr;
         }
         if (const char *v = getenv("MDFFGPU_PIM_SUBSET")) e.subset32 = atoi(v) != 0;
         // the rho and ion passes on the tensor cores (kspace_tc.cu, kspace_ion_tc.cu) from

@@ -221,10 +221,9 @@ struct Engine {
     int *d_nb = nullptr, *d_nbn = nullptr, *d_co = nullptr, *d_con = nullptr;
     double2 *d_coef = nullptr;   // [n][cap_co] cached dipole-field pair factors
     bool use32 = false;          // mixed precision: FP32 Ewald kernels
-    // parts of the mixed path (all on by default; MDFFGPU_MIXED_PARTS=real|rec|sr keeps
-    // only the named parts in FP32 -- real-space Ewald, k space, short-range pairs --,
-    // MDFFGPU_PIM_SUBSET=0 runs the CG field over all ions)
-    bool real32 = true, rec32 = true, subset32 = true, sr32 = true;
+    // parts of the mixed path (all on by default; MDFFGPU_MIXED_PARTS=real|rec keeps
+    // only that part in FP32, MDFFGPU_PIM_SUBSET=0 runs the CG field over all ions)
+    bool real32 = true, rec32 = true, subset32 = true;
     // mixed-precision real space (real32.cu), sized like the Coulomb list
     int *d_nl32 = nullptr, *d_nln32 = nullptr;   // in-cutoff neighbours [n][cap32]
     int *d_pl32 = nullptr, *d_pln32 = nullptr;   // polarisable neighbours of polarisable ions
@@ -271,7 +270,7 @@ struct Engine {
     // CG initial guess: polynomial extrapolation through the last extrapolate_order + 1
     // converged dipoles (false: the reference's ASPC coefficients)
     bool cg_poly = true;
-    float4 *d_qm_tc = nullptr;                          // its per-ion (q, 2 pi B mu)
+    float4 *d_qm_tc = nullptr;                          // per position of the order: (q, 2 pi B mu)
     float2 *d_rho_part32 = nullptr;                     // [rho32_chunks][nk]
     int ion32_slices = 0, nsm = 148;                    // most ion-pass slices; SMs
     double *d_ion_part32 = nullptr;                     // [slices][n][6]

@@ -99,40 +99,6 @@ __device__ __forceinline__ void bhm_pair_fast(const PairSR &P, double r2, int da
     w = (P.B * erh - (6.0 * ir6d + 8.0 * ir8d) * id + ir6 * fd6 + ir8 * fd8) * id;
 }
 
-// bhm_pair_fast in FP32 (the mixed path's short-range pairs): the same function and
-// operation order, FP32 arithmetic with expf and the reciprocal square root.  The
-// Tang-Toennies sums 1 - s_n(br) e^{-br} lose relative precision where br is small, but
-// there the damped dispersion is a small part of the pair force.
-__device__ __forceinline__ void bhm_pair32(float A, float B, float C, float D, float BD, float r2, int damped,
-                                           float &u, float &w) {
-    constexpr float E6 = 1.0f / 720.0f, E7 = 1.0f / 5040.0f, E8 = 1.0f / 40320.0f;
-    const float id = rsqrtf(r2), d = r2 * id, ir2 = id * id;
-    const float erh = A * expf(-B * d);
-    float ir6 = ir2 * ir2 * ir2, ir8 = ir6 * ir2;
-    ir6 *= C;
-    ir8 *= D;
-    float f6 = 1.0f, f8 = 1.0f, fd6 = 0.0f, fd8 = 0.0f;
-    if (damped) {
-        const float br = BD * d, ex = expf(-br);
-        float s6 = E6;
-        s6 = s6 * br + 1.0f / 120.0f;
-        s6 = s6 * br + 1.0f / 24.0f;
-        s6 = s6 * br + 1.0f / 6.0f;
-        s6 = s6 * br + 0.5f;
-        s6 = s6 * br + 1.0f;
-        s6 = s6 * br + 1.0f;
-        const float b2 = br * br, b4 = b2 * b2, b6 = b4 * b2;
-        const float s8 = s6 + b6 * br * (E7 + E8 * br);
-        f6 = 1.0f - s6 * ex;
-        f8 = 1.0f - s8 * ex;
-        fd6 = E6 * b6 * ex * BD;
-        fd8 = E8 * (b4 * b4) * ex * BD;
-    }
-    const float ir6d = ir6 * f6, ir8d = ir8 * f8;
-    u = erh - ir6d - ir8d;
-    w = (B * erh - (6.0f * ir6d + 8.0f * ir8d) * id + ir6 * fd6 + ir8 * fd8) * id;
-}
-
 // pair contribution to the per-ion force and to (u, virial): acc = u, Vxx Vxy Vxz Vyy Vyz Vzz
 // as sums over the full list of (r_a f_b + r_b f_a)
 __device__ __forceinline__ void sr_accumulate(double3 r, double u, double w, double &fx, double &fy, double &fz,
