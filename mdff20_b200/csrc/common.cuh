@@ -116,14 +116,14 @@ __device__ __forceinline__ void block_sum_to_part(double (&v)[NV], double *part,
 // exactly as k_reduce_slots does (same order), so the separate reduction launch is not
 // needed; ticket (zero between calls) counts the finished blocks.  The writers of the
 // partials fence their writes before arriving.
-__device__ __forceinline__ void last_block_slots(const double *part, int stride, int first, int nslots,
+__device__ __forceinline__ bool last_block_slots(const double *part, int stride, int first, int nslots,
                                                  double *scal, unsigned *ticket) {
     __shared__ bool last;
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
     __syncthreads();
-    if (!last) return;
+    if (!last) return false;
     __threadfence();
     __shared__ double sh[32];
     for (int sl = first; sl < first + nslots; sl++) {
@@ -141,6 +141,7 @@ __device__ __forceinline__ void last_block_slots(const double *part, int stride,
         __syncthreads();
     }
     if (threadIdx.x == 0) *ticket = 0u;
+    return true;
 }
 
 // Neumaier (compensated) summation for FP32 accumulations in the mixed path

@@ -43,12 +43,11 @@ __global__ void k_cg_ap(int n, const int *polar, const double *invpol, const dou
                         double3 *ap, double *part, int stride, double *scal, unsigned *ticket);
 __global__ void k_cg_rz(int n, const int *polar, const double *pol, const double3 *r, double3 *z, double *part,
                         int stride, double *scal, unsigned *ticket);
-__global__ void k_cg_dir(int n, const double *scal, const double3 *z, double3 *p);
+__global__ void k_cg_dir(int n, const double *scal, const double3 *z, double3 *p, CgTest t);
 __global__ void k_cg_step(int n, int nk, const int *polar, const double *pol, double *scal, const double3 *p,
                           const double3 *ap, double3 *x, double3 *r, double3 *z, const double2 *rho_p, double2 *acc,
-                          double *part, int stride, unsigned *ticket);
-__global__ void k_cg_check(cudaGraphConditionalHandle h, int first, const double *scal, DevScalars *out, int npol,
-                           double tol, int maxit, unsigned *status);
+                          double *part, int stride, unsigned *ticket, CgTest test);
+__global__ void k_cg_test(CgTest t, const double *scal);
 __global__ void k_upol_final(const double *scal, double coul, DevScalars *out);
 __global__ void k_vv1(int n, double dt, double dtsq2, const double *invm, double4 *r, const double3 *v,
                       const double3 *f, double3 *fs);
@@ -1009,8 +1008,17 @@ void Engine::pim_cg(bool fused) {
                 d_ticket + 1);
     MDFF_CK(cudaMemcpyAsync(d_cg_p, d_mu_save, sizeof(double3) * n, cudaMemcpyDeviceToDevice, stream));
     int maxit = std::max(p.max_scf_pim_iter, 1);
-    // one CG iteration up to the new residual norm (p <- z + beta p follows the test)
-    auto iteration = [&]() {
+    // one CG iteration up to the new residual norm and, recorded, the loop test in the
+    // same launch (p <- z + beta p follows the test)
+    CgTest test{};
+    test.mode = 1;
+    test.out = d_out;
+    test.npol = npol;
+    test.tol = p.conv_tol_ind;
+    test.maxit = maxit;
+    test.status = d_status;
+    test.guard = d_ticket + 4;
+    auto iteration = [&](CgTest t) {
         if (fused && subset32 && npol > 0) {
             // T p over the polarisable ions; Ap and p.Ap in the FP32 k-space combine, or
             // by k_cg_ap after the FP64 one
@@ -1027,19 +1035,19 @@ void Engine::pim_cg(bool fused) {
         // x, r update, rho(k) of the iterate, z = alpha r and the new r.z, r.r: one launch
         MDFF_LAUNCH(*this, k_cg_step, nb + (fused ? ceil_div(nk, 256) : 0), 256, 0, n, nk, d_polar, d_pol, d_scal,
                     d_cg_p, d_cg_ap, d_mu_ind, d_cg_r, d_mu_save, d_rho_it, fused ? d_rho_acc : nullptr, d_part,
-                    part_stride, d_ticket + 1);
+                    part_stride, d_ticket + 1, t);
     };
     if (capturing) {
         // graph: the loop is a while node whose condition the device test sets
         record_while(
             [&](cudaGraphConditionalHandle h) {
-                MDFF_LAUNCH(*this, k_cg_check, 1, 32, 0, h, 1, d_scal, d_out, npol, p.conv_tol_ind, maxit, d_status);
+                test.h = h;
+                MDFF_LAUNCH(*this, k_cg_test, 1, 32, 0, test, d_scal);
             },
             [&](cudaGraphConditionalHandle h) {
-                iteration();
-                MDFF_LAUNCH(*this, k_cg_check, 1, 32, 0, h, 0, d_scal, d_out, npol, p.conv_tol_ind, maxit,
-                            d_status);
-                MDFF_LAUNCH(*this, k_cg_dir, nb, 256, 0, n, d_scal, d_mu_save, d_cg_p);
+                test.h = h;
+                iteration(test);
+                MDFF_LAUNCH(*this, k_cg_dir, nb, 256, 0, n, d_scal, d_mu_save, d_cg_p, test);
             });
     } else {
         double rr = 0.0;
@@ -1047,15 +1055,16 @@ void Engine::pim_cg(bool fused) {
         MDFF_CK(cudaStreamSynchronize(stream));
         double rmsd = std::sqrt(rr / (double)std::max(npol, 1));
         int it = 0;
+        CgTest none{};
         while (rmsd > p.conv_tol_ind && it < maxit) {
-            iteration();
+            iteration(none);
             MDFF_CK(cudaMemcpyAsync(&rr, d_scal + S_RR, sizeof(double), cudaMemcpyDeviceToHost, stream));
             MDFF_CK(cudaStreamSynchronize(stream));
             rmsd = std::sqrt(rr / (double)std::max(npol, 1));
             if (!std::isfinite(rmsd)) throw Error(MDFFGPU_ERR_NONFINITE, "CG diverged");
             it++;
             if (rmsd <= p.conv_tol_ind) break;
-            MDFF_LAUNCH(*this, k_cg_dir, nb, 256, 0, n, d_scal, d_mu_save, d_cg_p);
+            MDFF_LAUNCH(*this, k_cg_dir, nb, 256, 0, n, d_scal, d_mu_save, d_cg_p, none);
         }
         if (rmsd > p.conv_tol_ind) throw Error(MDFFGPU_ERR_SCF, "CG did not converge in max_scf_pim_iter");
         last_scf_iter = it;

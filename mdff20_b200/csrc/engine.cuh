@@ -63,6 +63,25 @@ struct DevScalars {
     int scf_iter, nbuilds, rebuild, status;
 };
 
+// the stopping test of a recorded CG loop, evaluated by the last block of k_cg_step (or by
+// k_cg_test before the first iteration): mode 1, the induced-dipole test
+// rmsd = sqrt(r.r / npol) > tol (the reference's residual measure, src/pim.c:431-449);
+// mode 2, the adjoint test r.r > rtol2 r0.r0; mode 0, none (host-driven loops).  Sets the
+// while node's condition; the iteration limit or a non-finite residual raise status bits.
+struct CgTest {
+    cudaGraphConditionalHandle h;
+    int mode;
+    DevScalars *out;       // mode 1: iteration count and rmsd
+    int npol;
+    double tol;
+    double *rr0, *itc;     // mode 2: the initial r.r and the iteration count (fit slots)
+    double rtol2;
+    int maxit;
+    unsigned *status;
+    unsigned *guard;       // iterations counted by k_cg_dir, which ends the loop past maxit
+                           // whatever k_cg_step did (a backstop of the while node)
+};
+
 struct Engine;
 
 // zero-initialised device allocation; MDFFGPU_ERR_NOMEM on failure.  The zeroing runs on

@@ -45,8 +45,11 @@ __global__ void k_cg_ap(int n, const int *polar, const double *invpol, const dou
                         double3 *ap, double *part, int stride, double *scal, unsigned *ticket);
 __global__ void k_cg_rz(int n, const int *polar, const double *pol, const double3 *r, double3 *z, double *part,
                         int stride, double *scal, unsigned *ticket);
-__global__ void k_cg_update(int n, double *scal, const double3 *p, const double3 *ap, double3 *x, double3 *r);
-__global__ void k_cg_dir(int n, const double *scal, const double3 *z, double3 *p);
+__global__ void k_cg_step(int n, int nk, const int *polar, const double *pol, double *scal, const double3 *p,
+                          const double3 *ap, double3 *x, double3 *r, double3 *z, const double2 *rho_p, double2 *acc,
+                          double *part, int stride, unsigned *ticket, CgTest test);
+__global__ void k_cg_test(CgTest t, const double *scal);
+__global__ void k_cg_dir(int n, const double *scal, const double3 *z, double3 *p, CgTest t);
 
 struct TTd {
     double E[9];   // 1/k!
@@ -421,28 +424,6 @@ __global__ void k_fm_result(const double *__restrict__ sc, const double *__restr
     res[NRES - 1] = (double)*status;
 }
 
-// the adjoint CG's loop test (recorded loop): continue while |r|^2 > rtol^2 |r0|^2 and
-// the iteration limit is not reached; the limit or a non-finite residual sets a status bit
-__global__ void k_adj_check(cudaGraphConditionalHandle h, int first, const double *__restrict__ scal,
-                            double *__restrict__ fscal, double rtol2, int maxit, unsigned *status) {
-    if (threadIdx.x || blockIdx.x) return;
-    double rr = scal[S_RR];
-    if (first) {
-        fscal[F_ADJ_RR0] = rr;
-        fscal[F_ADJ_IT] = 0.0;
-    } else {
-        fscal[F_ADJ_IT] += 1.0;
-    }
-    int it = (int)fscal[F_ADJ_IT];
-    unsigned go = 0;
-    if (!isfinite(rr)) atomicOr(status, (unsigned)ST_NONFINITE);
-    else if (rr > rtol2 * fscal[F_ADJ_RR0] && rr > 0.0) {
-        if (it < maxit) go = 1;
-        else atomicOr(status, (unsigned)ST_SCF);
-    }
-    cudaGraphSetConditional(h, go);
-}
-
 // theta into the host copies of the parameters (p, the pair and damping tables, the
 // charges); set_fit_params then copies them to the device
 void Engine::fit_host_params(int tSi, int tO, const double *th) {
@@ -510,7 +491,7 @@ void Engine::fit_apply_theta(const double *d_th, int tSi, int tO) {
 }
 
 // CG on A x = b over the polarisable ions, x0 = 0, until |r| <= rtol |b|; while
-// recording, the loop is a device-controlled while node (k_adj_check)
+// recording, the loop is a device-controlled while node (the test in k_cg_step)
 void Engine::solve_pim(const double3 *d_b, double3 *d_x, double rtol, int maxit) {
     int nb = ceil_div(n, 256);
     MDFF_CK(cudaMemsetAsync(d_x, 0, sizeof(double3) * n, stream));
@@ -519,26 +500,36 @@ void Engine::solve_pim(const double3 *d_b, double3 *d_x, double rtol, int maxit)
                 d_ticket + 1);
     MDFF_CK(cudaMemcpyAsync(d_cg_p, d_mu_save, sizeof(double3) * n, cudaMemcpyDeviceToDevice, stream));
     // A p: the search direction vanishes off the polarisable ions, so the field passes
-    // run over those ions only
-    auto iteration = [&]() {
-        if (subset32 && npol > 0) field_pol(d_cg_p, d_ef_ind, nullptr, false);
+    // run over those ions only; A p and p.A p in the FP32 k-space combine (or k_cg_ap),
+    // then x, r, z and r.z, r.r in one launch, as the induced-dipole CG does
+    CgTest test{};
+    test.mode = 2;
+    test.rr0 = d_fscal + F_ADJ_RR0;
+    test.itc = d_fscal + F_ADJ_IT;
+    test.rtol2 = rtol * rtol;
+    test.maxit = maxit;
+    test.status = d_status;
+    test.guard = d_ticket + 4;
+    auto iteration = [&](CgTest t) {
+        const bool sub = subset32 && npol > 0, ap_in_combine = sub && use32 && rec32;
+        if (sub) field_pol(d_cg_p, d_ef_ind, nullptr, ap_in_combine);
         else field_of(d_qzero, d_cg_p, false, true, false, d_ef_ind);
-        MDFF_LAUNCH(*this, k_cg_ap, nb, 256, 0, n, d_polar, d_invpol, d_cg_p, d_ef_ind, d_cg_ap, d_part, part_stride,
-                    d_scal, d_ticket);
-        MDFF_LAUNCH(*this, k_cg_update, nb, 256, 0, n, d_scal, d_cg_p, d_cg_ap, d_x, d_cg_r);
-        MDFF_LAUNCH(*this, k_cg_rz, nb, 256, 0, n, d_polar, d_pol, d_cg_r, d_mu_save, d_part, part_stride, d_scal,
-                    d_ticket + 1);
+        if (!ap_in_combine)
+            MDFF_LAUNCH(*this, k_cg_ap, nb, 256, 0, n, d_polar, d_invpol, d_cg_p, d_ef_ind, d_cg_ap, d_part,
+                        part_stride, d_scal, d_ticket);
+        MDFF_LAUNCH(*this, k_cg_step, nb, 256, 0, n, 0, d_polar, d_pol, d_scal, d_cg_p, d_cg_ap, d_x, d_cg_r,
+                    d_mu_save, nullptr, nullptr, d_part, part_stride, d_ticket + 1, t);
     };
     if (capturing) {
-        double rtol2 = rtol * rtol;
         record_while(
             [&](cudaGraphConditionalHandle h) {
-                MDFF_LAUNCH(*this, k_adj_check, 1, 32, 0, h, 1, d_scal, d_fscal, rtol2, maxit, d_status);
+                test.h = h;
+                MDFF_LAUNCH(*this, k_cg_test, 1, 32, 0, test, d_scal);
             },
             [&](cudaGraphConditionalHandle h) {
-                iteration();
-                MDFF_LAUNCH(*this, k_adj_check, 1, 32, 0, h, 0, d_scal, d_fscal, rtol2, maxit, d_status);
-                MDFF_LAUNCH(*this, k_cg_dir, nb, 256, 0, n, d_scal, d_mu_save, d_cg_p);
+                test.h = h;
+                iteration(test);
+                MDFF_LAUNCH(*this, k_cg_dir, nb, 256, 0, n, d_scal, d_mu_save, d_cg_p, test);
             });
         return;
     }
@@ -547,13 +538,14 @@ void Engine::solve_pim(const double3 *d_b, double3 *d_x, double rtol, int maxit)
     MDFF_CK(cudaStreamSynchronize(stream));
     rr = rr0;
     int it = 0;
+    CgTest none{};
     while (rr > rtol * rtol * rr0 && rr > 0.0 && it < maxit) {
-        iteration();
+        iteration(none);
         MDFF_CK(cudaMemcpyAsync(&rr, d_scal + S_RR, sizeof(double), cudaMemcpyDeviceToHost, stream));
         MDFF_CK(cudaStreamSynchronize(stream));
         if (!std::isfinite(rr)) throw Error(MDFFGPU_ERR_NONFINITE, "adjoint CG diverged");
         it++;
-        MDFF_LAUNCH(*this, k_cg_dir, nb, 256, 0, n, d_scal, d_mu_save, d_cg_p);
+        MDFF_LAUNCH(*this, k_cg_dir, nb, 256, 0, n, d_scal, d_mu_save, d_cg_p, none);
     }
     if (rr > rtol * rtol * rr0 && rr > 0.0) throw Error(MDFFGPU_ERR_SCF, "adjoint CG did not converge");
     last_adj_iter = it;

@@ -308,20 +308,46 @@ __global__ void k_cg_rz(int n, const int *__restrict__ polar, const double *__re
     last_block_slots(part, stride, S_RZ, 2, scal, ticket);
 }
 
-// x += a p ; r -= a Ap, with a = rz / pAp read on the device; rz is kept as rz_old
-__global__ void k_cg_update(int n, double *__restrict__ scal, const double3 *__restrict__ p,
-                            const double3 *__restrict__ ap, double3 *__restrict__ x, double3 *__restrict__ r) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    double a = scal[S_RZ] / scal[S_PAP];
-    if (i == 0) scal[S_RZOLD] = scal[S_RZ];
-    if (i >= n) return;
-    double3 pp = p[i], q = ap[i], xx = x[i], rr = r[i];
-    x[i] = make_double3(xx.x + a * pp.x, xx.y + a * pp.y, xx.z + a * pp.z);
-    r[i] = make_double3(rr.x - a * q.x, rr.y - a * q.y, rr.z - a * q.z);
+// the loop test of CgTest (first: before the first iteration, iteration count 0)
+__device__ void cg_test(const CgTest &t, const double *scal, int first) {
+    const double rr = scal[S_RR];
+    unsigned go = 0;
+    if (t.mode == 1) {
+        const double rmsd = sqrt(rr / (double)(t.npol > 1 ? t.npol : 1));
+        const int it = first ? 0 : t.out->scf_iter + 1;
+        t.out->scf_iter = it;
+        t.out->scf_rmsd = rmsd;
+        if (!isfinite(rmsd)) atomicOr(t.status, (unsigned)ST_NONFINITE);
+        else if (rmsd > t.tol) {
+            if (it < t.maxit) go = 1;
+            else atomicOr(t.status, (unsigned)ST_SCF);
+        }
+    } else {
+        if (first) {
+            *t.rr0 = rr;
+            *t.itc = 0.0;
+        } else {
+            *t.itc += 1.0;
+        }
+        const int it = (int)*t.itc;
+        if (!isfinite(rr)) atomicOr(t.status, (unsigned)ST_NONFINITE);
+        else if (rr > t.rtol2 * *t.rr0 && rr > 0.0) {
+            if (it < t.maxit) go = 1;
+            else atomicOr(t.status, (unsigned)ST_SCF);
+        }
+    }
+    cudaGraphSetConditional(t.h, go);
+}
+
+// the test of a recorded loop before its first iteration
+__global__ void k_cg_test(CgTest t, const double *scal) {
+    if (threadIdx.x || blockIdx.x) return;
+    *t.guard = 0u;
+    cg_test(t, scal, 1);
 }
 
 // One CG update in a single launch: x += a p, r -= a Ap (a = rz / pAp, rz kept as rz_old),
-// z = alpha r and the partial sums of r.z and r.r (as k_cg_update then k_cg_rz), and in
+// z = alpha r and the partial sums of r.z and r.r (as k_cg_rz), and in
 // blocks past the ions (when acc is set) the rho(k) of the iterate, acc += a rho(p) (rho
 // is linear in the dipoles).  Those blocks add zero partials; the last block reduces the
 // slots as k_cg_rz does, so the scalars are the same bits.
@@ -329,7 +355,7 @@ __global__ void k_cg_step(int n, int nk, const int *__restrict__ polar, const do
                           double *scal, const double3 *__restrict__ p, const double3 *__restrict__ ap,
                           double3 *__restrict__ x, double3 *__restrict__ r, double3 *__restrict__ z,
                           const double2 *__restrict__ rho_p, double2 *__restrict__ acc, double *part, int stride,
-                          unsigned *ticket) {
+                          unsigned *ticket, CgTest test) {
     const double rz = scal[S_RZ];
     const double a = rz / scal[S_PAP];
     const int nbi = (n + blockDim.x - 1) / blockDim.x;
@@ -359,38 +385,23 @@ __global__ void k_cg_step(int n, int nk, const int *__restrict__ polar, const do
         }
     }
     block_sum_to_part<2>(v, part, S_RZ, stride);  // r.z, r.r
-    last_block_slots(part, stride, S_RZ, 2, scal, ticket);
+    const bool last = last_block_slots(part, stride, S_RZ, 2, scal, ticket);
+    if (last && threadIdx.x == 0 && test.mode) cg_test(test, scal, 0);
 }
 
-// p = z + beta p, beta = rz_new / rz_old
+// p = z + beta p, beta = rz_new / rz_old; in a recorded loop (t.mode set) also the
+// backstop of the loop: past maxit iterations it ends the loop and raises ST_SCF
 __global__ void k_cg_dir(int n, const double *__restrict__ scal, const double3 *__restrict__ z,
-                         double3 *__restrict__ p) {
+                         double3 *__restrict__ p, CgTest t) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0 && t.mode && ++*t.guard > (unsigned)t.maxit) {
+        atomicOr(t.status, (unsigned)ST_SCF);
+        cudaGraphSetConditional(t.h, 0);
+    }
     if (i >= n) return;
     double beta = scal[S_RZ] / scal[S_RZOLD];
     double3 zz = z[i], pp = p[i];
     p[i] = make_double3(zz.x + beta * pp.x, zz.y + beta * pp.y, zz.z + beta * pp.z);
-}
-
-// CG stopping test on the device (graph-captured steps): rmsd = sqrt(r.r / npol), the
-// reference's residual measure (src/pim.c:431-449).  first: before the iterations
-// (iteration count 0); otherwise after one.  Sets the while-loop condition: continue
-// while rmsd > tol and fewer than maxit iterations; non-finite residuals and
-// non-convergence raise status bits read by the host after the step.
-__global__ void k_cg_check(cudaGraphConditionalHandle h, int first, const double *scal, DevScalars *out, int npol,
-                           double tol, int maxit, unsigned *status) {
-    if (threadIdx.x || blockIdx.x) return;
-    double rmsd = sqrt(scal[S_RR] / (double)(npol > 1 ? npol : 1));
-    int it = first ? 0 : out->scf_iter + 1;
-    out->scf_iter = it;
-    out->scf_rmsd = rmsd;
-    unsigned go = 0;
-    if (!isfinite(rmsd)) atomicOr(status, (unsigned)ST_NONFINITE);
-    else if (rmsd > tol) {
-        if (it < maxit) go = 1;
-        else atomicOr(status, (unsigned)ST_SCF);
-    }
-    cudaGraphSetConditional(h, go);
 }
 
 // u_pol = 1/2 sum mu.alpha^-1.mu in energy units

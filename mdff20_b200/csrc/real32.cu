@@ -166,15 +166,29 @@ __global__ void __launch_bounds__(PW32 * 32) k_pol_field32(int n, const int *__r
     const int *L = pl + (size_t)i * cap;
     const float4 *U = pu + (size_t)i * cap;
     float ex = 0.f, ey = 0.f, ez = 0.f;
-    for (int k = lane; k < m; k += 32) {
-        int j = L[k];
-        float4 u = U[k];
-        double3 pd = p[j];
-        float px = (float)pd.x, py = (float)pd.y, pz = (float)pd.z;
-        float up = u.x * px + u.y * py + u.z * pz;
-        ex += up * u.x - u.w * px;
-        ey += up * u.y - u.w * py;
-        ez += up * u.z - u.w * pz;
+    // four records per lane in flight: their indices, records and dipole gathers are
+    // issued before any of them is used (the walk is bound by these loads)
+    constexpr int R = 4;
+    for (int k0 = lane; k0 < m; k0 += 32 * R) {
+        int j[R];
+        float4 u[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const int k = k0 + 32 * r;
+            j[r] = k < m ? L[k] : -1;
+            u[r] = k < m ? U[k] : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        double3 pd[R];
+#pragma unroll
+        for (int r = 0; r < R; r++) pd[r] = j[r] >= 0 ? p[j[r]] : make_double3(0.0, 0.0, 0.0);
+#pragma unroll
+        for (int r = 0; r < R; r++) {
+            const float px = (float)pd[r].x, py = (float)pd[r].y, pz = (float)pd[r].z;
+            const float up = u[r].x * px + u[r].y * py + u[r].z * pz;
+            ex += up * u[r].x - u[r].w * px;
+            ey += up * u[r].y - u[r].w * py;
+            ez += up * u[r].z - u[r].w * pz;
+        }
     }
     double dx = warp_sum((double)ex), dy = warp_sum((double)ey), dz = warp_sum((double)ez);
     if (lane == 0) ef[i] = make_double3(dx, dy, dz);

@@ -6,8 +6,8 @@ charge and total-moment passes over every ion go through it) for the N=24000 ben
 system (kmax 14: 29 of the 32 MMA columns), a small polarisable system (kmax 5, one
 64-row tile), a 450-ion system whose ion count is not a multiple of the 16-ion stage, a
 rigid-ion system (charges only); both ion passes beside it; and graph-replayed MD
-steps.  Bars: forces within 1e-5 RMS of FP64 and within 2x (+1e-6) of the CUDA-core
-pass's error, energies within 1e-5."""
+steps; and a triclinic cell with an unequal k box.  Bars: forces within 1e-5 RMS of FP64
+and within 2x (+1e-6) of the CUDA-core pass's error, energies within 1e-5."""
 import os
 
 import numpy as np
@@ -50,11 +50,27 @@ def _forces(s, pos, rho_tc, ion_tc=True, **kw):
     return out
 
 
+def _silica450_triclinic():
+    """The 450-ion system sheared into a triclinic cell (positions carried along in
+    fractional coordinates) with an unequal k box (kmax 5, 6, 7): the phase-table offsets
+    and E0 | E1 prefixes of the tensor-core passes in their general form."""
+    s = cases.silica450(True)
+    frac = s.pos @ np.linalg.inv(s.cell)
+    cell = s.cell.copy()
+    cell[1, 0] = 1.2
+    cell[2, 1] = -0.9
+    s.cell = cell
+    s.pos = frac @ cell
+    s.kES = (5, 6, 7)
+    return s
+
+
 SYSTEMS = {
     "config5": lambda: synth.config5(),
     "silica96": lambda: cases.silica96(True),
     "silica450": lambda: cases.silica450(True),
     "silica96_rigid": lambda: cases.silica96(False),
+    "silica450_triclinic": _silica450_triclinic,
 }
 
 
