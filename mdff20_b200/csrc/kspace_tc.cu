@@ -94,24 +94,29 @@ __host__ __device__ inline RtSmem rt_smem(int lz) {
 
 // ---------------------------------------------------------------- per-stage tables
 // Once per force evaluation, for position p of order (stage p / RT_SI, slot p % RT_SI):
-// the E0 | E1 prefix of the ion's phase-table row (lz float2, the values k_rho32 reads)
-// into etab, and the E operand (1, c_z, d_z of E2[z] = exp(2 pi i z t_z), the values of
-// the phase table's z blocks) split into TF32 h + l, K-major, into btab.  Positions past n
-// are zero.  One thread per (position, 16-byte unit of the E0 | E1 prefix or column).
+// the E0 | E1 prefix of the ion's phase-table row (lz complex values, the ones k_rho32
+// reads) into etab, interleaved by position pairs -- entry e of the pair (2m, 2m + 1) is
+// (x_2m, x_2m+1, y_2m, y_2m+1), the operand order of the pass's packed FP32x2 arithmetic --
+// and the E operand (1, c_z, d_z of E2[z] = exp(2 pi i z t_z), the values of the phase
+// table's z blocks) split into TF32 h + l, K-major, into btab.  Positions past n are zero.
+// One thread per (position pair, prefix entry) and per (position, column).
 __global__ void k_rho_tc_tables(int n, int npad, int lz, int tab_w, int K2, Cell c, const double4 *__restrict__ r,
-                                const int *__restrict__ order, const float4 *__restrict__ tab,
+                                const int *__restrict__ order, const float2 *__restrict__ tab,
                                 float4 *__restrict__ etab, float *__restrict__ btab) {
-    const int hl = lz / 2;   // 16-byte units of a prefix
-    const int per = hl + RT_N;
+    const long long ne = (long long)(npad / 2) * lz;   // pair entries, then (position, column) items
     long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= (long long)npad * per) return;
-    const int p = (int)(g / per), u = (int)(g - (long long)p * per);
-    const int ion = p < n ? order[p] : -1;
-    if (u < hl) {
-        etab[(size_t)p * hl + u] = ion >= 0 ? tab[(size_t)ion * (tab_w / 2) + u] : make_float4(0.f, 0.f, 0.f, 0.f);
+    if (g >= ne + (long long)npad * RT_N) return;
+    if (g < ne) {
+        const int m = (int)(g / lz), e = (int)(g - (long long)m * lz);
+        const int ia = 2 * m < n ? order[2 * m] : -1, ib = 2 * m + 1 < n ? order[2 * m + 1] : -1;
+        const float2 va = ia >= 0 ? tab[(size_t)ia * tab_w + e] : make_float2(0.f, 0.f);
+        const float2 vb = ib >= 0 ? tab[(size_t)ib * tab_w + e] : make_float2(0.f, 0.f);
+        etab[g] = make_float4(va.x, vb.x, va.y, vb.y);
         return;
     }
-    const int col = u - hl;
+    g -= ne;
+    const int p = (int)(g / RT_N), col = (int)(g - (long long)p * RT_N);
+    const int ion = p < n ? order[p] : -1;
     float v = 0.f;
     if (ion >= 0) {
         if (col == 0) {
@@ -132,27 +137,37 @@ __global__ void k_rho_tc_tables(int n, int npad, int lz, int tab_w, int K2, Cell
     *(float *)(T + RT_B_TERM + kmaj(col, j, RT_B_LBO)) = l;
 }
 
-// per pass: (q, 2 pi (B mu)) of positions 0..cnt-1 of order, as k_rho32 forms them
-__global__ void k_qm_tc(int cnt, const int *__restrict__ order, Cell c, const double *__restrict__ q,
-                        const double3 *__restrict__ mu, int lq, int ld, float4 *__restrict__ out) {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= cnt) return;
-    int ion = order[t];
+// per pass: (q, 2 pi (B mu)) of positions 0..cnt-1 of order, as k_rho32 forms them, zero
+// at the positions past them (their A values vanish without a test in the pass); stored by
+// position pairs (2m, 2m + 1) as (q_a, q_b, m0_a, m0_b), (m1_a, m1_b, m2_a, m2_b).  One
+// thread per pair.
+__device__ __forceinline__ float4 qm_of(int t, int cnt, const int *__restrict__ order, const Cell &c,
+                                        const double *__restrict__ q, const double3 *__restrict__ mu, int lq, int ld) {
+    if (t >= cnt) return make_float4(0.f, 0.f, 0.f, 0.f);
+    const int ion = order[t];
     const double tpi = TPI_D;
     float4 v = make_float4(lq ? (float)q[ion] : 0.f, 0.f, 0.f, 0.f);
     if (ld) {
-        double3 m3 = mu[ion];
+        const double3 m3 = mu[ion];
         v.y = (float)(tpi * (c.B[0][0] * m3.x + c.B[1][0] * m3.y + c.B[2][0] * m3.z));
         v.z = (float)(tpi * (c.B[0][1] * m3.x + c.B[1][1] * m3.y + c.B[2][1] * m3.z));
         v.w = (float)(tpi * (c.B[0][2] * m3.x + c.B[1][2] * m3.y + c.B[2][2] * m3.z));
     }
-    out[t] = v;
+    return v;
+}
+__global__ void k_qm_tc(int cnt, int npad, const int *__restrict__ order, Cell c, const double *__restrict__ q,
+                        const double3 *__restrict__ mu, int lq, int ld, float4 *__restrict__ out) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (2 * m >= npad) return;
+    const float4 a = qm_of(2 * m, cnt, order, c, q, mu, lq, ld), b = qm_of(2 * m + 1, cnt, order, c, q, mu, lq, ld);
+    out[2 * m] = make_float4(a.x, b.x, a.y, b.y);
+    out[2 * m + 1] = make_float4(a.z, b.z, a.w, b.w);
 }
 
 // ---------------------------------------------------------------- the pass
 struct RhoTcArgs {
     int cnt, chunk, nrow, nk, K2, K1, e1, lz;
-    const float4 *etab;      // [stage][RT_SI][lz / 2]
+    const float4 *etab;      // [stage][RT_SI / 2 position pairs][lz]
     const float4 *btab;      // [stage][RT_B_BYTES / 16]
     const float4 *qm;        // [position]
     const KRow *row;
@@ -312,28 +327,40 @@ __global__ void __launch_bounds__(RT_THREADS, 2) k_rho_tc(RhoTcArgs a) {
         R.nx = R.ny = R.z0 = R.cnt = R.koff = 0;
         if (rok) R = a.row[rr];
         const float fnx = (float)R.nx, fny = (float)R.ny;
+        const float2 fnx2 = make_float2(fnx, fnx), fny2 = make_float2(fny, fny);
         const int o0 = R.nx, o1 = a.e1 + a.K1 + R.ny;
         for (int s = 0; s < nst; s++) {
             const int b = s & 1, slot = s % RT_NIN;
             if (!__all_sync(0xffffffffu, wait(IN_FULL + slot, (s / RT_NIN) & 1))) break;
-            const int t0 = a0 + s * RT_SI;
-            const float2 *E = (const float2 *)(sE + slot * ebytes);
-            const float4 *Q = (const float4 *)(sQ + slot * RT_Q_BYTES);
+            const float4 *E = (const float4 *)(sE + slot * ebytes);   // [pair][lz]
+            const float4 *Q = (const float4 *)(sQ + slot * RT_Q_BYTES);  // [pair][2]
             float h[4][4], l[4][4];   // [coefficient][ion]
+            // two ions per FP32x2 operation; positions past the pass's ions have q = mu = 0
+            // (k_qm_tc), rows past nrow give accumulator rows the read-back skips: no tests
 #pragma unroll
-            for (int j = 0; j < 4; j++) {
-                const int jj = g * 4 + j;
-                const bool on = rok && t0 + jj < a1;
-                const float2 e0 = E[jj * a.lz + o0], e1 = E[jj * a.lz + o1];
-                const float4 qm = Q[jj];
-                const float bx = e0.x * e1.x - e0.y * e1.y, by = e0.x * e1.y + e0.y * e1.x;
-                const float c0 = fnx * qm.y + fny * qm.z;
-                const float v0 = qm.x * bx - c0 * by, v1 = qm.x * by + c0 * bx;
-                const float v2 = -qm.w * by, v3 = qm.w * bx;
-                split2(on ? v0 : 0.f, h[0][j], l[0][j]);
-                split2(on ? v1 : 0.f, h[1][j], l[1][j]);
-                split2(on ? v2 : 0.f, h[2][j], l[2][j]);
-                split2(on ? v3 : 0.f, h[3][j], l[3][j]);
+            for (int pp = 0; pp < 2; pp++) {
+                const int P = 2 * g + pp;
+                const float4 ea = E[P * a.lz + o0], eb = E[P * a.lz + o1];
+                const float2 e0x = make_float2(ea.x, ea.y), e0y = make_float2(ea.z, ea.w);
+                const float2 e1x = make_float2(eb.x, eb.y), e1y = make_float2(eb.z, eb.w);
+                const float4 qa = Q[2 * P], qb = Q[2 * P + 1];
+                const float2 qx = make_float2(qa.x, qa.y), qy = make_float2(qa.z, qa.w);
+                const float2 qz = make_float2(qb.x, qb.y), qw = make_float2(qb.z, qb.w);
+                const float2 bx = __ffma2_rn(make_float2(-e0y.x, -e0y.y), e1y, __fmul2_rn(e0x, e1x));
+                const float2 by = __ffma2_rn(e0y, e1x, __fmul2_rn(e0x, e1y));
+                const float2 c0 = __ffma2_rn(fny2, qz, __fmul2_rn(fnx2, qy));
+                const float2 v[4] = {__ffma2_rn(make_float2(-c0.x, -c0.y), by, __fmul2_rn(qx, bx)),
+                                     __ffma2_rn(c0, bx, __fmul2_rn(qx, by)),
+                                     __fmul2_rn(make_float2(-qw.x, -qw.y), by), __fmul2_rn(qw, bx)};
+#pragma unroll
+                for (int c = 0; c < 4; c++) {
+                    const float hx = tf32_round(v[c].x), hy = tf32_round(v[c].y);
+                    const float2 lv = __fadd2_rn(v[c], make_float2(-hx, -hy));
+                    h[c][2 * pp] = hx;
+                    h[c][2 * pp + 1] = hy;
+                    l[c][2 * pp] = lv.x;
+                    l[c][2 * pp + 1] = lv.y;
+                }
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(smem_u32(&bar[IN_EMPTY + slot]));   // E rows and qm read
@@ -455,9 +482,9 @@ void setup_rho_tc(Engine &e, int lz) {
 void launch_rho_tc_tables(Engine &e) {
     if (!e.d_rho_btab) return;
     const int npad = rt_npad(e), lz = e.rho_tc_lz;
-    const long long tot = (long long)npad * (lz / 2 + RT_N);
+    const long long tot = (long long)(npad / 2) * lz + (long long)npad * RT_N;
     MDFF_LAUNCH(e, k_rho_tc_tables, (unsigned)((tot + 255) / 256), 256, 0, e.n, npad, lz, e.tab_w, e.kmax[2], e.cell,
-                e.d_r, e.d_ion_order, (const float4 *)e.d_tab32, e.d_rho_etab, (float *)e.d_rho_btab);
+                e.d_r, e.d_ion_order, e.d_tab32, e.d_rho_etab, (float *)e.d_rho_btab);
 }
 
 // ions per chunk of a pass over `cnt` ions: a whole number of stages; by default two
@@ -475,8 +502,8 @@ bool launch_rho_tc(Engine &e, const double *q, const double3 *mu, bool lq, bool 
                    int z_off, int *chunks_used) {
     if (!e.d_rho_btab || cnt <= 0 || z_off != e.rho_tc_lz) return false;
     if (!(idx == nullptr && cnt == e.n) && !(idx == e.d_pidx && cnt == e.npol)) return false;
-    MDFF_LAUNCH(e, k_qm_tc, ceil_div(cnt, 256), 256, 0, cnt, e.d_ion_order, e.cell, q, mu, lq ? 1 : 0, ld ? 1 : 0,
-                e.d_qm_tc);
+    MDFF_LAUNCH(e, k_qm_tc, ceil_div(rt_npad(e) / 2, 256), 256, 0, cnt, rt_npad(e), e.d_ion_order, e.cell, q, mu,
+                lq ? 1 : 0, ld ? 1 : 0, e.d_qm_tc);
     RhoTcArgs a;
     a.cnt = cnt;
     a.chunk = rho_tc_chunk(e, cnt);

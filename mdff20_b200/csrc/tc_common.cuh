@@ -15,8 +15,9 @@ __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)_
 // x = h + l: h is x rounded to the TF32 grid (10 fraction bits; the half unit added to
 // the magnitude bits, so ties round away from zero), l = x - h exactly; the MMA reads l to
 // TF32 precision, so the pair carries about 21 bits of x
+__device__ __forceinline__ float tf32_round(float x) { return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xffffe000u); }
 __device__ __forceinline__ void split2(float x, float &h, float &l) {
-    h = __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xffffe000u);
+    h = tf32_round(x);
     l = x - h;
 }
 
