@@ -172,8 +172,10 @@ __global__ void __launch_bounds__(IT_THREADS, ItShape<NC>::MINB) k_ion_tc(IonTcA
     extern __shared__ __align__(1024) unsigned char sm[];
     unsigned char *sA = sm;                                   // the ion tile
     unsigned char *sB = sm + IT_A_BYTES;                      // [2] weight chunks
-    int2 *rnxy = (int2 *)(sB + 2 * S::BYTES);                 // (nx, ny) of the slice's rows
-    uint64_t *bar = (uint64_t *)(rnxy + a.rows_per_slice);
+    // per row of the slice: (nx, ny, 1 when the row continues the one before it in its
+    // row warp's group of IT_HALF -- same nx, ny one higher --, 0)
+    float4 *rowf = (float4 *)(sB + 2 * S::BYTES);
+    uint64_t *bar = (uint64_t *)(rowf + a.rows_per_slice);
     // bar: 0 tile landed, 1-2 chunk landed, 3-4 chunk consumed, 5-6 accumulator ready,
     // 7-8 accumulator read (one arrival per row warp)
     volatile int *abort_flag = (volatile int *)(bar + 9);
@@ -185,8 +187,13 @@ __global__ void __launch_bounds__(IT_THREADS, ItShape<NC>::MINB) k_ion_tc(IonTcA
     const int nch = (nrs + IT_RPC - 1) / IT_RPC, ch0 = r0 / IT_RPC;
 
     for (int e = tid; e < nrs; e += IT_THREADS) {
-        KRow R = a.row[r0 + e];
-        rnxy[e] = make_int2(R.nx, R.ny);
+        const KRow R = a.row[r0 + e];
+        bool step = false;
+        if (e % IT_HALF != 0) {
+            const KRow Q = a.row[r0 + e - 1];
+            step = R.nx == Q.nx && R.ny == Q.ny + 1;
+        }
+        rowf[e] = make_float4((float)R.nx, (float)R.ny, step ? 1.f : 0.f, 0.f);
     }
     if (tid == 0) {
         mbar_init(smem_u32(&bar[0]), 1);
@@ -296,8 +303,6 @@ __global__ void __launch_bounds__(IT_THREADS, ItShape<NC>::MINB) k_ion_tc(IonTcA
         }
         const float2 e1 = cis2pi32(ty);
         float2 w = make_float2(1.f, 0.f);
-        int2 Rp = make_int2(0, 0);
-        int run = IT_RUN;
         double S0 = 0, S1 = 0, S2 = 0, P0 = 0, P1 = 0, P2 = 0;
         const uint32_t lanebase = tmem + ((uint32_t)(qd * 32) << 16);
         bool ok = true;
@@ -325,20 +330,17 @@ __global__ void __launch_bounds__(IT_THREADS, ItShape<NC>::MINB) k_ion_tc(IonTcA
             for (int j = 0; j < IT_HALF; j++) {
                 const int rr = ch * IT_RPC + hsel * IT_HALF + j;
                 if (rr >= nrs) break;
-                const int2 R = rnxy[rr];
-                if (run < IT_RUN && R.x == Rp.x && R.y == Rp.y + 1) {
-                    w = cmul32(w, e1);
-                    run++;
-                } else {
-                    w = cis2pi32((double)R.x * tx + (double)R.y * ty);
-                    run = 1;
-                }
-                Rp = R;
+                const float4 R = rowf[rr];
+                // the row phase: from an FP64-reduced argument at rows 0 and IT_RUN of the
+                // group and wherever the row does not continue the one before, else by
+                // one FP32 step in ny
+                if (j % IT_RUN != 0 && R.z != 0.f) w = cmul32(w, e1);
+                else w = cis2pi32((double)R.x * tx + (double)R.y * ty);
                 const float *g = v + j * NC;
                 const float Gx = g[0], Gy = g[1], Hx = g[2], Hy = g[3];
                 // Im conj(w) G and Im conj(w) H
                 const float R1 = w.x * Gy - w.y * Gx, Rz = w.x * Hy - w.y * Hx;
-                const float fx = (float)R.x, fy = (float)R.y;
+                const float fx = R.x, fy = R.y;
                 s0 = fmaf(fx, R1, s0);
                 s1 = fmaf(fy, R1, s1);
                 s2 += Rz;
@@ -422,7 +424,7 @@ static void ion_tc_run(Engine &e, const IonTcArgs &a, int tiles, int slices, int
     using S = ItShape<NC>;
     MDFF_LAUNCH(e, k_ion_tc_weights<NC>, ceil_div(nchunk * S::N * (IT_KV / 4), 128), 128, 0, e.nrow, nchunk,
                 e.kmax[2], e.d_row, e.d_rho, e.d_ion_wtab);
-    size_t smem = S::SMEM + sizeof(int2) * a.rows_per_slice + 16 * sizeof(uint64_t);
+    size_t smem = S::SMEM + sizeof(float4) * a.rows_per_slice + 16 * sizeof(uint64_t);
     // the largest request once per process (the attribute call is not recorded in graphs)
     static std::once_flag once;
     std::call_once(once, [] {
