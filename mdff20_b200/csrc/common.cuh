@@ -50,6 +50,16 @@ struct Cell {
     int ortho;        // A and B diagonal
 };
 
+// First statement of every kernel (programmatic dependent launch): wait until the grids
+// this one depends on have completed and their writes are visible (returns at once for
+// a launch without a programmatic edge), then let this grid's dependents be scheduled;
+// a dependent grid runs nothing before its own wait, so only its launch overlaps this
+// grid's tail
+__device__ __forceinline__ void grid_dep() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Exactly-rounded FP64 products/sums: the reference's geometry is compiled without
 // FMA contraction (src/Makefile:17, no -mfma), and the neighbour-list pair set must
 // match it bit for bit, so these expressions are kept uncontracted.

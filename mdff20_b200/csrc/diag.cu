@@ -7,6 +7,7 @@ namespace mdffgpu {
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_fma_peak(T *out, int iters, T a, T b) {
+    grid_dep();
     T x0 = (T)threadIdx.x, x1 = x0 + (T)1, x2 = x0 + (T)2, x3 = x0 + (T)3;
     T x4 = x0 + (T)4, x5 = x0 + (T)5, x6 = x0 + (T)6, x7 = x0 + (T)7;
     for (int i = 0; i < iters; i++) {

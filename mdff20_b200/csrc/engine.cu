@@ -603,15 +603,18 @@ void Engine::alloc_lists(int cnb, int cco) {
 // the engine's double4 / double3 arrays by a kernel.  From page-locked host arrays the
 // copies are direct DMA; each call returns once its copies are done.
 __global__ void k_pack_r(int n, const double *__restrict__ soa, const double *__restrict__ q, double4 *__restrict__ r) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) r[i] = make_double4(soa[i], soa[n + i], soa[2 * (size_t)n + i], q[i]);
 }
 __global__ void k_pack_v(int n, const double *__restrict__ soa, double3 *__restrict__ v) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) v[i] = make_double3(soa[3 * (size_t)n + i], soa[4 * (size_t)n + i], soa[5 * (size_t)n + i]);
 }
 __global__ void k_unpack_state(int n, const double4 *__restrict__ r, const double3 *__restrict__ v,
                                const double3 *__restrict__ f, double *__restrict__ soa) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double4 a = r[i];

@@ -420,11 +420,34 @@ struct Engine {
     void reduce(int first_slot, int nslots, int nparts) { launch_reduce_slots(*this, first_slot, nslots, nparts); }
 };
 
+// Programmatic dependent launch: every kernel of this library opens with grid_dep()
+// (wait for the grids it depends on, then release its dependents), so each launch may
+// carry the programmatic-serialization attribute -- the grid is launched while the one
+// before it in the stream drains (a recorded graph keeps this as a programmatic edge)
+// and starts its work once that one has completed with its writes visible.
+// MDFFGPU_PDL=0 launches with full serialization.
+inline bool pdl_enabled() {
+    static const bool on = [] {
+        const char *v = getenv("MDFFGPU_PDL");
+        return !v || atoi(v) != 0;
+    }();
+    return on;
+}
+
 // launch bookkeeping: every kernel launch goes through this
 #define MDFF_LAUNCH(eng, kernel, grid, block, smem, ...)                               \
     do {                                                                               \
-        kernel<<<(grid), (block), (smem), (eng).stream>>>(__VA_ARGS__);                \
-        MDFF_CK(cudaGetLastError());                                                   \
+        cudaLaunchAttribute at_[1];                                                    \
+        at_[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;                \
+        at_[0].val.programmaticStreamSerializationAllowed = 1;                         \
+        cudaLaunchConfig_t cfg_ = {};                                                  \
+        cfg_.gridDim = dim3(grid);                                                     \
+        cfg_.blockDim = dim3(block);                                                   \
+        cfg_.dynamicSmemBytes = (smem);                                                \
+        cfg_.stream = (eng).stream;                                                    \
+        cfg_.attrs = at_;                                                              \
+        cfg_.numAttrs = pdl_enabled() ? 1 : 0;                                         \
+        MDFF_CK(cudaLaunchKernelEx(&cfg_, kernel, __VA_ARGS__));                       \
         (eng).launches++;                                                              \
     } while (0)
 

@@ -74,6 +74,7 @@ __device__ __forceinline__ void fit_block_sum(double (&v)[NV], double *part, int
 // w = scale (F - F_t); partial sums of |F - F_t|^2
 __global__ void k_fm_seed(int n, const double3 *__restrict__ f, const double3 *__restrict__ ft, double scale,
                           double3 *__restrict__ w, double *part, int stride) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double v[1] = {0.0};
     if (i < n) {
@@ -88,6 +89,7 @@ __global__ void k_fm_seed(int n, const double3 *__restrict__ f, const double3 *_
 // partial sums of a.b over the ions (mask: only polarisable ions when non-null)
 __global__ void k_dot3(int n, const double3 *__restrict__ a, const double3 *__restrict__ b,
                        const int *__restrict__ mask, double *part, int slot, int stride) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double v[1] = {0.0};
     if (i < n && (!mask || mask[i])) {
@@ -102,6 +104,7 @@ __global__ void k_dot3(int n, const double3 *__restrict__ a, const double3 *__re
 __global__ void k_adj_rhs(int n, const int *__restrict__ polar, double coul, const double3 *__restrict__ sdir,
                           const double3 *__restrict__ erw, const double *__restrict__ efg,
                           const double3 *__restrict__ w, double3 *__restrict__ s) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     if (!polar[i]) {
@@ -121,6 +124,7 @@ __global__ void k_adj_rhs(int n, const int *__restrict__ polar, double coul, con
 // drho_w(k) = i (kx rho_x + ky rho_y + kz rho_z)
 __global__ void k_drho_w(int nk, const double3 *__restrict__ kv, const double2 *__restrict__ rx,
                          const double2 *__restrict__ ry, const double2 *__restrict__ rz, double2 *__restrict__ out) {
+    grid_dep();
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nk) return;
     double3 kk = kv[k];
@@ -132,6 +136,7 @@ __global__ void k_drho_w(int nk, const double3 *__restrict__ kv, const double2 *
 // q w_a and mu w_a (a = 0, 1, 2): charges and dipoles of the rho passes of drho_w
 __global__ void k_scale_by_w(int n, int comp, const double *__restrict__ q, const double3 *__restrict__ mu,
                              const double3 *__restrict__ w, double *__restrict__ qo, double3 *__restrict__ muo) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double3 ww = w[i];
@@ -180,6 +185,7 @@ __device__ __forceinline__ void tt_param(const TTd &tt, double b, double c, doub
 // s_i (real space, electrostatic units) = - sum_j d/dmu_i [(w_i - w_j) . fij] at
 // polarisable i, fij the pair term of k_dir (force on i = -fij)
 __global__ void __launch_bounds__(FIT_WARPS * 32) k_adj_dir(AdjArgs a) {
+    grid_dep();
     int i = blockIdx.x * FIT_WARPS + (threadIdx.x >> 5);
     int lane = threadIdx.x & 31;
     double si3[3] = {0, 0, 0};
@@ -245,6 +251,7 @@ __global__ void __launch_bounds__(FIT_WARPS * 32) k_adj_dir(AdjArgs a) {
 // force terms), per block: w.dF/db, w.dF/dc (electrostatic units), lambda.dE_stat/db,
 // lambda.dE_stat/dc; the fit's b and c are those of every damped direction
 __global__ void __launch_bounds__(FIT_WARPS * 32) k_damp_sens(AdjArgs a) {
+    grid_dep();
     int i = blockIdx.x * FIT_WARPS + (threadIdx.x >> 5);
     int lane = threadIdx.x & 31;
     double acc[4] = {0, 0, 0, 0};
@@ -316,6 +323,7 @@ __global__ void __launch_bounds__(FIT_WARPS * 32) k_bhm_sens(int n, Cell c, cons
                                                              const int *__restrict__ nbn, int cap, double srcutsq,
                                                              int tSi, int tO, const double3 *__restrict__ w,
                                                              double *part, int stride) {
+    grid_dep();
     int i = blockIdx.x * FIT_WARPS + (threadIdx.x >> 5);
     int lane = threadIdx.x & 31;
     double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // A B C (Si-O), A B C (O-O), D (Si-O), D (O-O)
@@ -358,6 +366,7 @@ __global__ void __launch_bounds__(FIT_WARPS * 32) k_bhm_sens(int n, Cell c, cons
 // damped direction (one thread per type pair) ...
 __global__ void k_fit_tables(const double *__restrict__ th, int tSi, int tO, int nt, PairSR *__restrict__ pair,
                              PairDamp *__restrict__ damp) {
+    grid_dep();
     int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= nt * nt) return;
     int x = e / nt, y = e - x * nt;
@@ -388,6 +397,7 @@ __global__ void k_fit_tables(const double *__restrict__ th, int tSi, int tO, int
 __global__ void k_fit_ions(int n, const int *__restrict__ typ, const double *__restrict__ th, int tSi, int tO,
                            double *__restrict__ q, double4 *__restrict__ r, double *__restrict__ pol,
                            double *__restrict__ invpol) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int t = typ[i];
@@ -411,6 +421,7 @@ __global__ void k_fit_ions(int n, const int *__restrict__ typ, const double *__r
 // b and c terms); res[NRES - 1] = the context's status bits
 __global__ void k_fm_result(const double *__restrict__ sc, const double *__restrict__ th, double coul,
                             const unsigned *__restrict__ status, double *__restrict__ res) {
+    grid_dep();
     if (threadIdx.x || blockIdx.x) return;
     res[0] = sc[F_LOSS];
     for (int k = 0; k < 6; k++) res[1 + k] = sc[F_BHM + k];

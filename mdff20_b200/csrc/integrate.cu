@@ -9,6 +9,7 @@ namespace mdffgpu {
 // one block per slot; fixed-order tree over the block partials
 __global__ void k_reduce_slots(const double *__restrict__ part, int stride, int first, int nparts,
                                double *__restrict__ scal) {
+    grid_dep();
     int slot = first + blockIdx.x;
     const double *p = part + (size_t)slot * stride;
     double a = 0.0;
@@ -30,11 +31,13 @@ void launch_reduce_slots(Engine &e, int first_slot, int nslots, int nparts) {
 
 // ---------------------------------------------------------------- small helpers
 __global__ void k_fill3(int n, double3 *a, double3 v) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) a[i] = v;
 }
 
 __global__ void k_copy3(int n, const double3 *__restrict__ a, double3 *__restrict__ b) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) b[i] = a[i];
 }
@@ -42,6 +45,7 @@ __global__ void k_copy3(int n, const double3 *__restrict__ a, double3 *__restric
 // sum q^2 and |mu|^2 for the self terms (src/ewald.c:198-214)
 __global__ void k_self_sums(int n, const double *__restrict__ q, const double3 *__restrict__ mu, double *part,
                             int stride) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double v[2] = {0.0, 0.0};
     if (i < n) {
@@ -57,6 +61,7 @@ __global__ void k_self_sums(int n, const double *__restrict__ q, const double3 *
 // ef = self2*mu + ef_dir (used when the reciprocal part is skipped)
 __global__ void k_self_plus_dir(int n, double self2, const double3 *__restrict__ mu, const double3 *__restrict__ efd,
                                 double3 *__restrict__ ef) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double3 m = mu ? mu[i] : make_double3(0, 0, 0);
@@ -66,6 +71,7 @@ __global__ void k_self_plus_dir(int n, double self2, const double3 *__restrict__
 
 // f += f_dir * coul (when the reciprocal part is skipped)
 __global__ void k_axpy3(int n, double a, const double3 *__restrict__ x, double3 *__restrict__ y) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double3 u = x[i], v = y[i];
@@ -74,6 +80,7 @@ __global__ void k_axpy3(int n, double a, const double3 *__restrict__ x, double3 
 
 __global__ void k_efg_self_dir(int n, double self2, const double *__restrict__ q, const double *__restrict__ efgd,
                                double *__restrict__ efg) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     for (int p = 0; p < 3; p++)
@@ -90,6 +97,7 @@ __global__ void k_efg_self_dir(int n, double self2, const double *__restrict__ q
 // sum of r_a f_b + r_b f_a.
 __global__ void k_finalize_sr(const double *__restrict__ scal, int slot, double inveOmegaPU, double *u, double *pvir,
                               double *tau) {
+    grid_dep();
     if (threadIdx.x || blockIdx.x) return;
     *u = 0.5 * scal[slot];
     double t[6];
@@ -107,6 +115,7 @@ struct CoulFin {
     int do_dir, do_rec, do_stress;
 };
 __global__ void k_finalize_coul(const double *__restrict__ scal, CoulFin c, double *u, double *pvir, double *tau) {
+    grid_dep();
     if (threadIdx.x || blockIdx.x) return;
     const double rpi = 1.7724538509055160273;
     double alpha2 = c.alpha * c.alpha, selfa = c.alpha / rpi, selfa2 = 2.0 * selfa * alpha2 / 3.0;
@@ -142,6 +151,7 @@ __device__ __forceinline__ double3 pol_times(const double *P, double3 e) {
 
 __global__ void k_induced(int n, const int *__restrict__ polar, const double *__restrict__ pol,
                           const double3 *__restrict__ ef, double3 *__restrict__ mu) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || !polar[i]) return;
     mu[i] = pol_times(pol + (size_t)i * 9, ef[i]);
@@ -150,6 +160,7 @@ __global__ void k_induced(int n, const int *__restrict__ polar, const double *__
 // extrapolate_dipole_aspc predictor (src/pim.c:381-400) for order `e`, then the
 // history shift by `es` places
 __global__ void k_aspc_predict(int n, int e, int es, double *__restrict__ hist, double3 *__restrict__ mu, int poly) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double Bt[6][6] = {{1.0, 0, 0, 0, 0, 0},
@@ -177,6 +188,7 @@ __global__ void k_aspc_predict(int n, int e, int es, double *__restrict__ hist, 
 // corrector (src/pim.c:403-420): mu = W * alpha E + (1 - W) * mu_pred
 __global__ void k_aspc_correct(int n, double W, const int *__restrict__ polar, const double *__restrict__ pol,
                                const double3 *__restrict__ ef, double3 *__restrict__ mu) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double3 s = mu[i];
@@ -186,6 +198,7 @@ __global__ void k_aspc_correct(int n, double W, const int *__restrict__ polar, c
 
 // ef = a + b
 __global__ void k_add3(int n, const double3 *__restrict__ a, const double3 *__restrict__ b, double3 *__restrict__ c) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double3 x = a[i], y = b[i];
@@ -196,6 +209,7 @@ __global__ void k_add3(int n, const double3 *__restrict__ a, const double3 *__re
 __global__ void k_pim_sums(int n, const int *__restrict__ polar, const double *__restrict__ pol,
                            const double *__restrict__ invpol, const double3 *__restrict__ mu,
                            const double3 *__restrict__ ef, double *part, int stride) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double v[2] = {0.0, 0.0};
     if (i < n) {
@@ -219,6 +233,7 @@ __global__ void k_pim_sums(int n, const int *__restrict__ polar, const double *_
 }
 
 __global__ void k_hist_store(int n, const double3 *__restrict__ mu, double *__restrict__ hist) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double3 m = mu[i];
@@ -231,6 +246,7 @@ __global__ void k_hist_store(int n, const double3 *__restrict__ mu, double *__re
 // kO: f_ind = ef - mu * invpol_ii on polarisable ions (src/pim.c:561-567)
 __global__ void k_ko_find(int n, const int *__restrict__ polar, const double *__restrict__ invpol,
                           const double3 *__restrict__ ef, const double3 *__restrict__ mu, double3 *__restrict__ find) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n || !polar[i]) return;
     const double *I = invpol + (size_t)i * 9;
@@ -240,6 +256,7 @@ __global__ void k_ko_find(int n, const int *__restrict__ polar, const double *__
 
 // kO inner loop updates (src/pim.c:684-729)
 __global__ void k_scale_add3(int n, double a, const double3 *__restrict__ x, double b, double3 *__restrict__ y) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double3 u = x[i], v = y[i];
@@ -251,6 +268,7 @@ __global__ void k_scale_add3(int n, double a, const double3 *__restrict__ x, dou
 __global__ void k_cg_residual(int n, const int *__restrict__ polar, const double *__restrict__ invpol,
                               const double3 *__restrict__ efs, const double3 *__restrict__ tx,
                               const double3 *__restrict__ x, double3 *__restrict__ r) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     if (!polar[i]) {
@@ -268,6 +286,7 @@ __global__ void k_cg_residual(int n, const int *__restrict__ polar, const double
 __global__ void k_cg_ap(int n, const int *__restrict__ polar, const double *__restrict__ invpol,
                         const double3 *__restrict__ p, const double3 *__restrict__ tp, double3 *__restrict__ ap,
                         double *part, int stride, double *scal, unsigned *ticket) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double v[1] = {0.0};
     if (i < n) {
@@ -291,6 +310,7 @@ __global__ void k_cg_ap(int n, const int *__restrict__ polar, const double *__re
 __global__ void k_cg_rz(int n, const int *__restrict__ polar, const double *__restrict__ pol,
                         const double3 *__restrict__ r, double3 *__restrict__ z, double *part, int stride,
                         double *scal, unsigned *ticket) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double v[2] = {0.0, 0.0};
     if (i < n) {
@@ -341,6 +361,7 @@ __device__ void cg_test(const CgTest &t, const double *scal, int first) {
 
 // the test of a recorded loop before its first iteration
 __global__ void k_cg_test(CgTest t, const double *scal) {
+    grid_dep();
     if (threadIdx.x || blockIdx.x) return;
     *t.guard = 0u;
     cg_test(t, scal, 1);
@@ -356,6 +377,7 @@ __global__ void k_cg_step(int n, int nk, const int *__restrict__ polar, const do
                           double3 *__restrict__ x, double3 *__restrict__ r, double3 *__restrict__ z,
                           const double2 *__restrict__ rho_p, double2 *__restrict__ acc, double *part, int stride,
                           unsigned *ticket, CgTest test) {
+    grid_dep();
     const double rz = scal[S_RZ];
     const double a = rz / scal[S_PAP];
     const int nbi = (n + blockDim.x - 1) / blockDim.x;
@@ -393,6 +415,7 @@ __global__ void k_cg_step(int n, int nk, const int *__restrict__ polar, const do
 // backstop of the loop: past maxit iterations it ends the loop and raises ST_SCF
 __global__ void k_cg_dir(int n, const double *__restrict__ scal, const double3 *__restrict__ z,
                          double3 *__restrict__ p, CgTest t) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0 && t.mode && ++*t.guard > (unsigned)t.maxit) {
         atomicOr(t.status, (unsigned)ST_SCF);
@@ -406,6 +429,7 @@ __global__ void k_cg_dir(int n, const double *__restrict__ scal, const double3 *
 
 // u_pol = 1/2 sum mu.alpha^-1.mu in energy units
 __global__ void k_upol_final(const double *scal, double coul, DevScalars *out) {
+    grid_dep();
     if (threadIdx.x || blockIdx.x) return;
     out->u_pol = 0.5 * scal[S_UPOL] * coul;
 }
@@ -414,6 +438,7 @@ __global__ void k_upol_final(const double *scal, double coul, DevScalars *out) {
 // prop_velocity_verlet first half (src/integration.c:33-38)
 __global__ void k_vv1(int n, double dt, double dtsq2, const double *__restrict__ invm, double4 *__restrict__ r,
                       const double3 *__restrict__ v, const double3 *__restrict__ f, double3 *__restrict__ fs) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double4 x = r[i];
@@ -430,6 +455,7 @@ __global__ void k_vv1(int n, double dt, double dtsq2, const double *__restrict__
 __global__ void k_vv2(int n, double dt2, const double *__restrict__ invm, const double *__restrict__ mass,
                       double3 *__restrict__ v, const double3 *__restrict__ f, const double3 *__restrict__ fs,
                       double *part, int stride) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double k[1] = {0.0};
     if (i < n) {
@@ -447,6 +473,7 @@ __global__ void k_vv2(int n, double dt2, const double *__restrict__ invm, const 
 // prop_pos_vel_verlet (src/integration.c:66-90): half kick + drift ...
 __global__ void k_pv1(int n, double dt, double dt2, const double *__restrict__ invm, double4 *__restrict__ r,
                       double3 *__restrict__ v, const double3 *__restrict__ f) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double4 x = r[i];
@@ -465,6 +492,7 @@ __global__ void k_pv1(int n, double dt, double dt2, const double *__restrict__ i
 // ... and the second half kick + kinetic partials
 __global__ void k_pv2(int n, double dt2, const double *__restrict__ invm, const double *__restrict__ mass,
                       double3 *__restrict__ v, const double3 *__restrict__ f, double *part, int stride) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double k[1] = {0.0};
     if (i < n) {
@@ -482,6 +510,7 @@ __global__ void k_pv2(int n, double dt2, const double *__restrict__ invm, const 
 // kinetic partials, optionally after scaling v by the NHC factor s (src/integration.c:281-287)
 __global__ void k_scale_kin(int n, const DevScalars *__restrict__ out, int scale, const double *__restrict__ mass,
                             double3 *__restrict__ v, double *part, int stride) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double k[1] = {0.0};
     if (i < n) {
@@ -502,6 +531,7 @@ __global__ void k_scale_kin(int n, const DevScalars *__restrict__ out, int scale
 __global__ void k_lf(int n, double dtsq, double idt, const double *__restrict__ invm, const double *__restrict__ mass,
                      double4 *__restrict__ r, double3 *__restrict__ rs, double3 *__restrict__ v,
                      const double3 *__restrict__ f, double *part, int stride) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double k[1] = {0.0};
     if (i < n) {
@@ -532,6 +562,7 @@ struct NhcArgs {
 };
 template <int NN>
 __global__ void k_nhc_chain(NhcArgs a, double *__restrict__ nhc, const double *__restrict__ scal, DevScalars *out) {
+    grid_dep();
     if (threadIdx.x || blockIdx.x) return;
     constexpr int M = NN > 0 ? NN : 16;
     const int nn = NN > 0 ? NN : a.nn;
@@ -598,6 +629,7 @@ void launch_nhc_chain(Engine &e, const NhcArgs &a, double *nhc, const double *sc
 // e_kin and the NHC conserved-quantity term e_nvt (src/integration.c:156-176)
 __global__ void k_nhc_energy(int nn, double L, double temp, const double *__restrict__ nhc,
                              const double *__restrict__ scal, DevScalars *out) {
+    grid_dep();
     if (threadIdx.x || blockIdx.x) return;
     const double *xi = nhc, *vxi = nhc + 16, *Q = nhc + 32;
     out->e_kin = 0.5 * scal[S_KIN];
@@ -614,12 +646,14 @@ __global__ void k_nhc_energy(int nn, double L, double temp, const double *__rest
 }
 
 __global__ void k_set_ekin(const double *__restrict__ scal, DevScalars *out) {
+    grid_dep();
     if (threadIdx.x || blockIdx.x) return;
     out->e_kin = 0.5 * scal[S_KIN];
 }
 
 // non-finite guard on positions and forces (status word)
 __global__ void k_check_finite(int n, const double4 *__restrict__ r, const double3 *__restrict__ f, unsigned *status) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double4 x = r[i];

@@ -52,6 +52,7 @@ __global__ void __launch_bounds__(RHO_THREADS, RHO_MIN_BLOCKS) k_rho(int n, int 
                                                     const double3 *__restrict__ mu, int nseg,
                                                     const KSeg *__restrict__ seg, double2 *__restrict__ part,
                                                     int nk, const int *__restrict__ idx) {
+    grid_dep();
     extern __shared__ double2 sm[];
     const int W0 = K0 + 1, W1 = 2 * K1 + 1, W2 = 2 * K2 + 1, WT = W0 + W1 + W2;
     double2 *E = sm;                                   // [RHO_TI][WT]
@@ -182,6 +183,7 @@ __global__ void __launch_bounds__(256) k_rho_reduce(int nk, int nchunks, const P
                                                     const double3 *__restrict__ kv, double2 *__restrict__ rho_s,
                                                     double2 *__restrict__ rho_raw, double *__restrict__ ppart,
                                                     int slot, int stride) {
+    grid_dep();
     __shared__ double2 ws[8][RHOR_K];
     int w = threadIdx.x >> 5, l = threadIdx.x & 31;
     int k = blockIdx.x * RHOR_K + l;
@@ -221,6 +223,7 @@ __global__ void __launch_bounds__(32) k_rho_from_acc(int nk, const double2 *__re
                                                      const double *__restrict__ Ak, const double *__restrict__ kcoe,
                                                      const double3 *__restrict__ kv, double2 *__restrict__ rho_s,
                                                      double *__restrict__ ppart, int slot, int stride) {
+    grid_dep();
     int k = blockIdx.x * RHOR_K + threadIdx.x;
     double2 rho = k < nk ? acc[k] : make_double2(0.0, 0.0);
     rho_finish(k, nk, rho, Ak, kcoe, kv, rho_s, ppart, slot, stride);
@@ -255,6 +258,7 @@ struct IonArgs {
 // one slice of rows: S = sum_k n recarg, P = sum_k n (n.m) recarg2, H = sum_k n n^T recarg2
 template <bool WF, bool WEFG>
 __global__ void __launch_bounds__(ION_THREADS) k_rec_ion(IonArgs a) {
+    grid_dep();
     extern __shared__ double2 rk[];
     int ii = blockIdx.x * ION_THREADS + threadIdx.x;
     int tl = blockIdx.y;
@@ -378,6 +382,7 @@ __global__ void __launch_bounds__(ION_THREADS) k_rec_ion(IonArgs a) {
 // sum the slices of each ion (fixed order) and write field, force and EFG
 template <bool WF, bool WEFG>
 __global__ void k_rec_combine(IonArgs a) {
+    grid_dep();
     int ii = blockIdx.x * blockDim.x + threadIdx.x;
     if (ii >= a.n) return;
     int i = a.idx ? a.idx[ii] : ii;

@@ -63,6 +63,7 @@ struct TabLayout {
 
 // one thread per (ion, table entry)
 __global__ void k_phase32(int n, Cell c, const double4 *__restrict__ r, TabLayout L, float2 *__restrict__ tab) {
+    grid_dep();
     long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= (long long)n * L.w) return;
     int i = (int)(g / L.w), e = (int)(g - (long long)i * L.w);
@@ -117,6 +118,7 @@ __global__ void __launch_bounds__(RHO32_THREADS, RHO32_MIN_BLOCKS)
     k_rho32(int cnt, const int *__restrict__ idx, int chunk, TabLayout L, const float2 *__restrict__ tab,
             Cell c, const double *__restrict__ q, const double3 *__restrict__ mu, int nseg,
             const KSeg *__restrict__ seg, float2 *__restrict__ part, int nk) {
+    grid_dep();
     constexpr int NP = RZP / 2;
     extern __shared__ float4 sm4[];
     const int ha = L.z / 2, skip = (ZS / 2) * L.nzb_neg;   // 16-byte units
@@ -316,6 +318,7 @@ __device__ __forceinline__ void ion32_stage(const Ion32Args &a, float4 *rk4, int
 
 template <int KZ, bool WF>
 __global__ void __launch_bounds__(ION32_THREADS, ION32_MIN_BLOCKS) k_ion32(Ion32Args a) {
+    grid_dep();
     constexpr int NV = ion32_nv(WF), NP = KZ / 2, RS = 1 + NP * NV;
     extern __shared__ float4 rk4[];          // [rows of the slice][RS]
     int2 *rnxy = (int2 *)(rk4 + a.rows_per_slice * RS);   // (nx, ny) of the slice's rows
@@ -432,6 +435,7 @@ __global__ void __launch_bounds__(ION32_THREADS, ION32_MIN_BLOCKS) k_ion32(Ion32
 // ion as k_ion32<KZ, false>.
 template <int KZ>
 __global__ void __launch_bounds__(ION32_THREADS, ION32X2_MIN_BLOCKS) k_ion32x2(Ion32Args a) {
+    grid_dep();
     constexpr int NV = ion32_nv(false), NP = KZ / 2, RS = 1 + NP * NV;
     extern __shared__ float4 rk4[];          // [rows of the slice][RS]
     int2 *rnxy = (int2 *)(rk4 + a.rows_per_slice * RS);
@@ -530,6 +534,7 @@ struct Comb32Args {
 
 template <bool WF>
 __global__ void k_combine32(Comb32Args a) {
+    grid_dep();
     int li = blockIdx.x * blockDim.x + threadIdx.x;
     double pap[1] = {0.0};
     if (li < a.cnt) {

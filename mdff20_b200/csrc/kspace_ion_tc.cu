@@ -68,6 +68,7 @@ struct ItShape {
 // 128 positions with K = (h | h | l)
 __global__ void k_ion_tc_table(int n, int K2, Cell c, const double4 *__restrict__ r, const int *__restrict__ order,
                                float4 *__restrict__ atab) {
+    grid_dep();
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
     double4 ri = r[order[j]];
@@ -102,6 +103,7 @@ __global__ void k_ion_tc_table(int n, int K2, Cell c, const double4 *__restrict_
 template <int NC>
 __global__ void k_ion_tc_weights(int nrow, int nchunk, int K2, const KRow *__restrict__ row,
                                  const double2 *__restrict__ rho, float4 *__restrict__ wtab) {
+    grid_dep();
     using S = ItShape<NC>;
     constexpr int G = IT_KV / 4;
     int g = blockIdx.x * blockDim.x + threadIdx.x;
@@ -167,6 +169,7 @@ struct IonTcArgs {
 
 template <int NC>
 __global__ void __launch_bounds__(IT_THREADS, ItShape<NC>::MINB) k_ion_tc(IonTcArgs a) {
+    grid_dep();
     using S = ItShape<NC>;
     constexpr bool WF = NC == 6;
     extern __shared__ __align__(1024) unsigned char sm[];

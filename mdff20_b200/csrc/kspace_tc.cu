@@ -103,6 +103,7 @@ __host__ __device__ inline RtSmem rt_smem(int lz) {
 __global__ void k_rho_tc_tables(int n, int npad, int lz, int tab_w, int K2, Cell c, const double4 *__restrict__ r,
                                 const int *__restrict__ order, const float2 *__restrict__ tab,
                                 float4 *__restrict__ etab, float *__restrict__ btab) {
+    grid_dep();
     const long long ne = (long long)(npad / 2) * lz;   // pair entries, then (position, column) items
     long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= ne + (long long)npad * RT_N) return;
@@ -157,6 +158,7 @@ __device__ __forceinline__ float4 qm_of(int t, int cnt, const int *__restrict__ 
 }
 __global__ void k_qm_tc(int cnt, int npad, const int *__restrict__ order, Cell c, const double *__restrict__ q,
                         const double3 *__restrict__ mu, int lq, int ld, float4 *__restrict__ out) {
+    grid_dep();
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (2 * m >= npad) return;
     const float4 a = qm_of(2 * m, cnt, order, c, q, mu, lq, ld), b = qm_of(2 * m + 1, cnt, order, c, q, mu, lq, ld);
@@ -217,6 +219,7 @@ __device__ __forceinline__ void mma_stage(uint32_t h0, uint32_t h1, uint32_t s0,
 }
 
 __global__ void __launch_bounds__(RT_THREADS, 2) k_rho_tc(RhoTcArgs a) {
+    grid_dep();
     extern __shared__ __align__(1024) unsigned char sm[];
     const RtSmem L = rt_smem(a.lz);
     const uint32_t ebytes = (uint32_t)(RT_SI * a.lz * 8);

@@ -13,6 +13,7 @@ namespace mdffgpu {
 
 // s = kardir(r), w = charge
 __global__ void k_kardir(int n, Cell c, const double4 *__restrict__ r, double4 *__restrict__ s) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double4 ri = r[i];
@@ -37,6 +38,7 @@ __device__ __forceinline__ void top2_insert(double &m1, double &m2, double d) {
 
 __global__ void k_check_disp(int n, Cell c, const double4 *__restrict__ s, const double4 *__restrict__ svl,
                              double *__restrict__ part1, double *__restrict__ part2) {
+    grid_dep();
     __shared__ double sm1[32], sm2[32];
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double m1 = 0.0, m2 = 0.0;
@@ -73,6 +75,7 @@ __global__ void k_check_disp(int n, Cell c, const double4 *__restrict__ s, const
 
 __global__ void k_check_final(int nparts, const double *__restrict__ part1, const double *__restrict__ part2,
                               double skindiff, int *rebuild, DevScalars *out) {
+    grid_dep();
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     double m1 = 0.0, m2 = 0.0;
     for (int k = 0; k < nparts; k++) {
@@ -86,6 +89,7 @@ __global__ void k_check_final(int nparts, const double *__restrict__ part1, cons
 }
 
 __global__ void k_force_rebuild(int *rebuild, DevScalars *out) {
+    grid_dep();
     *rebuild = 1;
     out->rebuild = 1;
     out->nbuilds += 1;
@@ -108,6 +112,7 @@ __device__ __forceinline__ int cell_coord(double s, int ncd) {
 
 __global__ void k_bin(int n, int3 nc, const double4 *__restrict__ s, int *__restrict__ cell_of,
                       int *__restrict__ cnt, const int *__restrict__ rebuild) {
+    grid_dep();
     if (!*rebuild) return;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -121,6 +126,7 @@ __global__ void k_bin(int n, int3 nc, const double4 *__restrict__ s, int *__rest
 // exclusive scan of the cell counts (one block), resets the fill cursors
 __global__ void k_scan_cells(int ncell, const int *__restrict__ cnt, int *__restrict__ start, int *__restrict__ cur,
                              int cell_cap, unsigned *status, const int *__restrict__ rebuild) {
+    grid_dep();
     if (!*rebuild) return;
     __shared__ int carry;
     __shared__ int wsum[32];
@@ -160,6 +166,7 @@ __global__ void k_scan_cells(int ncell, const int *__restrict__ cnt, int *__rest
 
 __global__ void k_fill_cells(int n, const int *__restrict__ cell_of, const int *__restrict__ start,
                              int *__restrict__ cur, int *__restrict__ ions, const int *__restrict__ rebuild) {
+    grid_dep();
     if (!*rebuild) return;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -172,6 +179,7 @@ __global__ void k_fill_cells(int n, const int *__restrict__ cell_of, const int *
 // order, hence every pair sum, is the same from run to run
 __global__ void k_sort_cells(int ncell, int cell_cap, const int *__restrict__ start, const int *__restrict__ cnt,
                              int *__restrict__ ions, const int *__restrict__ rebuild) {
+    grid_dep();
     if (!*rebuild) return;
     extern __shared__ int sh[];
     int c = blockIdx.x;
@@ -210,6 +218,7 @@ __global__ void k_build(int n, Cell c, int3 nc, const double4 *__restrict__ s, c
                         double rsq_nb, double rsq_co, int cap_nb, int *__restrict__ nbl, int *__restrict__ nbn,
                         int cap_co, int *__restrict__ col, int *__restrict__ con, double4 *__restrict__ svl,
                         unsigned *status, const int *__restrict__ rebuild) {
+    grid_dep();
     if (!*rebuild) return;
     int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int lane = threadIdx.x & 31;

@@ -39,6 +39,7 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32, FAST ? 3 : 1) k_sr(int n, Cel
                                                         const int *__restrict__ nbn, int cap, double srcutsq,
                                                         int trunctype, int damped, TT tt, double3 *__restrict__ f,
                                                         double *__restrict__ part, int slot, int stride) {
+    grid_dep();
     int i = blockIdx.x * PAIR_WARPS + (threadIdx.x >> 5);
     int lane = threadIdx.x & 31;
     double acc[7] = {0, 0, 0, 0, 0, 0, 0};  // u, Vxx Vxy Vxz Vyy Vyz Vzz
@@ -136,6 +137,7 @@ struct DirArgs {
 
 template <bool FORCES, bool EF, bool EFG>
 __global__ void __launch_bounds__(PAIR_WARPS * 32) k_dir(DirArgs a) {
+    grid_dep();
     int i = blockIdx.x * PAIR_WARPS + (threadIdx.x >> 5);
     int lane = threadIdx.x & 31;
     double acc[7] = {0, 0, 0, 0, 0, 0, 0};   // u, V6
@@ -343,6 +345,7 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32) k_dir_prep(int n, Cell c, con
                                                              const int *__restrict__ col,
                                                              const int *__restrict__ con, int cap, double lrcutsq,
                                                              double alpha, double2 *__restrict__ coef) {
+    grid_dep();
     int i = blockIdx.x * PAIR_WARPS + (threadIdx.x >> 5);
     int lane = threadIdx.x & 31;
     if (i >= n) return;
@@ -378,6 +381,7 @@ __global__ void __launch_bounds__(PAIR_WARPS * 32) k_dir_field_cached(int n, Cel
                                                                      const double2 *__restrict__ coef,
                                                                      const double3 *__restrict__ mu,
                                                                      double3 *__restrict__ ef) {
+    grid_dep();
     int i = blockIdx.x * PAIR_WARPS + (threadIdx.x >> 5);
     int lane = threadIdx.x & 31;
     if (i >= n) return;

@@ -33,6 +33,7 @@ __global__ void k_kardir(int n, Cell c, const double4 *r, double4 *s);
 __global__ void __launch_bounds__(GR_TILE)
     k_gr_pairs(int n, Cell c, const double4 *__restrict__ s, const int *__restrict__ typ, int nt, int nbins,
                double cut2, double resg, unsigned long long *__restrict__ hist, int private_hist) {
+    grid_dep();
     extern __shared__ unsigned int h_sh[];
     __shared__ double4 tile[GR_TILE];
     __shared__ int ttile[GR_TILE];

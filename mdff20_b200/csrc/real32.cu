@@ -66,6 +66,7 @@ __device__ __forceinline__ void tt32(float b, float c, float r, int order, float
 
 __global__ void k_pack_mu32(int n, const double3 *__restrict__ mu, const int *__restrict__ typ,
                             float4 *__restrict__ out) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double3 m = mu ? mu[i] : make_double3(0, 0, 0);
@@ -89,6 +90,7 @@ struct Prep32Args {
 // The neighbour positions of the next chunk of 32 and the indices of the one after are
 // loaded while the current chunk is processed.
 __global__ void __launch_bounds__(PW32 * 32) k_pair_prep32(Prep32Args a) {
+    grid_dep();
     int i = blockIdx.x * PW32 + (threadIdx.x >> 5);
     int lane = threadIdx.x & 31;
     if (i >= a.n) return;
@@ -159,6 +161,7 @@ __global__ void __launch_bounds__(PW32 * 32) k_pol_field32(int n, const int *__r
                                                            const int *__restrict__ pln, int cap,
                                                            const double3 *__restrict__ p,
                                                            double3 *__restrict__ ef) {
+    grid_dep();
     int i = blockIdx.x * PW32 + (threadIdx.x >> 5);
     int lane = threadIdx.x & 31;
     if (i >= n) return;
@@ -214,6 +217,7 @@ struct Dir32bArgs {
 // multipole_ES_dir over the in-cutoff list: field (EF) or forces + energy + virial (FORCES)
 template <bool FORCES, bool EF, int KTT>
 __global__ void __launch_bounds__(PW32 * 32) k_dir32b(Dir32bArgs a) {
+    grid_dep();
     __shared__ DampF dt[NT * NT];
     for (int e = threadIdx.x; e < a.nt * a.nt; e += blockDim.x) {
         PairDamp D = a.damp[e];

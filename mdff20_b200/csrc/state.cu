@@ -35,6 +35,7 @@ constexpr int VERSION = 1;
 constexpr size_t WORDS_PER_ION = 3 * 6 + 18;
 
 __global__ void k_pack3(int n, const double4 *__restrict__ a, double *__restrict__ out) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) {
         double4 x = a[i];
@@ -45,6 +46,7 @@ __global__ void k_pack3(int n, const double4 *__restrict__ a, double *__restrict
 // xyz from `in`, w = charge (the layout of d_r and d_s)
 __global__ void k_unpack4(int n, const double *__restrict__ in, const double *__restrict__ q,
                           double4 *__restrict__ a) {
+    grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) a[i] = make_double4(in[3 * i], in[3 * i + 1], in[3 * i + 2], q[i]);
 }
