@@ -616,6 +616,12 @@ void Engine::fit_issue(const double3 *d_ft, double scale, int tSi, int tO, const
     if (!p.lcoulombic || !lpol) throw Error(MDFFGPU_ERR_STATE, "force matching needs the polarisable Coulomb model");
     if (pim_solver != MDFFGPU_PIM_CG && pim_solver != MDFFGPU_PIM_CG_FUSED)
         throw Error(MDFFGPU_ERR_STATE, "force matching needs a CG induced-dipole solver");
+    // fully serialised launches while an evaluation is issued (evaluations run concurrently)
+    struct NoPdl {
+        bool &f, old;
+        explicit NoPdl(bool &x) : f(x), old(x) { f = false; }
+        ~NoPdl() { f = old; }
+    } no_pdl(pdl);
     fit_alloc();
     const double *q = d_q;
     int nb = ceil_div(n, 256), nbw = ceil_div(n, FIT_WARPS);
@@ -739,10 +745,13 @@ void Engine::capture_fit(const double *d_th, int tSi, int tO, double scale, doub
     cudaGraph_t graph = nullptr;
     try {
         MDFF_CK(cudaMemsetAsync(d_status, 0, sizeof(unsigned), stream));
+        pdl = false;
         fit_apply_theta(d_th, tSi, tO);
+        pdl = true;
         fit_issue(d_ft, scale, tSi, tO, d_th, d_res);
     } catch (...) {
         capturing = false;
+        pdl = true;
         cudaStreamEndCapture(stream, &graph);
         if (graph) cudaGraphDestroy(graph);
         launches = l0;
