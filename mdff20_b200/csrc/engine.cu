@@ -27,7 +27,7 @@ struct CoulFin {
 };
 __global__ void k_finalize_coul(const double *scal, CoulFin c, double *u, double *pvir, double *tau);
 __global__ void k_induced(int n, const int *polar, const double *pol, const double3 *ef, double3 *mu);
-__global__ void k_aspc_predict(int n, int e, int es, double *hist, double3 *mu, int poly);
+__global__ void k_aspc_predict(int n, AspcCoef cf, int es, double *hist, double3 *mu);
 __global__ void k_aspc_correct(int n, double W, const int *polar, const double *pol, const double3 *ef,
                                double3 *mu);
 __global__ void k_add3(int n, const double3 *a, const double3 *b, double3 *c);
@@ -887,7 +887,7 @@ void Engine::pim_reference() {
     double upol_pre = 0.0;
     while (((iscf < p.max_scf_pim_iter) && (rmsd > p.conv_tol_ind)) || (iscf < p.min_scf_pim_iter)) {
         MDFF_CK(cudaMemsetAsync(d_mu_ind, 0, sizeof(double3) * n, stream));
-        if (!iscf) MDFF_LAUNCH(*this, k_aspc_predict, nb, 256, 0, n, e, es, d_hist, d_mu_ind, 0);
+        if (!iscf) MDFF_LAUNCH(*this, k_aspc_predict, nb, 256, 0, n, aspc_coef(e, false), es, d_hist, d_mu_ind);
         else MDFF_LAUNCH(*this, k_induced, nb, 256, 0, n, d_polar, d_pol, d_ef, d_mu_ind);
         if (!iscf) {  // u_pol of the predicted dipoles (src/pim.c:253), kept if the loop ends here
             MDFF_LAUNCH(*this, k_pim_sums, nb, 256, 0, n, d_polar, d_pol, d_invpol, d_mu_ind, d_ef, d_part,
@@ -978,7 +978,7 @@ void Engine::pim_cg(bool fused) {
     int e = (istep >= ord + 1) ? ord : (!istep ? 0 : istep - 1);
     int es = (e != ord) ? e + 1 : e;
     if (fused) {
-        MDFF_LAUNCH(*this, k_aspc_predict, nb, 256, 0, n, e, es, d_hist, d_mu_ind, cg_poly ? 1 : 0);
+        MDFF_LAUNCH(*this, k_aspc_predict, nb, 256, 0, n, aspc_coef(e, cg_poly), es, d_hist, d_mu_ind);
         MDFF_LAUNCH(*this, k_add3, nb, 256, 0, n, d_mu_static, d_mu_ind, d_mu_tot);
         // the residual reads the field at the polarisable ions only (FP64 real space
         // evaluates every ion; the k-space ion pass and FP32 real space only those)
@@ -1003,7 +1003,7 @@ void Engine::pim_cg(bool fused) {
         MDFF_LAUNCH(*this, k_cg_residual, nb, 256, 0, n, d_polar, d_invpol, d_muzero, d_ef_ind, d_mu_ind, d_cg_r);
     } else {
         field_of(d_q, d_mu_static, lqch != 0, ldip != 0, ldmp != 0, d_ef_stat);
-        MDFF_LAUNCH(*this, k_aspc_predict, nb, 256, 0, n, e, es, d_hist, d_mu_ind, cg_poly ? 1 : 0);
+        MDFF_LAUNCH(*this, k_aspc_predict, nb, 256, 0, n, aspc_coef(e, cg_poly), es, d_hist, d_mu_ind);
         field_of(d_qzero, d_mu_ind, false, true, false, d_ef_ind);
         MDFF_LAUNCH(*this, k_cg_residual, nb, 256, 0, n, d_polar, d_invpol, d_ef_stat, d_ef_ind, d_mu_ind, d_cg_r);
     }
@@ -1134,7 +1134,7 @@ void Engine::pim_ko() {
     double rmsd = 1.0e300, upol = 0.0;
     while (((iscf < p.max_scf_pim_iter) && (rmsd > p.conv_tol_ind)) || (iscf < p.min_scf_pim_iter)) {
         if ((!iscf) && (istep > 1)) {
-            MDFF_LAUNCH(*this, k_aspc_predict, nb, 256, 0, n, e, es, d_hist, d_mu_ind, 0);
+            MDFF_LAUNCH(*this, k_aspc_predict, nb, 256, 0, n, aspc_coef(e, false), es, d_hist, d_mu_ind);
         } else {
             ko_inner(d_cg_p, d_cg_r);
             MDFF_LAUNCH(*this, k_scale_add3, nb, 256, 0, n, 1.0, d_cg_p, 1.0, d_mu_ind);

@@ -153,6 +153,11 @@ void launch_rec(Engine &e, const double *q, const double3 *mu, bool lq, bool ld,
 void fit_status(unsigned status);
 constexpr int FIT_NRES = 1 + MDFFGPU_FIT_NPARAM + 1;   // loss, gradient, status bits per evaluation
 // integrate.cu
+struct AspcCoef {
+    int ne;          // values of the history used (order + 1)
+    double c[6];     // their coefficients, newest first
+};
+AspcCoef aspc_coef(int e, bool poly);
 void launch_reduce_slots(Engine &e, int first_slot, int nslots, int nparts);
 // true once the FP32 pair/k-space kernels exist in this build
 inline bool mixed_available() { return true; }

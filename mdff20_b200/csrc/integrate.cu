@@ -157,29 +157,41 @@ __global__ void k_induced(int n, const int *__restrict__ polar, const double *__
     mu[i] = pol_times(pol + (size_t)i * 9, ef[i]);
 }
 
-// extrapolate_dipole_aspc predictor (src/pim.c:381-400) for order `e`, then the
-// history shift by `es` places
-__global__ void k_aspc_predict(int n, int e, int es, double *__restrict__ hist, double3 *__restrict__ mu, int poly) {
+// extrapolate_dipole_aspc predictor coefficients (src/pim.c:381-400) of order e, or
+// (poly) those of the polynomial through the last e + 1 values, (-1)^k C(e + 1, k + 1);
+// computed here once per launch, so the kernel indexes no table by a runtime order
+AspcCoef aspc_coef(int e, bool poly) {
+    static const double Bt[6][6] = {{1.0, 0, 0, 0, 0, 0},
+                                    {2.0, -1.0, 0, 0, 0, 0},
+                                    {2.5, -2.0, 0.5, 0, 0, 0},
+                                    {2.8, -2.8, 1.2, -0.2, 0, 0},
+                                    {3.0, -24.0 / 7.0, 27.0 / 14.0, -4.0 / 7.0, 1.0 / 14.0, 0},
+                                    {22.0 / 7.0, -55.0 / 14.0, 55.0 / 21.0, -22.0 / 21.0, 5.0 / 21.0, -1.0 / 42.0}};
+    static const double Pt[6][6] = {{1.0, 0, 0, 0, 0, 0},
+                                    {2.0, -1.0, 0, 0, 0, 0},
+                                    {3.0, -3.0, 1.0, 0, 0, 0},
+                                    {4.0, -6.0, 4.0, -1.0, 0, 0},
+                                    {5.0, -10.0, 10.0, -5.0, 1.0, 0},
+                                    {6.0, -15.0, 20.0, -15.0, 6.0, -1.0}};
+    if (e < 0 || e > 5) throw Error(MDFFGPU_ERR_ARG, "extrapolate_order must be 0..5");
+    AspcCoef a;
+    a.ne = e + 1;
+    for (int k = 0; k < 6; k++) a.c[k] = poly ? Pt[e][k] : Bt[e][k];
+    return a;
+}
+
+// the predictor mu = sum_k c_k hist_k over the last cf.ne values, then the history
+// shift by `es` places
+__global__ void k_aspc_predict(int n, AspcCoef cf, int es, double *__restrict__ hist, double3 *__restrict__ mu) {
     grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const double Bt[6][6] = {{1.0, 0, 0, 0, 0, 0},
-                             {2.0, -1.0, 0, 0, 0, 0},
-                             {2.5, -2.0, 0.5, 0, 0, 0},
-                             {2.8, -2.8, 1.2, -0.2, 0, 0},
-                             {3.0, -24.0 / 7.0, 27.0 / 14.0, -4.0 / 7.0, 1.0 / 14.0, 0},
-                             {22.0 / 7.0, -55.0 / 14.0, 55.0 / 21.0, -22.0 / 21.0, 5.0 / 21.0, -1.0 / 42.0}};
-    // polynomial extrapolation through the last e + 1 values: (-1)^k C(e + 1, k + 1)
-    const double Pt[6][6] = {{1.0, 0, 0, 0, 0, 0},
-                             {2.0, -1.0, 0, 0, 0, 0},
-                             {3.0, -3.0, 1.0, 0, 0, 0},
-                             {4.0, -6.0, 4.0, -1.0, 0, 0},
-                             {5.0, -10.0, 10.0, -5.0, 1.0, 0},
-                             {6.0, -15.0, 20.0, -15.0, 6.0, -1.0}};
     double *h = hist + (size_t)i * ASPC_DEPTH * 3;
     double m[3] = {0.0, 0.0, 0.0};
-    for (int k = 0; k < e + 1; k++)
-        for (int c = 0; c < 3; c++) m[c] += (poly ? Pt[e][k] : Bt[e][k]) * h[3 * k + c];
+#pragma unroll
+    for (int k = 0; k < 6; k++)
+        if (k < cf.ne)
+            for (int c = 0; c < 3; c++) m[c] += cf.c[k] * h[3 * k + c];
     for (int k = es; k > 0; k--)
         for (int c = 0; c < 3; c++) h[3 * k + c] = h[3 * (k - 1) + c];
     mu[i] = make_double3(m[0], m[1], m[2]);

@@ -73,15 +73,27 @@ __global__ void k_check_disp(int n, Cell c, const double4 *__restrict__ s, const
     }
 }
 
+// one warp: strided top-2 of the block partials per lane, then the warp merge (the two
+// largest values, whatever the order they are met in)
 __global__ void k_check_final(int nparts, const double *__restrict__ part1, const double *__restrict__ part2,
                               double skindiff, int *rebuild, DevScalars *out) {
     grid_dep();
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (blockIdx.x) return;
+    const int l = threadIdx.x;
     double m1 = 0.0, m2 = 0.0;
-    for (int k = 0; k < nparts; k++) {
+    for (int k = l; k < nparts; k += 32) {
         top2_insert(m1, m2, part1[k]);
         top2_insert(m1, m2, part2[k]);
     }
+    for (int o = 16; o > 0; o >>= 1) {
+        double o1 = __shfl_xor_sync(0xffffffffu, m1, o);
+        double o2 = __shfl_xor_sync(0xffffffffu, m2, o);
+        double n1 = fmax(m1, o1);
+        double n2 = fmax(fmin(m1, o1), fmax(m2, o2));
+        m1 = n1;
+        m2 = n2;
+    }
+    if (l) return;
     int rb = (m1 + m2 > skindiff) ? 1 : 0;  // src/verlet.c:148
     *rebuild = rb;
     out->rebuild = rb;
