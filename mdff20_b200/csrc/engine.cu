@@ -118,6 +118,12 @@ Engine::Engine(const mdffgpu_params &prm, int dev) : p(prm) {
     MDFF_CK(cudaGetDevice(&device));
     MDFF_CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     MDFF_CK(cudaStreamCreateWithFlags(&body_stream, cudaStreamNonBlocking));
+    for (int k = 0; k < NSIDE; k++) {
+        MDFF_CK(cudaStreamCreateWithFlags(&side[k], cudaStreamNonBlocking));
+        MDFF_CK(cudaEventCreateWithFlags(&ev_fork[k], cudaEventDisableTiming));
+        MDFF_CK(cudaEventCreateWithFlags(&ev_join[k], cudaEventDisableTiming));
+    }
+    if (const char *v = getenv("MDFFGPU_SIDE_STREAMS")) side_on = atoi(v) != 0;
     setup_units_and_cell();
     setup_types();
     // device buffers
@@ -224,6 +230,11 @@ Engine::~Engine() {
     if (step_exec) cudaGraphExecDestroy(step_exec);
     if (fit_exec) cudaGraphExecDestroy(fit_exec);
     if (body_stream) cudaStreamDestroy(body_stream);
+    for (int k = 0; k < NSIDE; k++) {
+        if (ev_fork[k]) cudaEventDestroy(ev_fork[k]);
+        if (ev_join[k]) cudaEventDestroy(ev_join[k]);
+        if (side[k]) cudaStreamDestroy(side[k]);
+    }
     if (stream) cudaStreamDestroy(stream);
 }
 
@@ -1159,7 +1170,11 @@ void Engine::pim_ko() {
 void Engine::get_dipoles() {
     // mixed precision: in-cutoff list and dipole-field records of these positions (the
     // real-space kernels of this force evaluation read them)
-    if (use32 && real32) launch_pair_prep32(*this);
+    if (use32 && real32) {
+        if (prep_issued) join_side(SIDE_PREP);   // issued beside the k-space tables
+        else launch_pair_prep32(*this);
+        prep_issued = false;
+    }
     if (lpol) {
         // positions are fixed through the solve: cache the dipole-field pair factors
         struct CoefScope {
@@ -1196,20 +1211,36 @@ void Engine::engforce() {
     ensure_lists();
     MDFF_CK(cudaMemsetAsync(d_f, 0, sizeof(double3) * n, stream));
     launch_kardir(*this, d_r, d_s);
+    // side branches from here (they read the fractional coordinates): the short-range
+    // pairs, which add into d_f (joined before the k-space force combine reads it), and
+    // in mixed precision the in-cutoff lists (joined before the dipole solve)
+    if (p.lnmlj || p.lbhmft || p.lbhmftd)
+        on_side(SIDE_SR, [&] {
+            if (p.lnmlj) sr_forces(true, nullptr, nullptr, nullptr);
+            if (p.lbhmft || p.lbhmftd) sr_forces(false, nullptr, nullptr, nullptr);
+        });
+    if (p.lcoulombic && use32 && real32) {
+        on_side(SIDE_PREP, [&] { launch_pair_prep32(*this); });
+        prep_issued = true;
+    }
     if (use32) launch_coords32(*this);
-    if (p.lnmlj) sr_forces(true, nullptr, nullptr, nullptr);
-    if (p.lbhmft || p.lbhmftd) sr_forces(false, nullptr, nullptr, nullptr);
     if (p.lcoulombic) {
         rho_acc_ready = false;
         get_dipoles();
         bool ld = (ldip || lpol);
-        // direct space: forces, energy, virial (do_forces, do_stress; src/field.c:381-383)
-        if (use32 && real32)
-            launch_dir32(*this, d_q, d_mu_tot, p.alphaES, lqch != 0, ld, ldmp != 0, true, false, nullptr, d_tmp3);
-        else
-            launch_dir(*this, d_q, d_mu_tot, p.alphaES, lqch != 0, ld, ldmp != 0, true, false, false, false,
-                       nullptr, nullptr, d_tmp3);
-        reduce(S_DIR_U, 7, ceil_div(n, 8));
+        // direct space: forces, energy, virial (do_forces, do_stress; src/field.c:381-383);
+        // beside the k-space force pass in mixed precision (launch_combine32 joins it)
+        auto direct = [&] {
+            if (use32 && real32)
+                launch_dir32(*this, d_q, d_mu_tot, p.alphaES, lqch != 0, ld, ldmp != 0, true, false, nullptr, d_tmp3);
+            else
+                launch_dir(*this, d_q, d_mu_tot, p.alphaES, lqch != 0, ld, ldmp != 0, true, false, false, false,
+                           nullptr, nullptr, d_tmp3);
+            reduce(S_DIR_U, 7, ceil_div(n, 8));
+        };
+        if (use32 && rec32) on_side(SIDE_DIR, direct);
+        else direct();
+        if (!(use32 && rec32)) join_side(SIDE_SR);
         RecOut o;
         o.f = d_f;
         o.f_dir = d_tmp3;
@@ -1217,11 +1248,14 @@ void Engine::engforce() {
         if (rho_acc_ready) o.rho_acc = d_rho_acc;   // rho(k) of (q, mu_tot) from the fused CG
         rho_acc_ready = false;
         launch_rec(*this, d_q, d_mu_tot, lqch != 0, ld, o);
+        join_side(SIDE_DIR);
         int nb = ceil_div(n, 256);
         MDFF_LAUNCH(*this, k_self_sums, nb, 256, 0, n, d_q, d_mu_tot, d_part, part_stride);
         reduce(S_Q2, 2, nb);
         finalize_coul(true);
     }
+    for (int k = 0; k < NSIDE; k++) join_side(k);
+    prep_issued = false;
     MDFF_LAUNCH(*this, k_check_finite, ceil_div(n, 256), 256, 0, n, d_r, d_f, d_status);
 }
 

@@ -351,6 +351,46 @@ struct Engine {
     bool capturing = false;                 // launches are being recorded
     bool pdl = true;                        // launches may carry the programmatic-serialization attribute
     cudaStream_t body_stream = nullptr;     // records the CG loop body
+    // Independent parts of a force evaluation run on side streams (in a recorded step:
+    // parallel branches of the graph).  on_side(k, f) issues f on side stream k after
+    // all that `stream` has issued; join_side(k) makes `stream` wait for it.  Forks are
+    // joined before the first reader of what they write, inside the same evaluation.
+    static constexpr int SIDE_SR = 0;       // short-range pair forces (add into d_f)
+    static constexpr int SIDE_PREP = 1;     // FP32 in-cutoff lists and dipole-field records
+    static constexpr int SIDE_DIR = 2;      // real-space Ewald forces (d_tmp3, S_DIR_U slots)
+    static constexpr int NSIDE = 3;
+    cudaStream_t side[NSIDE] = {};
+    cudaEvent_t ev_fork[NSIDE] = {}, ev_join[NSIDE] = {};
+    bool side_open[NSIDE] = {};
+    bool side_on = true;                    // MDFFGPU_SIDE_STREAMS=0: everything on `stream`
+    bool prep_issued = false;               // this evaluation's FP32 lists are issued (SIDE_PREP)
+    template <class F>
+    void on_side(int k, F &&f) {
+        if (!side_on) {
+            f();
+            return;
+        }
+        join_side(k);
+        MDFF_CK(cudaEventRecord(ev_fork[k], stream));
+        MDFF_CK(cudaStreamWaitEvent(side[k], ev_fork[k], 0));
+        cudaStream_t main = stream;
+        stream = side[k];
+        try {
+            f();
+        } catch (...) {
+            stream = main;
+            if (cudaEventRecord(ev_join[k], side[k]) == cudaSuccess) cudaStreamWaitEvent(stream, ev_join[k], 0);
+            throw;
+        }
+        stream = main;
+        MDFF_CK(cudaEventRecord(ev_join[k], side[k]));
+        side_open[k] = true;
+    }
+    void join_side(int k) {
+        if (!side_open[k]) return;
+        side_open[k] = false;
+        MDFF_CK(cudaStreamWaitEvent(stream, ev_join[k], 0));
+    }
     cudaGraphExec_t step_exec = nullptr;
     long long gen = 0, graph_gen = -1;      // gen: bumped when buffers or modes change
     long long graph_outer = 0, graph_body = 0, body_count = 0;   // kernels per replay / per CG iteration

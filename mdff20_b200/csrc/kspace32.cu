@@ -778,6 +778,9 @@ void launch_ion32(Engine &e, const double *q, const double3 *mu, bool ld, const 
 // and turned into field / force / self terms at ion idx[li] (li when idx is null)
 void launch_combine32(Engine &e, const double *q, const double3 *mu, bool ld, const RecOut &o, const int *idx,
                       int cnt, int slices, bool wf) {
+    // the real-space terms and the short-range forces it adds to, when they ran beside
+    e.join_side(Engine::SIDE_DIR);
+    e.join_side(Engine::SIDE_SR);
     Comb32Args b;
     b.cnt = cnt;
     b.nslice = slices;
