@@ -616,12 +616,13 @@ void Engine::fit_issue(const double3 *d_ft, double scale, int tSi, int tO, const
     if (!p.lcoulombic || !lpol) throw Error(MDFFGPU_ERR_STATE, "force matching needs the polarisable Coulomb model");
     if (pim_solver != MDFFGPU_PIM_CG && pim_solver != MDFFGPU_PIM_CG_FUSED)
         throw Error(MDFFGPU_ERR_STATE, "force matching needs a CG induced-dipole solver");
-    // fully serialised launches while an evaluation is issued (evaluations run concurrently)
-    struct NoPdl {
+    // fully serialised launches on the one stream while an evaluation is issued (many
+    // evaluations run concurrently; measured: both overlaps cost configurations per second)
+    struct Off {
         bool &f, old;
-        explicit NoPdl(bool &x) : f(x), old(x) { f = false; }
-        ~NoPdl() { f = old; }
-    } no_pdl(pdl);
+        explicit Off(bool &x) : f(x), old(x) { f = false; }
+        ~Off() { f = old; }
+    } no_pdl(pdl), no_side(side_on);
     fit_alloc();
     const double *q = d_q;
     int nb = ceil_div(n, 256), nbw = ceil_div(n, FIT_WARPS);
