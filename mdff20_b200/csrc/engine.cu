@@ -994,12 +994,19 @@ void Engine::pim_cg(bool fused) {
         // the residual reads the field at the polarisable ions only (FP64 real space
         // evaluates every ion; the k-space ion pass and FP32 real space only those)
         bool sub = subset32 && npol > 0;
-        if (use32 && real32)
-            launch_dir32(*this, d_q, d_mu_tot, p.alphaES, lqch != 0, true, ldmp != 0, false, true, d_tmp3, nullptr,
-                         sub ? d_pidx : nullptr, npol);
-        else
+        if (use32 && real32) {
+            // on the branch of the in-cutoff lists, beside the k-space passes below (the
+            // FP32 k-space combine joins it)
+            auto dir = [&] {
+                launch_dir32(*this, d_q, d_mu_tot, p.alphaES, lqch != 0, true, ldmp != 0, false, true, d_tmp3,
+                             nullptr, sub ? d_pidx : nullptr, npol);
+            };
+            if (rec32) on_side(SIDE_PREP, dir);
+            else dir();
+        } else {
             launch_dir(*this, d_q, d_mu_tot, p.alphaES, lqch != 0, true, ldmp != 0, false, true, false, false,
                        d_tmp3, nullptr, nullptr);
+        }
         RecOut o;
         o.ef = d_ef_ind;
         o.ef_dir = d_tmp3;
@@ -1011,6 +1018,7 @@ void Engine::pim_cg(bool fused) {
             o.out_cnt = npol;
         }
         launch_rec(*this, d_q, d_mu_tot, lqch != 0, true, o);
+        join_side(SIDE_PREP);   // (joined by the combine already; the loop below reads the records)
         MDFF_LAUNCH(*this, k_cg_residual, nb, 256, 0, n, d_polar, d_invpol, d_muzero, d_ef_ind, d_mu_ind, d_cg_r);
     } else {
         field_of(d_q, d_mu_static, lqch != 0, ldip != 0, ldmp != 0, d_ef_stat);
@@ -1171,8 +1179,11 @@ void Engine::get_dipoles() {
     // mixed precision: in-cutoff list and dipole-field records of these positions (the
     // real-space kernels of this force evaluation read them)
     if (use32 && real32) {
-        if (prep_issued) join_side(SIDE_PREP);   // issued beside the k-space tables
-        else launch_pair_prep32(*this);
+        // issued beside the k-space tables; the fused CG's first field pass continues that
+        // branch with its real-space part and its k-space combine joins it
+        const bool cont = lpol && pim_solver == MDFFGPU_PIM_CG_FUSED && rec32;
+        if (!prep_issued) launch_pair_prep32(*this);
+        else if (!cont) join_side(SIDE_PREP);
         prep_issued = false;
     }
     if (lpol) {

@@ -353,10 +353,12 @@ struct Engine {
     cudaStream_t body_stream = nullptr;     // records the CG loop body
     // Independent parts of a force evaluation run on side streams (in a recorded step:
     // parallel branches of the graph).  on_side(k, f) issues f on side stream k after
-    // all that `stream` has issued; join_side(k) makes `stream` wait for it.  Forks are
-    // joined before the first reader of what they write, inside the same evaluation.
+    // all that `stream` has issued and after what side k already holds; join_side(k)
+    // makes `stream` wait for all of side k.  Forks are joined before the first reader
+    // of what they write, inside the same evaluation.
     static constexpr int SIDE_SR = 0;       // short-range pair forces (add into d_f)
-    static constexpr int SIDE_PREP = 1;     // FP32 in-cutoff lists and dipole-field records
+    static constexpr int SIDE_PREP = 1;     // FP32 in-cutoff lists and dipole-field records, then the
+                                            // real-space part of the solve's first field pass (d_tmp3)
     static constexpr int SIDE_DIR = 2;      // real-space Ewald forces (d_tmp3, S_DIR_U slots)
     static constexpr int NSIDE = 3;
     cudaStream_t side[NSIDE] = {};
@@ -370,7 +372,6 @@ struct Engine {
             f();
             return;
         }
-        join_side(k);
         MDFF_CK(cudaEventRecord(ev_fork[k], stream));
         MDFF_CK(cudaStreamWaitEvent(side[k], ev_fork[k], 0));
         cudaStream_t main = stream;

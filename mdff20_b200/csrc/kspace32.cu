@@ -781,6 +781,7 @@ void launch_combine32(Engine &e, const double *q, const double3 *mu, bool ld, co
     // the real-space terms and the short-range forces it adds to, when they ran beside
     e.join_side(Engine::SIDE_DIR);
     e.join_side(Engine::SIDE_SR);
+    e.join_side(Engine::SIDE_PREP);
     Comb32Args b;
     b.cnt = cnt;
     b.nslice = slices;
