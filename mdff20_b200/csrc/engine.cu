@@ -124,6 +124,12 @@ Engine::Engine(const mdffgpu_params &prm, int dev) : p(prm) {
         MDFF_CK(cudaEventCreateWithFlags(&ev_join[k], cudaEventDisableTiming));
     }
     if (const char *v = getenv("MDFFGPU_SIDE_STREAMS")) side_on = atoi(v) != 0;
+    {
+        int least = 0, greatest = 0;
+        MDFF_CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        prio_high = greatest;
+        if (const char *v = getenv("MDFFGPU_TC_PRIORITY")) prio_high = atoi(v) ? greatest : 0;
+    }
     setup_units_and_cell();
     setup_types();
     // device buffers
@@ -785,8 +791,13 @@ void Engine::field_of(const double *d_qv, const double3 *d_muv, bool lq, bool ld
 // field of a CG search direction p, which vanishes off the polarisable ions: the
 // k-space passes run over those ions only and the field is written there only
 void Engine::field_pol(const double3 *d_p, double3 *d_out, double2 *rho_raw, bool cg_ap) {
-    if (use32 && real32) launch_pol_field32(*this, d_p, d_tmp3);
-    else launch_dir_field_cached(*this, d_p, d_tmp3);
+    auto real = [&] {
+        if (use32 && real32) launch_pol_field32(*this, d_p, d_tmp3);
+        else launch_dir_field_cached(*this, d_p, d_tmp3);
+    };
+    // beside the k-space passes when launch_combine32 reads d_tmp3 (mixed k space)
+    if (use32 && rec32) on_side(stream == body_stream ? SIDE_BODY : SIDE_FIELD, real);
+    else real();
     RecOut o;
     o.ef = d_out;
     o.ef_dir = d_tmp3;
@@ -1485,7 +1496,7 @@ void Engine::capture_step(int step) {
     }
     capturing = false;
     MDFF_CK(cudaStreamEndCapture(stream, &graph));
-    cudaError_t err = cudaGraphInstantiate(&step_exec, graph, 0);
+    cudaError_t err = cudaGraphInstantiate(&step_exec, graph, cudaGraphInstantiateFlagUseNodePriority);
     cudaGraphDestroy(graph);
     if (err != cudaSuccess) {
         step_exec = nullptr;

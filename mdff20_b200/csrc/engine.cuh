@@ -350,6 +350,16 @@ struct Engine {
     bool graph_on = true;
     bool capturing = false;                 // launches are being recorded
     bool pdl = true;                        // launches may carry the programmatic-serialization attribute
+    // launch priority (0: the stream's).  The tensor-core k-space passes launch at the
+    // device's greatest priority (prio_high) so that, where a side branch runs beside
+    // them, the block scheduler places their large-shared-memory CTAs first and the
+    // side grid fills what is left; recorded graphs keep it per node.
+    int prio = 0, prio_high = 0;
+    struct HighPrio {
+        Engine &e;
+        explicit HighPrio(Engine &x) : e(x) { e.prio = e.prio_high; }
+        ~HighPrio() { e.prio = 0; }
+    };
     cudaStream_t body_stream = nullptr;     // records the CG loop body
     // Independent parts of a force evaluation run on side streams (in a recorded step:
     // parallel branches of the graph).  on_side(k, f) issues f on side stream k after
@@ -360,7 +370,12 @@ struct Engine {
     static constexpr int SIDE_PREP = 1;     // FP32 in-cutoff lists and dipole-field records, then the
                                             // real-space part of the solve's first field pass (d_tmp3)
     static constexpr int SIDE_DIR = 2;      // real-space Ewald forces (d_tmp3, S_DIR_U slots)
-    static constexpr int NSIDE = 3;
+    // the real-space field of a field pass (d_tmp3) beside its k-space passes: SIDE_BODY
+    // while a loop body is recorded (a stream that joined one capture cannot join the
+    // body's, which is recorded inside it), SIDE_FIELD otherwise
+    static constexpr int SIDE_BODY = 3;
+    static constexpr int SIDE_FIELD = 4;
+    static constexpr int NSIDE = 5;
     cudaStream_t side[NSIDE] = {};
     cudaEvent_t ev_fork[NSIDE] = {}, ev_join[NSIDE] = {};
     bool side_open[NSIDE] = {};
@@ -487,16 +502,23 @@ inline bool pdl_enabled() {
 // launch bookkeeping: every kernel launch goes through this
 #define MDFF_LAUNCH(eng, kernel, grid, block, smem, ...)                               \
     do {                                                                               \
-        cudaLaunchAttribute at_[1];                                                    \
-        at_[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;                \
-        at_[0].val.programmaticStreamSerializationAllowed = 1;                         \
+        cudaLaunchAttribute at_[2];                                                    \
+        unsigned na_ = 0;                                                              \
+        if ((eng).pdl && pdl_enabled()) {                                              \
+            at_[na_].id = cudaLaunchAttributeProgrammaticStreamSerialization;          \
+            at_[na_++].val.programmaticStreamSerializationAllowed = 1;                 \
+        }                                                                              \
+        if ((eng).prio) {                                                              \
+            at_[na_].id = cudaLaunchAttributePriority;                                 \
+            at_[na_++].val.priority = (eng).prio;                                      \
+        }                                                                              \
         cudaLaunchConfig_t cfg_ = {};                                                  \
         cfg_.gridDim = dim3(grid);                                                     \
         cfg_.blockDim = dim3(block);                                                   \
         cfg_.dynamicSmemBytes = (smem);                                                \
         cfg_.stream = (eng).stream;                                                    \
         cfg_.attrs = at_;                                                              \
-        cfg_.numAttrs = ((eng).pdl && pdl_enabled()) ? 1 : 0;                          \
+        cfg_.numAttrs = na_;                                                           \
         MDFF_CK(cudaLaunchKernelEx(&cfg_, kernel, __VA_ARGS__));                       \
         (eng).launches++;                                                              \
     } while (0)

@@ -760,7 +760,7 @@ void Engine::capture_fit(const double *d_th, int tSi, int tO, double scale, doub
     }
     capturing = false;
     MDFF_CK(cudaStreamEndCapture(stream, &graph));
-    cudaError_t err = cudaGraphInstantiate(&fit_exec, graph, 0);
+    cudaError_t err = cudaGraphInstantiate(&fit_exec, graph, cudaGraphInstantiateFlagUseNodePriority);
     cudaGraphDestroy(graph);
     if (err != cudaSuccess) {
         fit_exec = nullptr;

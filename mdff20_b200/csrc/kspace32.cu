@@ -782,6 +782,8 @@ void launch_combine32(Engine &e, const double *q, const double3 *mu, bool ld, co
     e.join_side(Engine::SIDE_DIR);
     e.join_side(Engine::SIDE_SR);
     e.join_side(Engine::SIDE_PREP);
+    e.join_side(Engine::SIDE_BODY);
+    e.join_side(Engine::SIDE_FIELD);
     Comb32Args b;
     b.cnt = cnt;
     b.nslice = slices;

@@ -433,6 +433,7 @@ static void ion_tc_run(Engine &e, const IonTcArgs &a, int tiles, int slices, int
     std::call_once(once, [] {
         MDFF_CK(cudaFuncSetAttribute(k_ion_tc<NC>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
     });
+    Engine::HighPrio hp(e);
     MDFF_LAUNCH(e, k_ion_tc<NC>, dim3(tiles, slices), IT_THREADS, smem, a);
 }
 

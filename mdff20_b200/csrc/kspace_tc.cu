@@ -528,6 +528,7 @@ bool launch_rho_tc(Engine &e, const double *q, const double3 *mu, bool lq, bool 
     std::call_once(once, [] {
         MDFF_CK(cudaFuncSetAttribute(k_rho_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
     });
+    Engine::HighPrio hp(e);
     MDFF_LAUNCH(e, k_rho_tc, dim3(ceil_div(e.nrow, RT_ROWS), chunks), RT_THREADS, rt_smem(a.lz).total, a);
     *chunks_used = chunks;
     return true;
