@@ -716,10 +716,14 @@ int Engine::check_verletlist(bool reset_status) {
         return 1;
     }
     if (reset_status) MDFF_CK(cudaMemsetAsync(d_status, 0, sizeof(unsigned), stream));
-    launch_kardir(*this, d_r, d_s);
+    if (capturing) {
+        // the rebuild as an IF node: on the steps without one its kernels do not launch
+        record_if([&](cudaGraphConditionalHandle h) { launch_check_list(*this, &h); },
+                  [&] { launch_build_lists(*this, false); });
+        return 0;   // the host reads the rebuild flag and status after the step
+    }
     launch_check_list(*this);
     launch_build_lists(*this, false);
-    if (capturing) return 0;   // the host reads the rebuild flag and status after the step
     int rb = 0;
     unsigned st = 0;
     MDFF_CK(cudaMemcpyAsync(&rb, d_rebuild, sizeof(int), cudaMemcpyDeviceToHost, stream));
@@ -938,6 +942,47 @@ void Engine::pim_reference() {
     double v = 0.5 * upol * coul_unit;   // get_upol returns 0.5*sum (src/pim.c:160)
     MDFF_CK(cudaMemcpyAsync(&d_out->u_pol, &v, sizeof(double), cudaMemcpyHostToDevice, stream));
     MDFF_CK(cudaStreamSynchronize(stream));
+}
+
+// While recording: a device-controlled branch.  `test` issues the kernel that sets the
+// condition through the handle, then an IF node is added and `body` is recorded into its
+// body graph on body_stream (if_count receives its launches).
+void Engine::record_if(const std::function<void(cudaGraphConditionalHandle)> &test,
+                       const std::function<void()> &body) {
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t cgraph = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    cudaGraphConditionalHandle h;
+    MDFF_CK(cudaStreamGetCaptureInfo(stream, &cs, nullptr, &cgraph, nullptr, nullptr));
+    MDFF_CK(cudaGraphConditionalHandleCreate(&h, cgraph, 0, 0));
+    test(h);
+    MDFF_CK(cudaStreamGetCaptureInfo(stream, &cs, nullptr, &cgraph, &deps, &ndeps));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    MDFF_CK(cudaGraphAddNode(&node, cgraph, deps, ndeps, &cp));
+    cudaGraph_t bgraph = cp.conditional.phGraph_out[0];
+    MDFF_CK(cudaStreamUpdateCaptureDependencies(stream, &node, 1, cudaStreamSetCaptureDependencies));
+    cudaStream_t outer = stream;
+    stream = body_stream;
+    MDFF_CK(cudaStreamBeginCaptureToGraph(stream, bgraph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    try {
+        long long b0 = launches;
+        body();
+        if_count += launches - b0;
+    } catch (...) {
+        cudaGraph_t g2 = nullptr;
+        cudaStreamEndCapture(stream, &g2);
+        stream = outer;
+        throw;
+    }
+    cudaGraph_t g2 = nullptr;
+    MDFF_CK(cudaStreamEndCapture(stream, &g2));
+    stream = outer;
 }
 
 // While recording: a device-controlled loop.  `first` issues the test that decides
@@ -1480,6 +1525,7 @@ void Engine::capture_step(int step) {
     MDFF_CK(cudaStreamSynchronize(stream));
     long long l0 = launches;
     body_count = 0;
+    if_count = 0;
     MDFF_CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     capturing = true;
     cudaGraph_t graph = nullptr;
@@ -1503,7 +1549,8 @@ void Engine::capture_step(int step) {
         MDFF_CK(err);
     }
     graph_body = body_count;
-    graph_outer = launches - l0 - body_count;
+    graph_if = if_count;
+    graph_outer = launches - l0 - body_count - if_count;
     launches = l0;
     graph_gen = gen;
 }
@@ -1525,7 +1572,7 @@ void Engine::md_steps(int first, int nsteps, double *thermo) {
         }
         sync_scalars();
         if (graphed) {
-            launches += graph_outer + graph_body * std::max(h_out->scf_iter, 0);
+            launches += graph_outer + graph_body * std::max(h_out->scf_iter, 0) + (h_out->rebuild ? graph_if : 0);
             if (p.lcoulombic && lpol) {
                 last_scf_iter = h_out->scf_iter;
                 last_rmsd = h_out->scf_rmsd;

@@ -102,7 +102,8 @@ inline T *dalloc(size_t count) {
 // ---------------------------------------------------------------- launchers
 // lists.cu
 void launch_kardir(Engine &e, const double4 *r, double4 *s);
-void launch_check_list(Engine &e);             // sets e.d_rebuild on the device
+// sets e.d_rebuild on the device (and, given a handle, the condition of a recorded IF node)
+void launch_check_list(Engine &e, const cudaGraphConditionalHandle *h = nullptr);
 void launch_build_lists(Engine &e, bool force); // gated by d_rebuild unless force
 // pair.cu
 void launch_sr(Engine &e, bool lj);            // adds forces into e.d_f, partials into slots
@@ -410,6 +411,7 @@ struct Engine {
     cudaGraphExec_t step_exec = nullptr;
     long long gen = 0, graph_gen = -1;      // gen: bumped when buffers or modes change
     long long graph_outer = 0, graph_body = 0, body_count = 0;   // kernels per replay / per CG iteration
+    long long graph_if = 0, if_count = 0;   // kernels of the list rebuild (an IF node) per rebuild
 
     explicit Engine(const mdffgpu_params &prm, int dev);
     ~Engine();
@@ -473,6 +475,7 @@ struct Engine {
     // launch shapes of the mixed k space timed on this system (the field pass of the CG):
     // choice = {tensor-core ion pass, rho chunks, ion-pass slices}, ms = its time
     void tune_launch(int reps, int *choice, double *ms);
+    void record_if(const std::function<void(cudaGraphConditionalHandle)> &test, const std::function<void()> &body);
     void record_while(const std::function<void(cudaGraphConditionalHandle)> &first,
                       const std::function<void(cudaGraphConditionalHandle)> &body);
     void drop_graph();

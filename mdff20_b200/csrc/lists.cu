@@ -36,18 +36,9 @@ __device__ __forceinline__ void top2_insert(double &m1, double &m2, double d) {
     }
 }
 
-__global__ void k_check_disp(int n, Cell c, const double4 *__restrict__ s, const double4 *__restrict__ svl,
-                             double *__restrict__ part1, double *__restrict__ part2) {
-    grid_dep();
-    __shared__ double sm1[32], sm2[32];
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    double m1 = 0.0, m2 = 0.0;
-    if (i < n) {
-        double4 a = s[i], b = svl[i];
-        double3 d = pbc_frac(c, dsub(a.x, b.x), dsub(a.y, b.y), dsub(a.z, b.z));
-        m1 = __dsqrt_rn(norm2_exact(d));
-    }
-    // warp top-2 merge
+// warp merge of per-lane top-2 pairs (the two largest values, whatever the order they
+// are met in)
+__device__ __forceinline__ void top2_warp(double &m1, double &m2) {
     for (int o = 16; o > 0; o >>= 1) {
         double o1 = __shfl_xor_sync(0xffffffffu, m1, o);
         double o2 = __shfl_xor_sync(0xffffffffu, m2, o);
@@ -56,7 +47,44 @@ __global__ void k_check_disp(int n, Cell c, const double4 *__restrict__ s, const
         m1 = n1;
         m2 = n2;
     }
-    int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+}
+
+// check_verletlist in one launch: the fractional coordinates of the current positions
+// (kardir, written to s for a rebuild), each ion's displacement since the last build and
+// per block its two largest (src/verlet.c:134-147); the last block to finish merges the
+// block pairs and tests them against the skin (src/verlet.c:148).  On a rebuild it also
+// zeroes the cell counts the binning adds to, and in a recorded step it sets the
+// condition of the IF node that holds the rebuild (use_h).
+struct CheckArgs {
+    int n, ncell;
+    Cell c;
+    const double4 *r;
+    double4 *s;
+    const double4 *svl;
+    double *part1, *part2;
+    unsigned *ticket;
+    double skindiff;
+    int *rebuild, *cell_cnt;
+    DevScalars *out;
+    cudaGraphConditionalHandle h;
+    int use_h;
+};
+__global__ void __launch_bounds__(256) k_check_list(CheckArgs a) {
+    grid_dep();
+    __shared__ double sm1[8], sm2[8];
+    __shared__ bool last;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double m1 = 0.0, m2 = 0.0;
+    if (i < a.n) {
+        const double4 ri = a.r[i];
+        const double3 f = kardir(a.c, ri.x, ri.y, ri.z);
+        a.s[i] = make_double4(f.x, f.y, f.z, ri.w);
+        const double4 b = a.svl[i];
+        const double3 d = pbc_frac(a.c, dsub(f.x, b.x), dsub(f.y, b.y), dsub(f.z, b.z));
+        m1 = __dsqrt_rn(norm2_exact(d));
+    }
+    top2_warp(m1, m2);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
     if (l == 0) {
         sm1[w] = m1;
         sm2[w] = m2;
@@ -68,36 +96,36 @@ __global__ void k_check_disp(int n, Cell c, const double4 *__restrict__ s, const
             top2_insert(a1, a2, sm1[k]);
             top2_insert(a1, a2, sm2[k]);
         }
-        part1[blockIdx.x] = a1;
-        part2[blockIdx.x] = a2;
+        a.part1[blockIdx.x] = a1;
+        a.part2[blockIdx.x] = a2;
+        __threadfence();
+        last = atomicAdd(a.ticket, 1u) == gridDim.x - 1;
     }
-}
-
-// one warp: strided top-2 of the block partials per lane, then the warp merge (the two
-// largest values, whatever the order they are met in)
-__global__ void k_check_final(int nparts, const double *__restrict__ part1, const double *__restrict__ part2,
-                              double skindiff, int *rebuild, DevScalars *out) {
-    grid_dep();
-    if (blockIdx.x) return;
-    const int l = threadIdx.x;
-    double m1 = 0.0, m2 = 0.0;
-    for (int k = l; k < nparts; k += 32) {
-        top2_insert(m1, m2, part1[k]);
-        top2_insert(m1, m2, part2[k]);
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    __shared__ int rb_s;
+    if (w == 0) {
+        const volatile double *p1 = a.part1, *p2 = a.part2;
+        double b1 = 0.0, b2 = 0.0;
+        for (int k = l; k < (int)gridDim.x; k += 32) {
+            top2_insert(b1, b2, p1[k]);
+            top2_insert(b1, b2, p2[k]);
+        }
+        top2_warp(b1, b2);
+        if (l == 0) {
+            const int rb = (b1 + b2 > a.skindiff) ? 1 : 0;   // src/verlet.c:148
+            *a.rebuild = rb;
+            a.out->rebuild = rb;
+            if (rb) a.out->nbuilds += 1;
+            if (a.use_h) cudaGraphSetConditional(a.h, rb ? 1u : 0u);
+            *a.ticket = 0u;
+            rb_s = rb;
+        }
     }
-    for (int o = 16; o > 0; o >>= 1) {
-        double o1 = __shfl_xor_sync(0xffffffffu, m1, o);
-        double o2 = __shfl_xor_sync(0xffffffffu, m2, o);
-        double n1 = fmax(m1, o1);
-        double n2 = fmax(fmin(m1, o1), fmax(m2, o2));
-        m1 = n1;
-        m2 = n2;
-    }
-    if (l) return;
-    int rb = (m1 + m2 > skindiff) ? 1 : 0;  // src/verlet.c:148
-    *rebuild = rb;
-    out->rebuild = rb;
-    if (rb) out->nbuilds += 1;
+    __syncthreads();
+    if (rb_s)
+        for (int k = threadIdx.x; k < a.ncell; k += blockDim.x) a.cell_cnt[k] = 0;
 }
 
 __global__ void k_force_rebuild(int *rebuild, DevScalars *out) {
@@ -107,12 +135,24 @@ __global__ void k_force_rebuild(int *rebuild, DevScalars *out) {
     out->nbuilds += 1;
 }
 
-void launch_check_list(Engine &e) {
-    int nb = ceil_div(e.n, 256);
-    double *p1 = e.d_part + (size_t)S_DISP1 * e.part_stride;
-    double *p2 = e.d_part + (size_t)S_DISP2 * e.part_stride;
-    MDFF_LAUNCH(e, k_check_disp, nb, 256, 0, e.n, e.cell, e.d_s, e.d_svl, p1, p2);
-    MDFF_LAUNCH(e, k_check_final, 1, 32, 0, nb, p1, p2, e.p.skindiff, e.d_rebuild, e.d_out);
+void launch_check_list(Engine &e, const cudaGraphConditionalHandle *h) {
+    CheckArgs a;
+    a.n = e.n;
+    a.ncell = e.ncell;
+    a.c = e.cell;
+    a.r = e.d_r;
+    a.s = e.d_s;
+    a.svl = e.d_svl;
+    a.part1 = e.d_part + (size_t)S_DISP1 * e.part_stride;
+    a.part2 = e.d_part + (size_t)S_DISP2 * e.part_stride;
+    a.ticket = e.d_ticket + 5;
+    a.skindiff = e.p.skindiff;
+    a.rebuild = e.d_rebuild;
+    a.cell_cnt = e.d_cell_cnt;
+    a.out = e.d_out;
+    a.h = h ? *h : cudaGraphConditionalHandle{};
+    a.use_h = h != nullptr;
+    MDFF_LAUNCH(e, k_check_list, ceil_div(e.n, 256), 256, 0, a);
 }
 
 // ---------------------------------------------------------------- cell binning
@@ -292,7 +332,8 @@ __global__ void k_build(int n, Cell c, int3 nc, const double4 *__restrict__ s, c
 void launch_build_lists(Engine &e, bool force) {
     if (force) MDFF_LAUNCH(e, k_force_rebuild, 1, 1, 0, e.d_rebuild, e.d_out);
     int3 nc = make_int3(e.nc[0], e.nc[1], e.nc[2]);
-    MDFF_CK(cudaMemsetAsync(e.d_cell_cnt, 0, sizeof(int) * e.ncell, e.stream));
+    // after k_check_list the counts are zero already when a rebuild is due
+    if (force) MDFF_CK(cudaMemsetAsync(e.d_cell_cnt, 0, sizeof(int) * e.ncell, e.stream));
     MDFF_LAUNCH(e, k_bin, ceil_div(e.n, 256), 256, 0, e.n, nc, e.d_s, e.d_cell_of, e.d_cell_cnt, e.d_rebuild);
     MDFF_LAUNCH(e, k_scan_cells, 1, 1024, 0, e.ncell, e.d_cell_cnt, e.d_cell_start, e.d_cell_cur, e.cell_cap,
                 e.d_status, e.d_rebuild);
