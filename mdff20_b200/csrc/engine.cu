@@ -55,9 +55,8 @@ __global__ void k_vv2(int n, double dt2, const double *invm, const double *mass,
                       const double3 *fs, double *part, int stride);
 __global__ void k_pv1(int n, double dt, double dt2, const double *invm, double4 *r, double3 *v, const double3 *f);
 __global__ void k_pv2(int n, double dt2, const double *invm, const double *mass, double3 *v, const double3 *f,
-                      double *part, int stride);
-__global__ void k_scale_kin(int n, const DevScalars *out, int scale, const double *mass, double3 *v, double *part,
-                            int stride);
+                      double *part, int stride, double *scal, unsigned *ticket, const double4 *r, unsigned *status);
+__global__ void k_scale_kin(ScaleKinArgs a);
 __global__ void k_lf(int n, double dtsq, double idt, const double *invm, const double *mass, double4 *r,
                      double3 *rs, double3 *v, const double3 *f, double *part, int stride);
 struct NhcArgs {
@@ -65,8 +64,6 @@ struct NhcArgs {
     double dt, temp, L, w[7];
 };
 void launch_nhc_chain(Engine &e, const NhcArgs &a, double *nhc, const double *scal, DevScalars *out);
-__global__ void k_nhc_energy(int nn, double L, double temp, const double *nhc, const double *scal,
-                             DevScalars *out);
 __global__ void k_set_ekin(const double *scal, DevScalars *out);
 __global__ void k_check_finite(int n, const double4 *r, const double3 *f, unsigned *status);
 __global__ void k_sort_cells(int ncell, int cell_cap, const int *start, const int *cnt, int *ions,
@@ -1274,7 +1271,7 @@ void Engine::finalize_coul(bool stress) {
 }
 
 // engforce, src/field.c:352-407
-void Engine::engforce() {
+void Engine::engforce(bool check_finite) {
     ensure_lists();
     MDFF_CK(cudaMemsetAsync(d_f, 0, sizeof(double3) * n, stream));
     launch_kardir(*this, d_r, d_s);
@@ -1323,7 +1320,7 @@ void Engine::engforce() {
     }
     for (int k = 0; k < NSIDE; k++) join_side(k);
     prep_issued = false;
-    MDFF_LAUNCH(*this, k_check_finite, ceil_div(n, 256), 256, 0, n, d_r, d_f, d_status);
+    if (check_finite) MDFF_LAUNCH(*this, k_check_finite, ceil_div(n, 256), 256, 0, n, d_r, d_f, d_status);
 }
 
 // multipole_ES on caller data (src/ewald.c:75-348)
@@ -1472,18 +1469,34 @@ void Engine::prop_agate(int step) {
         default: throw Error(MDFFGPU_ERR_ARG, "nhc_yosh_order must be 1, 3, 5 or 7");
         }
         if (a.nn < 2 || a.nn > 16) throw Error(MDFFGPU_ERR_ARG, "nhc_n must be in 2..16");
-        MDFF_LAUNCH(*this, k_scale_kin, nb, 256, 0, n, d_out, 0, d_mass, d_v, d_part, part_stride);
-        reduce(S_KIN, 1, nb);
+        // the kinetic sums are reduced by the last block of the kernel that forms them
+        ScaleKinArgs sk;
+        sk.n = n;
+        sk.energy = 0;
+        sk.nn = a.nn;
+        sk.L = a.L;
+        sk.temp = temp;
+        sk.out_s = d_out;
+        sk.mass = d_mass;
+        sk.nhc = d_nhc;
+        sk.v = d_v;
+        sk.part = d_part;
+        sk.scal = d_scal;
+        sk.stride = part_stride;
+        sk.ticket = d_ticket + 6;
+        sk.out = d_out;
+        sk.scale = 0;
+        MDFF_LAUNCH(*this, k_scale_kin, nb, 256, 0, sk);
         launch_nhc_chain(*this, a, d_nhc, d_scal, d_out);
-        MDFF_LAUNCH(*this, k_scale_kin, nb, 256, 0, n, d_out, 1, d_mass, d_v, d_part, part_stride);
+        sk.scale = 1;
+        MDFF_LAUNCH(*this, k_scale_kin, nb, 256, 0, sk);
         MDFF_LAUNCH(*this, k_pv1, nb, 256, 0, n, dt, dt * 0.5, d_invmass, d_r, d_v, d_f);
-        engforce();
-        MDFF_LAUNCH(*this, k_pv2, nb, 256, 0, n, dt * 0.5, d_invmass, d_mass, d_v, d_f, d_part, part_stride);
-        reduce(S_KIN, 1, nb);
+        engforce(false);   // the finiteness check runs in k_pv2
+        MDFF_LAUNCH(*this, k_pv2, nb, 256, 0, n, dt * 0.5, d_invmass, d_mass, d_v, d_f, d_part, part_stride,
+                    d_scal, d_ticket + 6, d_r, d_status);
         launch_nhc_chain(*this, a, d_nhc, d_scal, d_out);
-        MDFF_LAUNCH(*this, k_scale_kin, nb, 256, 0, n, d_out, 1, d_mass, d_v, d_part, part_stride);
-        reduce(S_KIN, 1, nb);
-        MDFF_LAUNCH(*this, k_nhc_energy, 1, 1, 0, a.nn, a.L, temp, d_nhc, d_scal, d_out);
+        sk.energy = 1;   // then e_kin and e_nvt
+        MDFF_LAUNCH(*this, k_scale_kin, nb, 256, 0, sk);
         break;
     }
     default: {  // prop_velocity_verlet, src/integration.c:22-63

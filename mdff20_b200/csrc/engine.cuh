@@ -159,6 +159,19 @@ struct AspcCoef {
     double c[6];     // their coefficients, newest first
 };
 AspcCoef aspc_coef(int e, bool poly);
+// k_scale_kin: v *= nhc_s (scale), the kinetic sum into scal[S_KIN], then (energy) e_kin
+// and e_nvt
+struct ScaleKinArgs {
+    int n, scale, energy, nn;
+    double L, temp;
+    const DevScalars *out_s;
+    const double *mass, *nhc;
+    double3 *v;
+    double *part, *scal;
+    int stride;
+    unsigned *ticket;
+    DevScalars *out;
+};
 void launch_reduce_slots(Engine &e, int first_slot, int nslots, int nparts);
 // true once the FP32 pair/k-space kernels exist in this build
 inline bool mixed_available() { return true; }
@@ -433,7 +446,7 @@ struct Engine {
     void gen_verletlist();
     int check_verletlist(bool reset_status = true);
     void ensure_lists();
-    void engforce();
+    void engforce(bool check_finite = true);   // check_finite: ST_NONFINITE from r and f
     void sr_forces(bool lj, double *u, double *pvir, double *tau);
     void sr_finish(bool lj);   // reduce the short-range slot, u / virial / stress into d_out
     void multipole_es_dev(const double *d_qv, const double3 *d_muv, double alpha, int flags, double3 *d_ef_out,

@@ -502,14 +502,24 @@ __global__ void k_pv1(int n, double dt, double dt2, const double *__restrict__ i
 }
 
 // ... and the second half kick + kinetic partials
-__global__ void k_pv2(int n, double dt2, const double *__restrict__ invm, const double *__restrict__ mass,
-                      double3 *__restrict__ v, const double3 *__restrict__ f, double *part, int stride) {
+// second half kick of prop_velocity_verlet within nhcn (src/integration.c:165-167), the
+// kinetic sum reduced by the last block into scal[S_KIN]; with r: the finiteness check of
+// positions and forces (ST_NONFINITE) in the same pass
+__global__ void __launch_bounds__(256) k_pv2(int n, double dt2, const double *__restrict__ invm,
+                                             const double *__restrict__ mass, double3 *__restrict__ v,
+                                             const double3 *__restrict__ f, double *part, int stride,
+                                             double *scal, unsigned *ticket, const double4 *__restrict__ r,
+                                             unsigned *status) {
     grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double k[1] = {0.0};
     if (i < n) {
         double3 vv = v[i], ff = f[i];
         double im = invm[i];
+        if (r) {
+            double4 x = r[i];
+            if (!isfinite(x.x + x.y + x.z + ff.x + ff.y + ff.z)) atomicOr(status, ST_NONFINITE);
+        }
         vv.x += ff.x * dt2 * im;
         vv.y += ff.y * dt2 * im;
         vv.z += ff.z * dt2 * im;
@@ -517,26 +527,49 @@ __global__ void k_pv2(int n, double dt2, const double *__restrict__ invm, const 
         k[0] = (vv.x * vv.x + vv.y * vv.y + vv.z * vv.z) * mass[i];
     }
     block_sum_to_part<1>(k, part, S_KIN, stride);
+    last_block_slots(part, stride, S_KIN, 1, scal, ticket);
 }
 
 // kinetic partials, optionally after scaling v by the NHC factor s (src/integration.c:281-287)
-__global__ void k_scale_kin(int n, const DevScalars *__restrict__ out, int scale, const double *__restrict__ mass,
-                            double3 *__restrict__ v, double *part, int stride) {
+// e_kin and the NHC conserved-quantity term e_nvt (src/integration.c:156-176) from the
+// kinetic sum in scal[S_KIN]; one thread
+__device__ void nhc_energy(int nn, double L, double temp, const double *__restrict__ nhc,
+                           const double *__restrict__ scal, DevScalars *out) {
+    const double *xi = nhc, *vxi = nhc + 16, *Q = nhc + 32;
+    out->e_kin = 0.5 * scal[S_KIN];
+    double nvt1 = L * temp * xi[0], nvt2 = vxi[0] * vxi[0] * 0.5 / Q[0], nvt3 = 0.0, nvt4 = 0.0;
+    for (int i = 1; i < nn; i++) {
+        nvt3 += vxi[i] * vxi[i] * 0.5 / Q[i];
+        nvt4 += temp * xi[i];
+    }
+    out->e_nvt = nvt1 + nvt2 + nvt3 + nvt4;
+    for (int i = 0; i < 16; i++) {
+        out->xi[i] = xi[i];
+        out->vxi[i] = vxi[i];
+    }
+}
+
+// v *= s (scale) and the kinetic sum sum m v^2: block partials in the S_KIN slot, which
+// the last block reduces into scal[S_KIN] as k_reduce_slots does (256-thread blocks);
+// energy: then e_kin and e_nvt (nhc_energy)
+__global__ void __launch_bounds__(256) k_scale_kin(ScaleKinArgs a) {
     grid_dep();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     double k[1] = {0.0};
-    if (i < n) {
-        double3 vv = v[i];
-        if (scale) {
-            double s = out->nhc_s;
+    if (i < a.n) {
+        double3 vv = a.v[i];
+        if (a.scale) {
+            double s = a.out_s->nhc_s;
             vv.x *= s;
             vv.y *= s;
             vv.z *= s;
-            v[i] = vv;
+            a.v[i] = vv;
         }
-        k[0] = (vv.x * vv.x + vv.y * vv.y + vv.z * vv.z) * mass[i];
+        k[0] = (vv.x * vv.x + vv.y * vv.y + vv.z * vv.z) * a.mass[i];
     }
-    block_sum_to_part<1>(k, part, S_KIN, stride);
+    block_sum_to_part<1>(k, a.part, S_KIN, a.stride);
+    const bool last = last_block_slots(a.part, a.stride, S_KIN, 1, a.scal, a.ticket);
+    if (last && a.energy && threadIdx.x == 0) nhc_energy(a.nn, a.L, a.temp, a.nhc, a.scal, a.out);
 }
 
 // leap-frog (src/integration.c:93-137)
@@ -635,25 +668,6 @@ void launch_nhc_chain(Engine &e, const NhcArgs &a, double *nhc, const double *sc
     case 4: MDFF_LAUNCH(e, k_nhc_chain<4>, 1, 1, 0, a, nhc, scal, out); break;
     case 5: MDFF_LAUNCH(e, k_nhc_chain<5>, 1, 1, 0, a, nhc, scal, out); break;
     default: MDFF_LAUNCH(e, k_nhc_chain<0>, 1, 1, 0, a, nhc, scal, out); break;
-    }
-}
-
-// e_kin and the NHC conserved-quantity term e_nvt (src/integration.c:156-176)
-__global__ void k_nhc_energy(int nn, double L, double temp, const double *__restrict__ nhc,
-                             const double *__restrict__ scal, DevScalars *out) {
-    grid_dep();
-    if (threadIdx.x || blockIdx.x) return;
-    const double *xi = nhc, *vxi = nhc + 16, *Q = nhc + 32;
-    out->e_kin = 0.5 * scal[S_KIN];
-    double nvt1 = L * temp * xi[0], nvt2 = vxi[0] * vxi[0] * 0.5 / Q[0], nvt3 = 0.0, nvt4 = 0.0;
-    for (int i = 1; i < nn; i++) {
-        nvt3 += vxi[i] * vxi[i] * 0.5 / Q[i];
-        nvt4 += temp * xi[i];
-    }
-    out->e_nvt = nvt1 + nvt2 + nvt3 + nvt4;
-    for (int i = 0; i < 16; i++) {
-        out->xi[i] = xi[i];
-        out->vxi[i] = vxi[i];
     }
 }
 
