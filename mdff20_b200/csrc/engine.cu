@@ -121,6 +121,7 @@ Engine::Engine(const mdffgpu_params &prm, int dev) : p(prm) {
         MDFF_CK(cudaEventCreateWithFlags(&ev_join[k], cudaEventDisableTiming));
     }
     if (const char *v = getenv("MDFFGPU_SIDE_STREAMS")) side_on = atoi(v) != 0;
+    if (const char *v = getenv("MDFFGPU_PDL")) pdl = atoi(v) != 0;
     {
         int least = 0, greatest = 0;
         MDFF_CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));

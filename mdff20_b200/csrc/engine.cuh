@@ -502,25 +502,18 @@ struct Engine {
 // (wait for the grids it depends on, then release its dependents), so each launch may
 // carry the programmatic-serialization attribute -- the grid is launched while the one
 // before it in the stream drains (a recorded graph keeps this as a programmatic edge)
-// and starts its work once that one has completed with its writes visible.
-// MDFFGPU_PDL=0 launches with full serialization, and so do the force-matching
-// evaluations (Engine::pdl false while they are issued): many of them run concurrently,
-// and blocks resident early while they wait for their prerequisite take SM slots from
-// the other streams' grids (measured: 2% fewer configurations per second with it).
-inline bool pdl_enabled() {
-    static const bool on = [] {
-        const char *v = getenv("MDFFGPU_PDL");
-        return !v || atoi(v) != 0;
-    }();
-    return on;
-}
+// and starts its work once that one has completed with its writes visible.  Engine::pdl
+// (MDFFGPU_PDL=0 at creation: off) selects it; the force-matching evaluations launch
+// fully serialised (many of them run concurrently, and blocks resident early while they
+// wait for their prerequisite take SM slots from the other streams' grids: measured 2%
+// fewer configurations per second with it).
 
 // launch bookkeeping: every kernel launch goes through this
 #define MDFF_LAUNCH(eng, kernel, grid, block, smem, ...)                               \
     do {                                                                               \
         cudaLaunchAttribute at_[2];                                                    \
         unsigned na_ = 0;                                                              \
-        if ((eng).pdl && pdl_enabled()) {                                              \
+        if ((eng).pdl) {                                                               \
             at_[na_].id = cudaLaunchAttributeProgrammaticStreamSerialization;          \
             at_[na_++].val.programmaticStreamSerializationAllowed = 1;                 \
         }                                                                              \
