@@ -19,7 +19,8 @@ ours      : state resident on the GPU; each timed step is bracketed by CUDA even
             the engine stream, with a 256 MB L2 flush between steps (not timed).
             `e2e` repeats the measurement through the C ABI with page-locked host
             arrays in the reference's per-component layout: positions and velocities
-            uploaded, one step, positions, velocities and forces downloaded, every step.
+            uploaded, one step, positions, velocities and forces downloaded, every step,
+            in one mdffgpu_md_steps_host call per step (one synchronisation).
 reference : the reference's own CPU code (oracle/_ref, -O3 -Ofast -fopenmp) on all host
             cores, on a bounded sample of steps of the same system.
 N > 1 GPUs: one process per GPU (torchrun).  MD: an independent replica per rank (the
@@ -60,7 +61,7 @@ def parse():
     ap.add_argument("--solver", choices=["cg", "fused", "reference"], default="fused")
     ap.add_argument("--fp64-steps", type=int, default=100, help="steps of the plain FP64 path timed beside")
     ap.add_argument("--force-check", type=int, default=1, help="mixed: force error against an FP64 evaluation")
-    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--e2e-steps", type=int, default=20)
     ap.add_argument("--roof-kernel", default="k_rho,k_rec_ion",
                     help="kernel families timed for the roofline (the one with the larger share is `roofline`)")
     ap.add_argument("--drift-steps", type=int, default=1000,
@@ -570,7 +571,8 @@ def run_ours(args):
 
     # ------------------------------------------------ end to end through the C ABI
     # page-locked host arrays in the reference's per-component layout (rx[], ry[], ...):
-    # positions and velocities in, positions, velocities and forces out, every step
+    # positions and velocities in, positions, velocities and forces out, every step (one
+    # C-ABI call: the copies are queued with the step and share its synchronisation)
     nE = max(1, args.e2e_steps)
     host = [torch.empty(s.nion, dtype=torch.float64).pin_memory().numpy() for _ in range(9)]
     eng.state_soa(*host)
@@ -582,10 +584,7 @@ def run_ours(args):
         with torch.cuda.stream(stream):
             flush.zero_()
         e_evs[k][0].record(stream)
-        eng.set_positions_soa(*host[0:3])
-        eng.set_velocities_soa(*host[3:6])
-        eng.md_steps(istep, 1)
-        eng.state_soa(*host)
+        eng.md_steps_host(istep, 1, host[0:6], host)
         e_evs[k][1].record(stream)
         istep += 1
     torch.cuda.synchronize()

@@ -204,6 +204,16 @@ int mdffgpu_prop_agate(mdffgpu_ctx *ctx, int istep);
  * nsteps records of 12 doubles: e_kin u_lj u_bhmftd u_coul u_pol e_nvt pvir_lj
  * pvir_bhmftd pvir_coul nlist_builds scf_iter scf_rmsd. */
 int mdffgpu_md_steps(mdffgpu_ctx *ctx, int first, int nsteps, double *thermo);
+/* No reference counterpart: mdffgpu_md_steps with the state on the host, as a caller
+ * that keeps rx..fz in its own arrays runs it (the reference's MD loop over its
+ * globals).  in (may be NULL): 6 arrays rx ry rz vx vy vz of nion doubles copied in
+ * before the steps (an entry NULL keeps that component's device values); out (may be
+ * NULL): 9 arrays rx ry rz vx vy vz fx fy fz the state after the last step is copied to
+ * (entries may be NULL).  The copies are queued with the steps: one call and, as in
+ * mdffgpu_md_steps, one synchronisation per step, the outgoing copies riding on the last
+ * one.  Equivalent to set_positions + set_velocities + md_steps + get_state. */
+int mdffgpu_md_steps_host(mdffgpu_ctx *ctx, int first, int nsteps, const double *const *in, double *thermo,
+                          double *const *out);
 
 /* Neighbour-list build that allocates no memory.  No counterpart in the reference; it
  * is for callers that cannot allocate device memory: an application that owns all GPU

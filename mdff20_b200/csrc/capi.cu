@@ -405,6 +405,12 @@ int mdffgpu_md_steps(mdffgpu_ctx *ctx, int first, int nsteps, double *thermo) {
     return guarded(ctx, [&](Engine &e) { e.md_steps(first, nsteps, thermo); });
 }
 
+int mdffgpu_md_steps_host(mdffgpu_ctx *ctx, int first, int nsteps, const double *const *in, double *thermo,
+                          double *const *out) {
+    if (nsteps < 0) return MDFFGPU_ERR_ARG;
+    return guarded(ctx, [&](Engine &e) { e.md_steps(first, nsteps, thermo, in, out); });
+}
+
 long long mdffgpu_launch_count(const mdffgpu_ctx *ctx) { return (ctx && ctx->e) ? ctx->e->launches : -1; }
 
 void *mdffgpu_stream(const mdffgpu_ctx *ctx) { return (ctx && ctx->e) ? (void *)ctx->e->stream : nullptr; }

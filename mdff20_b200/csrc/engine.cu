@@ -638,6 +638,13 @@ __global__ void k_unpack_state(int n, const double4 *__restrict__ r, const doubl
 #pragma unroll
     for (int k = 0; k < 9; k++) soa[(size_t)k * n + i] = x[k];
 }
+// component c of an array of `stride`-double records (positions double4, velocities
+// double3) into one component slot
+__global__ void k_unpack_comp(int n, int c, const double *__restrict__ src, int stride, double *__restrict__ dst) {
+    grid_dep();
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = src[(size_t)i * stride + c];
+}
 
 void Engine::set_positions(const double *rx, const double *ry, const double *rz) {
     const double *src[3] = {rx, ry, rz};
@@ -1570,7 +1577,42 @@ void Engine::capture_step(int step) {
 }
 
 // run_md's loop body (src/md.c:229-241)
-void Engine::md_steps(int first, int nsteps, double *thermo) {
+void Engine::md_steps(int first, int nsteps, double *thermo, const double *const *in, double *const *out) {
+    if (in) {
+        // the caller's positions and velocities, packed on the device (no synchronisation:
+        // the step's own one below, or the list build's, covers the copies)
+        for (int k = 0; k < 6; k++) {
+            double *dst = d_soa + (size_t)k * n;
+            if (in[k]) MDFF_CK(cudaMemcpyAsync(dst, in[k], sizeof(double) * n, cudaMemcpyHostToDevice, stream));
+        }
+        if (in[0] || in[1] || in[2]) {
+            // components not given keep their device values
+            for (int k = 0; k < 3; k++)
+                if (!in[k]) MDFF_LAUNCH(*this, k_unpack_comp, ceil_div(n, 256), 256, 0, n, k, (const double *)d_r, 4,
+                                        d_soa + (size_t)k * n);
+            MDFF_LAUNCH(*this, k_pack_r, ceil_div(n, 256), 256, 0, n, d_soa, d_q, d_r);
+            if (!p.lverletL) list_ready = false;
+        }
+        if (in[3] || in[4] || in[5]) {
+            for (int k = 3; k < 6; k++)
+                if (!in[k]) MDFF_LAUNCH(*this, k_unpack_comp, ceil_div(n, 256), 256, 0, n, k - 3, (const double *)d_v,
+                                        3, d_soa + (size_t)k * n);
+            MDFF_LAUNCH(*this, k_pack_v, ceil_div(n, 256), 256, 0, n, d_soa, d_v);
+        }
+    }
+    auto queue_out = [&] {
+        if (!out) return;
+        MDFF_LAUNCH(*this, k_unpack_state, ceil_div(n, 256), 256, 0, n, d_r, d_v, d_f, d_soa);
+        for (int k = 0; k < 9; k++)
+            if (out[k])
+                MDFF_CK(cudaMemcpyAsync(out[k], d_soa + (size_t)k * n, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                                        stream));
+    };
+    if (nsteps == 0) {
+        queue_out();
+        MDFF_CK(cudaStreamSynchronize(stream));
+        return;
+    }
     if (p.lverletL && !list_ready) gen_verletlist();
     for (int s = 0; s < nsteps; s++) {
         int step = first + s;
@@ -1584,6 +1626,7 @@ void Engine::md_steps(int first, int nsteps, double *thermo) {
             prop_agate(step);
             if (p.lverletL) check_verletlist(false);
         }
+        if (s == nsteps - 1) queue_out();   // on the last step's synchronisation
         sync_scalars();
         if (graphed) {
             launches += graph_outer + graph_body * std::max(h_out->scf_iter, 0) + (h_out->rebuild ? graph_if : 0);

@@ -463,7 +463,10 @@ struct Engine {
     void ko_inner(double3 *d_dmu, const double3 *d_find);
     double rmsd_of(const double3 *d_mu, const double3 *d_ef, double *upol_sum);
     void prop_agate(int step);
-    void md_steps(int first, int nsteps, double *thermo);
+    // in: 6 host arrays (rx..vz) copied in first, out: 9 host arrays (rx..fz) filled after
+    // the last step; both optional, entries may be null (mdffgpu_md_steps_host)
+    void md_steps(int first, int nsteps, double *thermo, const double *const *in = nullptr,
+                  double *const *out = nullptr);
     // force matching: theta = (A, B, C of Si-O, A, B, C of O-O, q_Si, alpha_O, b, c);
     // force_match: res[0] = sum |F - F_t|^2, res[1..10] = dL/dtheta for
     // L = scale/2 sum |F - F_t|^2 (w = scale (F - F_t))

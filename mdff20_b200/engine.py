@@ -160,7 +160,7 @@ EXPORTS = (
     "mdffgpu_set_dipole_history", "mdffgpu_get_dipole_history", "mdffgpu_set_nhc", "mdffgpu_get_nhc",
     "mdffgpu_get_thermo", "mdffgpu_gen_verletlist", "mdffgpu_check_verletlist", "mdffgpu_get_verletlist",
     "mdffgpu_engforce", "mdffgpu_engforce_nmlj", "mdffgpu_engforce_bhmftd", "mdffgpu_multipole_es",
-    "mdffgpu_get_dipoles", "mdffgpu_prop_agate", "mdffgpu_md_steps", "mdffgpu_launch_count",
+    "mdffgpu_get_dipoles", "mdffgpu_prop_agate", "mdffgpu_md_steps", "mdffgpu_md_steps_host", "mdffgpu_launch_count",
     "mdffgpu_stream", "mdffgpu_fma_peak", "mdffgpu_profile", "mdffgpu_profile_result",
     "mdffgpu_build_lists_noalloc", "mdffgpu_fit_set_params", "mdffgpu_force_match", "mdffgpu_fit_batch",
     "mdffgpu_fit_plan_create", "mdffgpu_fit_plan_eval", "mdffgpu_fit_plan_destroy", "mdffgpu_fit_plan_last_error",
@@ -219,6 +219,7 @@ def load_library(path: str = LIB_PATH):
         "mdffgpu_get_dipoles": [vp, dp, dp],
         "mdffgpu_prop_agate": [vp, I],
         "mdffgpu_md_steps": [vp, I, I, dp],
+        "mdffgpu_md_steps_host": [vp, I, I, C.POINTER(dp), dp, C.POINTER(dp)],
         "mdffgpu_fit_set_params": [vp, I, I, dp],
         "mdffgpu_force_match": [vp, I, I, dp, dp, dp, D, dp],
         "mdffgpu_fit_batch": [vpp, I, I, I, dp, C.POINTER(dp), D, I, dp],
@@ -466,6 +467,22 @@ class Engine:
     def md_steps(self, first: int, nsteps: int, record: bool = True):
         th = np.zeros((nsteps, 12)) if record else None
         self._check(self.L.mdffgpu_md_steps(self.h, first, nsteps, _dp(th)))
+        return th
+
+    def md_steps_host(self, first: int, nsteps: int, inp=None, out=None, record: bool = True):
+        """md_steps with the state on the host in the reference's per-component layout:
+        inp (rx ry rz vx vy vz; entries may be None) is copied in first, out (rx ry rz vx
+        vy vz fx fy fz; entries may be None) receives the state after the last step.
+        Arrays are contiguous float64 of length n (page-locked ones are copied by DMA)."""
+        def ptrs(arrs, k):
+            if arrs is None:
+                return None
+            if len(arrs) != k:
+                raise ValueError(f"md_steps_host takes {k} arrays here")
+            return (C.POINTER(C.c_double) * k)(*[None if x is None else _dp(_soa_arg(x, self.n)) for x in arrs])
+        pin, pout = ptrs(inp, 6), ptrs(out, 9)
+        th = np.zeros((nsteps, 12)) if record else None
+        self._check(self.L.mdffgpu_md_steps_host(self.h, first, nsteps, pin, _dp(th), pout))
         return th
 
     def launch_count(self) -> int:

@@ -99,3 +99,46 @@ def test_rebuild_if_node_matches_eager(precision):
     nbuilds = graph[0][:, 9]
     # the graph replays start at step extrapolate_order + 1; rebuilds must happen there
     assert nbuilds[-1] - nbuilds[s.extrapolate_order + 1] >= 3
+
+
+def test_md_steps_host_equals_separate_calls():
+    """mdffgpu_md_steps_host (state in, steps, state out, one call) gives what
+    set_positions + set_velocities + md_steps + get_state give, bit for bit; NULL input
+    components keep the device's values."""
+    s, p0 = _crist192()
+    n = len(p0)
+    rng = np.random.default_rng(3)
+    a = Engine(s, positions=p0, pim_solver=PIM_CG_FUSED, precision=MIXED)
+    b = Engine(s, positions=p0, pim_solver=PIM_CG_FUSED, precision=MIXED)
+    try:
+        for e in (a, b):
+            e.gen_verletlist()
+            e.engforce()
+            e.md_steps(1, 6)
+        pos = a.state()[0] + rng.normal(scale=1e-3, size=(n, 3))
+        vel = a.state()[1] * 1.01
+        comp = [np.ascontiguousarray(x[:, k]) for x in (pos, vel) for k in range(3)]
+        # separate calls
+        a.set_positions_soa(*comp[0:3])
+        a.set_velocities_soa(*comp[3:6])
+        ta = a.md_steps(7, 3)
+        oa = [np.empty(n) for _ in range(9)]
+        a.state_soa(*oa)
+        # one call
+        ob = [np.empty(n) for _ in range(9)]
+        tb = b.md_steps_host(7, 3, comp, ob)
+        assert np.array_equal(ta, tb)
+        for x, y in zip(oa, ob):
+            assert np.array_equal(x, y)
+        # None entries: velocities kept, out entries skipped
+        ta = a.md_steps(10, 1)
+        oa2 = [np.empty(n) for _ in range(9)]
+        a.state_soa(*oa2)
+        ob2 = [np.empty(n) if k in (0, 4, 8) else None for k in range(9)]
+        tb = b.md_steps_host(10, 1, [None] * 6, ob2)
+        assert np.array_equal(ta, tb)
+        for k in (0, 4, 8):
+            assert np.array_equal(oa2[k], ob2[k])
+    finally:
+        a.close()
+        b.close()
