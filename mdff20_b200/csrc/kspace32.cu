@@ -64,41 +64,43 @@ struct TabLayout {
 // one thread per (ion, table entry)
 __global__ void k_phase32(int n, Cell c, const double4 *__restrict__ r, TabLayout L, float2 *__restrict__ tab) {
     grid_dep();
-    long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= (long long)n * L.w) return;
-    int i = (int)(g / L.w), e = (int)(g - (long long)i * L.w);
-    int d = -1, m = 0;
-    if (e < L.K0 + 1) {
-        d = 0;
-        m = e;
-    } else if (e < L.e1 + 2 * L.K1 + 1) {
-        d = 1;
-        m = e - L.e1 - L.K1;
-    } else if (e >= L.z) {
-        // z blocks hold planar pairs: entry 2p = (x of z_2p, x of z_2p+1), entry 2p + 1 =
-        // their y; the thread of entry 2p writes both
-        int b = (e - L.z) / ZS, j = (e - L.z) - b * ZS;
-        if (j >= ZB) {
-            tab[g] = make_float2(0.f, 0.f);
-            return;
+    // one ion per warp row (threadIdx.y), its entries over the lanes
+    const int i = blockIdx.x * blockDim.y + threadIdx.y;
+    if (i >= n) return;
+    const double4 ri = r[i];
+    for (int e = threadIdx.x; e < L.w; e += blockDim.x) {
+        const size_t g = (size_t)i * L.w + e;
+        int d = -1, m = 0;
+        if (e < L.K0 + 1) {
+            d = 0;
+            m = e;
+        } else if (e < L.e1 + 2 * L.K1 + 1) {
+            d = 1;
+            m = e - L.e1 - L.K1;
+        } else if (e >= L.z) {
+            // z blocks hold planar pairs: entry 2p = (x of z_2p, x of z_2p+1), entry 2p + 1 =
+            // their y; the thread of entry 2p writes both
+            int b = (e - L.z) / ZS, j = (e - L.z) - b * ZS;
+            if (j >= ZB) {
+                tab[g] = make_float2(0.f, 0.f);
+                continue;
+            }
+            if (j & 1) continue;
+            int m0 = (b < L.nzb_neg) ? -L.K2 + ZB * b + j : 1 + ZB * (b - L.nzb_neg) + j;
+            bool ok0 = (b < L.nzb_neg) ? m0 <= 0 : m0 <= L.K2, ok1 = (b < L.nzb_neg) ? m0 + 1 <= 0 : m0 + 1 <= L.K2;
+            double t = c.B[0][2] * ri.x + c.B[1][2] * ri.y + c.B[2][2] * ri.z;
+            float2 v0 = ok0 ? cis2pi32((double)m0 * t) : make_float2(0.f, 0.f);
+            float2 v1 = ok1 ? cis2pi32((double)(m0 + 1) * t) : make_float2(0.f, 0.f);
+            *(float4 *)(tab + g) = make_float4(v0.x, v1.x, v0.y, v1.y);
+            continue;
         }
-        if (j & 1) return;
-        int m0 = (b < L.nzb_neg) ? -L.K2 + ZB * b + j : 1 + ZB * (b - L.nzb_neg) + j;
-        bool ok0 = (b < L.nzb_neg) ? m0 <= 0 : m0 <= L.K2, ok1 = (b < L.nzb_neg) ? m0 + 1 <= 0 : m0 + 1 <= L.K2;
-        double4 ri = r[i];
-        double t = c.B[0][2] * ri.x + c.B[1][2] * ri.y + c.B[2][2] * ri.z;
-        float2 v0 = ok0 ? cis2pi32((double)m0 * t) : make_float2(0.f, 0.f);
-        float2 v1 = ok1 ? cis2pi32((double)(m0 + 1) * t) : make_float2(0.f, 0.f);
-        *(float4 *)(tab + g) = make_float4(v0.x, v1.x, v0.y, v1.y);
-        return;
+        float2 v = make_float2(0.f, 0.f);
+        if (d >= 0) {
+            double t = c.B[0][d] * ri.x + c.B[1][d] * ri.y + c.B[2][d] * ri.z;
+            v = cis2pi32((double)m * t);
+        }
+        tab[g] = v;
     }
-    float2 v = make_float2(0.f, 0.f);
-    if (d >= 0) {
-        double4 ri = r[i];
-        double t = c.B[0][d] * ri.x + c.B[1][d] * ri.y + c.B[2][d] * ri.z;
-        v = cis2pi32((double)m * t);
-    }
-    tab[g] = v;
 }
 
 // ---------------------------------------------------------------- pass 1: rho(k)
@@ -680,8 +682,7 @@ static void ion32_slicing(const Engine &e, int cnt, bool wf, int &rows, int &sli
 
 void launch_phase32(Engine &e) {
     TabLayout L = layout_of(e);
-    long long tot = (long long)e.n * L.w;
-    MDFF_LAUNCH(e, k_phase32, (unsigned)((tot + 255) / 256), 256, 0, e.n, e.cell, e.d_r, L, e.d_tab32);
+    MDFF_LAUNCH(e, k_phase32, ceil_div(e.n, 8), dim3(32, 8), 0, e.n, e.cell, e.d_r, L, e.d_tab32);
 }
 
 void launch_coords32(Engine &e) {

@@ -104,11 +104,12 @@ __global__ void k_rho_tc_tables(int n, int npad, int lz, int tab_w, int K2, Cell
                                 const int *__restrict__ order, const float2 *__restrict__ tab,
                                 float4 *__restrict__ etab, float *__restrict__ btab) {
     grid_dep();
-    const long long ne = (long long)(npad / 2) * lz;   // pair entries, then (position, column) items
-    long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= ne + (long long)npad * RT_N) return;
+    // pair entries, then (position, column) items; below 2^31 in all (launch_rho_tc_tables)
+    const int ne = (npad / 2) * lz;
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= ne + npad * RT_N) return;
     if (g < ne) {
-        const int m = (int)(g / lz), e = (int)(g - (long long)m * lz);
+        const int m = g / lz, e = g - m * lz;
         const int ia = 2 * m < n ? order[2 * m] : -1, ib = 2 * m + 1 < n ? order[2 * m + 1] : -1;
         const float2 va = ia >= 0 ? tab[(size_t)ia * tab_w + e] : make_float2(0.f, 0.f);
         const float2 vb = ib >= 0 ? tab[(size_t)ib * tab_w + e] : make_float2(0.f, 0.f);
@@ -116,7 +117,7 @@ __global__ void k_rho_tc_tables(int n, int npad, int lz, int tab_w, int K2, Cell
         return;
     }
     g -= ne;
-    const int p = (int)(g / RT_N), col = (int)(g - (long long)p * RT_N);
+    const int p = g / RT_N, col = g - p * RT_N;
     const int ion = p < n ? order[p] : -1;
     float v = 0.f;
     if (ion >= 0) {
@@ -486,6 +487,7 @@ void launch_rho_tc_tables(Engine &e) {
     if (!e.d_rho_btab) return;
     const int npad = rt_npad(e), lz = e.rho_tc_lz;
     const long long tot = (long long)(npad / 2) * lz + (long long)npad * RT_N;
+    if (tot >= (1LL << 31)) throw Error(MDFFGPU_ERR_ARG, "system too large for the tensor-core rho tables");
     MDFF_LAUNCH(e, k_rho_tc_tables, (unsigned)((tot + 255) / 256), 256, 0, e.n, npad, lz, e.tab_w, e.kmax[2], e.cell,
                 e.d_r, e.d_ion_order, e.d_tab32, e.d_rho_etab, (float *)e.d_rho_btab);
 }
