@@ -1556,6 +1556,7 @@ void Engine::capture_step(int step) {
         check_verletlist(false);
     } catch (...) {
         capturing = false;
+        forget_sides();
         cudaStreamEndCapture(stream, &graph);
         if (graph) cudaGraphDestroy(graph);
         launches = l0;

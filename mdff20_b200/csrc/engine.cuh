@@ -421,6 +421,11 @@ struct Engine {
         side_open[k] = false;
         MDFF_CK(cudaStreamWaitEvent(stream, ev_join[k], 0));
     }
+    // after a recording that failed part way: its forks belong to the abandoned capture
+    void forget_sides() {
+        for (bool &o : side_open) o = false;
+        prep_issued = false;
+    }
     cudaGraphExec_t step_exec = nullptr;
     long long gen = 0, graph_gen = -1;      // gen: bumped when buffers or modes change
     long long graph_outer = 0, graph_body = 0, body_count = 0;   // kernels per replay / per CG iteration

@@ -753,6 +753,7 @@ void Engine::capture_fit(const double *d_th, int tSi, int tO, double scale, doub
     } catch (...) {
         capturing = false;
         pdl = true;
+        forget_sides();
         cudaStreamEndCapture(stream, &graph);
         if (graph) cudaGraphDestroy(graph);
         launches = l0;
