@@ -71,3 +71,5 @@ def test_null_arguments_rejected():
     assert L.mdffgpu_destroy(None) == 1
     assert L.mdffgpu_engforce(None) == 1
     assert L.mdffgpu_md_steps(None, 1, 1, None) == 1
+    assert L.mdffgpu_md_steps_host(None, 1, 1, None, None, None) == 1
+    assert L.mdffgpu_md_steps_host(None, 1, -1, None, None, None) == 1
